@@ -1,0 +1,160 @@
+/*
+ * kutta_b200: B200-native (sm_100a) pressure-correction linear solve.
+ *
+ * Plain C ABI. Every entry point takes plain pointers and sizes; device
+ * pointers are CUDA device addresses on the current device, host pointers are
+ * ordinary host memory. `stream` is a cudaStream_t passed as void* (NULL means
+ * the legacy default stream). Every call returns a b2_status; on failure the
+ * message is available from b2_last_error() (thread-local).
+ *
+ * The ABI replaces the reference's C++ linear-solver boundary
+ * (src/kutta/linalg/solver.hpp, amg.hpp, csr.hpp); each declaration names the
+ * reference interface it stands in for.
+ */
+#ifndef KUTTA_B200_H
+#define KUTTA_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Status codes. KUTTA's usage errors (KUTTA_REQUIRE -> kutta::Error,
+ * src/kutta/core/types.hpp:42-46) map to B2_INVALID_ARGUMENT; nonfinite input
+ * vectors (KUTTA_REQUIRE_FINITE -> kutta::NonfiniteError, types.hpp:48-52) map
+ * to B2_NONFINITE. Numerical non-convergence is NOT an error: it returns B2_OK
+ * with stats.converged = 0, as the reference does (solver.cpp:166-175). */
+typedef enum {
+  B2_OK = 0,
+  B2_INVALID_ARGUMENT = 1,
+  B2_NONFINITE = 2,
+  B2_DEVICE_ERROR = 3,
+  B2_TIMEOUT = 4,
+  B2_OUT_OF_MEMORY = 5,
+  B2_INTERNAL = 6
+} b2_status;
+
+/* SolverKind, src/kutta/linalg/solver.hpp:32-38 (same order and meaning). */
+typedef enum {
+  B2_JACOBI = 0,
+  B2_PCG_JACOBI = 1,
+  B2_BICGSTAB_JACOBI = 2,
+  B2_AMG_PCG = 3,
+  B2_AMG_BICGSTAB = 4
+} b2_solver_kind;
+
+/* NullSpace / OperatorStructure, solver.hpp:40-41. AmgCycle, amg.hpp:9. */
+typedef enum { B2_NULLSPACE_NONE = 0, B2_NULLSPACE_CONSTANT = 1 } b2_nullspace;
+typedef enum { B2_STRUCTURE_GENERAL = 0, B2_STRUCTURE_SYMMETRIC_M_MATRIX = 1 } b2_structure;
+typedef enum { B2_CYCLE_V = 0, B2_CYCLE_K = 1 } b2_cycle;
+
+typedef struct b2_workspace b2_workspace;
+typedef struct b2_solver b2_solver;
+typedef struct b2_hierarchy b2_hierarchy;
+
+/* AmgOptions (amg.hpp:8-20) plus SolverOptions (solver.hpp:66-72) in one
+ * struct. `workspace` may be NULL (private Krylov vectors). */
+typedef struct {
+  int cycle;               /* b2_cycle; default V */
+  int pre_sweeps;          /* default 5 */
+  int post_sweeps;         /* default 5 */
+  int coarse_sweeps;       /* default 32 */
+  int coarse_rows;         /* default 24 */
+  int max_levels;          /* default 24 */
+  int aggregation_passes;  /* default 3 */
+  double strength_threshold; /* default 0.25 */
+  int nullspace;           /* b2_nullspace; default none */
+  int structure;           /* b2_structure; default general */
+  b2_workspace* workspace; /* KrylovWorkspace (solver.hpp:47-64) or NULL */
+} b2_options;
+
+/* SolveControl, solver.hpp:18-23. */
+typedef struct {
+  double rel_tol;               /* default 1e-2 */
+  double abs_tol;               /* default 1e-12 */
+  int max_iter;                 /* default 200 */
+  int residual_check_interval;  /* default 8 */
+} b2_control;
+
+/* SolveStats, solver.hpp:25-30. */
+typedef struct {
+  int iterations;
+  int converged;
+  double initial_residual;
+  double final_residual;
+} b2_stats;
+
+/* Defaults of AmgOptions{} (amg.hpp:8-20) and SolveControl{} (solver.hpp:18-23). */
+void b2_options_default(b2_options* options);
+void b2_control_default(b2_control* control);
+
+/* Message of the last failed call on this thread; returns its full length. */
+size_t b2_last_error(char* buffer, size_t length);
+
+/* KrylovWorkspace(rows), solver.hpp:47-64: Krylov vectors shared by solvers of
+ * one size whose calls never run concurrently. Allocated on first use. */
+int b2_workspace_create(int rows, b2_workspace** out);
+void b2_workspace_destroy(b2_workspace* workspace);
+
+/* make_solver(kind, dev, a, SolverOptions) (solver.hpp:85-88; amg.cpp:384-406)
+ * when options == NULL or `use_amg_options` == 0, make_amg_solver(kind, dev, a,
+ * AmgOptions) (amg.hpp:26-27; amg.cpp:345-382) otherwise. The host CSR is the
+ * reference's CsrMatrixHost (csr.hpp:16-28): row_ptr[n+1], col[nnz] sorted per
+ * row, diag[n] the index of (i,i), val[nnz] as double. Setup runs on the host
+ * (aggregation) and uploads the hierarchy to the current device. */
+int b2_solver_create(int kind, int n, int nnz, const int32_t* row_ptr, const int32_t* col,
+                     const int32_t* diag, const double* val, const b2_options* options,
+                     int use_amg_options, b2_solver** out);
+
+/* LinearSolver::refresh(dev, a), solver.hpp:77. d_val: the device matrix
+ * values (nnz floats, same pattern as at create). */
+int b2_solver_refresh(b2_solver* solver, const float* d_val, void* stream);
+
+/* LinearSolver::solve(dev, a, x, b, control), solver.hpp:78-79. d_x holds the
+ * initial guess and receives the solution; d_b is the right-hand side; both n
+ * floats on the device and not aliased. d_val as for refresh. */
+int b2_solver_solve(b2_solver* solver, const float* d_val, float* d_x, const float* d_b,
+                    const b2_control* control, b2_stats* stats, void* stream);
+
+/* LinearSolver::describe(), solver.hpp:80. Returns the full length. */
+size_t b2_solver_describe(const b2_solver* solver, char* buffer, size_t length);
+
+void b2_solver_destroy(b2_solver* solver);
+
+/* spmv(dev, a, x, y) and residual(dev, a, x, b, r), csr.hpp:40-48 (kernels
+ * csr_spmv / csr_residual, linalg.kern.h:5-50): the same compensated float
+ * arithmetic on device CSR arrays. */
+int b2_csr_spmv(int n, int nnz, const int32_t* d_row_ptr, const int32_t* d_col,
+                const float* d_val, const float* d_x, float* d_y, void* stream);
+int b2_csr_residual(int n, int nnz, const int32_t* d_row_ptr, const int32_t* d_col,
+                    const float* d_val, const float* d_x, const float* d_b, float* d_r,
+                    void* stream);
+
+/* Hierarchy introspection (the captured-hierarchy checks of the reference's
+ * tests/linalg/test_solvers.cpp:487-555 read the same data back from launches).
+ * Level 0 is the input matrix. Copies are synchronous device-to-host reads on
+ * `stream`; any output pointer may be NULL. */
+int b2_solver_levels(const b2_solver* solver);
+int b2_solver_level_shape(const b2_solver* solver, int level, int* n, int* nnz);
+int b2_solver_level_copy(const b2_solver* solver, int level, int32_t* row_ptr, int32_t* col,
+                         float* val, float* inverse_l1, int32_t* aggregate, void* stream);
+
+/* Host-only AMG setup (no GPU needed): the aggregation hierarchy that
+ * b2_solver_create builds (Aggregation ctor, amg.cpp:200-226: pairs :25-75,
+ * coarsen :77-158, aggregate :160-174). Levels as above; values are the
+ * host-assembled coarse operators and L1 inverse diagonals. */
+int b2_hierarchy_build(int n, int nnz, const int32_t* row_ptr, const int32_t* col,
+                       const int32_t* diag, const double* val, const b2_options* options,
+                       int spd, b2_hierarchy** out);
+int b2_hierarchy_levels(const b2_hierarchy* h);
+int b2_hierarchy_level_shape(const b2_hierarchy* h, int level, int* n, int* nnz);
+int b2_hierarchy_level_copy(const b2_hierarchy* h, int level, int32_t* row_ptr, int32_t* col,
+                            float* val, float* inverse_l1, int32_t* aggregate);
+void b2_hierarchy_free(b2_hierarchy* h);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* KUTTA_B200_H */

@@ -1,0 +1,300 @@
+// extern "C" boundary (include/kutta_b200.h): status codes, thread-local error
+// text, and the mapping of the reference's linalg entry points onto kb2::Solver.
+#include "kutta_b200.h"
+
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <new>
+#include <string>
+
+#include "cuda/kernels.hpp"
+#include "host/setup.hpp"
+#include "host/solver.hpp"
+
+struct b2_workspace {
+  std::shared_ptr<kb2::Workspace> w;
+};
+struct b2_solver {
+  std::unique_ptr<kb2::Solver> s;
+};
+struct b2_hierarchy {
+  kb2::Hierarchy h;
+  kb2::HostCsr fine;
+};
+
+namespace {
+thread_local std::string g_error;
+
+int fail(int code, const char* message) {
+  g_error = message;
+  return code;
+}
+
+template <class F>
+int guarded(F&& f) {
+  try {
+    f();
+    return B2_OK;
+  } catch (const kb2::NonfiniteError& e) {
+    return fail(B2_NONFINITE, e.what());
+  } catch (const kb2::TimeoutError& e) {
+    return fail(B2_TIMEOUT, e.what());
+  } catch (const kb2::DeviceError& e) {
+    const bool oom = std::strstr(e.what(), "out of device memory") != nullptr;
+    return fail(oom ? B2_OUT_OF_MEMORY : B2_DEVICE_ERROR, e.what());
+  } catch (const kb2::Error& e) {
+    return fail(B2_INVALID_ARGUMENT, e.what());
+  } catch (const std::bad_alloc&) {
+    return fail(B2_OUT_OF_MEMORY, "host allocation failed");
+  } catch (const std::exception& e) {
+    return fail(B2_INTERNAL, e.what());
+  }
+}
+
+kb2::Options to_options(const b2_options* o) {
+  kb2::Options r;
+  if (!o) return r;
+  r.cycle = o->cycle == B2_CYCLE_K ? kb2::Cycle::K : kb2::Cycle::V;
+  KB2_REQUIRE(o->cycle == B2_CYCLE_V || o->cycle == B2_CYCLE_K, "AMG: invalid options");
+  r.pre_sweeps = o->pre_sweeps;
+  r.post_sweeps = o->post_sweeps;
+  r.coarse_sweeps = o->coarse_sweeps;
+  r.coarse_rows = o->coarse_rows;
+  r.max_levels = o->max_levels;
+  r.aggregation_passes = o->aggregation_passes;
+  r.strength_threshold = o->strength_threshold;
+  KB2_REQUIRE(o->nullspace == B2_NULLSPACE_NONE || o->nullspace == B2_NULLSPACE_CONSTANT,
+              "solver: invalid nullspace option");
+  r.nullspace = o->nullspace == B2_NULLSPACE_CONSTANT;
+  KB2_REQUIRE(o->structure == B2_STRUCTURE_GENERAL || o->structure == B2_STRUCTURE_SYMMETRIC_M_MATRIX,
+              "AMG: invalid operator structure");
+  r.m_matrix = o->structure == B2_STRUCTURE_SYMMETRIC_M_MATRIX;
+  return r;
+}
+
+kb2::CsrView view(int n, int nnz, const int32_t* row_ptr, const int32_t* col, const int32_t* diag,
+                  const double* val) {
+  KB2_REQUIRE(n >= 0 && nnz >= 0 && row_ptr != nullptr, "CSR: invalid array sizes");
+  return kb2::CsrView{n, nnz, row_ptr, col, diag, val};
+}
+
+cudaStream_t as_stream(void* s) { return static_cast<cudaStream_t>(s); }
+}  // namespace
+
+extern "C" {
+
+void b2_options_default(b2_options* o) {
+  if (!o) return;
+  o->cycle = B2_CYCLE_V;
+  o->pre_sweeps = 5;
+  o->post_sweeps = 5;
+  o->coarse_sweeps = 32;
+  o->coarse_rows = 24;
+  o->max_levels = 24;
+  o->aggregation_passes = 3;
+  o->strength_threshold = 0.25;
+  o->nullspace = B2_NULLSPACE_NONE;
+  o->structure = B2_STRUCTURE_GENERAL;
+  o->workspace = nullptr;
+}
+
+void b2_control_default(b2_control* c) {
+  if (!c) return;
+  c->rel_tol = 1e-2;
+  c->abs_tol = 1e-12;
+  c->max_iter = 200;
+  c->residual_check_interval = 8;
+}
+
+size_t b2_last_error(char* buffer, size_t length) {
+  if (buffer && length) std::snprintf(buffer, length, "%s", g_error.c_str());
+  return g_error.size();
+}
+
+int b2_workspace_create(int rows, b2_workspace** out) {
+  return guarded([&] {
+    KB2_REQUIRE(out != nullptr && rows >= 0, "workspace: invalid arguments");
+    *out = new b2_workspace{std::make_shared<kb2::Workspace>(rows)};
+  });
+}
+void b2_workspace_destroy(b2_workspace* w) { delete w; }
+
+int b2_solver_create(int kind, int n, int nnz, const int32_t* row_ptr, const int32_t* col,
+                     const int32_t* diag, const double* val, const b2_options* options,
+                     int use_amg_options, b2_solver** out) {
+  return guarded([&] {
+    KB2_REQUIRE(out != nullptr, "solver: null output handle");
+    *out = nullptr;
+    KB2_REQUIRE(kind >= B2_JACOBI && kind <= B2_AMG_BICGSTAB, "unknown SolverKind");
+    const auto k = static_cast<kb2::Kind>(kind);
+    const auto a = view(n, nnz, row_ptr, col, diag, val);
+    kb2::Options o;
+    if (options && use_amg_options) {
+      o = to_options(options);
+    } else if (options) {
+      // make_solver: AMG defaults with only nullspace and structure taken over
+      // (amg.cpp:388-396).
+      const auto given = to_options(options);
+      o.nullspace = given.nullspace;
+      o.m_matrix = given.m_matrix;
+    }
+    std::shared_ptr<kb2::Workspace> ws = options && options->workspace ? options->workspace->w : nullptr;
+    if (k == kb2::Kind::AmgPcg || k == kb2::Kind::AmgBicgstab) {
+      kb2::check_amg(k, a, o);
+    } else {
+      kb2::validate_host(a);
+      o.m_matrix = false;
+    }
+    auto solver = std::make_unique<kb2::Solver>(k, a, o, ws);
+    *out = new b2_solver{std::move(solver)};
+  });
+}
+
+int b2_solver_refresh(b2_solver* s, const float* d_val, void* stream) {
+  return guarded([&] {
+    KB2_REQUIRE(s && s->s, "solver: null handle");
+    KB2_REQUIRE(d_val != nullptr || s->s->entries() == 0, "solver: device or matrix mismatch");
+    s->s->refresh(d_val, as_stream(stream));
+  });
+}
+
+int b2_solver_solve(b2_solver* s, const float* d_val, float* d_x, const float* d_b,
+                    const b2_control* control, b2_stats* stats, void* stream) {
+  return guarded([&] {
+    KB2_REQUIRE(s && s->s, "solver: null handle");
+    KB2_REQUIRE(d_val != nullptr || s->s->entries() == 0, "solver: device or matrix mismatch");
+    kb2::Control c;
+    if (control) {
+      c.rel_tol = control->rel_tol;
+      c.abs_tol = control->abs_tol;
+      c.max_iter = control->max_iter;
+      c.residual_check_interval = control->residual_check_interval;
+    }
+    const auto r = s->s->solve(d_val, d_x, d_b, c, as_stream(stream));
+    if (stats) {
+      stats->iterations = r.iterations;
+      stats->converged = r.converged ? 1 : 0;
+      stats->initial_residual = r.initial_residual;
+      stats->final_residual = r.final_residual;
+    }
+  });
+}
+
+size_t b2_solver_describe(const b2_solver* s, char* buffer, size_t length) {
+  if (!s || !s->s) return 0;
+  const auto d = s->s->describe();
+  if (buffer && length) std::snprintf(buffer, length, "%s", d.c_str());
+  return d.size();
+}
+
+void b2_solver_destroy(b2_solver* s) { delete s; }
+
+int b2_csr_spmv(int n, int nnz, const int32_t* d_row_ptr, const int32_t* d_col,
+                const float* d_val, const float* d_x, float* d_y, void* stream) {
+  return guarded([&] {
+    KB2_REQUIRE(n >= 0 && nnz >= 0, "CSR: invalid array sizes");
+    KB2_REQUIRE(d_x != d_y || n == 0, "CSR: input/output aliasing is unsupported");
+    kb2::launch::spmv(n, d_row_ptr, d_col, d_val, d_x, d_y, nullptr, as_stream(stream));
+    kb2::cuda_check(cudaGetLastError(), "csr_spmv");
+  });
+}
+
+int b2_csr_residual(int n, int nnz, const int32_t* d_row_ptr, const int32_t* d_col,
+                    const float* d_val, const float* d_x, const float* d_b, float* d_r,
+                    void* stream) {
+  return guarded([&] {
+    KB2_REQUIRE(n >= 0 && nnz >= 0, "CSR: invalid array sizes");
+    KB2_REQUIRE((d_x != d_r && d_b != d_r) || n == 0, "CSR: residual RHS size or alias mismatch");
+    kb2::launch::residual(n, d_row_ptr, d_col, d_val, d_x, d_b, d_r, nullptr, as_stream(stream));
+    kb2::cuda_check(cudaGetLastError(), "csr_residual");
+  });
+}
+
+int b2_solver_levels(const b2_solver* s) { return s && s->s ? s->s->levels() : 0; }
+
+int b2_solver_level_shape(const b2_solver* s, int level, int* n, int* nnz) {
+  return guarded([&] {
+    KB2_REQUIRE(s && s->s && level >= 0 && level < s->s->levels(), "level out of range");
+    const auto& l = s->s->level(level);
+    if (n) *n = l.n;
+    if (nnz) *nnz = l.nnz;
+  });
+}
+
+int b2_solver_level_copy(const b2_solver* s, int level, int32_t* row_ptr, int32_t* col,
+                         float* val, float* inverse_l1, int32_t* aggregate, void* stream) {
+  return guarded([&] {
+    KB2_REQUIRE(s && s->s && level >= 0 && level < s->s->levels(), "level out of range");
+    const auto& l = s->s->level(level);
+    const auto st = as_stream(stream);
+    auto get = [&](void* dst, const void* src, std::size_t bytes) {
+      if (dst && src && bytes)
+        kb2::cuda_check(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, st), "level copy");
+    };
+    get(row_ptr, l.row_ptr.get(), sizeof(int) * (static_cast<std::size_t>(l.n) + 1));
+    get(col, l.col.get(), sizeof(int) * static_cast<std::size_t>(l.nnz));
+    const float* values = level == 0 ? s->s->current_values() : l.val.get();
+    get(val, values, sizeof(float) * static_cast<std::size_t>(l.nnz));
+    if (l.l1.allocated()) get(inverse_l1, l.l1.get(), sizeof(float) * static_cast<std::size_t>(l.n));
+    if (l.aggregate.allocated())
+      get(aggregate, l.aggregate.get(), sizeof(int) * static_cast<std::size_t>(l.n));
+    kb2::wait(st);
+  });
+}
+
+int b2_hierarchy_build(int n, int nnz, const int32_t* row_ptr, const int32_t* col,
+                       const int32_t* diag, const double* val, const b2_options* options,
+                       int spd, b2_hierarchy** out) {
+  return guarded([&] {
+    KB2_REQUIRE(out != nullptr, "hierarchy: null output handle");
+    *out = nullptr;
+    const auto a = view(n, nnz, row_ptr, col, diag, val);
+    const auto o = to_options(options);
+    kb2::check_amg(spd ? kb2::Kind::AmgPcg : kb2::Kind::AmgBicgstab, a, o);
+    auto* h = new b2_hierarchy;
+    try {
+      h->h = kb2::build_hierarchy(a, o);
+    } catch (...) {
+      delete h;
+      throw;
+    }
+    h->fine.n = n;
+    h->fine.row_ptr.assign(row_ptr, row_ptr + n + 1);
+    h->fine.col.assign(col, col + nnz);
+    h->fine.diag.assign(diag, diag + n);
+    h->fine.val.assign(val, val + nnz);
+    *out = h;
+  });
+}
+
+int b2_hierarchy_levels(const b2_hierarchy* h) { return h ? static_cast<int>(h->h.levels.size()) : 0; }
+
+int b2_hierarchy_level_shape(const b2_hierarchy* h, int level, int* n, int* nnz) {
+  return guarded([&] {
+    KB2_REQUIRE(h && level >= 0 && level < b2_hierarchy_levels(h), "level out of range");
+    const auto& m = level == 0 ? h->fine : h->h.levels[level].matrix;
+    if (n) *n = m.n;
+    if (nnz) *nnz = m.nnz();
+  });
+}
+
+int b2_hierarchy_level_copy(const b2_hierarchy* h, int level, int32_t* row_ptr, int32_t* col,
+                            float* val, float* inverse_l1, int32_t* aggregate) {
+  return guarded([&] {
+    KB2_REQUIRE(h && level >= 0 && level < b2_hierarchy_levels(h), "level out of range");
+    const auto& l = h->h.levels[level];
+    const auto& m = level == 0 ? h->fine : l.matrix;
+    if (row_ptr) std::memcpy(row_ptr, m.row_ptr.data(), sizeof(int) * m.row_ptr.size());
+    if (col) std::memcpy(col, m.col.data(), sizeof(int) * m.col.size());
+    if (val)
+      for (std::size_t j = 0; j < m.val.size(); ++j) val[j] = static_cast<float>(m.val[j]);
+    if (inverse_l1) std::memcpy(inverse_l1, l.l1.data(), sizeof(float) * l.l1.size());
+    if (aggregate && !l.transfer.aggregate.empty())
+      std::memcpy(aggregate, l.transfer.aggregate.data(), sizeof(int) * l.transfer.aggregate.size());
+  });
+}
+
+void b2_hierarchy_free(b2_hierarchy* h) { delete h; }
+
+}  // extern "C"

@@ -1,0 +1,576 @@
+// Reference-parity solver kernels for sm_100a (compiled with --fmad=false).
+//
+// Each kernel computes exactly the float operations, in exactly the order, of
+// the reference kernel it replaces (cited per kernel), so every per-row value is
+// bit-identical to the reference's CPU path. Reductions accumulate in FP64 in a
+// fixed tree; they are fused into the kernel that produces their operand and the
+// last block runs the reference's single-thread scalar update as an epilogue,
+// so a PCG iteration is a handful of launches instead of a dozen.
+#include "common.cuh"
+#include "kernels.hpp"
+
+namespace kb2 {
+namespace {
+using namespace dev;
+
+#define ROWS(i, n) \
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < (n); i += gridDim.x * blockDim.x)
+
+__device__ __forceinline__ Reducer as_reducer(DeviceReducer r) { return Reducer{r.partials, r.ticket}; }
+
+// ---- scalar updates, src/kutta/kernels/scalars.kern.h:51-121 -----------------
+__device__ void epilogue(Epilogue e, float* sc, int* st) {
+  switch (e) {
+    case Epilogue::None:
+      return;
+    case Epilogue::PcgAlpha: {  // solver_pcg_alpha :63-71
+      if (st[0] != 0) return;
+      const Pair rho = kp_load(sc, 0), pq = kp_load(sc, 2);
+      const Pair alpha = kp_div(rho, pq);
+      if (!kp_positive(rho) || !kp_positive(pq) || !kp_coefficient(alpha) || kp_zero(alpha))
+        st[0] = 2;
+      else
+        kp_store(sc, 8, alpha);
+      return;
+    }
+    case Epilogue::PcgBeta:
+    case Epilogue::PcgBetaFlexible: {  // solver_pcg_beta :72-80
+      if (st[0] != 0) return;
+      const Pair next = kp_load(sc, 4);
+      const Pair numer = e == Epilogue::PcgBetaFlexible
+                             ? kp_neg(kp_mul(kp_load(sc, 8), kp_load(sc, 6)))
+                             : next;
+      const Pair beta = kp_div(numer, kp_load(sc, 0));
+      if (!kp_positive(next) || !kp_coefficient(beta) || (kp_zero(beta) && !kp_zero(numer)))
+        st[0] = 2;
+      else {
+        kp_store(sc, 10, beta);
+        kp_store(sc, 0, next);
+      }
+      return;
+    }
+    case Epilogue::BicgBeta: {  // solver_bicg_beta :81-89
+      if (st[0] != 0) return;
+      const Pair rho = kp_load(sc, 0), omega = kp_load(sc, 12);
+      const Pair beta = kp_mul(kp_div(rho, kp_load(sc, 14)), kp_div(kp_load(sc, 8), omega));
+      if (kp_zero(rho) || !kp_finite(rho) || kp_zero(omega) || !kp_coefficient(omega) ||
+          !kp_coefficient(beta) || kp_zero(beta))
+        st[0] = 2;
+      else {
+        kp_store(sc, 10, beta);
+        st[2] = 0;
+      }
+      return;
+    }
+    case Epilogue::BicgAlpha: {  // solver_bicg_alpha :90-97
+      if (st[0] != 0) return;
+      const Pair rv = kp_load(sc, 2);
+      const Pair alpha = kp_div(kp_load(sc, 0), rv);
+      if (kp_zero(rv) || !kp_finite(rv) || !kp_coefficient(alpha) || kp_zero(alpha))
+        st[0] = 2;
+      else
+        kp_store(sc, 8, alpha);
+      return;
+    }
+    case Epilogue::BicgS: {  // solver_bicg_s :98-103
+      if (st[0] != 0) return;
+      ++st[1];
+      st[2] = kp_le(kp_load(sc, 16), kp_load(sc, 20)) ? 1 : 0;
+      return;
+    }
+    case Epilogue::BicgOmega: {  // solver_bicg_omega :104-112
+      if (st[0] != 0) return;
+      if (st[2] != 0) {
+        kp_store(sc, 12, kp(0.0f, 0.0f));
+        return;
+      }
+      const Pair tt = kp_load(sc, 2), ts = kp_load(sc, 4);
+      const Pair omega = kp_div(ts, tt);
+      if (!kp_positive(tt) || !kp_finite(tt) || kp_zero(omega) || !kp_coefficient(omega))
+        st[0] = 2;
+      else
+        kp_store(sc, 12, omega);
+      return;
+    }
+    case Epilogue::CheckPcg:
+    case Epilogue::CheckBicg: {  // solver_check :113-121
+      if (st[0] != 0) return;
+      const bool pcg = e == Epilogue::CheckPcg;
+      if (pcg) ++st[1];
+      const Pair rr = kp_load(sc, 18);
+      if (!kp_finite(rr) || kp_le(rr, kp_load(sc, 20)) || !kp_le(rr, kp_load(sc, 22)) ||
+          st[1] % 50 == 0)
+        st[0] = 1;
+      if (!pcg) kp_store(sc, 14, kp_load(sc, 0));
+      return;
+    }
+  }
+}
+
+// Block partial -> grid total -> pair store -> epilogue, in the last block.
+__device__ __forceinline__ void finish(const Reducer& red, double a, double b, bool dual,
+                                       float* scalars, int offset, int* status, Epilogue epi) {
+  __shared__ double shared[32];
+  a = block_sum(a, shared);
+  if (dual) b = block_sum(b, shared);
+  if (!publish(red, a, b, dual)) return;
+  const double total_a = gather(red, 0, shared);
+  const double total_b = dual ? gather(red, 1, shared) : 0.0;
+  if (threadIdx.x == 0) {
+    store_pair(scalars, offset, total_a);
+    if (dual) store_pair(scalars, offset + 2, total_b);
+    epilogue(epi, scalars, status);
+    *red.ticket = 0;
+  }
+}
+
+// ---- CSR row kernels --------------------------------------------------------
+// csr_spmv / csr_spmv_guarded, linalg.kern.h:5-16,111-114.
+__global__ void k_spmv(int n, const int* __restrict__ rows, const int* __restrict__ cols,
+                       const float* __restrict__ vals, const float* __restrict__ x,
+                       float* __restrict__ y, const int* __restrict__ status) {
+  if (status && status[0] != 0) return;
+  ROWS(i, n) {
+    float sum = 0.0f, error = 0.0f;
+    const int end = rows[i + 1];
+    for (int j = rows[i]; j < end; ++j) kahan_term(sum, error, vals[j], x[cols[j]]);
+    y[i] = sum;
+  }
+}
+
+// csr_spmv_guarded + dot_into(w, q) + a scalar kernel: PCG's p.q and alpha
+// (solver.cpp:288-290, w = p) or BiCGStab's rhat.q and alpha (:335-337, w = rhat).
+__global__ void k_spmv_dot(int n, const int* __restrict__ rows, const int* __restrict__ cols,
+                           const float* __restrict__ vals, const float* __restrict__ p,
+                           const float* __restrict__ w, float* __restrict__ q, DeviceReducer red,
+                           float* scalars, int offset, int* status, Epilogue epi) {
+  if (status[0] != 0) return;
+  double acc = 0;
+  ROWS(i, n) {
+    float sum = 0.0f, error = 0.0f;
+    const int end = rows[i + 1];
+    for (int j = rows[i]; j < end; ++j) kahan_term(sum, error, vals[j], p[cols[j]]);
+    q[i] = sum;
+    acc += static_cast<double>(w[i]) * static_cast<double>(sum);
+  }
+  finish(as_reducer(red), acc, 0, false, scalars, offset, status, epi);
+}
+
+// csr_residual / csr_residual_guarded, linalg.kern.h:32-50,115-118.
+__global__ void k_residual(int n, const int* __restrict__ rows, const int* __restrict__ cols,
+                           const float* __restrict__ vals, const float* __restrict__ x,
+                           const float* __restrict__ b, float* __restrict__ r,
+                           const int* __restrict__ status) {
+  if (status && status[0] != 0) return;
+  ROWS(i, n) {
+    float sum = b[i], error = 0.0f;
+    const int end = rows[i + 1];
+    for (int j = rows[i]; j < end; ++j) residual_term(sum, error, vals[j], x[cols[j]]);
+    r[i] = sum + error;
+  }
+}
+
+// amg_smooth (linalg.kern.h:150-156) and amg_smooth_zero (:162-170). The
+// zero-start form reads no x: the caller has just cleared it, so the ordinary
+// path (taken only for a nonfinite b) runs with x = 0.
+template <bool kZero>
+__global__ void k_smooth(int n, const int* __restrict__ rows, const int* __restrict__ cols,
+                         const float* __restrict__ vals, const float* __restrict__ x,
+                         const float* __restrict__ b, const float* __restrict__ inv,
+                         float* __restrict__ next, const int* __restrict__ status) {
+  if (status[0] != 0) return;
+  ROWS(i, n) {
+    const float bi = b[i];
+    if (kZero && !nonfinite(bi)) {
+      next[i] = 0.0f + (2.0f / 3.0f) * inv[i] * (bi + 0.0f);
+      continue;
+    }
+    float sum = bi, error = 0.0f;
+    const int end = rows[i + 1];
+    for (int j = rows[i]; j < end; ++j)
+      residual_term(sum, error, vals[j], kZero ? 0.0f : x[cols[j]]);
+    const float r = sum + error;
+    next[i] = (kZero ? 0.0f : x[i]) + (2.0f / 3.0f) * inv[i] * r;
+  }
+}
+
+// amg_coarse_solve, linalg.kern.h:126-147: whole <=24-row system in one thread.
+__global__ void k_coarse_solve(int count, const int* __restrict__ rows,
+                               const int* __restrict__ cols, const float* __restrict__ vals,
+                               float* __restrict__ x, const float* __restrict__ b,
+                               const float* __restrict__ inv, const int* __restrict__ status,
+                               int sweeps) {
+  if (threadIdx.x != 0 || blockIdx.x != 0 || status[0] != 0) return;
+  float current[24], r[24];
+  for (int row = 0; row < count; ++row) current[row] = 0.0f;
+  for (int sweep = 0; sweep < sweeps; ++sweep) {
+    for (int row = 0; row < count; ++row) {
+      float sum = b[row], error = 0.0f;
+      for (int j = rows[row]; j < rows[row + 1]; ++j)
+        residual_term(sum, error, vals[j], current[cols[j]]);
+      r[row] = sum + error;
+    }
+    for (int row = 0; row < count; ++row) current[row] += (2.0f / 3.0f) * inv[row] * r[row];
+  }
+  for (int row = 0; row < count; ++row) x[row] = current[row];
+}
+
+// krylov_diagonal, linalg.kern.h:52-70, with the refresh's max_abs check of the
+// invalid flags fused (amg.cpp:236-240).
+__global__ void k_diagonal(int n, const int* __restrict__ rows, const int* __restrict__ diag,
+                           const float* __restrict__ vals, float* __restrict__ inverse,
+                           int use_l1, DeviceReducer red, double* check, int slot) {
+  double worst = 0;
+  ROWS(i, n) {
+    const float d = vals[diag[i]];
+    float off = 0.0f, bad = 0.0f;
+    for (int j = rows[i]; j < rows[i + 1]; ++j) {
+      const float v = vals[j];
+      if (v - v != 0.0f) bad = 1.0f;
+      if (j != diag[i]) off += fabsf(v);
+    }
+    const float inv = d != 0.0f ? 1.0f / d : 0.0f;
+    const float l1 = fmaxf(fabsf(d), 0.5f * (fabsf(d) + off));
+    inverse[i] = use_l1 != 0 ? (l1 != 0.0f ? 1.0f / l1 : 0.0f) : inv;
+    const float invalid = (bad != 0.0f || inv - inv != 0.0f || l1 - l1 != 0.0f)
+                              ? 2.0f
+                              : (use_l1 != 0 && d < 0.0f ? 3.0f : (d == 0.0f ? 1.0f : 0.0f));
+    worst = nan_max(worst, static_cast<double>(invalid));
+  }
+  __shared__ double shared[32];
+  worst = block_max(worst, shared);
+  const Reducer r = as_reducer(red);
+  if (!publish(r, worst, 0, false)) return;
+  const double total = gather_max(r, shared);
+  if (threadIdx.x == 0) {
+    check[slot] = total;
+    *r.ticket = 0;
+  }
+}
+
+// ---- AMG transfer and Galerkin, src/kutta/kernels/amg.kern.h ------------------
+// amg_restrict(_guarded) :5-16,84-87: Kahan sum over the aggregate's members.
+__global__ void k_restrict(int nc, const int* __restrict__ offsets,
+                           const int* __restrict__ members, const float* __restrict__ fine,
+                           float* __restrict__ coarse, const int* __restrict__ status) {
+  if (status[0] != 0) return;
+  ROWS(g, nc) {
+    float sum = 0.0f, error = 0.0f;
+    for (int j = offsets[g]; j < offsets[g + 1]; ++j) {
+      const float term = fine[members[j]] - error;
+      const float next = sum + term;
+      error = (next - sum) - term;
+      sum = next;
+    }
+    coarse[g] = sum;
+  }
+}
+
+// amg_prolong(_guarded) :18-21,88-91.
+__global__ void k_prolong(int nf, const int* __restrict__ aggregate,
+                          const float* __restrict__ coarse, float* __restrict__ fine,
+                          const int* __restrict__ status) {
+  if (status[0] != 0) return;
+  ROWS(i, nf) {
+    const int g = aggregate[i];
+    if (g >= 0) fine[i] += coarse[g];
+  }
+}
+
+// amg_galerkin :27-38: Neumaier sum over the coarse entry's fine entries.
+__global__ void k_galerkin(int nnz_c, const int* __restrict__ offsets,
+                           const int* __restrict__ entries, const float* __restrict__ fine,
+                           float* __restrict__ coarse) {
+  ROWS(e, nnz_c) {
+    float sum = 0.0f, error = 0.0f;
+    for (int j = offsets[e]; j < offsets[e + 1]; ++j) neumaier_term(sum, error, fine[entries[j]]);
+    coarse[e] = sum + error;
+  }
+}
+
+// amg_m_matrix_diagonal :44-58.
+__global__ void k_m_matrix_diagonal(int nc, const int* __restrict__ offsets,
+                                    const int* __restrict__ members,
+                                    const int* __restrict__ fine_rows,
+                                    const int* __restrict__ fine_diag,
+                                    const float* __restrict__ fine, const int* __restrict__ rows,
+                                    const int* __restrict__ diag, float* coarse) {
+  ROWS(g, nc) {
+    UpperSum diagonal{0.0f, 0.0f};
+    for (int m = offsets[g]; m < offsets[g + 1]; ++m) {
+      const int row = members[m];
+      UpperSum surplus{fine[fine_diag[row]], 0.0f};
+      for (int j = fine_rows[row]; j < fine_rows[row + 1]; ++j)
+        if (j != fine_diag[row]) surplus = upper_add(surplus, fine[j]);
+      diagonal = upper_add(diagonal, upper_value(surplus));
+    }
+    for (int j = rows[g]; j < rows[g + 1]; ++j)
+      if (j != diag[g]) diagonal = upper_add(diagonal, -coarse[j]);
+    coarse[diag[g]] = upper_value(diagonal);
+  }
+}
+
+// ---- Krylov vector updates, scalars.kern.h:122-152 ---------------------------
+// solver_step :122-127 + dot_into(r, r -> 18) + solver_check(pcg) (solver.cpp:291-293).
+__global__ void k_pcg_step_dot(int n, float* __restrict__ x, float* __restrict__ r,
+                               const float* __restrict__ p, const float* __restrict__ q,
+                               DeviceReducer red, float* scalars, int* status) {
+  if (status[0] != 0) return;
+  const float alpha = kp_float(kp_load(scalars, 8));
+  double acc = 0;
+  ROWS(i, n) {
+    x[i] += alpha * p[i];
+    const float ri = r[i] - alpha * q[i];
+    r[i] = ri;
+    acc += static_cast<double>(ri) * static_cast<double>(ri);
+  }
+  finish(as_reducer(red), acc, 0, false, scalars, 18, status, Epilogue::CheckPcg);
+}
+
+// solver_direction :128-131.
+__global__ void k_direction(int n, const float* __restrict__ z, float* __restrict__ p,
+                            const float* __restrict__ scalars, const int* __restrict__ status) {
+  if (status[0] != 0) return;
+  const float beta = kp_float(kp_load(scalars, 10));
+  ROWS(i, n) p[i] = z[i] + beta * p[i];
+}
+
+// solver_bicg_direction :132-137.
+__global__ void k_bicg_direction(int n, const float* __restrict__ r, const float* __restrict__ v,
+                                 float* __restrict__ p, const float* __restrict__ scalars,
+                                 const int* __restrict__ status) {
+  if (status[0] != 0) return;
+  const float beta = kp_float(kp_load(scalars, 10)), omega = kp_float(kp_load(scalars, 12));
+  ROWS(i, n) p[i] = r[i] + beta * (p[i] - omega * v[i]);
+}
+
+// solver_bicg_difference :138-141.
+__global__ void k_bicg_difference(int n, const float* __restrict__ r, const float* __restrict__ q,
+                                  float* __restrict__ sv, const float* __restrict__ scalars,
+                                  const int* __restrict__ status) {
+  if (status[0] != 0) return;
+  const float alpha = kp_float(kp_load(scalars, 8));
+  ROWS(i, n) sv[i] = r[i] - alpha * q[i];
+}
+
+// solver_bicg_step :142-149.
+__global__ void k_bicg_step(int n, float* __restrict__ x, float* __restrict__ r,
+                            const float* __restrict__ z, const float* __restrict__ zs,
+                            const float* __restrict__ sv, const float* __restrict__ t,
+                            const float* __restrict__ scalars, const int* __restrict__ status) {
+  if (status[0] != 0) return;
+  const float alpha = kp_float(kp_load(scalars, 8)), omega = kp_float(kp_load(scalars, 12));
+  const bool s_only = status[2] != 0;
+  ROWS(i, n) {
+    if (s_only) {
+      x[i] += alpha * z[i];
+      r[i] = sv[i];
+    } else {
+      x[i] += alpha * z[i] + omega * zs[i];
+      r[i] = sv[i] - omega * t[i];
+    }
+  }
+}
+
+// krylov_multiply(_guarded), linalg.kern.h:72-75,119-122.
+__global__ void k_multiply(int n, const float* __restrict__ r, const float* __restrict__ inverse,
+                           float* __restrict__ z, const int* __restrict__ status) {
+  if (status && status[0] != 0) return;
+  ROWS(i, n) z[i] = r[i] * inverse[i];
+}
+
+// axpy, blas.kern.h:5.
+__global__ void k_axpy(int n, float* __restrict__ y, const float* __restrict__ x, float a) {
+  ROWS(i, n) y[i] = y[i] + a * x[i];
+}
+
+__global__ void k_fill(int n, float* __restrict__ x, float value) { ROWS(i, n) x[i] = value; }
+
+// ---- reductions ---------------------------------------------------------------
+// Device::reduce_into (device.hpp:186-202) with FP64 accumulation.
+__global__ void k_reduce_into(ReduceMode mode, int n, const float* __restrict__ x,
+                              const float* __restrict__ y, const float* __restrict__ u,
+                              const float* __restrict__ v, DeviceReducer red, float* scalars,
+                              int offset, int* status, bool guard, Epilogue epi) {
+  if (guard && status[0] != 0) return;
+  double a = 0, b = 0;
+  const bool dual = mode == ReduceMode::Dot2;
+  ROWS(i, n) {
+    a += mode == ReduceMode::Sum ? static_cast<double>(x[i])
+                                 : static_cast<double>(x[i]) * static_cast<double>(y[i]);
+    if (dual) b += static_cast<double>(u[i]) * static_cast<double>(v[i]);
+  }
+  finish(as_reducer(red), a, b, dual, scalars, offset, status, epi);
+}
+
+// Host reductions (Device::sum/dot/max_abs): the FP64 value into out[slot].
+__global__ void k_reduce_value(ReduceMode mode, int n, const float* __restrict__ x,
+                               const float* __restrict__ y, DeviceReducer red, double* out,
+                               int slot) {
+  __shared__ double shared[32];
+  double a = 0;
+  ROWS(i, n) {
+    if (mode == ReduceMode::MaxAbs) a = nan_max(a, fabs(static_cast<double>(x[i])));
+    else if (mode == ReduceMode::Sum) a += static_cast<double>(x[i]);
+    else a += static_cast<double>(x[i]) * static_cast<double>(y[i]);
+  }
+  const Reducer r = as_reducer(red);
+  a = mode == ReduceMode::MaxAbs ? block_max(a, shared) : block_sum(a, shared);
+  if (!publish(r, a, 0, false)) return;
+  const double total = mode == ReduceMode::MaxAbs ? gather_max(r, shared) : gather(r, 0, shared);
+  if (threadIdx.x == 0) {
+    out[slot] = total;
+    *r.ticket = 0;
+  }
+}
+
+// solver_limits :51-55 (all 24 slots).
+__global__ void k_solver_limits(float* scalars, float th, float tl, float dh, float dl) {
+  const int i = threadIdx.x;
+  if (i < 24)
+    scalars[i] = i == 20 ? th : (i == 21 ? tl : (i == 22 ? dh : (i == 23 ? dl : 0.0f)));
+}
+
+// solver_reset :56-62.
+__global__ void k_solver_reset(float* scalars, int* status, int iterations) {
+  status[0] = 0;
+  status[1] = iterations;
+  status[2] = 0;
+  scalars[8] = 1.0f;
+  scalars[9] = 0.0f;
+  scalars[12] = 1.0f;
+  scalars[13] = 0.0f;
+  scalars[14] = 1.0f;
+  scalars[15] = 0.0f;
+}
+
+// solver_project :150-152.
+__global__ void k_project(int n, float* __restrict__ x, const float* __restrict__ sum,
+                          float count_hi, float count_lo) {
+  const float mean = kp_float(kp_div(kp_load(sum, 0), kp(count_hi, count_lo)));
+  ROWS(i, n) x[i] -= mean;
+}
+
+inline int blocks(int n) { return grid_for(n); }
+static_assert(kReducePartials == kPartials, "reduction scratch size");
+
+}  // namespace
+
+namespace launch {
+
+void spmv(int n, const int* rows, const int* cols, const float* vals, const float* x, float* y,
+          const int* status, cudaStream_t s) {
+  if (n <= 0) return;
+  k_spmv<<<blocks(n), kBlock, 0, s>>>(n, rows, cols, vals, x, y, status);
+}
+void spmv_dot(int n, const int* rows, const int* cols, const float* vals, const float* p,
+              const float* w, float* q, DeviceReducer red, float* scalars, int offset,
+              int* status, Epilogue epi, cudaStream_t s) {
+  k_spmv_dot<<<blocks(n), kBlock, 0, s>>>(n, rows, cols, vals, p, w, q, red, scalars, offset,
+                                          status, epi);
+}
+void residual(int n, const int* rows, const int* cols, const float* vals, const float* x,
+              const float* b, float* r, const int* status, cudaStream_t s) {
+  if (n <= 0) return;
+  k_residual<<<blocks(n), kBlock, 0, s>>>(n, rows, cols, vals, x, b, r, status);
+}
+void smooth(int n, const int* rows, const int* cols, const float* vals, const float* x,
+            const float* b, const float* inv, float* next, const int* status, bool zero_start,
+            cudaStream_t s) {
+  if (n <= 0) return;
+  if (zero_start)
+    k_smooth<true><<<blocks(n), kBlock, 0, s>>>(n, rows, cols, vals, x, b, inv, next, status);
+  else
+    k_smooth<false><<<blocks(n), kBlock, 0, s>>>(n, rows, cols, vals, x, b, inv, next, status);
+}
+void coarse_solve(int count, const int* rows, const int* cols, const float* vals, float* x,
+                  const float* b, const float* inv, const int* status, int sweeps,
+                  cudaStream_t s) {
+  k_coarse_solve<<<1, 32, 0, s>>>(count, rows, cols, vals, x, b, inv, status, sweeps);
+}
+void diagonal(int n, const int* rows, const int* diag, const float* vals, float* inverse,
+              int use_l1, DeviceReducer red, double* check, int slot, cudaStream_t s) {
+  k_diagonal<<<blocks(n), kBlock, 0, s>>>(n, rows, diag, vals, inverse, use_l1, red, check, slot);
+}
+void restrict_(int nc, const int* offsets, const int* members, const float* fine, float* coarse,
+               const int* status, cudaStream_t s) {
+  if (nc <= 0) return;
+  k_restrict<<<blocks(nc), kBlock, 0, s>>>(nc, offsets, members, fine, coarse, status);
+}
+void prolong(int nf, const int* aggregate, const float* coarse, float* fine, const int* status,
+             cudaStream_t s) {
+  if (nf <= 0) return;
+  k_prolong<<<blocks(nf), kBlock, 0, s>>>(nf, aggregate, coarse, fine, status);
+}
+void galerkin(int nnz_c, const int* offsets, const int* entries, const float* fine, float* coarse,
+              cudaStream_t s) {
+  if (nnz_c <= 0) return;
+  k_galerkin<<<blocks(nnz_c), kBlock, 0, s>>>(nnz_c, offsets, entries, fine, coarse);
+}
+void m_matrix_diagonal(int nc, const int* offsets, const int* members, const int* fine_rows,
+                       const int* fine_diag, const float* fine, const int* rows, const int* diag,
+                       float* coarse, cudaStream_t s) {
+  if (nc <= 0) return;
+  k_m_matrix_diagonal<<<blocks(nc), kBlock, 0, s>>>(nc, offsets, members, fine_rows, fine_diag,
+                                                    fine, rows, diag, coarse);
+}
+void pcg_step_dot(int n, float* x, float* r, const float* p, const float* q, DeviceReducer red,
+                  float* scalars, int* status, cudaStream_t s) {
+  k_pcg_step_dot<<<blocks(n), kBlock, 0, s>>>(n, x, r, p, q, red, scalars, status);
+}
+void direction(int n, const float* z, float* p, const float* scalars, const int* status,
+               cudaStream_t s) {
+  if (n <= 0) return;
+  k_direction<<<blocks(n), kBlock, 0, s>>>(n, z, p, scalars, status);
+}
+void bicg_direction(int n, const float* r, const float* v, float* p, const float* scalars,
+                    const int* status, cudaStream_t s) {
+  if (n <= 0) return;
+  k_bicg_direction<<<blocks(n), kBlock, 0, s>>>(n, r, v, p, scalars, status);
+}
+void bicg_difference(int n, const float* r, const float* q, float* sv, const float* scalars,
+                     const int* status, cudaStream_t s) {
+  if (n <= 0) return;
+  k_bicg_difference<<<blocks(n), kBlock, 0, s>>>(n, r, q, sv, scalars, status);
+}
+void bicg_step(int n, float* x, float* r, const float* z, const float* zs, const float* sv,
+               const float* t, const float* scalars, const int* status, cudaStream_t s) {
+  if (n <= 0) return;
+  k_bicg_step<<<blocks(n), kBlock, 0, s>>>(n, x, r, z, zs, sv, t, scalars, status);
+}
+void multiply(int n, const float* r, const float* inverse, float* z, const int* status,
+              cudaStream_t s) {
+  if (n <= 0) return;
+  k_multiply<<<blocks(n), kBlock, 0, s>>>(n, r, inverse, z, status);
+}
+void axpy(int n, float* y, const float* x, float a, cudaStream_t s) {
+  if (n <= 0) return;
+  k_axpy<<<blocks(n), kBlock, 0, s>>>(n, y, x, a);
+}
+void fill(int n, float* x, float value, cudaStream_t s) {
+  if (n <= 0) return;
+  k_fill<<<blocks(n), kBlock, 0, s>>>(n, x, value);
+}
+void reduce_into(ReduceMode mode, int n, const float* x, const float* y, const float* u,
+                 const float* v, DeviceReducer red, float* scalars, int offset, int* status,
+                 bool guard, Epilogue epi, cudaStream_t s) {
+  k_reduce_into<<<blocks(n), kBlock, 0, s>>>(mode, n, x, y, u, v, red, scalars, offset, status,
+                                             guard, epi);
+}
+void reduce_value(ReduceMode mode, int n, const float* x, const float* y, DeviceReducer red,
+                  double* out, int slot, cudaStream_t s) {
+  k_reduce_value<<<blocks(n), kBlock, 0, s>>>(mode, n, x, y, red, out, slot);
+}
+void solver_limits(float* scalars, float th, float tl, float dh, float dl, cudaStream_t s) {
+  k_solver_limits<<<1, 32, 0, s>>>(scalars, th, tl, dh, dl);
+}
+void solver_reset(float* scalars, int* status, int iterations, cudaStream_t s) {
+  k_solver_reset<<<1, 1, 0, s>>>(scalars, status, iterations);
+}
+void project(int n, float* x, const float* sum, float count_hi, float count_lo, cudaStream_t s) {
+  if (n <= 0) return;
+  k_project<<<blocks(n), kBlock, 0, s>>>(n, x, sum, count_hi, count_lo);
+}
+
+}  // namespace launch
+}  // namespace kb2

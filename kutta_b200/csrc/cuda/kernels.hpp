@@ -1,0 +1,111 @@
+// Host launchers for the sm_100a solver kernels. Plain pointers and sizes;
+// every launcher enqueues on `stream` and never synchronises.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace kb2 {
+
+// Scalar epilogues run by the last block of a fused reduction, after the
+// reduced value is stored as a (hi, lo) pair: the single-thread scalar kernels
+// of src/kutta/kernels/scalars.kern.h:51-121.
+enum class Epilogue : int {
+  None = 0,
+  PcgAlpha,         // solver_pcg_alpha
+  CheckPcg,         // solver_check(pcg = 1)
+  CheckBicg,        // solver_check(pcg = 0)
+  PcgBeta,          // solver_pcg_beta(flexible = 0)
+  PcgBetaFlexible,  // solver_pcg_beta(flexible = 1)
+  BicgBeta,         // solver_bicg_beta
+  BicgAlpha,        // solver_bicg_alpha
+  BicgS,            // solver_bicg_s
+  BicgOmega,        // solver_bicg_omega
+};
+
+// Reduction modes of Device::reduce_into / host reductions.
+enum class ReduceMode : int { Sum = 0, Dot = 1, Dot2 = 2, MaxAbs = 3 };
+
+// Doubles of reduction scratch per reducer: two partials per block for at most
+// 148 SMs x 8 blocks.
+constexpr int kReducePartials = 2 * 148 * 8;
+
+struct DeviceReducer {
+  double* partials;   // 2 * kMaxBlocks doubles
+  unsigned* ticket;   // zero-initialised counter
+};
+
+namespace launch {
+
+// ---- CSR row kernels (one row per thread, grid-stride) -------------------
+// y = A x, Kahan-compensated (csr_spmv). status may be null (unguarded).
+void spmv(int n, const int* rows, const int* cols, const float* vals, const float* x, float* y,
+          const int* status, cudaStream_t s);
+// q = A p and w.q -> scalars[offset] as a pair, then `epi` (guarded by status).
+void spmv_dot(int n, const int* rows, const int* cols, const float* vals, const float* p,
+              const float* w, float* q, DeviceReducer red, float* scalars, int offset,
+              int* status, Epilogue epi, cudaStream_t s);
+// r = b - A x, Neumaier + Dekker compensated (csr_residual). status may be null.
+void residual(int n, const int* rows, const int* cols, const float* vals, const float* x,
+              const float* b, float* r, const int* status, cudaStream_t s);
+// next = x + (2/3) inv (b - A x)  (amg_smooth); zero_start: x treated as the
+// zero vector without reading it (amg_smooth_zero).
+void smooth(int n, const int* rows, const int* cols, const float* vals, const float* x,
+            const float* b, const float* inv, float* next, const int* status, bool zero_start,
+            cudaStream_t s);
+// <=24-row coarsest level, `sweeps` Jacobi sweeps in one thread (amg_coarse_solve).
+void coarse_solve(int count, const int* rows, const int* cols, const float* vals, float* x,
+                  const float* b, const float* inv, const int* status, int sweeps,
+                  cudaStream_t s);
+// Inverse (L1) diagonal and invalid flags (krylov_diagonal); the max of the
+// flags is written to check[slot] as a double (no host wait).
+void diagonal(int n, const int* rows, const int* diag, const float* vals, float* inverse,
+              int use_l1, DeviceReducer red, double* check, int slot, cudaStream_t s);
+
+// ---- AMG transfer and Galerkin --------------------------------------------
+void restrict_(int nc, const int* offsets, const int* members, const float* fine, float* coarse,
+               const int* status, cudaStream_t s);
+void prolong(int nf, const int* aggregate, const float* coarse, float* fine, const int* status,
+             cudaStream_t s);
+void galerkin(int nnz_c, const int* offsets, const int* entries, const float* fine, float* coarse,
+              cudaStream_t s);
+void m_matrix_diagonal(int nc, const int* offsets, const int* members, const int* fine_rows,
+                       const int* fine_diag, const float* fine, const int* rows, const int* diag,
+                       float* coarse, cudaStream_t s);
+
+// ---- Krylov vector updates (guarded by status) ----------------------------
+// x += a p; r -= a q; then r.r -> scalars[18] and solver_check(pcg = 1).
+void pcg_step_dot(int n, float* x, float* r, const float* p, const float* q, DeviceReducer red,
+                  float* scalars, int* status, cudaStream_t s);
+void direction(int n, const float* z, float* p, const float* scalars, const int* status,
+               cudaStream_t s);
+void bicg_direction(int n, const float* r, const float* v, float* p, const float* scalars,
+                    const int* status, cudaStream_t s);
+void bicg_difference(int n, const float* r, const float* q, float* sv, const float* scalars,
+                     const int* status, cudaStream_t s);
+void bicg_step(int n, float* x, float* r, const float* z, const float* zs, const float* sv,
+               const float* t, const float* scalars, const int* status, cudaStream_t s);
+void multiply(int n, const float* r, const float* inverse, float* z, const int* status,
+              cudaStream_t s);
+void axpy(int n, float* y, const float* x, float a, cudaStream_t s);
+void fill(int n, float* x, float value, cudaStream_t s);
+
+// ---- reductions -----------------------------------------------------------
+// Sum / Dot / Dot2 of the first n entries, FP64, written as pair(s) into
+// scalars[offset..]; then `epi`. guard: skip entirely when status[0] != 0
+// (every consumer of these slots is itself guarded).
+void reduce_into(ReduceMode mode, int n, const float* x, const float* y, const float* u,
+                 const float* v, DeviceReducer red, float* scalars, int offset, int* status,
+                 bool guard, Epilogue epi, cudaStream_t s);
+// Host reductions: FP64 value into out[slot] (device double array).
+void reduce_value(ReduceMode mode, int n, const float* x, const float* y, DeviceReducer red,
+                  double* out, int slot, cudaStream_t s);
+
+// ---- single-thread scalar kernels -------------------------------------------
+void solver_limits(float* scalars, float th, float tl, float dh, float dl, cudaStream_t s);
+void solver_reset(float* scalars, int* status, int iterations, cudaStream_t s);
+// x -= mean(x) using the pair sum at sum[0..1] (solver_project).
+void project(int n, float* x, const float* sum, float count_hi, float count_lo, cudaStream_t s);
+
+}  // namespace launch
+}  // namespace kb2

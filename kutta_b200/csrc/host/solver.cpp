@@ -1,0 +1,491 @@
+// Krylov drivers and the aggregation-AMG preconditioner on sm_100a kernels.
+//
+// The host-side control flow follows the reference's Krylov class exactly
+// (src/kutta/linalg/solver.cpp:75-393: batched status polls, reliable residual
+// replacement, best-iterate restore, small-system speculation) and its
+// Aggregation preconditioner (amg.cpp:198-342: refresh with one host wait,
+// V-cycle with ping-pong smoothing), so iteration counts and returned iterates
+// follow the reference's. All vector and scalar work runs on the device.
+#include "solver.hpp"
+
+#include <algorithm>
+#include <array>
+#include <cmath>
+#include <cstring>
+#include <iomanip>
+#include <sstream>
+
+namespace kb2 {
+
+namespace {
+constexpr int kSpeculativeRows = 1 << 17;  // solver.cpp:387
+}
+
+Solver::Solver(Kind kind, const CsrView& a, const Options& options,
+               std::shared_ptr<Workspace> workspace)
+    : kind_(kind), options_(options), n_(a.n), nnz_(a.nnz), nullspace_(options.nullspace),
+      workspace_(std::move(workspace)) {
+  cuda_check(cudaGetDevice(&device_), "cudaGetDevice");
+  if (!workspace_) workspace_ = std::make_shared<Workspace>(a.n);
+  KB2_REQUIRE(workspace_->rows() == a.n, "Krylov workspace size mismatch");
+  cudaStream_t s = nullptr;
+  // Level 0 pattern: the solver's own device copy of the caller's pattern.
+  levels_.reserve(static_cast<std::size_t>(std::max(1, options.max_levels)));
+  levels_.emplace_back();
+  {
+    auto& l = levels_.back();
+    l.n = a.n;
+    l.nnz = a.nnz;
+    l.row_ptr.reset(static_cast<std::size_t>(a.n) + 1);
+    l.row_ptr.upload(a.row_ptr, static_cast<std::size_t>(a.n) + 1, s);
+    l.col.reset(static_cast<std::size_t>(a.nnz));
+    l.col.upload(a.col, static_cast<std::size_t>(a.nnz), s);
+    l.diag.reset(static_cast<std::size_t>(a.n));
+    l.diag.upload(a.diag, static_cast<std::size_t>(a.n), s);
+  }
+  if (amg()) {
+    // Aggregation ctor (amg.cpp:200-226): host hierarchy, then uploads.
+    const Hierarchy h = build_hierarchy(a, options_);
+    complexity_ = h.complexity;
+    for (std::size_t i = 0; i < h.levels.size(); ++i) {
+      if (i > 0) {
+        levels_.emplace_back();
+        auto& l = levels_.back();
+        const auto& m = h.levels[i].matrix;
+        l.n = m.n;
+        l.nnz = m.nnz();
+        l.row_ptr.upload(m.row_ptr, s);
+        l.col.upload(m.col, s);
+        l.diag.upload(m.diag, s);
+        std::vector<float> v(m.val.begin(), m.val.end());
+        l.val.upload(v, s);
+        l.xa.reset(static_cast<std::size_t>(m.n));
+        l.b.reset(static_cast<std::size_t>(m.n));
+        l.x = l.xa.get();
+      }
+      auto& l = levels_.back();
+      l.l1.upload(h.levels[i].l1, s);
+      l.ra.reset(static_cast<std::size_t>(l.n));
+      l.r = l.ra.get();
+      if (nullspace_) l.projection.reset(2);
+      const auto& t = h.levels[i].transfer;
+      if (i + 1 < h.levels.size()) {
+        l.aggregate.upload(t.aggregate, s);
+        l.member_offsets.upload(t.member_offsets, s);
+        l.members.upload(t.members, s);
+        l.entry_offsets.upload(t.entry_offsets, s);
+        l.entries.upload(t.entries, s);
+      }
+    }
+  } else {
+    // Jacobi preconditioner (solver.cpp:56-73).
+    jacobi_inverse_.upload(diagonal_values(a, false, false), s);
+  }
+  // Krylov ctor (solver.cpp:77-90).
+  r_ = workspace_->vector(Workspace::R);
+  z_ = workspace_->vector(Workspace::Z);
+  if (kind_ != Kind::Jacobi) {
+    p_ = workspace_->vector(Workspace::P);
+    q_ = workspace_->vector(Workspace::Q);
+  }
+  if (bicg()) {
+    shadow_ = workspace_->vector(Workspace::Shadow);
+    s_ = workspace_->vector(Workspace::S);
+    t_ = workspace_->vector(Workspace::T);
+    zs_ = workspace_->vector(Workspace::Zs);
+  }
+  best_ = workspace_->vector(Workspace::Best);
+  if (!amg()) scratch_ = workspace_->vector(Workspace::Scratch);
+  scalars_.reset(24);
+  status_.reset(3);
+  projection_.reset(nullspace_ ? 2 : 0);
+  partials_.reset(kReducePartials);
+  values_.reset(64);
+  ticket_.reset(1);
+  cuda_check(cudaMemsetAsync(ticket_.get(), 0, sizeof(unsigned), s), "memset");
+  cuda_check(cudaMemsetAsync(scalars_.get(), 0, 24 * sizeof(float), s), "memset");
+  cuda_check(cudaMemsetAsync(status_.get(), 0, 3 * sizeof(int), s), "memset");
+  speculate_ = kind_ != Kind::Jacobi && n_ <= kSpeculativeRows;
+  wait(s);
+}
+
+// ---------------------------------------------------------------- primitives --
+void Solver::residual(const float* x, const float* b, float* r) {
+  launch::residual(n_, rows0(), cols0(), val_, x, b, r, nullptr, stream_);
+}
+
+std::vector<double> Solver::host_reduce(std::initializer_list<Request> requests) {
+  int slot = 0;
+  for (const auto& q : requests)
+    launch::reduce_value(q.mode, q.n, q.x, q.y, reducer(), values_.get(), slot++, stream_);
+  cuda_check(cudaMemcpyAsync(host_values_.get(), values_.get(), sizeof(double) * slot,
+                             cudaMemcpyDeviceToHost, stream_),
+             "reduction readback");
+  wait(stream_);
+  cuda_check(cudaGetLastError(), "reduction");
+  return std::vector<double>(host_values_.get(), host_values_.get() + slot);
+}
+
+double Solver::norm(const float* x) {
+  return std::sqrt(host_reduce({{ReduceMode::Dot, x, x, n_}})[0]);
+}
+
+void Solver::copy(float* dst, const float* src, int n) {
+  if (n > 0 && dst != src)
+    cuda_check(cudaMemcpyAsync(dst, src, sizeof(float) * static_cast<std::size_t>(n),
+                               cudaMemcpyDeviceToDevice, stream_),
+               "copy");
+}
+
+// linalg_detail::project, detail.hpp:13-19.
+void Solver::project(float* x, int n, float* projection) {
+  if (n == 0) return;
+  launch::reduce_into(ReduceMode::Sum, n, x, x, x, x, reducer(), projection, 0, status_.get(),
+                      false, Epilogue::None, stream_);
+  const float count = static_cast<float>(n);
+  launch::project(n, x, projection, count,
+                  static_cast<float>(static_cast<double>(n) - static_cast<double>(count)), stream_);
+}
+
+void Solver::reset(int iterations) { launch::solver_reset(scalars_.get(), status_.get(), iterations, stream_); }
+
+// ------------------------------------------------------------ preconditioner --
+void Solver::smooth(DevLevel& l, const int* rows, const int* cols, const float* vals,
+                    const float* b, float*& x, int sweeps, bool zero_start) {
+  for (int sweep = 0; sweep < sweeps; ++sweep) {
+    launch::smooth(l.n, rows, cols, vals, x, b, l.l1.get(), l.r, status_.get(),
+                   zero_start && sweep == 0, stream_);
+    std::swap(x, l.r);  // ping-pong: the two buffers exchange roles (amg.cpp:280)
+  }
+}
+
+// Aggregation::cycle, amg.cpp:283-310.
+void Solver::cycle(std::size_t index, const float* b, float*& x) {
+  auto& l = levels_[index];
+  const int* rows = l.row_ptr.get();
+  const int* cols = l.col.get();
+  const float* vals = index == 0 ? val_ : l.val.get();
+  // x is not cleared: every first step below writes it without reading it.
+  if (index + 1 == levels_.size()) {
+    if (l.n <= 24)
+      launch::coarse_solve(l.n, rows, cols, vals, x, b, l.l1.get(), status_.get(),
+                           options_.coarse_sweeps, stream_);
+    else
+      smooth(l, rows, cols, vals, b, x, options_.coarse_sweeps, true);
+  } else {
+    smooth(l, rows, cols, vals, b, x, options_.pre_sweeps, true);
+    launch::residual(l.n, rows, cols, vals, x, b, l.r, status_.get(), stream_);
+    auto& c = levels_[index + 1];
+    launch::restrict_(c.n, l.member_offsets.get(), l.members.get(), l.r, c.b.get(),
+                      status_.get(), stream_);
+    if (nullspace_) project(c.b.get(), c.n, c.projection.get());
+    cycle(index + 1, c.b.get(), c.x);
+    launch::prolong(l.n, l.aggregate.get(), c.x, x, status_.get(), stream_);
+    smooth(l, rows, cols, vals, b, x, options_.post_sweeps, false);
+  }
+  if (nullspace_ && index != 0) project(x, l.n, l.projection.get());
+}
+
+// Krylov::apply (solver.cpp:197-200) with the AMG (amg.cpp:258-261) or Jacobi
+// (solver.cpp:65-68) preconditioner.
+void Solver::apply(const float* r, float*& z) {
+  if (amg()) cycle(0, r, z);
+  else launch::multiply(n_, r, jacobi_inverse_.get(), z, status_.get(), stream_);
+  if (nullspace_) project(z, n_, projection_.get());
+}
+
+// Krylov::refresh (solver.cpp:92-95) + Aggregation::refresh (amg.cpp:228-256) or
+// Jacobi::refresh (solver.cpp:61-64). One host wait for all validity checks.
+void Solver::refresh(const float* val, cudaStream_t s) {
+  stream_ = s;
+  val_ = val;
+  if (!amg()) {
+    launch::diagonal(n_, rows0(), levels_[0].diag.get(), val, jacobi_inverse_.get(), 0, reducer(),
+                     values_.get(), 0, s);
+    cuda_check(cudaMemcpyAsync(host_values_.get(), values_.get(), sizeof(double),
+                               cudaMemcpyDeviceToHost, s),
+               "refresh readback");
+    wait(s);
+    cuda_check(cudaGetLastError(), "refresh");
+    KB2_REQUIRE(host_values_[0] == 0, "Jacobi: invalid values or zero diagonal");
+    return;
+  }
+  const float* matrix = val;
+  std::vector<double> allowed;
+  for (std::size_t i = 0; i < levels_.size(); ++i) {
+    auto& l = levels_[i];
+    launch::diagonal(l.n, l.row_ptr.get(), l.diag.get(), matrix, l.l1.get(), 1, reducer(),
+                     values_.get(), static_cast<int>(i), s);
+    allowed.push_back(nullspace_ && l.n == 1 ? 1 : 0);
+    if (i + 1 < levels_.size()) {
+      auto& c = levels_[i + 1];
+      launch::galerkin(c.nnz, l.entry_offsets.get(), l.entries.get(), matrix, c.val.get(), s);
+      if (options_.m_matrix)
+        launch::m_matrix_diagonal(c.n, l.member_offsets.get(), l.members.get(), l.row_ptr.get(),
+                                  l.diag.get(), matrix, c.row_ptr.get(), c.diag.get(),
+                                  c.val.get(), s);
+      matrix = c.val.get();
+    }
+  }
+  cuda_check(cudaMemcpyAsync(host_values_.get(), values_.get(), sizeof(double) * levels_.size(),
+                             cudaMemcpyDeviceToHost, s),
+             "refresh readback");
+  wait(s);
+  cuda_check(cudaGetLastError(), "refresh");
+  for (std::size_t i = 0; i < levels_.size(); ++i) {
+    const double invalid = host_values_[i];
+    KB2_REQUIRE(invalid != 3, "AMG: requires positive diagonals");
+    KB2_REQUIRE(invalid <= allowed[i], "AMG: invalid values or zero diagonal");
+  }
+}
+
+// --------------------------------------------------------------------- Krylov --
+bool Solver::verified(float* x, const float* b, double target, Stats& stats) {
+  if (speculated_) {
+    // The same kernels already ran on copies of this exact x; adopt them.
+    if (nullspace_) copy(x, speculative_x(), n_);
+    copy(r_, speculative_r(), n_);
+    stats.final_residual = *speculated_;
+    speculated_.reset();
+  } else {
+    if (nullspace_) project(x, n_, projection_.get());
+    residual(x, b, r_);
+    stats.final_residual = norm(r_);
+  }
+  verified_current_ = true;
+  stats.converged = std::isfinite(stats.final_residual) && stats.final_residual <= target;
+  if (stats.final_residual < best_residual_) {
+    best_residual_ = stats.final_residual;
+    copy(best_, x, n_);
+  }
+  if (nullspace_) project(r_, n_, projection_.get());
+  return stats.converged;
+}
+
+std::vector<int> Solver::poll(const float* x, const float* b) {
+  if (speculate_) {
+    const float* source = x;
+    if (nullspace_) {
+      copy(speculative_x(), x, n_);
+      project(speculative_x(), n_, projection_.get());
+      source = speculative_x();
+    }
+    float* r = speculative_r();
+    residual(source, b, r);
+    speculated_ = std::sqrt(host_reduce({{ReduceMode::Dot, r, r, n_}})[0]);
+  }
+  cuda_check(cudaMemcpyAsync(host_status_.get(), status_.get(), 3 * sizeof(int),
+                             cudaMemcpyDeviceToHost, stream_),
+             "status readback");
+  wait(stream_);
+  cuda_check(cudaGetLastError(), "solve");
+  return {host_status_[0], host_status_[1], host_status_[2]};
+}
+
+bool Solver::replacement(float* x, const float* b, double target, Stats& stats, int& restarts,
+                         double& last_verified) {
+  if (verified(x, b, target, stats) || diverged(stats)) return false;
+  restarts = stats.final_residual >= 0.9 * last_verified ? restarts + 1 : 0;
+  last_verified = stats.final_residual;
+  return restarts < 12;
+}
+
+// Krylov::pcg, solver.cpp:271-313. Per update: SpMV fused with p.q and alpha;
+// the x/r update fused with r.r and the convergence check; the preconditioner;
+// r.z fused with beta; the direction update.
+void Solver::pcg(float* x, const float* b, const Control& c, double target, Stats& stats) {
+  auto restart = [&] {
+    reset(stats.iterations);
+    apply(r_, z_);
+    copy(p_, z_, n_);
+    launch::reduce_into(ReduceMode::Dot, n_, r_, z_, r_, z_, reducer(), scalars_.get(), 0,
+                        status_.get(), true, Epilogue::None, stream_);
+  };
+  restart();
+  int restarts = 0;
+  double last_verified = stats.initial_residual;
+  int check_interval = batch_interval(c);
+  while (stats.iterations < c.max_iter) {
+    const int batch = std::min(check_interval, c.max_iter - stats.iterations);
+    verified_current_ = false;
+    speculated_.reset();
+    for (int j = 0; j < batch; ++j) {
+      launch::spmv_dot(n_, rows0(), cols0(), val_, p_, p_, q_, reducer(), scalars_.get(), 2,
+                       status_.get(), Epilogue::PcgAlpha, stream_);
+      launch::pcg_step_dot(n_, x, r_, p_, q_, reducer(), scalars_.get(), status_.get(), stream_);
+      if (stats.iterations + j + 1 == c.max_iter) continue;
+      apply(r_, z_);
+      if (variable())
+        launch::reduce_into(ReduceMode::Dot2, n_, r_, z_, z_, q_, reducer(), scalars_.get(), 4,
+                            status_.get(), true, Epilogue::PcgBetaFlexible, stream_);
+      else
+        launch::reduce_into(ReduceMode::Dot, n_, r_, z_, r_, z_, reducer(), scalars_.get(), 4,
+                            status_.get(), true, Epilogue::PcgBeta, stream_);
+      launch::direction(n_, z_, p_, scalars_.get(), status_.get(), stream_);
+    }
+    const auto state = poll(x, b);
+    stats.iterations = state[1];
+    if (state[0] == 2) break;
+    if (state[0] == 1) {
+      if (!replacement(x, b, target, stats, restarts, last_verified) ||
+          stats.iterations == c.max_iter)
+        break;
+      // Near a float residual floor, repeated candidates can stop after one update.
+      if (stats.final_residual <= 10 * target) check_interval = 1;
+      restart();
+    }
+  }
+}
+
+// Krylov::bicgstab, solver.cpp:314-361.
+void Solver::bicgstab(float* x, const float* b, const Control& c, double target, Stats& stats) {
+  auto restart = [&] {
+    reset(stats.iterations);
+    copy(shadow_, r_, n_);
+    launch::fill(n_, p_, 0.0f, stream_);
+    launch::fill(n_, q_, 0.0f, stream_);
+  };
+  restart();
+  int restarts = 0;
+  double last_verified = stats.initial_residual;
+  int check_interval = batch_interval(c);
+  float* sc = scalars_.get();
+  while (stats.iterations < c.max_iter) {
+    const int batch = std::min(check_interval, c.max_iter - stats.iterations);
+    verified_current_ = false;
+    speculated_.reset();
+    for (int j = 0; j < batch; ++j) {
+      (void)j;
+      launch::reduce_into(ReduceMode::Dot, n_, shadow_, r_, shadow_, r_, reducer(), sc, 0,
+                          status_.get(), true, Epilogue::BicgBeta, stream_);
+      launch::bicg_direction(n_, r_, q_, p_, sc, status_.get(), stream_);
+      apply(p_, z_);
+      launch::spmv_dot(n_, rows0(), cols0(), val_, z_, shadow_, q_, reducer(), sc, 2,
+                       status_.get(), Epilogue::BicgAlpha, stream_);
+      launch::bicg_difference(n_, r_, q_, s_, sc, status_.get(), stream_);
+      launch::reduce_into(ReduceMode::Dot, n_, s_, s_, s_, s_, reducer(), sc, 16, status_.get(),
+                          true, Epilogue::BicgS, stream_);
+      apply(s_, zs_);
+      launch::spmv(n_, rows0(), cols0(), val_, zs_, t_, status_.get(), stream_);
+      launch::reduce_into(ReduceMode::Dot2, n_, t_, t_, t_, s_, reducer(), sc, 2, status_.get(),
+                          true, Epilogue::BicgOmega, stream_);
+      launch::bicg_step(n_, x, r_, z_, zs_, s_, t_, sc, status_.get(), stream_);
+      launch::reduce_into(ReduceMode::Dot, n_, r_, r_, r_, r_, reducer(), sc, 18, status_.get(),
+                          true, Epilogue::CheckBicg, stream_);
+    }
+    const auto state = poll(x, b);
+    stats.iterations = state[1];
+    if (state[0] == 2) break;
+    if (state[0] == 1) {
+      if (!replacement(x, b, target, stats, restarts, last_verified) ||
+          stats.iterations == c.max_iter)
+        break;
+      if (stats.final_residual <= 10 * target) check_interval = 1;
+      restart();
+    }
+  }
+}
+
+// Krylov::solve, solver.cpp:97-176.
+Stats Solver::solve(const float* val, float* x, const float* b, const Control& c, cudaStream_t s) {
+  stream_ = s;
+  val_ = val;
+  KB2_REQUIRE((n_ == 0 || (x != nullptr && b != nullptr)) && (x != b || n_ == 0),
+              "solve: vector size or alias mismatch");
+  KB2_REQUIRE(c.max_iter >= 0 && std::isfinite(c.rel_tol) && c.rel_tol >= 0 &&
+                  std::isfinite(c.abs_tol) && c.abs_tol >= 0 && c.residual_check_interval > 0,
+              "solve: invalid control");
+  speculated_.reset();
+  if (!nullspace_) residual(x, b, r_);
+  const auto entry = nullspace_
+      ? host_reduce({{ReduceMode::Dot, b, b, n_}, {ReduceMode::Dot, x, x, n_},
+                     {ReduceMode::Sum, b, b, n_}})
+      : host_reduce({{ReduceMode::Dot, b, b, n_}, {ReduceMode::Dot, x, x, n_},
+                     {ReduceMode::Dot, r_, r_, n_}});
+  const double bnorm = std::sqrt(entry[0]);
+  if (!(std::isfinite(bnorm) && std::isfinite(std::sqrt(entry[1]))))
+    throw NonfiniteError("solve: nonfinite input vector");
+  Stats stats;
+  if (nullspace_) {
+    if (n_ != 0) {
+      KB2_REQUIRE(std::fabs(entry[2]) <= 1e-6 * std::sqrt(static_cast<double>(n_)) * bnorm,
+                  "solve: incompatible RHS for constant Neumann nullspace");
+      project(x, n_, projection_.get());
+    }
+    residual(x, b, r_);
+    stats.initial_residual = norm(r_);
+  } else {
+    stats.initial_residual = std::sqrt(entry[2]);
+  }
+  stats.final_residual = stats.initial_residual;
+  verified_current_ = true;
+  const double target = std::max(c.abs_tol, c.rel_tol * stats.initial_residual);
+  if (!std::isfinite(stats.initial_residual)) return stats;
+  if (stats.final_residual <= target) {
+    stats.converged = true;
+    return stats;
+  }
+  if (nullspace_) project(r_, n_, projection_.get());
+  best_residual_ = stats.initial_residual;
+  copy(best_, x, n_);
+  if (kind_ != Kind::Jacobi) {
+    std::array<float, 4> limits{};
+    auto pair = [&](int at, double value) {
+      limits[at] = static_cast<float>(value);
+      limits[at + 1] = std::isfinite(limits[at])
+                           ? static_cast<float>(value - static_cast<double>(limits[at]))
+                           : 0.0f;
+    };
+    pair(0, target * target);
+    pair(2, 1e6 * stats.initial_residual * stats.initial_residual);
+    launch::solver_limits(scalars_.get(), limits[0], limits[1], limits[2], limits[3], stream_);
+  }
+  reset(0);
+  if (kind_ == Kind::Jacobi) {
+    for (int i = 0; i < c.max_iter; ++i) {
+      apply(r_, z_);
+      launch::axpy(n_, x, z_, 2.0f / 3.0f, stream_);
+      verified_current_ = false;
+      ++stats.iterations;
+      if (stats.iterations % c.residual_check_interval == 0 || stats.iterations == c.max_iter) {
+        if (verified(x, b, target, stats) || diverged(stats)) break;
+      } else {
+        residual(x, b, r_);
+      }
+    }
+  } else if (kind_ == Kind::PcgJacobi || kind_ == Kind::AmgPcg) {
+    pcg(x, b, c, target, stats);
+  } else {
+    bicgstab(x, b, c, target, stats);
+  }
+  // All exits report the actual residual; restore the best verified iterate.
+  if (!verified_current_ || nullspace_) verified(x, b, target, stats);
+  if (!std::isfinite(stats.final_residual) || stats.final_residual > best_residual_) {
+    copy(x, best_, n_);
+    verified(x, b, target, stats);
+  }
+  previous_iterations_ = stats.converged ? stats.iterations : 0;
+  wait(stream_);
+  cuda_check(cudaGetLastError(), "solve");
+  return stats;
+}
+
+std::string Solver::describe() const {
+  const char* name = kind_ == Kind::Jacobi
+                         ? "damped Jacobi"
+                         : (kind_ == Kind::PcgJacobi || kind_ == Kind::AmgPcg
+                                ? (variable() ? "flexible PCG" : "PCG")
+                                : "BiCGStab");
+  std::ostringstream out;
+  out << name << ", ";
+  if (amg())
+    out << "aggregation AMG " << (options_.cycle == Cycle::K ? 'K' : 'V') << "-cycle, "
+        << levels_.size() << " levels, op complexity " << std::fixed << std::setprecision(3)
+        << complexity_;
+  else
+    out << "Jacobi";
+  if (nullspace_) out << ", constant-nullspace projection";
+  return out.str();
+}
+
+}  // namespace kb2

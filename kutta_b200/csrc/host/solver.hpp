@@ -1,0 +1,153 @@
+// The LinearSolver of the reference's linalg boundary (src/kutta/linalg/solver.hpp),
+// re-implemented over sm_100a kernels: Krylov drivers (Jacobi, PCG, BiCGStab) with
+// device-resident float-pair scalars, and the aggregation-AMG preconditioner.
+#pragma once
+
+#include <cmath>
+#include <initializer_list>
+#include <memory>
+#include <optional>
+#include <string>
+#include <vector>
+
+#include "../cuda/kernels.hpp"
+#include "device.hpp"
+#include "setup.hpp"
+
+namespace kb2 {
+
+struct Control {  // SolveControl, solver.hpp:18-23
+  double rel_tol = 1e-2, abs_tol = 1e-12;
+  int max_iter = 200, residual_check_interval = 8;
+};
+struct Stats {  // SolveStats, solver.hpp:25-30
+  int iterations = 0;
+  double initial_residual = 0, final_residual = 0;
+  bool converged = false;
+};
+
+// KrylovWorkspace, solver.hpp:47-64: vectors allocated on first use and shared by
+// solvers of one size whose calls never run concurrently.
+class Workspace {
+ public:
+  enum Slot { R, Z, P, Q, Shadow, S, T, Zs, Best, Scratch, Count };
+  explicit Workspace(int rows) : rows_(rows) {}
+  int rows() const { return rows_; }
+  float* vector(Slot slot) {
+    int device = 0;
+    cuda_check(cudaGetDevice(&device), "cudaGetDevice");
+    KB2_REQUIRE(device_ < 0 || device_ == device, "Krylov workspace shared across devices");
+    device_ = device;
+    auto& v = v_[slot];
+    if (!v.allocated()) v.reset(static_cast<std::size_t>(rows_));
+    return v.get();
+  }
+
+ private:
+  int rows_;
+  int device_ = -1;
+  DArray<float> v_[Count];
+};
+
+struct DevLevel {
+  int n = 0, nnz = 0;
+  DArray<int> row_ptr, col, diag;
+  DArray<float> val;            // coarse levels (level 0 uses the caller's values)
+  DArray<float> l1;             // inverse L1 diagonal
+  DArray<float> xa, ra, b;      // storage; x/r below name the current roles
+  float* x = nullptr;
+  float* r = nullptr;
+  DArray<float> projection;     // constant-nullspace sum pair
+  // transfer to level + 1
+  DArray<int> aggregate, member_offsets, members, entry_offsets, entries;
+};
+
+class Solver {
+ public:
+  Solver(Kind kind, const CsrView& a, const Options& options, std::shared_ptr<Workspace> workspace);
+  void refresh(const float* val, cudaStream_t s);
+  Stats solve(const float* val, float* x, const float* b, const Control& c, cudaStream_t s);
+  std::string describe() const;
+
+  int levels() const { return static_cast<int>(levels_.size()); }
+  const DevLevel& level(int i) const { return levels_[static_cast<std::size_t>(i)]; }
+  int rows() const { return n_; }
+  int entries() const { return nnz_; }
+  const float* current_values() const { return val_; }
+
+ private:
+  bool amg() const { return kind_ == Kind::AmgPcg || kind_ == Kind::AmgBicgstab; }
+  bool bicg() const { return kind_ == Kind::BicgstabJacobi || kind_ == Kind::AmgBicgstab; }
+  bool variable() const { return amg() && options_.cycle == Cycle::K; }
+  const int* rows0() const { return levels_[0].row_ptr.get(); }
+  const int* cols0() const { return levels_[0].col.get(); }
+
+  // Device primitives on stream_.
+  void residual(const float* x, const float* b, float* r);
+  struct Request {
+    ReduceMode mode;
+    const float* x;
+    const float* y;
+    int n;
+  };
+  // Device::reduce_many: several FP64 reductions behind one host wait.
+  std::vector<double> host_reduce(std::initializer_list<Request> requests);
+  double norm(const float* x);
+  void copy(float* dst, const float* src, int n);
+  void project(float* x, int n, float* projection);
+  void reset(int iterations);
+
+  // Preconditioner.
+  void apply(const float* r, float*& z);
+  void cycle(std::size_t index, const float* b, float*& x);
+  void smooth(DevLevel& l, const int* rows, const int* cols, const float* vals, const float* b,
+              float*& x, int sweeps, bool zero_start);
+
+  // Krylov driver (solver.cpp:97-393).
+  bool verified(float* x, const float* b, double target, Stats& stats);
+  bool diverged(const Stats& stats) const {
+    return !std::isfinite(stats.final_residual) ||
+           stats.final_residual > 1e3 * stats.initial_residual;
+  }
+  std::vector<int> poll(const float* x, const float* b);
+  bool replacement(float* x, const float* b, double target, Stats& stats, int& restarts,
+                   double& last_verified);
+  void pcg(float* x, const float* b, const Control& c, double target, Stats& stats);
+  void bicgstab(float* x, const float* b, const Control& c, double target, Stats& stats);
+  int batch_interval(const Control& c) const {
+    return previous_iterations_ > 0 && previous_iterations_ < c.residual_check_interval
+               ? previous_iterations_ + 1
+               : c.residual_check_interval;
+  }
+  float* speculative_r() { return bicg() ? t_ : q_; }
+  float*& speculative_x() { return bicg() ? s_ : z_; }
+  DeviceReducer reducer() const { return DeviceReducer{partials_.get(), ticket_.get()}; }
+
+  Kind kind_;
+  Options options_;
+  int n_, nnz_;
+  bool nullspace_;
+  int device_ = 0;
+  std::shared_ptr<Workspace> workspace_;
+  std::vector<DevLevel> levels_;
+  double complexity_ = 0;
+  DArray<float> jacobi_inverse_;  // Jacobi preconditioner
+  float *r_ = nullptr, *z_ = nullptr, *p_ = nullptr, *q_ = nullptr, *shadow_ = nullptr,
+        *s_ = nullptr, *t_ = nullptr, *zs_ = nullptr, *best_ = nullptr, *scratch_ = nullptr;
+  DArray<float> scalars_, projection_;
+  DArray<int> status_;
+  DArray<double> partials_, values_;
+  DArray<unsigned> ticket_;
+  Pinned<double> host_values_{64};
+  Pinned<int> host_status_{4};
+  bool speculate_ = false;
+  std::optional<double> speculated_;
+  double best_residual_ = 0;
+  int previous_iterations_ = 0;
+  bool verified_current_ = false;
+  // Per-call state.
+  cudaStream_t stream_ = nullptr;
+  const float* val_ = nullptr;
+};
+
+}  // namespace kb2

@@ -1,0 +1,418 @@
+"""Python mirror of the reference's linear-solver boundary over the C ABI.
+
+Same names, argument meaning and error behaviour as ``src/kutta/linalg``
+(solver.hpp, amg.hpp, csr.hpp): ``make_solver`` / ``make_amg_solver`` build a
+solver from a host CSR (setup on the host, hierarchy uploaded to the GPU);
+``LinearSolver.refresh`` recomputes value-dependent data on the device;
+``LinearSolver.solve`` runs the Krylov iteration on the device and returns
+``SolveStats``. Usage errors raise :class:`KuttaError` (kutta::Error),
+nonfinite input vectors :class:`NonfiniteError` (kutta::NonfiniteError).
+
+Device vectors are CUDA ``torch.Tensor`` s (float32 values, int32 indices); the
+work is enqueued on torch's current stream. Every compute call goes through
+``libkutta_b200.so``; there is no other implementation behind these names.
+"""
+from __future__ import annotations
+
+import ctypes
+import dataclasses
+import enum
+import pathlib
+
+import numpy as np
+
+_LIB_PATH = pathlib.Path(__file__).resolve().parent / "_lib" / "libkutta_b200.so"
+
+
+class KuttaError(RuntimeError):
+    """kutta::Error: invalid CSR, options, controls or matrix values."""
+
+
+class NonfiniteError(KuttaError):
+    """kutta::NonfiniteError: a nonfinite input vector."""
+
+
+class DeviceError(KuttaError):
+    """A CUDA runtime failure (or out of device memory)."""
+
+
+class DeviceTimeout(DeviceError):
+    """A bounded host wait on the device ran out."""
+
+
+class SolverKind(enum.IntEnum):  # solver.hpp:32-38
+    Jacobi = 0
+    PcgJacobi = 1
+    BicgstabJacobi = 2
+    AmgPcg = 3
+    AmgBicgstab = 4
+
+
+class NullSpace(enum.IntEnum):  # solver.hpp:40
+    None_ = 0
+    Constant = 1
+
+
+class OperatorStructure(enum.IntEnum):  # solver.hpp:41
+    General = 0
+    SymmetricMMatrix = 1
+
+
+class AmgCycle(enum.IntEnum):  # amg.hpp:9
+    V = 0
+    K = 1
+
+
+@dataclasses.dataclass
+class SolveControl:  # solver.hpp:18-23
+    rel_tol: float = 1e-2
+    abs_tol: float = 1e-12
+    max_iter: int = 200
+    residual_check_interval: int = 8
+
+
+@dataclasses.dataclass
+class SolveStats:  # solver.hpp:25-30
+    iterations: int = 0
+    initial_residual: float = 0.0
+    final_residual: float = 0.0
+    converged: bool = False
+
+
+class KrylovWorkspace:  # solver.hpp:47-64
+    def __init__(self, rows: int):
+        lib = _load()
+        handle = ctypes.c_void_p()
+        _check(lib.b2_workspace_create(int(rows), ctypes.byref(handle)))
+        self._handle = handle
+        self._rows = int(rows)
+
+    def rows(self) -> int:
+        return self._rows
+
+    def __del__(self):
+        if getattr(self, "_handle", None) and _lib is not None:
+            _lib.b2_workspace_destroy(self._handle)
+            self._handle = None
+
+
+@dataclasses.dataclass
+class SolverOptions:  # solver.hpp:66-72
+    nullspace: NullSpace = NullSpace.None_
+    structure: OperatorStructure = OperatorStructure.General
+    workspace: KrylovWorkspace | None = None
+
+
+@dataclasses.dataclass
+class AmgOptions:  # amg.hpp:8-20
+    cycle: AmgCycle = AmgCycle.V
+    pre_sweeps: int = 5
+    post_sweeps: int = 5
+    coarse_sweeps: int = 32
+    coarse_rows: int = 24
+    max_levels: int = 24
+    aggregation_passes: int = 3
+    strength_threshold: float = 0.25
+    nullspace: NullSpace = NullSpace.None_
+    structure: OperatorStructure = OperatorStructure.General
+    workspace: KrylovWorkspace | None = None
+
+
+class _Options(ctypes.Structure):
+    _fields_ = [("cycle", ctypes.c_int), ("pre_sweeps", ctypes.c_int),
+                ("post_sweeps", ctypes.c_int), ("coarse_sweeps", ctypes.c_int),
+                ("coarse_rows", ctypes.c_int), ("max_levels", ctypes.c_int),
+                ("aggregation_passes", ctypes.c_int), ("strength_threshold", ctypes.c_double),
+                ("nullspace", ctypes.c_int), ("structure", ctypes.c_int),
+                ("workspace", ctypes.c_void_p)]
+
+
+class _Control(ctypes.Structure):
+    _fields_ = [("rel_tol", ctypes.c_double), ("abs_tol", ctypes.c_double),
+                ("max_iter", ctypes.c_int), ("residual_check_interval", ctypes.c_int)]
+
+
+class _Stats(ctypes.Structure):
+    _fields_ = [("iterations", ctypes.c_int), ("converged", ctypes.c_int),
+                ("initial_residual", ctypes.c_double), ("final_residual", ctypes.c_double)]
+
+
+# Every symbol include/kutta_b200.h declares, with its ctypes signature.
+_I = ctypes.c_int
+_P = ctypes.c_void_p
+_SIGNATURES = {
+    "b2_options_default": (None, [_P]),
+    "b2_control_default": (None, [_P]),
+    "b2_last_error": (ctypes.c_size_t, [ctypes.c_char_p, ctypes.c_size_t]),
+    "b2_workspace_create": (_I, [_I, _P]),
+    "b2_workspace_destroy": (None, [_P]),
+    "b2_solver_create": (_I, [_I, _I, _I, _P, _P, _P, _P, _P, _I, _P]),
+    "b2_solver_refresh": (_I, [_P, _P, _P]),
+    "b2_solver_solve": (_I, [_P, _P, _P, _P, _P, _P, _P]),
+    "b2_solver_describe": (ctypes.c_size_t, [_P, ctypes.c_char_p, ctypes.c_size_t]),
+    "b2_solver_destroy": (None, [_P]),
+    "b2_csr_spmv": (_I, [_I, _I, _P, _P, _P, _P, _P, _P]),
+    "b2_csr_residual": (_I, [_I, _I, _P, _P, _P, _P, _P, _P, _P]),
+    "b2_solver_levels": (_I, [_P]),
+    "b2_solver_level_shape": (_I, [_P, _I, _P, _P]),
+    "b2_solver_level_copy": (_I, [_P, _I, _P, _P, _P, _P, _P, _P]),
+    "b2_hierarchy_build": (_I, [_I, _I, _P, _P, _P, _P, _P, _I, _P]),
+    "b2_hierarchy_levels": (_I, [_P]),
+    "b2_hierarchy_level_shape": (_I, [_P, _I, _P, _P]),
+    "b2_hierarchy_level_copy": (_I, [_P, _I, _P, _P, _P, _P, _P]),
+    "b2_hierarchy_free": (None, [_P]),
+}
+
+_lib = None
+
+
+def library_path() -> pathlib.Path:
+    return _LIB_PATH
+
+
+def _load():
+    """Loads libkutta_b200.so; fails loudly when the native build is missing."""
+    global _lib
+    if _lib is None:
+        if not _LIB_PATH.exists():
+            raise RuntimeError(
+                f"kutta_b200 native library missing ({_LIB_PATH}); build it with "
+                "`python -m kutta_b200.build` (there is no fallback implementation)")
+        lib = ctypes.CDLL(str(_LIB_PATH))
+        for name, (res, args) in _SIGNATURES.items():
+            fn = getattr(lib, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = lib
+    return _lib
+
+
+def last_error() -> str:
+    lib = _load()
+    buf = ctypes.create_string_buffer(4096)
+    lib.b2_last_error(buf, 4096)
+    return buf.value.decode(errors="replace")
+
+
+def _check(code: int):
+    if code == 0:
+        return
+    msg = last_error()
+    if code == 2:
+        raise NonfiniteError(msg)
+    if code == 4:
+        raise DeviceTimeout(msg)
+    if code in (3, 5):
+        raise DeviceError(msg)
+    raise KuttaError(msg)
+
+
+def _ptr(a: np.ndarray):
+    return ctypes.c_void_p(a.ctypes.data) if a is not None and a.size else None
+
+
+def _tptr(t):
+    return ctypes.c_void_p(t.data_ptr()) if t is not None and t.numel() else None
+
+
+def _stream():
+    import torch
+    return ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+
+
+@dataclasses.dataclass
+class CsrMatrixHost:
+    """csr.hpp:16-28 (pattern + double values)."""
+    n_rows: int
+    row_ptr: np.ndarray
+    col: np.ndarray
+    diag: np.ndarray
+    val: np.ndarray
+
+    @classmethod
+    def of(cls, system) -> "CsrMatrixHost":
+        return cls(int(system.row_ptr.shape[0] - 1), system.row_ptr, system.col, system.diag,
+                   system.val)
+
+    def arrays(self):
+        return (np.ascontiguousarray(self.row_ptr, np.int32), np.ascontiguousarray(self.col, np.int32),
+                np.ascontiguousarray(self.diag, np.int32), np.ascontiguousarray(self.val, np.float64))
+
+    @property
+    def nnz(self) -> int:
+        return int(self.col.shape[0])
+
+
+def _host(a) -> CsrMatrixHost:
+    return a if isinstance(a, CsrMatrixHost) else CsrMatrixHost.of(a)
+
+
+@dataclasses.dataclass
+class CsrMatrix:
+    """Device CSR (csr.hpp:31-38); ``val`` is the only part expected to change."""
+    n_rows: int
+    nnz: int
+    row_ptr: "torch.Tensor"
+    col: "torch.Tensor"
+    diag: "torch.Tensor"
+    val: "torch.Tensor"
+
+
+def upload(a, device="cuda") -> CsrMatrix:
+    """upload(dev, CsrMatrixHost), csr.cpp:61-73: values stored as float32."""
+    import torch
+    h = _host(a)
+    row_ptr, col, diag, val = h.arrays()
+    if not np.all(np.isfinite(val)) or np.any(np.abs(val) > np.finfo(np.float32).max):
+        raise KuttaError("CSR: nonfinite or out-of-range value")
+    return CsrMatrix(h.n_rows, h.nnz, torch.from_numpy(row_ptr).to(device),
+                     torch.from_numpy(col).to(device), torch.from_numpy(diag).to(device),
+                     torch.from_numpy(val.astype(np.float32)).to(device))
+
+
+def _options_struct(o, use_amg: bool) -> _Options:
+    s = _Options()
+    _load().b2_options_default(ctypes.byref(s))
+    if isinstance(o, AmgOptions):
+        s.cycle, s.pre_sweeps, s.post_sweeps = int(o.cycle), o.pre_sweeps, o.post_sweeps
+        s.coarse_sweeps, s.coarse_rows, s.max_levels = o.coarse_sweeps, o.coarse_rows, o.max_levels
+        s.aggregation_passes, s.strength_threshold = o.aggregation_passes, o.strength_threshold
+    if o is not None:
+        s.nullspace, s.structure = int(o.nullspace), int(o.structure)
+        s.workspace = o.workspace._handle if o.workspace is not None else None
+    return s
+
+
+class LinearSolver:
+    """solver.hpp:74-81."""
+
+    def __init__(self, kind: SolverKind, a, options, use_amg: bool):
+        lib = _load()
+        h = _host(a)
+        row_ptr, col, diag, val = h.arrays()
+        opts = _options_struct(options, use_amg)
+        handle = ctypes.c_void_p()
+        _check(lib.b2_solver_create(int(kind), h.n_rows, h.nnz, _ptr(row_ptr), _ptr(col),
+                                    _ptr(diag), _ptr(val), ctypes.byref(opts), int(use_amg),
+                                    ctypes.byref(handle)))
+        self._handle = handle
+        self._workspace = getattr(options, "workspace", None)  # keep alive
+        self.kind = SolverKind(kind)
+        self.n_rows = h.n_rows
+        self.nnz = h.nnz
+
+    def _check_matrix(self, a: CsrMatrix):
+        if a.n_rows != self.n_rows or a.nnz != self.nnz or a.val.numel() != self.nnz:
+            raise KuttaError("solver: device or matrix mismatch")
+
+    def refresh(self, a: CsrMatrix) -> None:
+        self._check_matrix(a)
+        _check(_load().b2_solver_refresh(self._handle, _tptr(a.val), _stream()))
+
+    def solve(self, a: CsrMatrix, x, b, control: SolveControl | None = None) -> SolveStats:
+        self._check_matrix(a)
+        if x.numel() != self.n_rows or b.numel() != self.n_rows or (
+                x.numel() and x.data_ptr() == b.data_ptr()):
+            raise KuttaError("solve: vector size or alias mismatch")
+        control = control or SolveControl()
+        c = _Control(control.rel_tol, control.abs_tol, control.max_iter,
+                     control.residual_check_interval)
+        st = _Stats()
+        _check(_load().b2_solver_solve(self._handle, _tptr(a.val), _tptr(x), _tptr(b),
+                                       ctypes.byref(c), ctypes.byref(st), _stream()))
+        return SolveStats(st.iterations, st.initial_residual, st.final_residual, bool(st.converged))
+
+    def describe(self) -> str:
+        buf = ctypes.create_string_buffer(512)
+        _load().b2_solver_describe(self._handle, buf, 512)
+        return buf.value.decode()
+
+    def levels(self):
+        """The device hierarchy read back: [(n, row_ptr, col, val, inverse_l1, aggregate)]."""
+        lib = _load()
+        out = []
+        for lv in range(lib.b2_solver_levels(self._handle)):
+            n, nnz = ctypes.c_int(), ctypes.c_int()
+            _check(lib.b2_solver_level_shape(self._handle, lv, ctypes.byref(n), ctypes.byref(nnz)))
+            rp = np.zeros(n.value + 1, np.int32)
+            cl = np.zeros(nnz.value, np.int32)
+            vl = np.zeros(nnz.value, np.float32)
+            l1 = np.zeros(n.value, np.float32)
+            ag = np.full(n.value, -2, np.int32)
+            _check(lib.b2_solver_level_copy(self._handle, lv, _ptr(rp), _ptr(cl), _ptr(vl),
+                                            _ptr(l1), _ptr(ag), _stream()))
+            out.append((n.value, rp, cl, vl, l1, ag))
+        return out
+
+    def __del__(self):
+        if getattr(self, "_handle", None) and _lib is not None:
+            _lib.b2_solver_destroy(self._handle)
+            self._handle = None
+
+
+def make_solver(kind: SolverKind, a, options: SolverOptions | None = None) -> LinearSolver:
+    """solver.hpp:85-88 / amg.cpp:384-406."""
+    return LinearSolver(kind, a, options or SolverOptions(), use_amg=False)
+
+
+def make_amg_solver(kind: SolverKind, a, options: AmgOptions) -> LinearSolver:
+    """amg.hpp:26-27 / amg.cpp:345-382."""
+    return LinearSolver(kind, a, options, use_amg=True)
+
+
+def spmv(a: CsrMatrix, x, y) -> None:
+    """csr.hpp:40-41: y = A x (Kahan-compensated float)."""
+    if x.numel() != a.n_rows or y.numel() != a.n_rows:
+        raise KuttaError("CSR: vector size mismatch")
+    if a.n_rows and x.data_ptr() == y.data_ptr():
+        raise KuttaError("CSR: input/output aliasing is unsupported")
+    _check(_load().b2_csr_spmv(a.n_rows, a.nnz, _tptr(a.row_ptr), _tptr(a.col), _tptr(a.val),
+                               _tptr(x), _tptr(y), _stream()))
+
+
+def residual(a: CsrMatrix, x, b, r) -> None:
+    """csr.hpp:43-46: r = b - A x (Neumaier + Dekker compensated float)."""
+    if x.numel() != a.n_rows or r.numel() != a.n_rows or b.numel() != a.n_rows:
+        raise KuttaError("CSR: vector size mismatch")
+    if a.n_rows and (x.data_ptr() == r.data_ptr() or b.data_ptr() == r.data_ptr()):
+        raise KuttaError("CSR: residual RHS size or alias mismatch")
+    _check(_load().b2_csr_residual(a.n_rows, a.nnz, _tptr(a.row_ptr), _tptr(a.col), _tptr(a.val),
+                                   _tptr(x), _tptr(b), _tptr(r), _stream()))
+
+
+@dataclasses.dataclass
+class HostLevel:
+    n: int
+    row_ptr: np.ndarray
+    col: np.ndarray
+    val: np.ndarray
+    inverse_l1: np.ndarray
+    aggregate: np.ndarray | None
+
+
+def build_hierarchy(a, options: AmgOptions | None = None, spd: bool = True) -> list[HostLevel]:
+    """The host AMG setup alone (no GPU): aggregates, coarse operators, L1 diagonals."""
+    lib = _load()
+    h = _host(a)
+    row_ptr, col, diag, val = h.arrays()
+    opts = _options_struct(options or AmgOptions(), True)
+    handle = ctypes.c_void_p()
+    _check(lib.b2_hierarchy_build(h.n_rows, h.nnz, _ptr(row_ptr), _ptr(col), _ptr(diag),
+                                  _ptr(val), ctypes.byref(opts), int(spd), ctypes.byref(handle)))
+    out = []
+    try:
+        count = lib.b2_hierarchy_levels(handle)
+        for lv in range(count):
+            n, nnz = ctypes.c_int(), ctypes.c_int()
+            _check(lib.b2_hierarchy_level_shape(handle, lv, ctypes.byref(n), ctypes.byref(nnz)))
+            rp = np.zeros(n.value + 1, np.int32)
+            cl = np.zeros(nnz.value, np.int32)
+            vl = np.zeros(nnz.value, np.float32)
+            l1 = np.zeros(n.value, np.float32)
+            ag = np.zeros(n.value, np.int32) if lv + 1 < count else None
+            _check(lib.b2_hierarchy_level_copy(handle, lv, _ptr(rp), _ptr(cl), _ptr(vl), _ptr(l1),
+                                               _ptr(ag) if ag is not None else None))
+            out.append(HostLevel(n.value, rp, cl, vl, l1, ag))
+    finally:
+        lib.b2_hierarchy_free(handle)
+    return out

@@ -1,0 +1,292 @@
+// Test infrastructure only: a C-ABI shim over the reference library's own CPU
+// path (kutta::make_solver / make_amg_solver on the serial CPU Device), built by
+// oracle/build_ref.sh from the reference sources into oracle/_ref/. Only the
+// tests, the golden-fixture generator and bench.py's reference/CPU-baseline arm
+// load it; the product never does.
+//
+// It exposes two things:
+//   kref_solve      set up, refresh and solve one system exactly as the reference
+//                   does (src/kutta/linalg/amg.cpp:345-406, solver.cpp:97-176);
+//   kref_hierarchy  capture the AMG hierarchy the reference actually solves with
+//                   (aggregates, coarse CSR patterns and values, L1 inverse
+//                   diagonals) from the kernels its V-cycle launches, the way
+//                   tests/linalg/test_solvers.cpp:509-521 reads them back.
+#include <chrono>
+#include <cstring>
+#include <functional>
+#include <map>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "kernels.hpp"
+#include "kutta/linalg/amg.hpp"
+
+namespace {
+using namespace kutta;
+
+// Forwards every Device call to the serial CPU backend while letting the shim
+// observe kernel launches. Buffers are wrapped so the wrapper owns the handle
+// identity the solver sees; launches translate them back.
+class WatchDevice final : public Device {
+  struct Wrapped final : BufferHandle {
+    Buffer<float> inner;
+    explicit Wrapped(Buffer<float> b) : inner(std::move(b)) {}
+    std::size_t bytes() const override { return inner.size() * sizeof(float); }
+  };
+  static Buffer<float>& in(const BufferHandle& h) {
+    return const_cast<Wrapped&>(static_cast<const Wrapped&>(h)).inner;
+  }
+
+ public:
+  WatchDevice() : cpu_(Device::create(Backend::Cpu)) {}
+  Backend backend() const override { return Backend::Cpu; }
+  std::string name() const override { return cpu_->name(); }
+  double sum(const Buffer<float>& x, std::size_t n) override { return cpu_->sum(in(*x.handle()), n); }
+  double dot(const Buffer<float>& x, const Buffer<float>& y, std::size_t n) override {
+    return cpu_->dot(in(*x.handle()), in(*y.handle()), n);
+  }
+  double max_abs(const Buffer<float>& x, std::size_t n) override {
+    return cpu_->max_abs(in(*x.handle()), n);
+  }
+  void launch(KernelId id, std::size_t n, std::span<const KernelArg> args) override {
+    std::vector<KernelArg> inner(args.begin(), args.end());
+    for (auto& a : inner)
+      if (a.kind == KernelArg::Kind::Buffer) a.buffer = in(*a.buffer).handle();
+    cpu_->launch(id, n, inner);
+    if (observer) observer(id, n, args);
+  }
+  void synchronize() override { cpu_->synchronize(); }
+  template <class T>
+  std::vector<T> read(const BufferHandle* h) {
+    const auto words = cpu_->download(in(*h));
+    std::vector<T> out(words.size());
+    if (!words.empty()) std::memcpy(out.data(), words.data(), words.size() * sizeof(float));
+    return out;
+  }
+  std::function<void(KernelId, std::size_t, std::span<const KernelArg>)> observer;
+
+ protected:
+  void reduce_into(const Buffer<float>& x, const Buffer<float>& y, const Buffer<float>& u,
+                   const Buffer<float>& v, std::size_t n, Buffer<float>& dst,
+                   std::size_t offset, Reduction mode) override {
+    check_reduction(x, y, u, v, n, dst, offset, mode);
+    auto& out = in(*dst.handle());
+    if (mode == Reduction::Sum) cpu_->sum_into(in(*x.handle()), n, out, offset);
+    else if (mode == Reduction::Dot) cpu_->dot_into(in(*x.handle()), in(*y.handle()), n, out, offset);
+    else cpu_->dot2_into(in(*x.handle()), in(*y.handle()), in(*u.handle()), in(*v.handle()), n, out, offset);
+  }
+  void host_reductions(std::span<const HostReduction> requests, std::span<double> out) override {
+    std::vector<HostReduction> inner(requests.begin(), requests.end());
+    for (auto& r : inner) { r.x = &in(*r.x->handle()); r.y = &in(*r.y->handle()); }
+    const auto values = cpu_->reduce_many(inner);
+    std::copy(values.begin(), values.end(), out.begin());
+  }
+  std::unique_ptr<BufferHandle> alloc_bytes(std::size_t bytes) override {
+    return std::make_unique<Wrapped>(cpu_->alloc<float>((bytes + 3) / 4));
+  }
+  void upload_bytes(BufferHandle& dst, const void* src, std::size_t bytes) override {
+    std::vector<float> words(in(dst).size());
+    if (bytes) std::memcpy(words.data(), src, bytes);
+    cpu_->upload<float>(in(dst), words);
+  }
+  void download_bytes(const BufferHandle& src, void* dst, std::size_t bytes) override {
+    const auto words = cpu_->download(in(src));
+    if (bytes) std::memcpy(dst, words.data(), bytes);
+  }
+  void copy_bytes(BufferHandle& dst, const BufferHandle& src, std::size_t) override {
+    cpu_->copy(in(dst), in(src));
+  }
+  void fill_bytes(BufferHandle& dst, const void* value, std::size_t size, std::size_t) override {
+    float word = 0;
+    std::memcpy(&word, value, size);
+    cpu_->fill(in(dst), word);
+  }
+
+ private:
+  std::unique_ptr<Device> cpu_;
+};
+
+}  // namespace
+
+extern "C" {
+
+struct kref_options {
+  int kind;           // 0 Jacobi, 1 PcgJacobi, 2 BicgstabJacobi, 3 AmgPcg, 4 AmgBicgstab
+  int cycle;          // 0 V, 1 K
+  int pre_sweeps, post_sweeps, coarse_sweeps, coarse_rows, max_levels, passes;
+  double threshold;
+  int nullspace;      // 0 None, 1 Constant
+  int structure;      // 0 General, 1 SymmetricMMatrix
+  int use_make_solver;  // 1: make_solver(kind, dev, a, {nullspace, structure}) defaults
+};
+struct kref_control { double rel_tol, abs_tol; int max_iter, interval; };
+struct kref_stats {
+  int iterations, converged, levels, pad;
+  double initial_residual, final_residual, setup_s, refresh_s, solve_s;
+};
+
+static thread_local std::string g_error;
+const char* kref_last_error() { return g_error.c_str(); }
+
+static CsrMatrixHost host_matrix(int n, int nnz, const int* row_ptr, const int* col,
+                                 const int* diag, const double* val) {
+  CsrMatrixHost a;
+  a.pattern.n_rows = n;
+  a.pattern.row_ptr.assign(row_ptr, row_ptr + n + 1);
+  a.pattern.col.assign(col, col + nnz);
+  a.pattern.diag.assign(diag, diag + n);
+  a.val.assign(val, val + nnz);
+  return a;
+}
+
+static std::unique_ptr<LinearSolver> build(Device& dev, const CsrMatrixHost& a,
+                                           const kref_options& o) {
+  const auto kind = static_cast<SolverKind>(o.kind);
+  if (o.use_make_solver || (kind != SolverKind::AmgPcg && kind != SolverKind::AmgBicgstab)) {
+    SolverOptions so;
+    so.nullspace = static_cast<NullSpace>(o.nullspace);
+    so.structure = static_cast<OperatorStructure>(o.structure);
+    return make_solver(kind, dev, a, so);
+  }
+  AmgOptions ao;
+  ao.cycle = o.cycle ? AmgCycle::K : AmgCycle::V;
+  ao.pre_sweeps = o.pre_sweeps;
+  ao.post_sweeps = o.post_sweeps;
+  ao.coarse_sweeps = o.coarse_sweeps;
+  ao.coarse_rows = o.coarse_rows;
+  ao.max_levels = o.max_levels;
+  ao.aggregation_passes = o.passes;
+  ao.strength_threshold = o.threshold;
+  ao.nullspace = static_cast<NullSpace>(o.nullspace);
+  ao.structure = static_cast<OperatorStructure>(o.structure);
+  return make_amg_solver(kind, dev, a, ao);
+}
+
+// Full reference lifecycle: setup from host values, refresh, solve. x holds the
+// initial guess on entry and the solution on return. Returns 0, or -1 with the
+// reference's exception text in kref_last_error().
+int kref_solve(int n, int nnz, const int* row_ptr, const int* col, const int* diag,
+               const double* val, const float* b, float* x, const kref_options* o,
+               const kref_control* c, kref_stats* s, char* describe, int describe_len) {
+  try {
+    using Clock = std::chrono::steady_clock;
+    auto dev = Device::create(Backend::Cpu);
+    const auto a = host_matrix(n, nnz, row_ptr, col, diag, val);
+    auto matrix = upload(*dev, a);
+    auto t0 = Clock::now();
+    auto solver = build(*dev, a, *o);
+    auto t1 = Clock::now();
+    solver->refresh(*dev, matrix);
+    auto t2 = Clock::now();
+    auto db = dev->upload<float>(std::span<const float>(b, n));
+    auto dx = dev->upload<float>(std::span<const float>(x, n));
+    auto t3 = Clock::now();
+    const auto st = solver->solve(*dev, matrix, dx, db,
+                                  {c->rel_tol, c->abs_tol, c->max_iter, c->interval});
+    auto t4 = Clock::now();
+    dev->download(dx, std::span<float>(x, n));
+    s->iterations = st.iterations;
+    s->converged = st.converged ? 1 : 0;
+    s->initial_residual = st.initial_residual;
+    s->final_residual = st.final_residual;
+    s->setup_s = std::chrono::duration<double>(t1 - t0).count();
+    s->refresh_s = std::chrono::duration<double>(t2 - t1).count();
+    s->solve_s = std::chrono::duration<double>(t4 - t3).count();
+    if (describe && describe_len > 0) {
+      const auto d = solver->describe();
+      std::snprintf(describe, describe_len, "%s", d.c_str());
+    }
+    return 0;
+  } catch (const std::exception& e) {
+    g_error = e.what();
+    return -1;
+  }
+}
+
+// Captured hierarchy: level 0 is the input matrix, levels 1.. are the coarse
+// operators the V-cycle really used; aggregate[l] maps level-l rows to level
+// l+1 rows (-1 for rows left out).
+struct KrefHierarchy {
+  struct Level {
+    int n = 0;
+    std::vector<int> row_ptr, col, aggregate;
+    std::vector<float> val, l1;
+  };
+  std::vector<Level> levels;
+};
+
+void* kref_hierarchy(int n, int nnz, const int* row_ptr, const int* col, const int* diag,
+                     const double* val, const kref_options* o) {
+  try {
+    WatchDevice dev;
+    const auto a = host_matrix(n, nnz, row_ptr, col, diag, val);
+    auto matrix = upload(dev, a);
+    auto solver = build(dev, a, *o);
+    solver->refresh(dev, matrix);
+    std::map<std::size_t, KrefHierarchy::Level> ops;
+    std::map<std::size_t, std::vector<int>> aggregates;
+    std::map<std::size_t, std::vector<float>> inverse_l1;
+    dev.observer = [&](KernelId id, std::size_t count, std::span<const KernelArg> args) {
+      // Argument positions follow the kernel signatures in
+      // src/kutta/kernels/linalg.kern.h and amg.kern.h.
+      if (id == KernelId::amg_coarse_solve) count = static_cast<std::size_t>(args[7].get<int>());
+      const bool smooth = id == KernelId::amg_smooth || id == KernelId::amg_smooth_zero;
+      if ((id == KernelId::csr_residual_guarded || smooth || id == KernelId::amg_coarse_solve) &&
+          !ops.contains(count)) {
+        auto& l = ops[count];
+        l.n = static_cast<int>(count);
+        l.row_ptr = dev.read<int>(args[0].buffer);
+        l.col = dev.read<int>(args[1].buffer);
+        l.val = dev.read<float>(args[2].buffer);
+      }
+      if ((smooth || id == KernelId::amg_coarse_solve) && !inverse_l1.contains(count))
+        inverse_l1[count] = dev.read<float>(args[5].buffer);
+      if (id == KernelId::amg_prolong_guarded && !aggregates.contains(count))
+        aggregates[count] = dev.read<int>(args[0].buffer);
+    };
+    auto db = dev.upload<float>(std::vector<float>(n, 1.0f));
+    auto dx = dev.alloc<float>(n);
+    dev.fill(dx, 0.0f);
+    solver->solve(dev, matrix, dx, db, {0, 0, 1, 8});
+    auto* h = new KrefHierarchy;
+    for (auto it = ops.rbegin(); it != ops.rend(); ++it) {
+      auto l = std::move(it->second);
+      l.row_ptr.resize(l.n + 1);
+      l.col.resize(l.row_ptr.back());
+      l.val.resize(l.row_ptr.back());
+      l.l1 = inverse_l1[it->first];
+      l.l1.resize(l.n);
+      if (aggregates.contains(it->first)) {
+        l.aggregate = aggregates[it->first];
+        l.aggregate.resize(l.n);
+      }
+      h->levels.push_back(std::move(l));
+    }
+    return h;
+  } catch (const std::exception& e) {
+    g_error = e.what();
+    return nullptr;
+  }
+}
+
+int kref_hierarchy_levels(void* h) { return static_cast<int>(static_cast<KrefHierarchy*>(h)->levels.size()); }
+void kref_hierarchy_shape(void* h, int level, int* n, int* nnz, int* has_aggregate) {
+  const auto& l = static_cast<KrefHierarchy*>(h)->levels[level];
+  *n = l.n;
+  *nnz = l.row_ptr.empty() ? 0 : l.row_ptr.back();
+  *has_aggregate = l.aggregate.empty() ? 0 : 1;
+}
+void kref_hierarchy_copy(void* h, int level, int* row_ptr, int* col, float* val, float* l1,
+                         int* aggregate) {
+  const auto& l = static_cast<KrefHierarchy*>(h)->levels[level];
+  std::memcpy(row_ptr, l.row_ptr.data(), l.row_ptr.size() * sizeof(int));
+  std::memcpy(col, l.col.data(), l.col.size() * sizeof(int));
+  std::memcpy(val, l.val.data(), l.val.size() * sizeof(float));
+  std::memcpy(l1, l.l1.data(), l.l1.size() * sizeof(float));
+  if (aggregate && !l.aggregate.empty())
+    std::memcpy(aggregate, l.aggregate.data(), l.aggregate.size() * sizeof(int));
+}
+void kref_hierarchy_free(void* h) { delete static_cast<KrefHierarchy*>(h); }
+
+}  // extern "C"
