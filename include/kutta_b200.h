@@ -132,6 +132,30 @@ int b2_csr_residual(int n, int nnz, const int32_t* d_row_ptr, const int32_t* d_c
                     const float* d_val, const float* d_x, const float* d_b, float* d_r,
                     void* stream);
 
+/* Measurement (no reference counterpart; the reference's bench counts its
+ * launches through its InstrumentedDevice, tests/linalg/instrumented_device.hpp).
+ * With profiling on, every fine-level smoother sweep of a solve is bracketed by
+ * CUDA events on the solve stream, and the algorithmic bytes of every kernel
+ * the solve launches are tallied (stored operands, each read or written once). */
+typedef struct {
+  long long launches;        /* kernels this solver launched since profiling was enabled */
+  long long fine_sweeps;     /* fine-level amg_smooth launches timed */
+  double fine_sweep_ms;      /* their total device time */
+  double fine_sweep_bytes;   /* algorithmic bytes of one fine-level sweep */
+  double algorithmic_bytes;  /* all kernels of the profiled solves */
+  long long solves;
+} b2_profile;
+int b2_solver_profile(b2_solver* solver, int enable);
+int b2_solver_profile_read(b2_solver* solver, b2_profile* out);
+/* Process-wide count of kernels launched by this library. */
+long long b2_kernel_launches(void);
+
+/* One damped L1-Jacobi sweep (amg_smooth / amg_smooth_zero,
+ * src/kutta/kernels/linalg.kern.h:150-170): next = x + (2/3) inv (b - A x). */
+int b2_amg_smooth(int n, const int32_t* d_row_ptr, const int32_t* d_col, const float* d_val,
+                  const float* d_x, const float* d_b, const float* d_inverse, float* d_next,
+                  int zero_start, void* stream);
+
 /* Hierarchy introspection (the captured-hierarchy checks of the reference's
  * tests/linalg/test_solvers.cpp:487-555 read the same data back from launches).
  * Level 0 is the input matrix. Copies are synchronous device-to-host reads on

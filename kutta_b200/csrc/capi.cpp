@@ -211,6 +211,40 @@ int b2_csr_residual(int n, int nnz, const int32_t* d_row_ptr, const int32_t* d_c
   });
 }
 
+int b2_solver_profile(b2_solver* s, int enable) {
+  return guarded([&] {
+    KB2_REQUIRE(s && s->s, "solver: null handle");
+    s->s->set_profile(enable != 0);
+  });
+}
+
+int b2_solver_profile_read(b2_solver* s, b2_profile* out) {
+  return guarded([&] {
+    KB2_REQUIRE(s && s->s && out, "solver: null handle");
+    const auto p = s->s->profile();
+    out->launches = p.launches;
+    out->fine_sweeps = p.fine_sweeps;
+    out->fine_sweep_ms = p.fine_sweep_ms;
+    out->fine_sweep_bytes = p.fine_sweep_bytes;
+    out->algorithmic_bytes = p.algorithmic_bytes;
+    out->solves = p.solves;
+  });
+}
+
+long long b2_kernel_launches(void) { return kb2::launch::counter.load(); }
+
+int b2_amg_smooth(int n, const int32_t* d_row_ptr, const int32_t* d_col, const float* d_val,
+                  const float* d_x, const float* d_b, const float* d_inverse, float* d_next,
+                  int zero_start, void* stream) {
+  return guarded([&] {
+    KB2_REQUIRE(n >= 0, "CSR: invalid array sizes");
+    KB2_REQUIRE((d_next != d_x && d_next != d_b) || n == 0, "smooth: output aliases an input");
+    kb2::launch::smooth(n, d_row_ptr, d_col, d_val, d_x, d_b, d_inverse, d_next, nullptr,
+                        zero_start != 0, as_stream(stream));
+    kb2::cuda_check(cudaGetLastError(), "amg_smooth");
+  });
+}
+
 int b2_solver_levels(const b2_solver* s) { return s && s->s ? s->s->levels() : 0; }
 
 int b2_solver_level_shape(const b2_solver* s, int level, int* n, int* nnz) {

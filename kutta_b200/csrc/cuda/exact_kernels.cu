@@ -9,6 +9,8 @@
 #include "common.cuh"
 #include "kernels.hpp"
 
+#include <atomic>
+
 namespace kb2 {
 namespace {
 using namespace dev;
@@ -178,7 +180,7 @@ __global__ void k_smooth(int n, const int* __restrict__ rows, const int* __restr
                          const float* __restrict__ vals, const float* __restrict__ x,
                          const float* __restrict__ b, const float* __restrict__ inv,
                          float* __restrict__ next, const int* __restrict__ status) {
-  if (status[0] != 0) return;
+  if (status && status[0] != 0) return;
   ROWS(i, n) {
     const float bi = b[i];
     if (kZero && !nonfinite(bi)) {
@@ -458,26 +460,32 @@ static_assert(kReducePartials == kPartials, "reduction scratch size");
 
 namespace launch {
 
+std::atomic<long long> counter{0};
+
 void spmv(int n, const int* rows, const int* cols, const float* vals, const float* x, float* y,
           const int* status, cudaStream_t s) {
   if (n <= 0) return;
+  ++counter;
   k_spmv<<<blocks(n), kBlock, 0, s>>>(n, rows, cols, vals, x, y, status);
 }
 void spmv_dot(int n, const int* rows, const int* cols, const float* vals, const float* p,
               const float* w, float* q, DeviceReducer red, float* scalars, int offset,
               int* status, Epilogue epi, cudaStream_t s) {
+  ++counter;
   k_spmv_dot<<<blocks(n), kBlock, 0, s>>>(n, rows, cols, vals, p, w, q, red, scalars, offset,
                                           status, epi);
 }
 void residual(int n, const int* rows, const int* cols, const float* vals, const float* x,
               const float* b, float* r, const int* status, cudaStream_t s) {
   if (n <= 0) return;
+  ++counter;
   k_residual<<<blocks(n), kBlock, 0, s>>>(n, rows, cols, vals, x, b, r, status);
 }
 void smooth(int n, const int* rows, const int* cols, const float* vals, const float* x,
             const float* b, const float* inv, float* next, const int* status, bool zero_start,
             cudaStream_t s) {
   if (n <= 0) return;
+  ++counter;
   if (zero_start)
     k_smooth<true><<<blocks(n), kBlock, 0, s>>>(n, rows, cols, vals, x, b, inv, next, status);
   else
@@ -486,89 +494,108 @@ void smooth(int n, const int* rows, const int* cols, const float* vals, const fl
 void coarse_solve(int count, const int* rows, const int* cols, const float* vals, float* x,
                   const float* b, const float* inv, const int* status, int sweeps,
                   cudaStream_t s) {
+  ++counter;
   k_coarse_solve<<<1, 32, 0, s>>>(count, rows, cols, vals, x, b, inv, status, sweeps);
 }
 void diagonal(int n, const int* rows, const int* diag, const float* vals, float* inverse,
               int use_l1, DeviceReducer red, double* check, int slot, cudaStream_t s) {
+  ++counter;
   k_diagonal<<<blocks(n), kBlock, 0, s>>>(n, rows, diag, vals, inverse, use_l1, red, check, slot);
 }
 void restrict_(int nc, const int* offsets, const int* members, const float* fine, float* coarse,
                const int* status, cudaStream_t s) {
   if (nc <= 0) return;
+  ++counter;
   k_restrict<<<blocks(nc), kBlock, 0, s>>>(nc, offsets, members, fine, coarse, status);
 }
 void prolong(int nf, const int* aggregate, const float* coarse, float* fine, const int* status,
              cudaStream_t s) {
   if (nf <= 0) return;
+  ++counter;
   k_prolong<<<blocks(nf), kBlock, 0, s>>>(nf, aggregate, coarse, fine, status);
 }
 void galerkin(int nnz_c, const int* offsets, const int* entries, const float* fine, float* coarse,
               cudaStream_t s) {
   if (nnz_c <= 0) return;
+  ++counter;
   k_galerkin<<<blocks(nnz_c), kBlock, 0, s>>>(nnz_c, offsets, entries, fine, coarse);
 }
 void m_matrix_diagonal(int nc, const int* offsets, const int* members, const int* fine_rows,
                        const int* fine_diag, const float* fine, const int* rows, const int* diag,
                        float* coarse, cudaStream_t s) {
   if (nc <= 0) return;
+  ++counter;
   k_m_matrix_diagonal<<<blocks(nc), kBlock, 0, s>>>(nc, offsets, members, fine_rows, fine_diag,
                                                     fine, rows, diag, coarse);
 }
 void pcg_step_dot(int n, float* x, float* r, const float* p, const float* q, DeviceReducer red,
                   float* scalars, int* status, cudaStream_t s) {
+  ++counter;
   k_pcg_step_dot<<<blocks(n), kBlock, 0, s>>>(n, x, r, p, q, red, scalars, status);
 }
 void direction(int n, const float* z, float* p, const float* scalars, const int* status,
                cudaStream_t s) {
   if (n <= 0) return;
+  ++counter;
   k_direction<<<blocks(n), kBlock, 0, s>>>(n, z, p, scalars, status);
 }
 void bicg_direction(int n, const float* r, const float* v, float* p, const float* scalars,
                     const int* status, cudaStream_t s) {
   if (n <= 0) return;
+  ++counter;
   k_bicg_direction<<<blocks(n), kBlock, 0, s>>>(n, r, v, p, scalars, status);
 }
 void bicg_difference(int n, const float* r, const float* q, float* sv, const float* scalars,
                      const int* status, cudaStream_t s) {
   if (n <= 0) return;
+  ++counter;
   k_bicg_difference<<<blocks(n), kBlock, 0, s>>>(n, r, q, sv, scalars, status);
 }
 void bicg_step(int n, float* x, float* r, const float* z, const float* zs, const float* sv,
                const float* t, const float* scalars, const int* status, cudaStream_t s) {
   if (n <= 0) return;
+  ++counter;
   k_bicg_step<<<blocks(n), kBlock, 0, s>>>(n, x, r, z, zs, sv, t, scalars, status);
 }
 void multiply(int n, const float* r, const float* inverse, float* z, const int* status,
               cudaStream_t s) {
   if (n <= 0) return;
+  ++counter;
   k_multiply<<<blocks(n), kBlock, 0, s>>>(n, r, inverse, z, status);
 }
 void axpy(int n, float* y, const float* x, float a, cudaStream_t s) {
   if (n <= 0) return;
+  ++counter;
   k_axpy<<<blocks(n), kBlock, 0, s>>>(n, y, x, a);
 }
 void fill(int n, float* x, float value, cudaStream_t s) {
   if (n <= 0) return;
+  ++counter;
   k_fill<<<blocks(n), kBlock, 0, s>>>(n, x, value);
 }
 void reduce_into(ReduceMode mode, int n, const float* x, const float* y, const float* u,
                  const float* v, DeviceReducer red, float* scalars, int offset, int* status,
                  bool guard, Epilogue epi, cudaStream_t s) {
+  ++counter;
   k_reduce_into<<<blocks(n), kBlock, 0, s>>>(mode, n, x, y, u, v, red, scalars, offset, status,
                                              guard, epi);
 }
 void reduce_value(ReduceMode mode, int n, const float* x, const float* y, DeviceReducer red,
                   double* out, int slot, cudaStream_t s) {
+  ++counter;
   k_reduce_value<<<blocks(n), kBlock, 0, s>>>(mode, n, x, y, red, out, slot);
 }
 void solver_limits(float* scalars, float th, float tl, float dh, float dl, cudaStream_t s) {
+  ++counter;
   k_solver_limits<<<1, 32, 0, s>>>(scalars, th, tl, dh, dl);
 }
 void solver_reset(float* scalars, int* status, int iterations, cudaStream_t s) {
+  ++counter;
   k_solver_reset<<<1, 1, 0, s>>>(scalars, status, iterations);
 }
 void project(int n, float* x, const float* sum, float count_hi, float count_lo, cudaStream_t s) {
   if (n <= 0) return;
+  ++counter;
   k_project<<<blocks(n), kBlock, 0, s>>>(n, x, sum, count_hi, count_lo);
 }
 

@@ -2,6 +2,7 @@
 // every launcher enqueues on `stream` and never synchronises.
 #pragma once
 
+#include <atomic>
 #include <cstdint>
 #include <cuda_runtime.h>
 
@@ -36,6 +37,9 @@ struct DeviceReducer {
 };
 
 namespace launch {
+
+// Kernels launched by this library since load (every launcher increments it).
+extern std::atomic<long long> counter;
 
 // ---- CSR row kernels (one row per thread, grid-stride) -------------------
 // y = A x, Kahan-compensated (csr_spmv). status may be null (unguarded).

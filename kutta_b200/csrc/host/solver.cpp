@@ -112,12 +112,50 @@ Solver::Solver(Kind kind, const CsrView& a, const Options& options,
 // ---------------------------------------------------------------- primitives --
 void Solver::residual(const float* x, const float* b, float* r) {
   launch::residual(n_, rows0(), cols0(), val_, x, b, r, nullptr, stream_);
+  tally(8.0 * nnz_ + 4.0 * (n_ + 1) + 12.0 * n_);
+}
+
+Solver::~Solver() {
+  for (auto e : events_) cudaEventDestroy(e);
+}
+
+void Solver::set_profile(bool on) {
+  profiling_ = on;
+  prof_ = Profile{};
+  prof_.fine_sweep_bytes = 8.0 * nnz_ + 4.0 * (n_ + 1) + 16.0 * n_;
+  launch_mark_ = launch::counter.load();
+  events_used_ = 0;
+}
+
+void Solver::collect_events() {
+  std::vector<float> times;
+  for (std::size_t k = 0; k + 1 < events_used_; k += 2) {
+    float ms = 0;
+    cuda_check(cudaEventElapsedTime(&ms, events_[k], events_[k + 1]), "cudaEventElapsedTime");
+    times.push_back(ms);
+  }
+  events_used_ = 0;
+  if (!times.empty()) {
+    // Sweeps queued after a convergence candidate return at once (status guard);
+    // they are not sweeps of the matrix and are left out of the kernel time.
+    std::vector<float> sorted = times;
+    std::nth_element(sorted.begin(), sorted.begin() + sorted.size() / 2, sorted.end());
+    const float median = sorted[sorted.size() / 2];
+    for (float ms : times)
+      if (ms >= 0.25f * median) {
+        prof_.fine_sweep_ms += ms;
+        ++prof_.fine_sweeps;
+      }
+  }
+  prof_.launches = launch::counter.load() - launch_mark_;
 }
 
 std::vector<double> Solver::host_reduce(std::initializer_list<Request> requests) {
   int slot = 0;
-  for (const auto& q : requests)
+  for (const auto& q : requests) {
     launch::reduce_value(q.mode, q.n, q.x, q.y, reducer(), values_.get(), slot++, stream_);
+    tally((q.mode == ReduceMode::Dot && q.x != q.y ? 8.0 : 4.0) * q.n);
+  }
   cuda_check(cudaMemcpyAsync(host_values_.get(), values_.get(), sizeof(double) * slot,
                              cudaMemcpyDeviceToHost, stream_),
              "reduction readback");
@@ -131,10 +169,12 @@ double Solver::norm(const float* x) {
 }
 
 void Solver::copy(float* dst, const float* src, int n) {
-  if (n > 0 && dst != src)
+  if (n > 0 && dst != src) {
     cuda_check(cudaMemcpyAsync(dst, src, sizeof(float) * static_cast<std::size_t>(n),
                                cudaMemcpyDeviceToDevice, stream_),
                "copy");
+    tally(8.0 * n);
+  }
 }
 
 // linalg_detail::project, detail.hpp:13-19.
@@ -152,9 +192,23 @@ void Solver::reset(int iterations) { launch::solver_reset(scalars_.get(), status
 // ------------------------------------------------------------ preconditioner --
 void Solver::smooth(DevLevel& l, const int* rows, const int* cols, const float* vals,
                     const float* b, float*& x, int sweeps, bool zero_start) {
+  const bool fine = &l == &levels_[0];
   for (int sweep = 0; sweep < sweeps; ++sweep) {
-    launch::smooth(l.n, rows, cols, vals, x, b, l.l1.get(), l.r, status_.get(),
-                   zero_start && sweep == 0, stream_);
+    const bool zero = zero_start && sweep == 0;
+    // Every 8th fine-level sweep is bracketed by events: enough samples for the
+    // average launch time, little added host work inside a timed solve.
+    const bool timed = profiling_ && fine && !zero && (sampled_++ % 8 == 0);
+    if (timed) {
+      while (events_.size() < events_used_ + 2) {
+        cudaEvent_t e;
+        cuda_check(cudaEventCreate(&e), "cudaEventCreate");
+        events_.push_back(e);
+      }
+      cuda_check(cudaEventRecord(events_[events_used_++], stream_), "cudaEventRecord");
+    }
+    launch::smooth(l.n, rows, cols, vals, x, b, l.l1.get(), l.r, status_.get(), zero, stream_);
+    if (timed) cuda_check(cudaEventRecord(events_[events_used_++], stream_), "cudaEventRecord");
+    tally(zero ? 12.0 * l.n : 8.0 * l.nnz + 4.0 * (l.n + 1) + 16.0 * l.n);
     std::swap(x, l.r);  // ping-pong: the two buffers exchange roles (amg.cpp:280)
   }
 }
@@ -178,9 +232,11 @@ void Solver::cycle(std::size_t index, const float* b, float*& x) {
     auto& c = levels_[index + 1];
     launch::restrict_(c.n, l.member_offsets.get(), l.members.get(), l.r, c.b.get(),
                       status_.get(), stream_);
+    tally(8.0 * l.nnz + 4.0 * (l.n + 1) + 12.0 * l.n + 4.0 * (c.n + 1) + 8.0 * l.n + 4.0 * c.n);
     if (nullspace_) project(c.b.get(), c.n, c.projection.get());
     cycle(index + 1, c.b.get(), c.x);
     launch::prolong(l.n, l.aggregate.get(), c.x, x, status_.get(), stream_);
+    tally(12.0 * l.n + 4.0 * c.n);
     smooth(l, rows, cols, vals, b, x, options_.post_sweeps, false);
   }
   if (nullspace_ && index != 0) project(x, l.n, l.projection.get());
@@ -313,8 +369,10 @@ void Solver::pcg(float* x, const float* b, const Control& c, double target, Stat
       launch::spmv_dot(n_, rows0(), cols0(), val_, p_, p_, q_, reducer(), scalars_.get(), 2,
                        status_.get(), Epilogue::PcgAlpha, stream_);
       launch::pcg_step_dot(n_, x, r_, p_, q_, reducer(), scalars_.get(), status_.get(), stream_);
+      tally(8.0 * nnz_ + 4.0 * (n_ + 1) + 8.0 * n_ + 24.0 * n_);
       if (stats.iterations + j + 1 == c.max_iter) continue;
       apply(r_, z_);
+      tally((variable() ? 12.0 : 8.0) * n_ + 12.0 * n_);
       if (variable())
         launch::reduce_into(ReduceMode::Dot2, n_, r_, z_, z_, q_, reducer(), scalars_.get(), 4,
                             status_.get(), true, Epilogue::PcgBetaFlexible, stream_);
@@ -372,6 +430,7 @@ void Solver::bicgstab(float* x, const float* b, const Control& c, double target,
       launch::bicg_step(n_, x, r_, z_, zs_, s_, t_, sc, status_.get(), stream_);
       launch::reduce_into(ReduceMode::Dot, n_, r_, r_, r_, r_, reducer(), sc, 18, status_.get(),
                           true, Epilogue::CheckBicg, stream_);
+      tally(2.0 * (8.0 * nnz_ + 4.0 * (n_ + 1)) + 104.0 * n_);
     }
     const auto state = poll(x, b);
     stats.iterations = state[1];
@@ -467,6 +526,10 @@ Stats Solver::solve(const float* val, float* x, const float* b, const Control& c
   previous_iterations_ = stats.converged ? stats.iterations : 0;
   wait(stream_);
   cuda_check(cudaGetLastError(), "solve");
+  if (profiling_) {
+    collect_events();
+    ++prof_.solves;
+  }
   return stats;
 }
 

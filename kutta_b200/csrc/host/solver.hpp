@@ -62,9 +62,19 @@ struct DevLevel {
   DArray<int> aggregate, member_offsets, members, entry_offsets, entries;
 };
 
+// Solve-time measurement: device time of every fine-level smoother sweep (CUDA
+// events on the solve stream) and the algorithmic bytes of every launch.
+struct Profile {
+  long long launches = 0, fine_sweeps = 0, solves = 0;
+  double fine_sweep_ms = 0, fine_sweep_bytes = 0, algorithmic_bytes = 0;
+};
+
 class Solver {
  public:
   Solver(Kind kind, const CsrView& a, const Options& options, std::shared_ptr<Workspace> workspace);
+  ~Solver();
+  void set_profile(bool on);
+  Profile profile() const { return prof_; }
   void refresh(const float* val, cudaStream_t s);
   Stats solve(const float* val, float* x, const float* b, const Control& c, cudaStream_t s);
   std::string describe() const;
@@ -148,6 +158,17 @@ class Solver {
   // Per-call state.
   cudaStream_t stream_ = nullptr;
   const float* val_ = nullptr;
+  // Measurement.
+  void tally(double bytes) {
+    if (profiling_) prof_.algorithmic_bytes += bytes;
+  }
+  void collect_events();
+  bool profiling_ = false;
+  Profile prof_;
+  long long launch_mark_ = 0;
+  std::vector<cudaEvent_t> events_;
+  std::size_t events_used_ = 0;
+  long long sampled_ = 0;
 };
 
 }  // namespace kb2

@@ -132,6 +132,12 @@ class _Control(ctypes.Structure):
                 ("max_iter", ctypes.c_int), ("residual_check_interval", ctypes.c_int)]
 
 
+class _Profile(ctypes.Structure):
+    _fields_ = [("launches", ctypes.c_longlong), ("fine_sweeps", ctypes.c_longlong),
+                ("fine_sweep_ms", ctypes.c_double), ("fine_sweep_bytes", ctypes.c_double),
+                ("algorithmic_bytes", ctypes.c_double), ("solves", ctypes.c_longlong)]
+
+
 class _Stats(ctypes.Structure):
     _fields_ = [("iterations", ctypes.c_int), ("converged", ctypes.c_int),
                 ("initial_residual", ctypes.c_double), ("final_residual", ctypes.c_double)]
@@ -153,6 +159,10 @@ _SIGNATURES = {
     "b2_solver_destroy": (None, [_P]),
     "b2_csr_spmv": (_I, [_I, _I, _P, _P, _P, _P, _P, _P]),
     "b2_csr_residual": (_I, [_I, _I, _P, _P, _P, _P, _P, _P, _P]),
+    "b2_solver_profile": (_I, [_P, _I]),
+    "b2_solver_profile_read": (_I, [_P, _P]),
+    "b2_kernel_launches": (ctypes.c_longlong, []),
+    "b2_amg_smooth": (_I, [_I, _P, _P, _P, _P, _P, _P, _P, _I, _P]),
     "b2_solver_levels": (_I, [_P]),
     "b2_solver_level_shape": (_I, [_P, _I, _P, _P]),
     "b2_solver_level_copy": (_I, [_P, _I, _P, _P, _P, _P, _P, _P]),
@@ -327,6 +337,15 @@ class LinearSolver:
         _load().b2_solver_describe(self._handle, buf, 512)
         return buf.value.decode()
 
+    def profile(self, enable: bool) -> None:
+        """Turns solve-time measurement on (resetting it) or off."""
+        _check(_load().b2_solver_profile(self._handle, int(enable)))
+
+    def profile_read(self) -> dict:
+        p = _Profile()
+        _check(_load().b2_solver_profile_read(self._handle, ctypes.byref(p)))
+        return {f: getattr(p, f) for f, _ in _Profile._fields_}
+
     def levels(self):
         """The device hierarchy read back: [(n, row_ptr, col, val, inverse_l1, aggregate)]."""
         lib = _load()
@@ -368,6 +387,17 @@ def spmv(a: CsrMatrix, x, y) -> None:
         raise KuttaError("CSR: input/output aliasing is unsupported")
     _check(_load().b2_csr_spmv(a.n_rows, a.nnz, _tptr(a.row_ptr), _tptr(a.col), _tptr(a.val),
                                _tptr(x), _tptr(y), _stream()))
+
+
+def kernel_launches() -> int:
+    """Kernels this library has launched in this process."""
+    return int(_load().b2_kernel_launches())
+
+
+def amg_smooth(a: CsrMatrix, x, b, inverse, out, zero_start=False) -> None:
+    """One damped L1-Jacobi sweep (amg_smooth / amg_smooth_zero)."""
+    _check(_load().b2_amg_smooth(a.n_rows, _tptr(a.row_ptr), _tptr(a.col), _tptr(a.val), _tptr(x),
+                                 _tptr(b), _tptr(inverse), _tptr(out), int(zero_start), _stream()))
 
 
 def residual(a: CsrMatrix, x, b, r) -> None:
