@@ -13,6 +13,7 @@
 #include <cmath>
 #include <cstring>
 #include <iomanip>
+#include <numeric>
 #include <sstream>
 
 namespace kb2 {
@@ -20,6 +21,7 @@ namespace kb2 {
 namespace {
 constexpr int kSpeculativeRows = 1 << 17;  // solver.cpp:387
 }
+
 
 Solver::Solver(Kind kind, const CsrView& a, const Options& options,
                std::shared_ptr<Workspace> workspace)
@@ -221,11 +223,12 @@ void Solver::cycle(std::size_t index, const float* b, float*& x) {
   const float* vals = index == 0 ? val_ : l.val.get();
   // x is not cleared: every first step below writes it without reading it.
   if (index + 1 == levels_.size()) {
-    if (l.n <= 24)
+    if (l.n <= 24) {
       launch::coarse_solve(l.n, rows, cols, vals, x, b, l.l1.get(), status_.get(),
                            options_.coarse_sweeps, stream_);
-    else
+    } else {
       smooth(l, rows, cols, vals, b, x, options_.coarse_sweeps, true);
+    }
   } else {
     smooth(l, rows, cols, vals, b, x, options_.pre_sweeps, true);
     launch::residual(l.n, rows, cols, vals, x, b, l.r, status_.get(), stream_);
