@@ -156,6 +156,61 @@ int b2_amg_smooth(int n, const int32_t* d_row_ptr, const int32_t* d_col, const f
                   const float* d_x, const float* d_b, const float* d_inverse, float* d_next,
                   int zero_start, void* stream);
 
+/* ---- Mixed-precision solve (no reference counterpart) --------------------
+ * The same pressure system solved to a tolerance below the FP32 floor: FP64
+ * iterative refinement (true residual b - A x and inner products in FP64, the
+ * solution kept in FP64) around an inner FP32 PCG whose V-cycle stores the
+ * coarse operators in BF16 with symmetric per-row scales and solves the
+ * coarsest level with a dense FP64 Cholesky factorisation. The hierarchy
+ * pairs rows like the reference's aggregation and lets rows left unpaired join
+ * their strongest paired neighbour, so coarsening reaches the dense size. */
+typedef struct {
+  b2_options amg;            /* threshold, passes, sweeps, structure (coarse_rows ignored) */
+  int absorb_singletons;     /* default 1 */
+  int dense_rows;            /* coarsen until a level has <= this many rows (default 512) */
+  int coarse_bf16;           /* default 1: levels >= 1 stored as BF16 x row scales */
+  double inner_rel_tol;      /* residual reduction per refinement step (default 1e-3) */
+  int inner_max_iter;        /* inner PCG iterations per refinement step (default 300) */
+  int max_refinements;       /* default 30 */
+} b2_mixed_options;
+
+typedef struct {
+  int refinements;           /* outer FP64 refinement steps */
+  int iterations;            /* inner PCG iterations, all steps */
+  int converged;
+  double initial_residual;   /* ||b - A x0||, FP64 */
+  double final_residual;     /* ||b - A x||, FP64, of the returned FP64 x */
+} b2_mixed_stats;
+
+typedef struct b2_mixed b2_mixed;
+
+void b2_mixed_options_default(b2_mixed_options* options);
+int b2_mixed_create(int n, int nnz, const int32_t* row_ptr, const int32_t* col,
+                    const int32_t* diag, const double* val, const b2_mixed_options* options,
+                    b2_mixed** out);
+int b2_mixed_refresh(b2_mixed* solver, const float* d_val, void* stream);
+/* d_x: n doubles, initial guess in, FP64 solution out. d_b: n floats. */
+int b2_mixed_solve(b2_mixed* solver, const float* d_val, double* d_x, const float* d_b,
+                   const b2_control* control, b2_mixed_stats* stats, void* stream);
+size_t b2_mixed_describe(const b2_mixed* solver, char* buffer, size_t length);
+void b2_mixed_destroy(b2_mixed* solver);
+/* The mixed solve's coarsest-level step on its own: the dense FP64 Cholesky
+ * factorisation of a small SPD CSR operator (n <= 1024) and its explicit
+ * inverse, computed in one thread block. d_inverse: n*n doubles, row-major.
+ * *d_not_spd (a device double) is written 1.0 if a pivot was not positive,
+ * else 0.0. Enqueued on `stream`; the n*n factor scratch is allocated and
+ * released stream-ordered (cudaMallocAsync / cudaFreeAsync). */
+int b2_dense_inverse(int n, const int32_t* d_row_ptr, const int32_t* d_col, const float* d_val,
+                     double* d_inverse, double* d_not_spd, void* stream);
+
+/* As b2_solver_profile / _read, for the inner solve plus the FP64 refinement. */
+int b2_mixed_profile(b2_mixed* solver, int enable);
+int b2_mixed_profile_read(b2_mixed* solver, b2_profile* out);
+/* Host-only mixed hierarchy (as b2_hierarchy_build). */
+int b2_mixed_hierarchy_build(int n, int nnz, const int32_t* row_ptr, const int32_t* col,
+                             const int32_t* diag, const double* val,
+                             const b2_mixed_options* options, b2_hierarchy** out);
+
 /* Hierarchy introspection (the captured-hierarchy checks of the reference's
  * tests/linalg/test_solvers.cpp:487-555 read the same data back from launches).
  * Level 0 is the input matrix. Copies are synchronous device-to-host reads on

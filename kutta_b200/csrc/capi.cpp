@@ -2,6 +2,7 @@
 // text, and the mapping of the reference's linalg entry points onto kb2::Solver.
 #include "kutta_b200.h"
 
+#include <cmath>
 #include <cstdio>
 #include <cstring>
 #include <memory>
@@ -9,6 +10,7 @@
 #include <string>
 
 #include "cuda/kernels.hpp"
+#include "host/mixed.hpp"
 #include "host/setup.hpp"
 #include "host/solver.hpp"
 
@@ -21,6 +23,9 @@ struct b2_solver {
 struct b2_hierarchy {
   kb2::Hierarchy h;
   kb2::HostCsr fine;
+};
+struct b2_mixed {
+  std::unique_ptr<kb2::MixedSolver> s;
 };
 
 namespace {
@@ -71,6 +76,14 @@ kb2::Options to_options(const b2_options* o) {
               "AMG: invalid operator structure");
   r.m_matrix = o->structure == B2_STRUCTURE_SYMMETRIC_M_MATRIX;
   return r;
+}
+
+kb2::Options mixed_options(const b2_mixed_options& m) {
+  auto o = to_options(&m.amg);
+  o.absorb_singletons = m.absorb_singletons != 0;
+  KB2_REQUIRE(m.dense_rows >= 1 && m.dense_rows <= 4096, "mixed: dense_rows must be in [1, 4096]");
+  o.coarse_rows = m.dense_rows;
+  return o;
 }
 
 kb2::CsrView view(int n, int nnz, const int32_t* row_ptr, const int32_t* col, const int32_t* diag,
@@ -330,5 +343,144 @@ int b2_hierarchy_level_copy(const b2_hierarchy* h, int level, int32_t* row_ptr, 
 }
 
 void b2_hierarchy_free(b2_hierarchy* h) { delete h; }
+
+void b2_mixed_options_default(b2_mixed_options* o) {
+  if (!o) return;
+  b2_options_default(&o->amg);
+  o->amg.structure = B2_STRUCTURE_SYMMETRIC_M_MATRIX;
+  o->amg.pre_sweeps = o->amg.post_sweeps = 2;
+  o->absorb_singletons = 1;
+  o->dense_rows = 512;
+  o->coarse_bf16 = 1;
+  o->inner_rel_tol = 1e-3;
+  o->inner_max_iter = 300;
+  o->max_refinements = 30;
+}
+
+int b2_mixed_create(int n, int nnz, const int32_t* row_ptr, const int32_t* col,
+                    const int32_t* diag, const double* val, const b2_mixed_options* options,
+                    b2_mixed** out) {
+  return guarded([&] {
+    KB2_REQUIRE(out != nullptr, "solver: null output handle");
+    *out = nullptr;
+    b2_mixed_options defaults;
+    b2_mixed_options_default(&defaults);
+    const b2_mixed_options& m = options ? *options : defaults;
+    const auto a = view(n, nnz, row_ptr, col, diag, val);
+    kb2::MixedOptions o;
+    o.amg = mixed_options(m);
+    o.amg.coarse_bf16 = m.coarse_bf16 != 0;
+    o.amg.dense_coarsest = true;
+    KB2_REQUIRE(std::isfinite(m.inner_rel_tol) && m.inner_rel_tol > 0 && m.inner_rel_tol < 1 &&
+                    m.inner_max_iter > 0 && m.max_refinements > 0,
+                "mixed: invalid refinement options");
+    o.inner_rel_tol = m.inner_rel_tol;
+    o.inner_max_iter = m.inner_max_iter;
+    o.max_refinements = m.max_refinements;
+    kb2::check_amg(kb2::Kind::AmgPcg, a, o.amg);
+    *out = new b2_mixed{std::make_unique<kb2::MixedSolver>(a, o)};
+  });
+}
+
+int b2_mixed_refresh(b2_mixed* s, const float* d_val, void* stream) {
+  return guarded([&] {
+    KB2_REQUIRE(s && s->s, "solver: null handle");
+    s->s->refresh(d_val, as_stream(stream));
+  });
+}
+
+int b2_mixed_solve(b2_mixed* s, const float* d_val, double* d_x, const float* d_b,
+                   const b2_control* control, b2_mixed_stats* stats, void* stream) {
+  return guarded([&] {
+    KB2_REQUIRE(s && s->s, "solver: null handle");
+    kb2::Control c;
+    if (control) {
+      c.rel_tol = control->rel_tol;
+      c.abs_tol = control->abs_tol;
+      c.max_iter = control->max_iter;
+      c.residual_check_interval = control->residual_check_interval;
+    }
+    const auto r = s->s->solve(d_val, d_x, d_b, c, as_stream(stream));
+    if (stats) {
+      stats->refinements = r.refinements;
+      stats->iterations = r.iterations;
+      stats->converged = r.converged ? 1 : 0;
+      stats->initial_residual = r.initial_residual;
+      stats->final_residual = r.final_residual;
+    }
+  });
+}
+
+size_t b2_mixed_describe(const b2_mixed* s, char* buffer, size_t length) {
+  if (!s || !s->s) return 0;
+  const auto d = s->s->describe();
+  if (buffer && length) std::snprintf(buffer, length, "%s", d.c_str());
+  return d.size();
+}
+
+void b2_mixed_destroy(b2_mixed* s) { delete s; }
+
+int b2_dense_inverse(int n, const int32_t* d_row_ptr, const int32_t* d_col, const float* d_val,
+                     double* d_inverse, double* d_not_spd, void* stream) {
+  return guarded([&] {
+    KB2_REQUIRE(n >= 1 && n <= 1024, "dense inverse: n must be in [1, 1024]");
+    KB2_REQUIRE(d_row_ptr && d_col && d_val && d_inverse && d_not_spd,
+                "dense inverse: null argument");
+    const auto st = as_stream(stream);
+    double* lower = nullptr;
+    kb2::cuda_check(cudaMallocAsync(reinterpret_cast<void**>(&lower),
+                                    sizeof(double) * static_cast<std::size_t>(n) * n, st),
+                    "cudaMallocAsync");
+    kb2::launch::dense_inverse(n, d_row_ptr, d_col, d_val, lower, d_inverse, d_not_spd, st);
+    const cudaError_t launched = cudaGetLastError();
+    kb2::cuda_check(cudaFreeAsync(lower, st), "cudaFreeAsync");
+    kb2::cuda_check(launched, "dense_inverse");
+  });
+}
+
+int b2_mixed_profile(b2_mixed* s, int enable) {
+  return guarded([&] {
+    KB2_REQUIRE(s && s->s, "solver: null handle");
+    s->s->inner().set_profile(enable != 0);
+  });
+}
+
+int b2_mixed_profile_read(b2_mixed* s, b2_profile* out) {
+  return guarded([&] {
+    KB2_REQUIRE(s && s->s && out, "solver: null handle");
+    const auto p = s->s->inner().profile();
+    out->launches = p.launches;
+    out->fine_sweeps = p.fine_sweeps;
+    out->fine_sweep_ms = p.fine_sweep_ms;
+    out->fine_sweep_bytes = p.fine_sweep_bytes;
+    out->algorithmic_bytes = p.algorithmic_bytes;
+    out->solves = p.solves;
+  });
+}
+
+int b2_mixed_hierarchy_build(int n, int nnz, const int32_t* row_ptr, const int32_t* col,
+                             const int32_t* diag, const double* val,
+                             const b2_mixed_options* options, b2_hierarchy** out) {
+  return guarded([&] {
+    KB2_REQUIRE(out != nullptr && options != nullptr, "hierarchy: null argument");
+    *out = nullptr;
+    const auto a = view(n, nnz, row_ptr, col, diag, val);
+    auto o = mixed_options(*options);
+    kb2::check_amg(kb2::Kind::AmgPcg, a, o);
+    auto* h = new b2_hierarchy;
+    try {
+      h->h = kb2::build_hierarchy(a, o);
+    } catch (...) {
+      delete h;
+      throw;
+    }
+    h->fine.n = n;
+    h->fine.row_ptr.assign(row_ptr, row_ptr + n + 1);
+    h->fine.col.assign(col, col + nnz);
+    h->fine.diag.assign(diag, diag + n);
+    h->fine.val.assign(val, val + nnz);
+    *out = h;
+  });
+}
 
 }  // extern "C"

@@ -105,6 +105,31 @@ void reduce_into(ReduceMode mode, int n, const float* x, const float* y, const f
 void reduce_value(ReduceMode mode, int n, const float* x, const float* y, DeviceReducer red,
                   double* out, int slot, cudaStream_t s);
 
+// ---- mixed precision (no reference counterpart) ---------------------------
+// Coarse operator as BF16 times a per-row FP32 scale (max |a_ij|).
+void bf16_pack(int n, const int* rows, const float* vals, unsigned short* v16, float* scale,
+               cudaStream_t s);
+void bf16_smooth(int n, const int* rows, const int* cols, const unsigned short* v16,
+                 const float* scale, const float* x, const float* b, const float* inv, float* next,
+                 const int* status, bool zero_start, cudaStream_t s);
+void bf16_residual(int n, const int* rows, const int* cols, const unsigned short* v16,
+                   const float* scale, const float* x, const float* b, float* r, const int* status,
+                   cudaStream_t s);
+// Dense FP64 Cholesky of an n <= 1024 CSR operator and its explicit inverse
+// (n x n, row-major, into `inverse`; `lower` is n x n scratch); *error = 1 if
+// the operator is not SPD.
+void dense_inverse(int n, const int* rows, const int* cols, const float* vals, double* lower,
+                   double* inverse, double* error, cudaStream_t s);
+// x = inverse * b (FP64 accumulation).
+void dense_solve(int n, const double* inverse, const float* b, float* x, const int* status,
+                 cudaStream_t s);
+// rf = float(b - A x) with x FP64, ||b - A x||^2 (FP64) into out[slot].
+void residual64(int n, const int* rows, const int* cols, const float* vals, const double* x,
+                const float* b, float* rf, DeviceReducer red, double* out, int slot,
+                cudaStream_t s);
+// x += e.
+void update64(int n, double* x, const float* e, cudaStream_t s);
+
 // ---- single-thread scalar kernels -------------------------------------------
 void solver_limits(float* scalars, float th, float tl, float dh, float dl, cudaStream_t s);
 void solver_reset(float* scalars, int* status, int iterations, cudaStream_t s);

@@ -1,0 +1,45 @@
+// Mixed-precision pressure solve (no reference counterpart): FP64 iterative
+// refinement around the FP32 AMG-PCG of solver.hpp in its mixed mode.
+#pragma once
+
+#include <string>
+
+#include "solver.hpp"
+
+namespace kb2 {
+
+struct MixedOptions {
+  Options amg;                // pairing, sweeps, structure; coarse_bf16 / dense_coarsest / absorb
+  double inner_rel_tol = 1e-3;
+  int inner_max_iter = 300;
+  int max_refinements = 30;
+};
+
+struct MixedStats {
+  int refinements = 0, iterations = 0;
+  bool converged = false;
+  double initial_residual = 0, final_residual = 0;
+};
+
+class MixedSolver {
+ public:
+  MixedSolver(const CsrView& a, const MixedOptions& o);
+  void refresh(const float* val, cudaStream_t s) { inner_.refresh(val, s); }
+  // x: FP64 solution (initial guess in); b: FP32 right-hand side.
+  MixedStats solve(const float* val, double* x, const float* b, const Control& c, cudaStream_t s);
+  std::string describe() const;
+  Solver& inner() { return inner_; }
+
+ private:
+  double residual(const float* val, const double* x, const float* b, cudaStream_t s);
+
+  MixedOptions o_;
+  Solver inner_;
+  int n_;
+  DArray<float> rf_, e_;
+  DArray<double> partials_, norm_;
+  DArray<unsigned> ticket_;
+  Pinned<double> host_{2};
+};
+
+}  // namespace kb2

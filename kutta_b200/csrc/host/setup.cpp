@@ -138,10 +138,11 @@ Coarsening coarsen(const CsrView& fine, std::vector<int> aggregate, bool entry_m
 // passes on the intermediate coarse operator (rebuilt from the fine matrix each
 // time), composing the maps; the final transfer carries the entry map.
 Coarsening aggregate(const CsrView& a, const Options& o) {
-  auto map = pairs(a, o.strength_threshold, true);
+  auto map = pairs(a, o.strength_threshold, true, o.absorb_singletons);
   for (int pass = 1; pass < o.aggregation_passes; ++pass) {
     auto intermediate = coarsen(a, std::move(map), false, o.m_matrix);
-    const auto next = pairs(CsrView::of(intermediate.matrix), o.strength_threshold, false);
+    const auto next = pairs(CsrView::of(intermediate.matrix), o.strength_threshold, false,
+                            o.absorb_singletons);
     map = std::move(intermediate.t.aggregate);
     for (auto& g : map)
       if (g >= 0) g = next[g];
@@ -157,7 +158,8 @@ Coarsening aggregate(const CsrView& a, const Options& o) {
 // unassigned neighbour whose weight is >= threshold * its strongest weight
 // (strict > keeps the lowest column on ties). With exclude_isolated, rows with
 // no nonzero neighbour stay unassigned (-1).
-std::vector<int> pairs(const CsrView& a, double threshold, bool exclude_isolated) {
+std::vector<int> pairs(const CsrView& a, double threshold, bool exclude_isolated,
+                       bool absorb_singletons) {
   const int n = a.n;
   std::vector<int> offsets(static_cast<std::size_t>(n) + 1, 0), sources(a.nnz);
   for (int j = 0; j < a.nnz; ++j) ++offsets[a.col[j] + 1];
@@ -170,10 +172,9 @@ std::vector<int> pairs(const CsrView& a, double threshold, bool exclude_isolated
   std::vector<int> map(n, -1);
   std::vector<int> cand_col;
   std::vector<double> cand_w;
-  int next = 0;
-  for (int i = 0; i < n; ++i) {
-    if (map[i] != -1) continue;
-    // Merge outgoing (row i) and incoming (column i) neighbours in column order.
+  // Merges outgoing (row i) and incoming (column i) neighbours in column order;
+  // returns the strongest weight.
+  auto neighbours = [&](int i) {
     cand_col.clear();
     cand_w.clear();
     int out = a.row_ptr[i], incoming = offsets[i];
@@ -195,6 +196,12 @@ std::vector<int> pairs(const CsrView& a, double threshold, bool exclude_isolated
         strongest = std::max(strongest, weight);
       }
     }
+    return strongest;
+  };
+  int next = 0;
+  for (int i = 0; i < n; ++i) {
+    if (map[i] != -1) continue;
+    const double strongest = neighbours(i);
     if (exclude_isolated && strongest == 0) continue;
     int partner = -1;
     double weight = 0;
@@ -209,6 +216,35 @@ std::vector<int> pairs(const CsrView& a, double threshold, bool exclude_isolated
     if (partner != -1) map[partner] = next;
     ++next;
   }
+  if (!absorb_singletons) return map;
+  // A row left alone joins the pair of its strongest neighbour that belongs to
+  // a pair (rows in row order; aggregates then renumbered in their old order).
+  std::vector<int> size(static_cast<std::size_t>(next), 0);
+  for (int g : map)
+    if (g >= 0) ++size[g];
+  for (int i = 0; i < n; ++i) {
+    if (map[i] < 0 || size[map[i]] != 1) continue;
+    neighbours(i);
+    int best = -1;
+    double weight = 0;
+    for (std::size_t k = 0; k < cand_col.size(); ++k) {
+      const int g = map[cand_col[k]];
+      if (g >= 0 && g != map[i] && size[g] >= 2 && cand_w[k] > weight) {
+        best = g;
+        weight = cand_w[k];
+      }
+    }
+    if (best < 0) continue;
+    size[map[i]] = 0;
+    map[i] = best;
+    ++size[best];
+  }
+  std::vector<int> renumber(static_cast<std::size_t>(next), -1);
+  int kept = 0;
+  for (int g = 0; g < next; ++g)
+    if (size[g] > 0) renumber[g] = kept++;
+  for (auto& g : map)
+    if (g >= 0) g = renumber[g];
   return map;
 }
 

@@ -43,6 +43,14 @@ struct Options {  // AmgOptions, src/kutta/linalg/amg.hpp:8-20
   double strength_threshold = 0.25;
   bool nullspace = false;  // NullSpace::Constant
   bool m_matrix = false;   // OperatorStructure::SymmetricMMatrix
+  // Mixed-precision hierarchy only (no reference counterpart): after each
+  // pairing pass, a row left unpaired joins the pair of its strongest paired
+  // neighbour, so coarsening does not stall on singletons.
+  bool absorb_singletons = false;
+  // Mixed-precision V-cycle: levels >= 1 stored as BF16 x row scales, and the
+  // coarsest level (<= 1024 rows) solved with a dense FP64 inverse.
+  bool coarse_bf16 = false;
+  bool dense_coarsest = false;
 };
 
 // CsrMatrixHost (src/kutta/linalg/csr.hpp:16-28). val holds float-representable
@@ -93,6 +101,7 @@ void check_amg(Kind kind, const CsrView& a, const Options& o);
 Hierarchy build_hierarchy(const CsrView& a, const Options& o);
 
 // Exposed for tests.
-std::vector<int> pairs(const CsrView& a, double threshold, bool exclude_isolated);
+std::vector<int> pairs(const CsrView& a, double threshold, bool exclude_isolated,
+                       bool absorb_singletons = false);
 
 }  // namespace kb2

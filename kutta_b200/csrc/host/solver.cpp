@@ -108,7 +108,43 @@ Solver::Solver(Kind kind, const CsrView& a, const Options& options,
   cuda_check(cudaMemsetAsync(scalars_.get(), 0, 24 * sizeof(float), s), "memset");
   cuda_check(cudaMemsetAsync(status_.get(), 0, 3 * sizeof(int), s), "memset");
   speculate_ = kind_ != Kind::Jacobi && n_ <= kSpeculativeRows;
+  if (amg() && (options_.coarse_bf16 || options_.dense_coarsest)) {
+    for (std::size_t i = 1; i < levels_.size(); ++i) {
+      auto& l = levels_[i];
+      if (options_.coarse_bf16) {
+        l.v16.reset(static_cast<std::size_t>(l.nnz));
+        l.scale.reset(static_cast<std::size_t>(l.n));
+      }
+    }
+    auto& c = levels_.back();
+    if (options_.dense_coarsest && levels_.size() > 1 && c.n <= 1024) {
+      c.dense_lower.reset(static_cast<std::size_t>(c.n) * c.n);
+      c.dense_inverse.reset(static_cast<std::size_t>(c.n) * c.n);
+    }
+    // Usable before the first refresh, from the setup values.
+    prepare_mixed(s, 0);
+    cuda_check(cudaMemcpyAsync(host_values_.get(), values_.get(), sizeof(double),
+                               cudaMemcpyDeviceToHost, s),
+               "setup readback");
+    wait(s);
+    KB2_REQUIRE(host_values_[0] == 0, "mixed: coarsest operator is not SPD");
+  }
   wait(s);
+}
+
+// BF16 copies of the coarse operators and the dense inverse of the coarsest,
+// from the current FP32 coarse values; the dense SPD check lands in values_[0].
+void Solver::prepare_mixed(cudaStream_t s, int slot) {
+  double* error = values_.get() + slot;
+  cuda_check(cudaMemsetAsync(error, 0, sizeof(double), s), "memset");
+  for (std::size_t i = 1; i < levels_.size(); ++i) {
+    auto& l = levels_[i];
+    if (l.v16.allocated())
+      launch::bf16_pack(l.n, l.row_ptr.get(), l.val.get(), l.v16.get(), l.scale.get(), s);
+    if (dense(l))
+      launch::dense_inverse(l.n, l.row_ptr.get(), l.col.get(), l.val.get(), l.dense_lower.get(),
+                            l.dense_inverse.get(), error, s);
+  }
 }
 
 // ---------------------------------------------------------------- primitives --
@@ -208,7 +244,11 @@ void Solver::smooth(DevLevel& l, const int* rows, const int* cols, const float* 
       }
       cuda_check(cudaEventRecord(events_[events_used_++], stream_), "cudaEventRecord");
     }
-    launch::smooth(l.n, rows, cols, vals, x, b, l.l1.get(), l.r, status_.get(), zero, stream_);
+    if (l.v16.allocated())
+      launch::bf16_smooth(l.n, rows, cols, l.v16.get(), l.scale.get(), x, b, l.l1.get(), l.r,
+                          status_.get(), zero, stream_);
+    else
+      launch::smooth(l.n, rows, cols, vals, x, b, l.l1.get(), l.r, status_.get(), zero, stream_);
     if (timed) cuda_check(cudaEventRecord(events_[events_used_++], stream_), "cudaEventRecord");
     tally(zero ? 12.0 * l.n : 8.0 * l.nnz + 4.0 * (l.n + 1) + 16.0 * l.n);
     std::swap(x, l.r);  // ping-pong: the two buffers exchange roles (amg.cpp:280)
@@ -223,7 +263,10 @@ void Solver::cycle(std::size_t index, const float* b, float*& x) {
   const float* vals = index == 0 ? val_ : l.val.get();
   // x is not cleared: every first step below writes it without reading it.
   if (index + 1 == levels_.size()) {
-    if (l.n <= 24) {
+    if (dense(l)) {
+      launch::dense_solve(l.n, l.dense_inverse.get(), b, x, status_.get(), stream_);
+      tally(8.0 * l.n * l.n + 8.0 * l.n);
+    } else if (l.n <= 24) {
       launch::coarse_solve(l.n, rows, cols, vals, x, b, l.l1.get(), status_.get(),
                            options_.coarse_sweeps, stream_);
     } else {
@@ -231,7 +274,11 @@ void Solver::cycle(std::size_t index, const float* b, float*& x) {
     }
   } else {
     smooth(l, rows, cols, vals, b, x, options_.pre_sweeps, true);
-    launch::residual(l.n, rows, cols, vals, x, b, l.r, status_.get(), stream_);
+    if (l.v16.allocated())
+      launch::bf16_residual(l.n, rows, cols, l.v16.get(), l.scale.get(), x, b, l.r,
+                            status_.get(), stream_);
+    else
+      launch::residual(l.n, rows, cols, vals, x, b, l.r, status_.get(), stream_);
     auto& c = levels_[index + 1];
     launch::restrict_(c.n, l.member_offsets.get(), l.members.get(), l.r, c.b.get(),
                       status_.get(), stream_);
@@ -286,8 +333,10 @@ void Solver::refresh(const float* val, cudaStream_t s) {
       matrix = c.val.get();
     }
   }
-  cuda_check(cudaMemcpyAsync(host_values_.get(), values_.get(), sizeof(double) * levels_.size(),
-                             cudaMemcpyDeviceToHost, s),
+  const int slots = static_cast<int>(levels_.size());
+  if (mixed()) prepare_mixed(s, slots);
+  cuda_check(cudaMemcpyAsync(host_values_.get(), values_.get(),
+                             sizeof(double) * (slots + (mixed() ? 1 : 0)), cudaMemcpyDeviceToHost, s),
              "refresh readback");
   wait(s);
   cuda_check(cudaGetLastError(), "refresh");
@@ -296,6 +345,7 @@ void Solver::refresh(const float* val, cudaStream_t s) {
     KB2_REQUIRE(invalid != 3, "AMG: requires positive diagonals");
     KB2_REQUIRE(invalid <= allowed[i], "AMG: invalid values or zero diagonal");
   }
+  if (mixed()) KB2_REQUIRE(host_values_[slots] == 0, "mixed: coarsest operator is not SPD");
 }
 
 // --------------------------------------------------------------------- Krylov --
@@ -544,12 +594,18 @@ std::string Solver::describe() const {
                                 : "BiCGStab");
   std::ostringstream out;
   out << name << ", ";
-  if (amg())
+  if (amg()) {
     out << "aggregation AMG " << (options_.cycle == Cycle::K ? 'K' : 'V') << "-cycle, "
         << levels_.size() << " levels, op complexity " << std::fixed << std::setprecision(3)
         << complexity_;
-  else
+    if (mixed())
+      out << " (V(" << options_.pre_sweeps << "," << options_.post_sweeps << ")"
+          << (options_.absorb_singletons ? ", singletons absorbed" : "")
+          << (options_.coarse_bf16 ? ", BF16 coarse levels" : "")
+          << (dense(levels_.back()) ? ", dense FP64 coarsest" : "") << ")";
+  } else {
     out << "Jacobi";
+  }
   if (nullspace_) out << ", constant-nullspace projection";
   return out.str();
 }

@@ -58,6 +58,10 @@ struct DevLevel {
   float* x = nullptr;
   float* r = nullptr;
   DArray<float> projection;     // constant-nullspace sum pair
+  // Mixed precision: BF16 operator with row scales; dense FP64 inverse.
+  DArray<unsigned short> v16;
+  DArray<float> scale;
+  DArray<double> dense_lower, dense_inverse;
   // transfer to level + 1
   DArray<int> aggregate, member_offsets, members, entry_offsets, entries;
 };
@@ -74,7 +78,13 @@ class Solver {
   Solver(Kind kind, const CsrView& a, const Options& options, std::shared_ptr<Workspace> workspace);
   ~Solver();
   void set_profile(bool on);
-  Profile profile() const { return prof_; }
+  Profile profile() const {
+    Profile p = prof_;
+    p.launches = launch::counter.load() - launch_mark_;
+    return p;
+  }
+  // Bytes of kernels a wrapping driver launched (the FP64 refinement).
+  void add_bytes(double bytes) { tally(bytes); }
   void refresh(const float* val, cudaStream_t s);
   Stats solve(const float* val, float* x, const float* b, const Control& c, cudaStream_t s);
   std::string describe() const;
@@ -88,7 +98,12 @@ class Solver {
  private:
   bool amg() const { return kind_ == Kind::AmgPcg || kind_ == Kind::AmgBicgstab; }
   bool bicg() const { return kind_ == Kind::BicgstabJacobi || kind_ == Kind::AmgBicgstab; }
-  bool variable() const { return amg() && options_.cycle == Cycle::K; }
+  // A variable preconditioner needs the flexible beta (solver.cpp:296-298): the
+  // K-cycle, and the mixed V-cycle (BF16 rounding breaks exact symmetry).
+  bool variable() const { return amg() && (options_.cycle == Cycle::K || options_.coarse_bf16); }
+  bool dense(const DevLevel& l) const { return l.dense_inverse.allocated(); }
+  void prepare_mixed(cudaStream_t s, int error_slot);
+  bool mixed() const { return options_.coarse_bf16 || options_.dense_coarsest; }
   const int* rows0() const { return levels_[0].row_ptr.get(); }
   const int* cols0() const { return levels_[0].col.get(); }
 

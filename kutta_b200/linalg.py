@@ -171,6 +171,16 @@ _SIGNATURES = {
     "b2_hierarchy_level_shape": (_I, [_P, _I, _P, _P]),
     "b2_hierarchy_level_copy": (_I, [_P, _I, _P, _P, _P, _P, _P]),
     "b2_hierarchy_free": (None, [_P]),
+    "b2_mixed_options_default": (None, [_P]),
+    "b2_mixed_create": (_I, [_I, _I, _P, _P, _P, _P, _P, _P]),
+    "b2_mixed_refresh": (_I, [_P, _P, _P]),
+    "b2_mixed_solve": (_I, [_P, _P, _P, _P, _P, _P, _P]),
+    "b2_mixed_describe": (ctypes.c_size_t, [_P, ctypes.c_char_p, ctypes.c_size_t]),
+    "b2_mixed_destroy": (None, [_P]),
+    "b2_mixed_hierarchy_build": (_I, [_I, _I, _P, _P, _P, _P, _P, _P]),
+    "b2_dense_inverse": (_I, [_I, _P, _P, _P, _P, _P, _P]),
+    "b2_mixed_profile": (_I, [_P, _I]),
+    "b2_mixed_profile_read": (_I, [_P, _P]),
 }
 
 _lib = None
@@ -408,6 +418,144 @@ def residual(a: CsrMatrix, x, b, r) -> None:
         raise KuttaError("CSR: residual RHS size or alias mismatch")
     _check(_load().b2_csr_residual(a.n_rows, a.nnz, _tptr(a.row_ptr), _tptr(a.col), _tptr(a.val),
                                    _tptr(x), _tptr(b), _tptr(r), _stream()))
+
+
+@dataclasses.dataclass
+class MixedOptions:
+    """b2_mixed_options: the mixed-precision solve (no reference counterpart)."""
+    amg: AmgOptions = dataclasses.field(default_factory=lambda: AmgOptions(
+        pre_sweeps=2, post_sweeps=2, structure=OperatorStructure.SymmetricMMatrix))
+    absorb_singletons: bool = True
+    dense_rows: int = 512
+    coarse_bf16: bool = True
+    inner_rel_tol: float = 1e-3
+    inner_max_iter: int = 300
+    max_refinements: int = 30
+
+
+@dataclasses.dataclass
+class MixedStats:
+    refinements: int = 0
+    iterations: int = 0
+    converged: bool = False
+    initial_residual: float = 0.0
+    final_residual: float = 0.0
+
+
+class _MixedOptions(ctypes.Structure):
+    _fields_ = [("amg", _Options), ("absorb_singletons", ctypes.c_int),
+                ("dense_rows", ctypes.c_int), ("coarse_bf16", ctypes.c_int),
+                ("inner_rel_tol", ctypes.c_double), ("inner_max_iter", ctypes.c_int),
+                ("max_refinements", ctypes.c_int)]
+
+
+class _MixedStats(ctypes.Structure):
+    _fields_ = [("refinements", ctypes.c_int), ("iterations", ctypes.c_int),
+                ("converged", ctypes.c_int), ("initial_residual", ctypes.c_double),
+                ("final_residual", ctypes.c_double)]
+
+
+def _mixed_struct(o: MixedOptions) -> _MixedOptions:
+    s = _MixedOptions()
+    _load().b2_mixed_options_default(ctypes.byref(s))
+    s.amg = _options_struct(o.amg, True)
+    s.absorb_singletons, s.dense_rows, s.coarse_bf16 = int(o.absorb_singletons), o.dense_rows, int(o.coarse_bf16)
+    s.inner_rel_tol, s.inner_max_iter, s.max_refinements = o.inner_rel_tol, o.inner_max_iter, o.max_refinements
+    return s
+
+
+class MixedSolver:
+    """FP64 iterative refinement around the FP32 AMG-PCG with BF16 coarse
+    levels and a dense FP64 coarsest solve; the solution is FP64."""
+
+    def __init__(self, a, options: MixedOptions | None = None):
+        lib = _load()
+        h = _host(a)
+        row_ptr, col, diag, val = h.arrays()
+        opts = _mixed_struct(options or MixedOptions())
+        handle = ctypes.c_void_p()
+        _check(lib.b2_mixed_create(h.n_rows, h.nnz, _ptr(row_ptr), _ptr(col), _ptr(diag), _ptr(val),
+                                   ctypes.byref(opts), ctypes.byref(handle)))
+        self._handle = handle
+        self.n_rows, self.nnz = h.n_rows, h.nnz
+
+    def refresh(self, a: CsrMatrix) -> None:
+        _check(_load().b2_mixed_refresh(self._handle, _tptr(a.val), _stream()))
+
+    def solve(self, a: CsrMatrix, x64, b, control: SolveControl | None = None) -> MixedStats:
+        """x64: float64 CUDA tensor (initial guess in, solution out); b: float32."""
+        import torch
+        if x64.dtype != torch.float64 or x64.numel() != self.n_rows or b.numel() != self.n_rows:
+            raise KuttaError("solve: vector size or alias mismatch")
+        control = control or SolveControl()
+        c = _Control(control.rel_tol, control.abs_tol, control.max_iter,
+                     control.residual_check_interval)
+        st = _MixedStats()
+        _check(_load().b2_mixed_solve(self._handle, _tptr(a.val), _tptr(x64), _tptr(b),
+                                      ctypes.byref(c), ctypes.byref(st), _stream()))
+        return MixedStats(st.refinements, st.iterations, bool(st.converged), st.initial_residual,
+                          st.final_residual)
+
+    def describe(self) -> str:
+        buf = ctypes.create_string_buffer(512)
+        _load().b2_mixed_describe(self._handle, buf, 512)
+        return buf.value.decode()
+
+    def profile(self, enable: bool) -> None:
+        _check(_load().b2_mixed_profile(self._handle, int(enable)))
+
+    def profile_read(self) -> dict:
+        p = _Profile()
+        _check(_load().b2_mixed_profile_read(self._handle, ctypes.byref(p)))
+        return {f: getattr(p, f) for f, _ in _Profile._fields_}
+
+    def __del__(self):
+        if getattr(self, "_handle", None) and _lib is not None:
+            _lib.b2_mixed_destroy(self._handle)
+            self._handle = None
+
+
+def dense_inverse(a: CsrMatrix, inverse, not_spd) -> None:
+    """Dense FP64 Cholesky inverse of a small SPD CSR operator (n <= 1024):
+    inverse (n*n float64 CUDA tensor, row-major) and not_spd (1 float64 flag)."""
+    _check(_load().b2_dense_inverse(a.n_rows, _tptr(a.row_ptr), _tptr(a.col), _tptr(a.val),
+                                    _tptr(inverse), _tptr(not_spd), _stream()))
+
+
+def make_mixed_solver(a, options: MixedOptions | None = None) -> MixedSolver:
+    return MixedSolver(a, options)
+
+
+def build_mixed_hierarchy(a, options: MixedOptions | None = None) -> list:
+    """The mixed solve's host hierarchy (no GPU)."""
+    lib = _load()
+    h = _host(a)
+    row_ptr, col, diag, val = h.arrays()
+    opts = _mixed_struct(options or MixedOptions())
+    handle = ctypes.c_void_p()
+    _check(lib.b2_mixed_hierarchy_build(h.n_rows, h.nnz, _ptr(row_ptr), _ptr(col), _ptr(diag),
+                                        _ptr(val), ctypes.byref(opts), ctypes.byref(handle)))
+    return _read_hierarchy(lib, handle)
+
+
+def _read_hierarchy(lib, handle) -> list:
+    out = []
+    try:
+        count = lib.b2_hierarchy_levels(handle)
+        for lv in range(count):
+            n, nnz = ctypes.c_int(), ctypes.c_int()
+            _check(lib.b2_hierarchy_level_shape(handle, lv, ctypes.byref(n), ctypes.byref(nnz)))
+            rp = np.zeros(n.value + 1, np.int32)
+            cl = np.zeros(nnz.value, np.int32)
+            vl = np.zeros(nnz.value, np.float32)
+            l1 = np.zeros(n.value, np.float32)
+            ag = np.zeros(n.value, np.int32) if lv + 1 < count else None
+            _check(lib.b2_hierarchy_level_copy(handle, lv, _ptr(rp), _ptr(cl), _ptr(vl), _ptr(l1),
+                                               _ptr(ag) if ag is not None else None))
+            out.append(HostLevel(n.value, rp, cl, vl, l1, ag))
+    finally:
+        lib.b2_hierarchy_free(handle)
+    return out
 
 
 @dataclasses.dataclass

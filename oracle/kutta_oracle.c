@@ -327,7 +327,7 @@ static int find_entry(const hcsr* a, int row, int column) { /* lower_bound */
 }
 
 /* pairs(), src/kutta/linalg/amg.cpp:25-75. */
-static int* pairs(const hcsr* a, double threshold, int exclude_isolated) {
+static int* pairs(const hcsr* a, double threshold, int exclude_isolated, int absorb) {
   int n = a->n;
   int* offsets = xcalloc((size_t)n + 1, sizeof(int));
   int* sources = xmalloc(sizeof(int) * (size_t)a->nnz);
@@ -373,6 +373,44 @@ static int* pairs(const hcsr* a, double threshold, int exclude_isolated) {
     map[i] = next;
     if (partner != -1) map[partner] = next;
     ++next;
+  }
+  if (absorb) {
+    /* Mixed-precision hierarchy (kutta_b200's own method, no reference
+     * counterpart): an unpaired row joins the pair of its strongest neighbour
+     * that belongs to a pair; rows in order, aggregates renumbered in order. */
+    int* size = xcalloc((size_t)(next > 0 ? next : 1), sizeof(int));
+    for (int i = 0; i < n; ++i) if (map[i] >= 0) ++size[map[i]];
+    for (int i = 0; i < n; ++i) {
+      if (map[i] < 0 || size[map[i]] != 1) continue;
+      int best = -1;
+      double bw = 0;
+      int out = a->row_ptr[i], in = offsets[i];
+      while (out < a->row_ptr[i + 1] || in < offsets[i + 1]) {
+        int oc = out < a->row_ptr[i + 1] ? a->col[out] : n;
+        int ic = in < offsets[i + 1] ? sources[in] : n;
+        int column = oc < ic ? oc : ic;
+        double w = 0;
+        if (oc == column) w = fabs(a->val[out++]);
+        if (ic == column) {
+          double t = fabs(a->val[find_entry(a, column, i)]);
+          w = w > t ? w : t;
+          ++in;
+        }
+        if (column != i && w != 0) {
+          int g = map[column];
+          if (g >= 0 && g != map[i] && size[g] >= 2 && w > bw) { best = g; bw = w; }
+        }
+      }
+      if (best < 0) continue;
+      size[map[i]] = 0;
+      map[i] = best;
+      ++size[best];
+    }
+    int* renumber = xmalloc(sizeof(int) * (size_t)(next > 0 ? next : 1));
+    int kept = 0;
+    for (int g = 0; g < next; ++g) renumber[g] = size[g] > 0 ? kept++ : -1;
+    for (int i = 0; i < n; ++i) if (map[i] >= 0) map[i] = renumber[map[i]];
+    free(size); free(renumber);
   }
   free(offsets); free(sources);
   return map;
@@ -477,11 +515,11 @@ static void coarsen(const hcsr* fine, int* aggregate, int entry_map, int m_matri
 
 /* aggregate(), amg.cpp:160-174. */
 static void aggregate_level(const hcsr* a, const ko_options* o, hcsr* cm, transfer* t) {
-  int* map = pairs(a, o->threshold, 1);
+  int* map = pairs(a, o->threshold, 1, o->absorb);
   for (int pass = 1; pass < o->passes; ++pass) {
     hcsr im; transfer it;
     coarsen(a, map, 0, o->m_matrix, &im, &it);
-    int* next = pairs(&im, o->threshold, 0);
+    int* next = pairs(&im, o->threshold, 0, o->absorb);
     map = it.aggregate;
     it.aggregate = NULL;
     for (int i = 0; i < a->n; ++i) if (map[i] >= 0) map[i] = next[map[i]];

@@ -21,6 +21,7 @@ typedef struct {
   double threshold;
   int nullspace;     /* 1: constant nullspace */
   int m_matrix;      /* 1: SymmetricMMatrix */
+  int absorb;        /* 1: singleton absorption (the mixed solve's hierarchy) */
 } ko_options;
 
 typedef struct { double rel_tol, abs_tol; int max_iter, interval; } ko_control;

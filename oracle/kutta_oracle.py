@@ -25,7 +25,7 @@ class Options(ctypes.Structure):
                 ("coarse_sweeps", ctypes.c_int), ("coarse_rows", ctypes.c_int),
                 ("max_levels", ctypes.c_int), ("passes", ctypes.c_int),
                 ("threshold", ctypes.c_double), ("nullspace", ctypes.c_int),
-                ("m_matrix", ctypes.c_int)]
+                ("m_matrix", ctypes.c_int), ("absorb", ctypes.c_int)]
 
 
 class Control(ctypes.Structure):
@@ -103,9 +103,10 @@ class OracleNonfinite(OracleError):
 
 
 def options(kind=AMG_PCG, *, pre_sweeps=5, post_sweeps=5, coarse_sweeps=32, coarse_rows=24,
-            max_levels=24, passes=3, threshold=0.25, nullspace=False, m_matrix=False) -> Options:
+            max_levels=24, passes=3, threshold=0.25, nullspace=False, m_matrix=False,
+            absorb=False) -> Options:
     return Options(kind, 0, pre_sweeps, post_sweeps, coarse_sweeps, coarse_rows, max_levels,
-                   passes, threshold, int(nullspace), int(m_matrix))
+                   passes, threshold, int(nullspace), int(m_matrix), int(absorb))
 
 
 class Solver:

@@ -1,0 +1,162 @@
+"""The mixed-precision solve (no reference counterpart).
+
+CPU: its hierarchy (pairing with singleton absorption) equals the oracle's
+restatement bit for bit and reaches the dense size where the reference's
+pairing stalls. GPU: it converges below the FP32 rounding floor, judged by the
+FP64 true residual of the returned FP64 solution and by the error against the
+FP64 CG oracle."""
+import numpy as np
+import pytest
+
+from kutta_b200 import harness
+from kutta_b200 import linalg as L
+from oracle import kutta_oracle as O
+
+
+def _oracle_levels(s, dense_rows=512):
+    o = O.Solver(s, O.options(O.AMG_PCG, pre_sweeps=2, post_sweeps=2, coarse_rows=dense_rows,
+                              m_matrix=True, absorb=True))
+    return o.levels()
+
+
+@pytest.mark.parametrize("seed,tet", [(1, True), (2, False)])
+def test_mixed_hierarchy_matches_oracle(seed, tet):
+    s = harness.box_system(20, 20, 20, tet=tet, seed=seed)
+    mine = L.build_mixed_hierarchy(s)
+    theirs = _oracle_levels(s)
+    assert [m.n for m in mine] == [t["n"] for t in theirs]
+    assert mine[-1].n <= 512
+    for i, (m, t) in enumerate(zip(mine, theirs)):
+        assert np.array_equal(m.row_ptr, t["row_ptr"]) and np.array_equal(m.col, t["col"])
+        if i > 0:
+            assert np.array_equal(m.val.view(np.uint32), t["val"].view(np.uint32))
+        assert np.array_equal(m.inverse_l1.view(np.uint32), t["l1"].view(np.uint32))
+        if t["aggregate"] is not None:
+            assert np.array_equal(m.aggregate, t["aggregate"])
+
+
+def test_absorption_removes_the_stall():
+    """The reference's pairing stops coarsening at a large level on random
+    coefficients; absorption keeps coarsening down to the dense size."""
+    s = harness.box_system(24, 24, 24, tet=True, seed=3)
+    plain = L.build_hierarchy(s, L.AmgOptions(structure=L.OperatorStructure.SymmetricMMatrix,
+                                              coarse_rows=512))
+    mixed = L.build_mixed_hierarchy(s)
+    assert plain[-1].n > 2000
+    assert mixed[-1].n <= 512
+    assert sum(lv.row_ptr[-1] for lv in mixed) < sum(lv.row_ptr[-1] for lv in plain)
+
+
+def _fp64_true(s, x64, b):
+    import scipy.sparse as sp
+    A = sp.csr_matrix((s.val, s.col, s.row_ptr), shape=(s.n, s.n))
+    return float(np.linalg.norm(b.astype(np.float64) - A @ x64))
+
+
+CASES = [
+    ("hex20", lambda: harness.box_system(20, 20, 20, tet=False, seed=5), 1e-6),
+    ("tet16", lambda: harness.box_system(16, 16, 16, tet=True, seed=6), 1e-6),
+    ("tet16_graded_1e-8", lambda: harness.box_system(16, 16, 16, tet=True, seed=7, band_layers=6,
+                                                     dmin=1e-6, dmax=1.0), 1e-8),
+]
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name,make,tol", CASES, ids=[c[0] for c in CASES])
+def test_mixed_converges_below_fp32_floor(cuda, name, make, tol):
+    import torch
+    s = make()
+    solver = L.make_mixed_solver(s)
+    a = L.upload(s)
+    solver.refresh(a)
+    b = torch.from_numpy(s.b).cuda()
+    x = torch.zeros(s.n, dtype=torch.float64, device="cuda")
+    st = solver.solve(a, x, b, L.SolveControl(tol, 1e-30, 3000))
+    torch.cuda.synchronize()
+    xr = x.cpu().numpy()
+    true = _fp64_true(s, xr, s.b)
+    assert st.converged, st
+    assert true <= tol * st.initial_residual * 1.0001
+    assert true == pytest.approx(st.final_residual, rel=1e-3)
+    x64, _ = O.cg64(s, rel_tol=1e-14)
+    err = np.linalg.norm(xr - x64) / np.linalg.norm(x64)
+    # A float32 x cannot reach this residual: the rounded exact solution sits above it.
+    floor = _fp64_true(s, x64.astype(np.float32).astype(np.float64), s.b) / st.initial_residual
+    print(f"{name}: refinements={st.refinements} inner iterations={st.iterations} "
+          f"rel={true / st.initial_residual:.2e} |x-x64|/|x64|={err:.2e} fp32 floor={floor:.2e}")
+    assert err < 1e-3
+
+
+@pytest.mark.gpu
+def test_mixed_refresh_tracks_new_values(cuda):
+    """After a value change and refresh the solve meets the tolerance for the
+    new matrix (BF16 copies and the dense inverse are rebuilt)."""
+    import torch
+    s = harness.box_system(14, 14, 14, tet=True, seed=8)
+    solver = L.make_mixed_solver(s)
+    a = L.upload(s)
+    scaled = s.val * 1.5
+    scaled[s.diag] += 0.01 * np.abs(s.val[s.diag])
+    a.val.copy_(torch.from_numpy(scaled.astype(np.float32)))
+    solver.refresh(a)
+    b = torch.from_numpy(s.b).cuda()
+    x = torch.zeros(s.n, dtype=torch.float64, device="cuda")
+    st = solver.solve(a, x, b, L.SolveControl(1e-7, 1e-30, 2000))
+    t = harness.HostSystem(s.row_ptr, s.col, s.diag, scaled.astype(np.float32).astype(np.float64), s.b)
+    assert st.converged
+    assert _fp64_true(t, x.cpu().numpy(), s.b) <= 1e-7 * st.initial_residual * 1.0001
+
+
+def _coarsest(n_side=6, seed=4):
+    s = harness.box_system(n_side, n_side, n_side, tet=True, seed=seed)
+    return s
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("n_side", [3, 4, 5])
+def test_dense_inverse_matches_fp64(cuda, n_side):
+    """The coarsest-level dense FP64 Cholesky inverse against numpy in FP64."""
+    import torch
+    s = _coarsest(n_side)
+    n = s.n
+    assert n <= 1024
+    a = L.upload(s)
+    inv = torch.empty(n * n, dtype=torch.float64, device="cuda")
+    flag = torch.full((1,), 7.0, dtype=torch.float64, device="cuda")
+    L.dense_inverse(a, inv, flag)
+    torch.cuda.synchronize()
+    assert flag.item() == 0.0
+    dense = np.zeros((n, n))
+    for i in range(n):
+        for j in range(s.row_ptr[i], s.row_ptr[i + 1]):
+            dense[i, s.col[j]] = np.float32(s.val[j])
+    got = inv.cpu().numpy().reshape(n, n)
+    want = np.linalg.inv(dense)
+    assert np.max(np.abs(got - want)) <= 1e-9 * np.max(np.abs(want))
+
+
+@pytest.mark.gpu
+def test_dense_inverse_flags_non_spd(cuda):
+    import torch
+    s = _coarsest(3)
+    bad = s.val.copy()
+    bad[s.diag[0]] = -1.0
+    a = L.upload(harness.HostSystem(s.row_ptr, s.col, s.diag, bad, s.b))
+    inv = torch.empty(s.n * s.n, dtype=torch.float64, device="cuda")
+    flag = torch.zeros(1, dtype=torch.float64, device="cuda")
+    L.dense_inverse(a, inv, flag)
+    torch.cuda.synchronize()
+    assert flag.item() == 1.0
+
+
+@pytest.mark.gpu
+def test_mixed_rejects_nonfinite_rhs(cuda):
+    import torch
+    s = harness.box_system(6, 6, 6, tet=True, seed=1)
+    solver = L.make_mixed_solver(s)
+    a = L.upload(s)
+    b = torch.from_numpy(s.b).cuda()
+    b[3] = float("nan")
+    x = torch.zeros(s.n, dtype=torch.float64, device="cuda")
+    with pytest.raises(L.NonfiniteError):
+        solver.solve(a, x, b)
