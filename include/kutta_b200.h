@@ -203,6 +203,21 @@ void b2_mixed_destroy(b2_mixed* solver);
 int b2_dense_inverse(int n, const int32_t* d_row_ptr, const int32_t* d_col, const float* d_val,
                      double* d_inverse, double* d_not_spd, void* stream);
 
+/* b2_dense_inverse for callers that cannot allocate device memory (no
+ * counterpart in the reference): hosts that give the solver a fixed device
+ * memory budget, real-time loops that must not take the allocator's locks or
+ * risk running out of memory mid-step, and work queued while another
+ * component records the stream. The same computation, with the n*n factor
+ * scratch taken from a 2 MiB array built into the library (so n <= 512; larger
+ * n is rejected with B2_INVALID_ARGUMENT). It calls no allocator. The array is
+ * shared by all calls on a device: calls that overlap on the GPU race, so the
+ * caller orders them. The first call on each device looks the array's address
+ * up (and may load the library's device code); make it before any stream
+ * capture. */
+int b2_dense_inverse_noalloc(int n, const int32_t* d_row_ptr, const int32_t* d_col,
+                             const float* d_val, double* d_inverse, double* d_not_spd,
+                             void* stream);
+
 /* As b2_solver_profile / _read, for the inner solve plus the FP64 refinement. */
 int b2_mixed_profile(b2_mixed* solver, int enable);
 int b2_mixed_profile_read(b2_mixed* solver, b2_profile* out);

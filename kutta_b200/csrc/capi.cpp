@@ -95,6 +95,12 @@ kb2::CsrView view(int n, int nnz, const int32_t* row_ptr, const int32_t* col, co
 cudaStream_t as_stream(void* s) { return static_cast<cudaStream_t>(s); }
 }  // namespace
 
+namespace kb2 {
+// Sets the text b2_last_error() returns, for entry points defined in other
+// translation units.
+int report_error(int code, const char* message) { return fail(code, message); }
+}  // namespace kb2
+
 extern "C" {
 
 void b2_options_default(b2_options* o) {

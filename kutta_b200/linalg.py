@@ -179,6 +179,7 @@ _SIGNATURES = {
     "b2_mixed_destroy": (None, [_P]),
     "b2_mixed_hierarchy_build": (_I, [_I, _I, _P, _P, _P, _P, _P, _P]),
     "b2_dense_inverse": (_I, [_I, _P, _P, _P, _P, _P, _P]),
+    "b2_dense_inverse_noalloc": (_I, [_I, _P, _P, _P, _P, _P, _P]),
     "b2_mixed_profile": (_I, [_P, _I]),
     "b2_mixed_profile_read": (_I, [_P, _P]),
 }
@@ -520,6 +521,16 @@ def dense_inverse(a: CsrMatrix, inverse, not_spd) -> None:
     inverse (n*n float64 CUDA tensor, row-major) and not_spd (1 float64 flag)."""
     _check(_load().b2_dense_inverse(a.n_rows, _tptr(a.row_ptr), _tptr(a.col), _tptr(a.val),
                                     _tptr(inverse), _tptr(not_spd), _stream()))
+
+
+def dense_inverse_noalloc(a: CsrMatrix, inverse, not_spd) -> None:
+    """dense_inverse for callers that cannot allocate device memory (n <= 512):
+    the factor scratch is a 2 MiB array built into the library, shared by every
+    call on the device, so calls that overlap on the GPU race. The first call on
+    a device looks that array up; make it before any stream capture."""
+    _check(_load().b2_dense_inverse_noalloc(a.n_rows, _tptr(a.row_ptr), _tptr(a.col),
+                                            _tptr(a.val), _tptr(inverse), _tptr(not_spd),
+                                            _stream()))
 
 
 def make_mixed_solver(a, options: MixedOptions | None = None) -> MixedSolver:
