@@ -465,6 +465,56 @@ __global__ void k_project(int n, float* __restrict__ x, const float* __restrict_
   ROWS(i, n) x[i] -= mean;
 }
 
+// ---- K-cycle inner corrections (scalars.kern.h:154-186) ------------------------
+// Per-level scalars: [0] p.q (q.q for GCR), [2] b.p / t.p (b.q / t.q), [4] t.t or
+// z.q, [6] b.b, [8] alpha, [10] beta. The level's status: 0 running, 1 keep the
+// accepted first correction, 2 fall back to the plain first cycle.
+__global__ void k_inner_alpha(float* scalars, int* status, const int* parent, int first) {
+  if (first != 0) status[0] = parent[0] == 0 ? 0 : 2;
+  if (status[0] != 0) return;
+  const Pair denom = kp_load(scalars, 0);
+  const Pair alpha = kp_div(kp_load(scalars, 2), denom);
+  if (!kp_positive(denom) || !kp_coefficient(alpha) ||
+      (kp_zero(alpha) && !kp_zero(kp_load(scalars, 2))))
+    status[0] = first != 0 ? 2 : 1;
+  else
+    kp_store(scalars, 8, alpha);
+}
+
+__global__ void k_inner_first(int n, const float* __restrict__ b, const float* __restrict__ p,
+                              const float* __restrict__ q, float* __restrict__ x,
+                              float* __restrict__ t, const float* __restrict__ scalars,
+                              const int* __restrict__ status) {
+  const bool running = status[0] == 0;
+  const float alpha = kp_float(kp_load(scalars, 8));
+  ROWS(i, n) {
+    x[i] = running ? alpha * p[i] : p[i];
+    t[i] = running ? b[i] - alpha * q[i] : 0.0f;
+  }
+}
+
+// Adaptive exit: keep the first correction when |t|^2 <= |b|^2 / 16.
+__global__ void k_inner_check(const float* scalars, int* status) {
+  if (status[0] != 0) return;
+  if (kp_le(kp_load(scalars, 4), kp_mul(kp(0.0625f, 0.0f), kp_load(scalars, 6)))) status[0] = 1;
+}
+
+__global__ void k_inner_beta(float* scalars, int* status) {
+  if (status[0] != 0) return;
+  const Pair beta = kp_div(kp_neg(kp_load(scalars, 4)), kp_load(scalars, 0));
+  if (!kp_coefficient(beta) || (kp_zero(beta) && !kp_zero(kp_load(scalars, 4))))
+    status[0] = 1;
+  else
+    kp_store(scalars, 10, beta);
+}
+
+__global__ void k_inner_step(int n, float* __restrict__ x, const float* __restrict__ p,
+                             const float* __restrict__ scalars, const int* __restrict__ status) {
+  if (status[0] != 0) return;
+  const float alpha = kp_float(kp_load(scalars, 8));
+  ROWS(i, n) x[i] += alpha * p[i];
+}
+
 inline int blocks(int n) { return grid_for(n); }
 // Kernels without a reduction: one row per thread below ~2M rows, where that
 // measured fastest; above, the 1184-block grid-stride form measured faster
@@ -616,6 +666,30 @@ void project(int n, float* x, const float* sum, float count_hi, float count_lo, 
   if (n <= 0) return;
   ++counter;
   k_project<<<blocks(n), kBlock, 0, s>>>(n, x, sum, count_hi, count_lo);
+}
+void inner_alpha(float* scalars, int* status, const int* parent, int first, cudaStream_t s) {
+  ++counter;
+  k_inner_alpha<<<1, 1, 0, s>>>(scalars, status, parent, first);
+}
+void inner_first(int n, const float* b, const float* p, const float* q, float* x, float* t,
+                 const float* scalars, const int* status, cudaStream_t s) {
+  if (n <= 0) return;
+  ++counter;
+  k_inner_first<<<blocks(n), kBlock, 0, s>>>(n, b, p, q, x, t, scalars, status);
+}
+void inner_check(const float* scalars, int* status, cudaStream_t s) {
+  ++counter;
+  k_inner_check<<<1, 1, 0, s>>>(scalars, status);
+}
+void inner_beta(float* scalars, int* status, cudaStream_t s) {
+  ++counter;
+  k_inner_beta<<<1, 1, 0, s>>>(scalars, status);
+}
+void inner_step(int n, float* x, const float* p, const float* scalars, const int* status,
+                cudaStream_t s) {
+  if (n <= 0) return;
+  ++counter;
+  k_inner_step<<<blocks(n), kBlock, 0, s>>>(n, x, p, scalars, status);
 }
 
 }  // namespace launch

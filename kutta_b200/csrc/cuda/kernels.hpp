@@ -136,5 +136,19 @@ void solver_reset(float* scalars, int* status, int iterations, cudaStream_t s);
 // x -= mean(x) using the pair sum at sum[0..1] (solver_project).
 void project(int n, float* x, const float* sum, float count_hi, float count_lo, cudaStream_t s);
 
+// ---- K-cycle inner corrections (amg_inner_*, scalars.kern.h:154-186) --------
+// alpha = scalars[2] / scalars[0] -> scalars[8]; first != 0 also restarts the
+// level status from the parent's.
+void inner_alpha(float* scalars, int* status, const int* parent, int first, cudaStream_t s);
+// x = alpha p, t = b - alpha q (running) or x = p, t = 0 (fallback).
+void inner_first(int n, const float* b, const float* p, const float* q, float* x, float* t,
+                 const float* scalars, const int* status, cudaStream_t s);
+void inner_check(const float* scalars, int* status, cudaStream_t s);
+// beta = -scalars[4] / scalars[0] -> scalars[10].
+void inner_beta(float* scalars, int* status, cudaStream_t s);
+// x += alpha p.
+void inner_step(int n, float* x, const float* p, const float* scalars, const int* status,
+                cudaStream_t s);
+
 }  // namespace launch
 }  // namespace kb2

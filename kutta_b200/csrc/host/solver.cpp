@@ -79,6 +79,23 @@ Solver::Solver(Kind kind, const CsrView& a, const Options& options,
         l.entries.upload(t.entries, s);
       }
     }
+    // K-cycle work vectors on the levels reached through inner() (Level ctor,
+    // amg.cpp:179-195): every coarse level but the coarsest.
+    if (options_.cycle == Cycle::K) {
+      for (std::size_t i = 1; i + 1 < levels_.size(); ++i) {
+        auto& l = levels_[i];
+        const auto rows = static_cast<std::size_t>(l.n);
+        l.za.reset(rows);
+        l.p.reset(rows);
+        l.q.reset(rows);
+        l.t.reset(rows);
+        l.scalars.reset(12);
+        l.status.reset(1);
+        l.z = l.za.get();
+        cuda_check(cudaMemsetAsync(l.scalars.get(), 0, 12 * sizeof(float), s), "memset");
+        cuda_check(cudaMemsetAsync(l.status.get(), 0, sizeof(int), s), "memset");
+      }
+    }
   } else {
     // Jacobi preconditioner (solver.cpp:56-73).
     jacobi_inverse_.upload(diagonal_values(a, false, false), s);
@@ -229,7 +246,7 @@ void Solver::reset(int iterations) { launch::solver_reset(scalars_.get(), status
 
 // ------------------------------------------------------------ preconditioner --
 void Solver::smooth(DevLevel& l, const int* rows, const int* cols, const float* vals,
-                    const float* b, float*& x, int sweeps, bool zero_start) {
+                    const float* b, float*& x, int sweeps, bool zero_start, const int* status) {
   const bool fine = &l == &levels_[0];
   for (int sweep = 0; sweep < sweeps; ++sweep) {
     const bool zero = zero_start && sweep == 0;
@@ -246,9 +263,9 @@ void Solver::smooth(DevLevel& l, const int* rows, const int* cols, const float* 
     }
     if (l.v16.allocated())
       launch::bf16_smooth(l.n, rows, cols, l.v16.get(), l.scale.get(), x, b, l.l1.get(), l.r,
-                          status_.get(), zero, stream_);
+                          status, zero, stream_);
     else
-      launch::smooth(l.n, rows, cols, vals, x, b, l.l1.get(), l.r, status_.get(), zero, stream_);
+      launch::smooth(l.n, rows, cols, vals, x, b, l.l1.get(), l.r, status, zero, stream_);
     if (timed) cuda_check(cudaEventRecord(events_[events_used_++], stream_), "cudaEventRecord");
     tally(zero ? 12.0 * l.n : 8.0 * l.nnz + 4.0 * (l.n + 1) + 16.0 * l.n);
     std::swap(x, l.r);  // ping-pong: the two buffers exchange roles (amg.cpp:280)
@@ -256,46 +273,101 @@ void Solver::smooth(DevLevel& l, const int* rows, const int* cols, const float* 
 }
 
 // Aggregation::cycle, amg.cpp:283-310.
-void Solver::cycle(std::size_t index, const float* b, float*& x) {
+void Solver::cycle(std::size_t index, const float* b, float*& x, const int* status) {
   auto& l = levels_[index];
   const int* rows = l.row_ptr.get();
   const int* cols = l.col.get();
   const float* vals = index == 0 ? val_ : l.val.get();
   // x is not cleared: every first step below writes it without reading it.
+  // While status[0] != 0 nothing is written and x is never read.
   if (index + 1 == levels_.size()) {
     if (dense(l)) {
-      launch::dense_solve(l.n, l.dense_inverse.get(), b, x, status_.get(), stream_);
+      launch::dense_solve(l.n, l.dense_inverse.get(), b, x, status, stream_);
       tally(8.0 * l.n * l.n + 8.0 * l.n);
     } else if (l.n <= 24) {
-      launch::coarse_solve(l.n, rows, cols, vals, x, b, l.l1.get(), status_.get(),
+      launch::coarse_solve(l.n, rows, cols, vals, x, b, l.l1.get(), status,
                            options_.coarse_sweeps, stream_);
     } else {
-      smooth(l, rows, cols, vals, b, x, options_.coarse_sweeps, true);
+      smooth(l, rows, cols, vals, b, x, options_.coarse_sweeps, true, status);
     }
   } else {
-    smooth(l, rows, cols, vals, b, x, options_.pre_sweeps, true);
+    smooth(l, rows, cols, vals, b, x, options_.pre_sweeps, true, status);
     if (l.v16.allocated())
-      launch::bf16_residual(l.n, rows, cols, l.v16.get(), l.scale.get(), x, b, l.r,
-                            status_.get(), stream_);
+      launch::bf16_residual(l.n, rows, cols, l.v16.get(), l.scale.get(), x, b, l.r, status,
+                            stream_);
     else
-      launch::residual(l.n, rows, cols, vals, x, b, l.r, status_.get(), stream_);
+      launch::residual(l.n, rows, cols, vals, x, b, l.r, status, stream_);
     auto& c = levels_[index + 1];
-    launch::restrict_(c.n, l.member_offsets.get(), l.members.get(), l.r, c.b.get(),
-                      status_.get(), stream_);
+    launch::restrict_(c.n, l.member_offsets.get(), l.members.get(), l.r, c.b.get(), status,
+                      stream_);
     tally(8.0 * l.nnz + 4.0 * (l.n + 1) + 12.0 * l.n + 4.0 * (c.n + 1) + 8.0 * l.n + 4.0 * c.n);
     if (nullspace_) project(c.b.get(), c.n, c.projection.get());
-    cycle(index + 1, c.b.get(), c.x);
-    launch::prolong(l.n, l.aggregate.get(), c.x, x, status_.get(), stream_);
+    if (options_.cycle == Cycle::K && index + 2 < levels_.size())
+      inner(index + 1, status);
+    else
+      cycle(index + 1, c.b.get(), c.x, status);
+    launch::prolong(l.n, l.aggregate.get(), c.x, x, status, stream_);
     tally(12.0 * l.n + 4.0 * c.n);
-    smooth(l, rows, cols, vals, b, x, options_.post_sweeps, false);
+    smooth(l, rows, cols, vals, b, x, options_.post_sweeps, false, status);
   }
   if (nullspace_ && index != 0) project(x, l.n, l.projection.get());
+}
+
+void Solver::reduce_into(ReduceMode mode, int n, const float* x, const float* y, const float* u,
+                         const float* v, float* scalars, int offset, const int* guard) {
+  // Without an epilogue the reduction only reads the guard.
+  launch::reduce_into(mode, n, x, y, u, v, reducer(), scalars, offset, const_cast<int*>(guard),
+                      true, Epilogue::None, stream_);
+  tally((mode == ReduceMode::Dot2 ? 16.0 : 8.0) * n);
+}
+
+// Aggregation::inner, amg.cpp:312-338: two preconditioned Krylov steps on the
+// coarse equation of level `index` (A-conjugate directions for SPD, GCR
+// otherwise), leaving the correction in l.x for the prolongation. The first
+// cycle runs under the parent's status, the rest under the level's own; a
+// reduction is skipped exactly when every reader of its slots is.
+void Solver::inner(std::size_t index, const int* parent) {
+  auto& l = levels_[index];
+  const int n = l.n;
+  const int* rows = l.row_ptr.get();
+  const int* cols = l.col.get();
+  const float* vals = l.val.get();
+  const bool spd = kind_ == Kind::AmgPcg;
+  float* sc = l.scalars.get();
+  int* st = l.status.get();
+  float *p = l.p.get(), *q = l.q.get(), *t = l.t.get();
+  const double spmv_bytes = 8.0 * l.nnz + 4.0 * (n + 1) + 8.0 * n;
+
+  cycle(index, l.b.get(), l.z, parent);
+  copy(p, l.z, n);
+  launch::spmv(n, rows, cols, vals, p, q, parent, stream_);
+  tally(spmv_bytes);
+  reduce_into(ReduceMode::Dot2, n, spd ? p : q, q, l.b.get(), spd ? p : q, sc, 0, parent);
+  launch::inner_alpha(sc, st, parent, 1, stream_);
+  launch::inner_first(n, l.b.get(), p, q, l.x, t, sc, st, stream_);
+  tally(24.0 * n);
+  reduce_into(ReduceMode::Dot2, n, t, t, l.b.get(), l.b.get(), sc, 4, st);
+  launch::inner_check(sc, st, stream_);
+  cycle(index, t, l.z, st);
+  if (!spd) {
+    launch::spmv(n, rows, cols, vals, l.z, l.r, st, stream_);
+    tally(spmv_bytes);
+  }
+  reduce_into(ReduceMode::Dot, n, spd ? l.z : l.r, q, nullptr, nullptr, sc, 4, st);
+  launch::inner_beta(sc, st, stream_);
+  launch::direction(n, l.z, p, sc, st, stream_);
+  launch::spmv(n, rows, cols, vals, p, q, st, stream_);
+  tally(12.0 * n + spmv_bytes);
+  reduce_into(ReduceMode::Dot2, n, spd ? p : q, q, t, spd ? p : q, sc, 0, st);
+  launch::inner_alpha(sc, st, parent, 0, stream_);
+  launch::inner_step(n, l.x, p, sc, st, stream_);
+  tally(12.0 * n);
 }
 
 // Krylov::apply (solver.cpp:197-200) with the AMG (amg.cpp:258-261) or Jacobi
 // (solver.cpp:65-68) preconditioner.
 void Solver::apply(const float* r, float*& z) {
-  if (amg()) cycle(0, r, z);
+  if (amg()) cycle(0, r, z, status_.get());
   else launch::multiply(n_, r, jacobi_inverse_.get(), z, status_.get(), stream_);
   if (nullspace_) project(z, n_, projection_.get());
 }
@@ -599,7 +671,8 @@ std::string Solver::describe() const {
         << levels_.size() << " levels, op complexity " << std::fixed << std::setprecision(3)
         << complexity_;
     if (mixed())
-      out << " (V(" << options_.pre_sweeps << "," << options_.post_sweeps << ")"
+      out << " (" << (options_.cycle == Cycle::K ? 'K' : 'V') << "(" << options_.pre_sweeps
+          << "," << options_.post_sweeps << ")"
           << (options_.absorb_singletons ? ", singletons absorbed" : "")
           << (options_.coarse_bf16 ? ", BF16 coarse levels" : "")
           << (dense(levels_.back()) ? ", dense FP64 coarsest" : "") << ")";

@@ -58,6 +58,11 @@ struct DevLevel {
   float* x = nullptr;
   float* r = nullptr;
   DArray<float> projection;     // constant-nullspace sum pair
+  // K-cycle inner corrections (coarse levels): z ping-pongs with r, x is the
+  // correction handed to the prolongation.
+  DArray<float> za, p, q, t, scalars;
+  DArray<int> status;
+  float* z = nullptr;
   // Mixed precision: BF16 operator with row scales; dense FP64 inverse.
   DArray<unsigned short> v16;
   DArray<float> scale;
@@ -124,9 +129,14 @@ class Solver {
 
   // Preconditioner.
   void apply(const float* r, float*& z);
-  void cycle(std::size_t index, const float* b, float*& x);
+  // Work queued by cycle/smooth/inner is skipped on the device while
+  // status[0] != 0 (the outer solve's status, or a K-cycle level's own).
+  void cycle(std::size_t index, const float* b, float*& x, const int* status);
+  void inner(std::size_t index, const int* parent);
   void smooth(DevLevel& l, const int* rows, const int* cols, const float* vals, const float* b,
-              float*& x, int sweeps, bool zero_start);
+              float*& x, int sweeps, bool zero_start, const int* status);
+  void reduce_into(ReduceMode mode, int n, const float* x, const float* y, const float* u,
+                   const float* v, float* scalars, int offset, const int* guard);
 
   // Krylov driver (solver.cpp:97-393).
   bool verified(float* x, const float* b, double target, Stats& stats);

@@ -104,3 +104,44 @@ def test_device_hierarchy_matches_reference_bitwise(cuda):
         assert np.array_equal(l1.view(np.uint32), r.l1.view(np.uint32))
         if r.aggregate is not None:
             assert np.array_equal(ag, r.aggregate)
+
+
+def _neumann_forcing(s):
+    """Integer-valued compatible forcing (tests/linalg/test_solvers.cpp:20-23)."""
+    s.b = np.zeros(s.n, np.float32)
+    s.b[0], s.b[-1] = 1.0, -1.0
+    return s
+
+
+K_CASES = [
+    # test_solvers.cpp:97-98: K-cycle AMG-BiCGStab on the upwind Poisson matrix.
+    ("poisson_wind3_bicg", lambda: _rhs(harness.poisson(20, 18, 1, 1, False, False, 3)), 4,
+     False, False),
+    # test_solvers.cpp:146-151: K-cycle AMG-PCG on poisson(14, 13, 8).
+    ("poisson14x13x8", lambda: _rhs(harness.poisson(14, 13, 8)), 3, False, False),
+    # test_solvers.cpp:634-647: K-cycle with the constant-nullspace projection.
+    ("poisson12x10x4_neumann", lambda: _neumann_forcing(harness.poisson(12, 10, 4, 1, False, True)),
+     3, False, True),
+    ("poisson32_random_forcing", lambda: _forced(harness.poisson(32, 32, 32)), 3, False, False),
+    ("hex16_pressure", lambda: harness.box_system(16, 16, 16, tet=False, seed=5), 3, True, False),
+    ("tet12_pressure", lambda: harness.box_system(12, 12, 12, tet=True, seed=7), 3, True, False),
+    ("tet10_convection_bicg", lambda: harness.box_system(10, 10, 10, tet=True, seed=2,
+                                                          convection=1e-3), 4, False, False),
+]
+
+
+@needs_ref
+@pytest.mark.parametrize("name,make,kind,m_matrix,neumann", K_CASES, ids=[c[0] for c in K_CASES])
+def test_k_cycle_matches_reference(cuda, name, make, kind, m_matrix, neumann):
+    """amg.cpp:283-338: the K-cycle's two inner Krylov corrections per coarse
+    level (flexible CG for SPD, GCR otherwise), against the reference library."""
+    s = make()
+    opts = L.AmgOptions(cycle=L.AmgCycle.K,
+                        structure=M if m_matrix else L.OperatorStructure.General,
+                        nullspace=L.NullSpace.Constant if neumann else L.NullSpace.None_)
+    st, x, solver = _solve_gpu(s, L.SolverKind(kind), amg_options=opts)
+    r = ref.solve(s, opts=ref.options(kind, cycle=1, structure=int(m_matrix), nullspace=int(neumann)),
+                  rel_tol=1e-6, abs_tol=1e-12, max_iter=2000)
+    assert "K-cycle" in r.describe
+    assert solver.describe() == r.describe
+    _compare(st, x, r)
