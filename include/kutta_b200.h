@@ -165,13 +165,20 @@ int b2_amg_smooth(int n, const int32_t* d_row_ptr, const int32_t* d_col, const f
  * pairs rows like the reference's aggregation and lets rows left unpaired join
  * their strongest paired neighbour, so coarsening reaches the dense size. */
 typedef struct {
-  b2_options amg;            /* threshold, passes, sweeps, structure (coarse_rows ignored) */
+  b2_options amg;            /* cycle (default K), sweeps (default 1,1), threshold,
+                                passes, structure (coarse_rows ignored) */
   int absorb_singletons;     /* default 1 */
   int dense_rows;            /* coarsen until a level has <= this many rows (default 512) */
   int coarse_bf16;           /* default 1: levels >= 1 stored as BF16 x row scales */
   double inner_rel_tol;      /* residual reduction per refinement step (default 1e-3) */
   int inner_max_iter;        /* inner PCG iterations per refinement step (default 300) */
   int max_refinements;       /* default 30 */
+  int fused_coarse;          /* default 1: the coarse levels below 16,384 rows run as one
+                                thread-block-cluster launch per V-cycle (BF16, no
+                                nullspace, below any K-cycle inner steps) */
+  int k_cycle_levels;        /* with amg.cycle = K: coarse levels 1..k take the inner
+                                Krylov step, the rest a V-cycle; 0 = every level
+                                (default 1) */
 } b2_mixed_options;
 
 typedef struct {

@@ -40,6 +40,7 @@ CXX_FLAGS = ["-O3", "-std=c++17", "-fPIC", "-ffp-contract=off", "-Wall", "-Wextr
 PRODUCT_CU = {
     "exact_kernels.cu": EXACT,
     "mixed_kernels.cu": [],
+    "tail_cycle.cu": [],
     "noalloc.cu": [],
 }
 PRODUCT_CPP = ["host/setup.cpp", "host/solver.cpp", "host/mixed.cpp", "capi.cpp"]

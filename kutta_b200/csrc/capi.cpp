@@ -354,13 +354,16 @@ void b2_mixed_options_default(b2_mixed_options* o) {
   if (!o) return;
   b2_options_default(&o->amg);
   o->amg.structure = B2_STRUCTURE_SYMMETRIC_M_MATRIX;
-  o->amg.pre_sweeps = o->amg.post_sweeps = 2;
+  o->amg.cycle = B2_CYCLE_K;
+  o->amg.pre_sweeps = o->amg.post_sweeps = 1;
   o->absorb_singletons = 1;
   o->dense_rows = 512;
   o->coarse_bf16 = 1;
   o->inner_rel_tol = 1e-3;
   o->inner_max_iter = 300;
   o->max_refinements = 30;
+  o->fused_coarse = 1;
+  o->k_cycle_levels = 1;
 }
 
 int b2_mixed_create(int n, int nnz, const int32_t* row_ptr, const int32_t* col,
@@ -377,6 +380,9 @@ int b2_mixed_create(int n, int nnz, const int32_t* row_ptr, const int32_t* col,
     o.amg = mixed_options(m);
     o.amg.coarse_bf16 = m.coarse_bf16 != 0;
     o.amg.dense_coarsest = true;
+    o.amg.fused_tail = m.fused_coarse != 0;
+    KB2_REQUIRE(m.k_cycle_levels >= 0, "mixed: k_cycle_levels must be >= 0");
+    o.amg.k_levels = m.k_cycle_levels;
     KB2_REQUIRE(std::isfinite(m.inner_rel_tol) && m.inner_rel_tol > 0 && m.inner_rel_tol < 1 &&
                     m.inner_max_iter > 0 && m.max_refinements > 0,
                 "mixed: invalid refinement options");

@@ -130,6 +130,39 @@ void residual64(int n, const int* rows, const int* cols, const float* vals, cons
 // x += e.
 void update64(int n, double* x, const float* e, cudaStream_t s);
 
+// ---- mixed V-cycle tail: the small coarse levels in one cluster launch ------
+// Rows of a tail level are split in power-of-two chunks of (1 << shift) rows,
+// chunk k owned by CTA k of the cluster; x, r and b are offsets (in floats)
+// of that CTA's chunks in dynamic shared memory.
+constexpr int kMaxTailLevels = 8;
+constexpr int kTailSharedBytes = 200 * 1024;  // dynamic shared memory per CTA, at most
+struct TailLevel {
+  int n, shift;
+  const int* rows;
+  const int* cols;
+  const unsigned short* v16;
+  const float* scale;
+  const float* inv;
+  // transfer to the next tail level (unused on the coarsest)
+  const int* aggregate;
+  const int* offsets;
+  const int* members;
+  int x, r, b;
+};
+struct TailPlan {
+  int levels, pre, post, coarse_sweeps, cluster, smem_bytes;
+  int gathered;            // shared offset of the gathered coarsest b (dense solve)
+  const double* dense;     // coarsest dense FP64 inverse, or null for sweeps
+  TailLevel level[kMaxTailLevels];
+};
+// Whether a cluster of `cluster` CTAs (16 or 8) with this much shared memory
+// per CTA can run the tail on the current device (sets the kernel's
+// shared-memory and cluster-size attributes).
+bool tail_cluster_fits(int cluster, int smem_bytes);
+// x = V-cycle of the tail levels applied to b (both level-0 vectors of the
+// tail, in global memory); skipped while status[0] != 0.
+void tail_cycle(const TailPlan& plan, const float* b, float* x, const int* status, cudaStream_t s);
+
 // ---- single-thread scalar kernels -------------------------------------------
 void solver_limits(float* scalars, float th, float tl, float dh, float dl, cudaStream_t s);
 void solver_reset(float* scalars, int* status, int iterations, cudaStream_t s);

@@ -51,6 +51,13 @@ struct Options {  // AmgOptions, src/kutta/linalg/amg.hpp:8-20
   // coarsest level (<= 1024 rows) solved with a dense FP64 inverse.
   bool coarse_bf16 = false;
   bool dense_coarsest = false;
+  // Mixed V-cycle: the coarse levels below 16,384 rows run as one
+  // thread-block-cluster launch (needs coarse_bf16, no nullspace, and no
+  // K-cycle inner step on those levels).
+  bool fused_tail = false;
+  // K-cycle depth: coarse levels 1..k_levels take the inner Krylov step and
+  // the levels below them a V-cycle; 0 means every level (the reference).
+  int k_levels = 0;
 };
 
 // CsrMatrixHost (src/kutta/linalg/csr.hpp:16-28). val holds float-representable

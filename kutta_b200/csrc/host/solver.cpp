@@ -82,7 +82,7 @@ Solver::Solver(Kind kind, const CsrView& a, const Options& options,
     // K-cycle work vectors on the levels reached through inner() (Level ctor,
     // amg.cpp:179-195): every coarse level but the coarsest.
     if (options_.cycle == Cycle::K) {
-      for (std::size_t i = 1; i + 1 < levels_.size(); ++i) {
+      for (std::size_t i = 1; i + 1 < levels_.size() && inner_level(i); ++i) {
         auto& l = levels_[i];
         const auto rows = static_cast<std::size_t>(l.n);
         l.za.reset(rows);
@@ -145,8 +145,83 @@ Solver::Solver(Kind kind, const CsrView& a, const Options& options,
                "setup readback");
     wait(s);
     KB2_REQUIRE(host_values_[0] == 0, "mixed: coarsest operator is not SPD");
+    if (options_.fused_tail && options_.coarse_bf16 && !nullspace_) plan_tail();
   }
   wait(s);
+}
+
+// The tail starts at the first coarse level with at most 16,384 rows (about a
+// row per thread of a 16-CTA cluster: larger levels run faster spread over
+// every SM) and needs at least two levels. Each level gets three chunks (x, r,
+// b) of 2^shift >= ceil(n / cluster) floats per CTA; the dense coarsest also
+// gets room for its whole right-hand side.
+void Solver::plan_tail() {
+  constexpr int kTailRows = 1 << 14;
+  const std::size_t count = levels_.size();
+  // The tail runs plain V-cycles, so it starts below the K-cycle inner levels.
+  std::size_t start = 0;
+  for (std::size_t i = 1; i < count; ++i)
+    if (levels_[i].n <= kTailRows && !(options_.cycle == Cycle::K && inner_level(i))) {
+      start = i;
+      break;
+    }
+  if (start == 0 || count - start < 2 || count - start > launch::kMaxTailLevels) return;
+  const DevLevel& coarsest = levels_.back();
+  for (int cluster : {16, 8}) {
+    launch::TailPlan p{};
+    p.levels = static_cast<int>(count - start);
+    p.pre = options_.pre_sweeps;
+    p.post = options_.post_sweeps;
+    p.coarse_sweeps = options_.coarse_sweeps;
+    p.cluster = cluster;
+    p.dense = dense(coarsest) ? coarsest.dense_inverse.get() : nullptr;
+    int offset = 0;
+    double bytes = 0;
+    for (int k = 0; k < p.levels; ++k) {
+      const DevLevel& l = levels_[start + static_cast<std::size_t>(k)];
+      auto& t = p.level[k];
+      const int per_cta = (l.n + cluster - 1) / cluster;
+      int shift = 0;
+      while ((1 << shift) < per_cta) ++shift;
+      KB2_REQUIRE(static_cast<long long>(cluster) << shift >= l.n, "tail: chunking");
+      t.n = l.n;
+      t.shift = shift;
+      t.rows = l.row_ptr.get();
+      t.cols = l.col.get();
+      t.v16 = l.v16.get();
+      t.scale = l.scale.get();
+      t.inv = l.l1.get();
+      const bool last = k + 1 == p.levels;
+      t.aggregate = last ? nullptr : l.aggregate.get();
+      t.offsets = last ? nullptr : l.member_offsets.get();
+      t.members = last ? nullptr : l.members.get();
+      t.x = offset;
+      t.r = offset + (1 << shift);
+      t.b = offset + 2 * (1 << shift);
+      offset += 3 * (1 << shift);
+      const double sweep = 6.0 * l.nnz + 4.0 * (l.n + 1) + 16.0 * l.n;
+      if (!last) {
+        const double nc = levels_[start + static_cast<std::size_t>(k) + 1].n;
+        bytes += 12.0 * l.n + (p.pre - 1 + p.post) * sweep + (sweep - 4.0 * l.n) +
+                 4.0 * (nc + 1) + 8.0 * l.n + 4.0 * nc + 12.0 * l.n + 4.0 * nc;
+      } else if (p.dense) {
+        bytes += 8.0 * l.n * l.n + 8.0 * l.n;
+      } else {
+        bytes += 12.0 * l.n + (p.coarse_sweeps - 1) * sweep;
+      }
+    }
+    if (p.dense) {
+      p.gathered = offset;
+      offset += coarsest.n;
+    }
+    p.smem_bytes = offset * static_cast<int>(sizeof(float));
+    if (!launch::tail_cluster_fits(cluster, p.smem_bytes)) continue;
+    tail_ = p;
+    tail_start_ = start;
+    tail_bytes_ = bytes;
+    tail_on_ = true;
+    return;
+  }
 }
 
 // BF16 copies of the coarse operators and the dense inverse of the coarsest,
@@ -280,6 +355,11 @@ void Solver::cycle(std::size_t index, const float* b, float*& x, const int* stat
   const float* vals = index == 0 ? val_ : l.val.get();
   // x is not cleared: every first step below writes it without reading it.
   // While status[0] != 0 nothing is written and x is never read.
+  if (tail_on_ && index == tail_start_) {
+    launch::tail_cycle(tail_, b, x, status, stream_);
+    tally(tail_bytes_);
+    return;
+  }
   if (index + 1 == levels_.size()) {
     if (dense(l)) {
       launch::dense_solve(l.n, l.dense_inverse.get(), b, x, status, stream_);
@@ -302,7 +382,7 @@ void Solver::cycle(std::size_t index, const float* b, float*& x, const int* stat
                       stream_);
     tally(8.0 * l.nnz + 4.0 * (l.n + 1) + 12.0 * l.n + 4.0 * (c.n + 1) + 8.0 * l.n + 4.0 * c.n);
     if (nullspace_) project(c.b.get(), c.n, c.projection.get());
-    if (options_.cycle == Cycle::K && index + 2 < levels_.size())
+    if (options_.cycle == Cycle::K && index + 2 < levels_.size() && inner_level(index + 1))
       inner(index + 1, status);
     else
       cycle(index + 1, c.b.get(), c.x, status);
@@ -673,9 +753,16 @@ std::string Solver::describe() const {
     if (mixed())
       out << " (" << (options_.cycle == Cycle::K ? 'K' : 'V') << "(" << options_.pre_sweeps
           << "," << options_.post_sweeps << ")"
+          << (options_.cycle == Cycle::K && options_.k_levels > 0
+                  ? ", inner Krylov steps on levels 1-" + std::to_string(options_.k_levels)
+                  : std::string())
           << (options_.absorb_singletons ? ", singletons absorbed" : "")
           << (options_.coarse_bf16 ? ", BF16 coarse levels" : "")
-          << (dense(levels_.back()) ? ", dense FP64 coarsest" : "") << ")";
+          << (dense(levels_.back()) ? ", dense FP64 coarsest" : "");
+    if (tail_on_)
+      out << ", levels " << tail_start_ << "-" << levels_.size() - 1 << " in one "
+          << tail_.cluster << "-CTA cluster launch";
+    if (mixed()) out << ")";
   } else {
     out << "Jacobi";
   }

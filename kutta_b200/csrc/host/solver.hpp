@@ -107,7 +107,18 @@ class Solver {
   // K-cycle, and the mixed V-cycle (BF16 rounding breaks exact symmetry).
   bool variable() const { return amg() && (options_.cycle == Cycle::K || options_.coarse_bf16); }
   bool dense(const DevLevel& l) const { return l.dense_inverse.allocated(); }
+  // Whether coarse level `index` takes the K-cycle's inner Krylov step (given
+  // a K-cycle and a level above the coarsest two).
+  bool inner_level(std::size_t index) const {
+    return options_.k_levels <= 0 || index <= static_cast<std::size_t>(options_.k_levels);
+  }
   void prepare_mixed(cudaStream_t s, int error_slot);
+  // Cluster-fused tail of the mixed V-cycle: levels >= tail_start_ in one launch.
+  void plan_tail();
+  bool tail_on_ = false;
+  std::size_t tail_start_ = 0;
+  double tail_bytes_ = 0;
+  launch::TailPlan tail_{};
   bool mixed() const { return options_.coarse_bf16 || options_.dense_coarsest; }
   const int* rows0() const { return levels_[0].row_ptr.get(); }
   const int* cols0() const { return levels_[0].col.get(); }

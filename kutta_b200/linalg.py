@@ -425,13 +425,16 @@ def residual(a: CsrMatrix, x, b, r) -> None:
 class MixedOptions:
     """b2_mixed_options: the mixed-precision solve (no reference counterpart)."""
     amg: AmgOptions = dataclasses.field(default_factory=lambda: AmgOptions(
-        pre_sweeps=2, post_sweeps=2, structure=OperatorStructure.SymmetricMMatrix))
+        cycle=AmgCycle.K, pre_sweeps=1, post_sweeps=1,
+        structure=OperatorStructure.SymmetricMMatrix))
     absorb_singletons: bool = True
     dense_rows: int = 512
     coarse_bf16: bool = True
     inner_rel_tol: float = 1e-3
     inner_max_iter: int = 300
     max_refinements: int = 30
+    fused_coarse: bool = True
+    k_cycle_levels: int = 1
 
 
 @dataclasses.dataclass
@@ -447,7 +450,8 @@ class _MixedOptions(ctypes.Structure):
     _fields_ = [("amg", _Options), ("absorb_singletons", ctypes.c_int),
                 ("dense_rows", ctypes.c_int), ("coarse_bf16", ctypes.c_int),
                 ("inner_rel_tol", ctypes.c_double), ("inner_max_iter", ctypes.c_int),
-                ("max_refinements", ctypes.c_int)]
+                ("max_refinements", ctypes.c_int), ("fused_coarse", ctypes.c_int),
+                ("k_cycle_levels", ctypes.c_int)]
 
 
 class _MixedStats(ctypes.Structure):
@@ -462,6 +466,8 @@ def _mixed_struct(o: MixedOptions) -> _MixedOptions:
     s.amg = _options_struct(o.amg, True)
     s.absorb_singletons, s.dense_rows, s.coarse_bf16 = int(o.absorb_singletons), o.dense_rows, int(o.coarse_bf16)
     s.inner_rel_tol, s.inner_max_iter, s.max_refinements = o.inner_rel_tol, o.inner_max_iter, o.max_refinements
+    s.fused_coarse = int(o.fused_coarse)
+    s.k_cycle_levels = int(o.k_cycle_levels)
     return s
 
 

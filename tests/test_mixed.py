@@ -160,3 +160,50 @@ def test_mixed_rejects_nonfinite_rhs(cuda):
     x = torch.zeros(s.n, dtype=torch.float64, device="cuda")
     with pytest.raises(L.NonfiniteError):
         solver.solve(a, x, b)
+
+
+def _v11():
+    return L.AmgOptions(pre_sweeps=1, post_sweeps=1, structure=L.OperatorStructure.SymmetricMMatrix)
+
+
+def _default_amg():
+    return L.MixedOptions().amg
+
+
+FUSED_CASES = [
+    # V-cycle: the tail starts at level 1.
+    ("tet16_v", lambda: harness.box_system(16, 16, 16, tet=True, seed=6), _v11),
+    ("hex24_v", lambda: harness.box_system(24, 24, 24, tet=False, seed=12), _v11),
+    # Default K-cycle with the inner step on level 1: the tail starts below it.
+    ("tet40_graded_k", lambda: harness.box_system(40, 40, 40, tet=True, seed=13, band_layers=6,
+                                                  dmin=1e-6, dmax=1.0), _default_amg),
+]
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name,make,amg", FUSED_CASES, ids=[c[0] for c in FUSED_CASES])
+def test_fused_coarse_levels_match_separate_launches(cuda, name, make, amg):
+    """The small coarse levels as one thread-block-cluster launch give the same
+    solve as their separate BF16 kernels: same convergence, iteration counts
+    within one, and both solutions within the tolerance of the FP64 oracle."""
+    import torch
+    s = make()
+    a = L.upload(s)
+    b = torch.from_numpy(s.b).cuda()
+    results = {}
+    for fused in (True, False):
+        solver = L.make_mixed_solver(s, L.MixedOptions(amg=amg(), fused_coarse=fused))
+        assert ("cluster launch" in solver.describe()) == fused, solver.describe()
+        solver.refresh(a)
+        x = torch.zeros(s.n, dtype=torch.float64, device="cuda")
+        st = solver.solve(a, x, b, L.SolveControl(1e-8, 1e-30, 3000))
+        torch.cuda.synchronize()
+        assert st.converged, (fused, st)
+        xr = x.cpu().numpy()
+        assert _fp64_true(s, xr, s.b) <= 1e-8 * st.initial_residual * 1.0001
+        results[fused] = (st, xr)
+    (sf, xf), (su, xu) = results[True], results[False]
+    assert abs(sf.iterations - su.iterations) <= max(1, su.iterations // 20), (sf, su)
+    x64, _ = O.cg64(s, rel_tol=1e-14)
+    for xr in (xf, xu):
+        assert np.linalg.norm(xr - x64) / np.linalg.norm(x64) < 1e-5
