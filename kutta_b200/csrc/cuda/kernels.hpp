@@ -132,8 +132,8 @@ void update64(int n, double* x, const float* e, cudaStream_t s);
 
 // ---- mixed V-cycle tail: the small coarse levels in one cluster launch ------
 // Rows of a tail level are split in power-of-two chunks of (1 << shift) rows,
-// chunk k owned by CTA k of the cluster; x, r and b are offsets (in floats)
-// of that CTA's chunks in dynamic shared memory.
+// chunk k owned by CTA k of the cluster. xg, rg, bg are the level's vectors in
+// global memory (the first tail level's b is its input and xg its output).
 constexpr int kMaxTailLevels = 8;
 constexpr int kTailSharedBytes = 200 * 1024;  // dynamic shared memory per CTA, at most
 struct TailLevel {
@@ -147,11 +147,13 @@ struct TailLevel {
   const int* aggregate;
   const int* offsets;
   const int* members;
-  int x, r, b;
+  float* xg;
+  float* rg;
+  float* bg;
 };
 struct TailPlan {
   int levels, pre, post, coarse_sweeps, cluster, smem_bytes;
-  int gathered;            // shared offset of the gathered coarsest b (dense solve)
+  int gathered, solution;  // shared offsets of the dense coarsest b and x (n each)
   const double* dense;     // coarsest dense FP64 inverse, or null for sweeps
   TailLevel level[kMaxTailLevels];
 };
@@ -159,9 +161,9 @@ struct TailPlan {
 // per CTA can run the tail on the current device (sets the kernel's
 // shared-memory and cluster-size attributes).
 bool tail_cluster_fits(int cluster, int smem_bytes);
-// x = V-cycle of the tail levels applied to b (both level-0 vectors of the
-// tail, in global memory); skipped while status[0] != 0.
-void tail_cycle(const TailPlan& plan, const float* b, float* x, const int* status, cudaStream_t s);
+// level[0].xg = V-cycle of the tail levels applied to level[0].bg; skipped
+// while status[0] != 0.
+void tail_cycle(const TailPlan& plan, const int* status, cudaStream_t s);
 
 // ---- single-thread scalar kernels -------------------------------------------
 void solver_limits(float* scalars, float th, float tl, float dh, float dl, cudaStream_t s);

@@ -5,11 +5,20 @@
 // sweep, residual, restriction or prolongation costs a launch and a few
 // microseconds whatever its size. Here one thread-block cluster (16 CTAs of
 // 1024 threads where the device allows, else 8) runs the whole V-cycle of
-// those levels. Each CTA owns a power-of-two chunk of rows per level and keeps
-// that chunk's x, r and b in its shared memory; a row's neighbours are read
-// from whichever CTA owns them through distributed shared memory, and each
-// step ends with a cluster barrier. The operators are the BF16 copies with
-// row scales, read from global memory (they stay in L2).
+// those levels, with a cluster barrier between dependent steps.
+//
+// Each CTA owns a power-of-two chunk of rows per level. The level vectors stay
+// in global memory, where they are L2-resident: values written during the
+// launch are read with L2-only loads, which keeps them coherent across the
+// cluster's SMs (for these scattered gathers L2 measured faster than reading
+// other CTAs' shared memory), while the operators, constant during the launch,
+// are read through the read-only cache, where a CTA's rows stay between steps.
+//
+// Steps are merged where no neighbour value is needed: the zero-start sweep of
+// a level is done by whoever writes its right-hand side (the first step, or
+// the restriction), and every CTA solves the dense coarsest level itself, so
+// the prolongation from it reads the correction from the CTA's own shared
+// memory.
 #include <cooperative_groups.h>
 #include <cuda_bf16.h>
 
@@ -26,18 +35,11 @@ using launch::TailLevel;
 using launch::TailPlan;
 
 constexpr int kTailThreads = 1024;
+constexpr int kBatch = 8;
+constexpr float kOmega = 2.0f / 3.0f;
 
 __device__ __forceinline__ float bf(unsigned short v) {
   return __bfloat162float(__ushort_as_bfloat16(v));
-}
-
-// Value j of a level vector whose chunks start at `offset` in every CTA's
-// shared memory.
-__device__ __forceinline__ float remote(cg::cluster_group& cluster, float* shared, int offset,
-                                        int shift, int j) {
-  const int owner = j >> shift;
-  const int local = j & ((1 << shift) - 1);
-  return *cluster.map_shared_rank(shared + offset + local, owner);
 }
 
 struct Rows {
@@ -48,171 +50,181 @@ __device__ __forceinline__ Rows owned(const TailLevel& l, int rank) {
   return Rows{base, max(0, min(1 << l.shift, l.n - base))};
 }
 
-// sum_j a_ij x_j with the BF16 operator (without the row scale). Columns and
-// values are loaded eight at a time before the neighbour reads, so a thread
-// keeps several loads in flight instead of one dependent chain per entry.
-__device__ __forceinline__ float row_product(cg::cluster_group& cluster, float* shared,
-                                             const TailLevel& l, int x, int i) {
-  constexpr int kBatch = 8;
+// sum_j a_ij x_j of row i with the BF16 operator (without the row scale). The
+// entries are taken eight at a time, their neighbour values all requested
+// before any is used, so a thread keeps several loads in flight.
+__device__ __forceinline__ float row_product(const TailLevel& l, const float* x, int i) {
   float acc = 0.0f;
-  const int end = l.rows[i + 1];
-  for (int j0 = l.rows[i]; j0 < end; j0 += kBatch) {
-    int col[kBatch];
-    float val[kBatch];
+  const int end = __ldg(l.rows + i + 1);
+  for (int j0 = __ldg(l.rows + i); j0 < end; j0 += kBatch) {
+    int c[kBatch];
+    float a[kBatch];
 #pragma unroll
     for (int u = 0; u < kBatch; ++u) {
-      const bool in = j0 + u < end;
-      col[u] = in ? l.cols[j0 + u] : -1;
-      val[u] = in ? bf(l.v16[j0 + u]) : 0.0f;
+      c[u] = j0 + u < end ? __ldg(l.cols + j0 + u) : -1;
+      a[u] = j0 + u < end ? bf(__ldg(l.v16 + j0 + u)) : 0.0f;
     }
+    float v[kBatch];
 #pragma unroll
-    for (int u = 0; u < kBatch; ++u)
-      if (col[u] >= 0) acc = fmaf(val[u], remote(cluster, shared, x, l.shift, col[u]), acc);
+    for (int u = 0; u < kBatch; ++u) v[u] = c[u] >= 0 ? __ldcg(x + c[u]) : 0.0f;
+#pragma unroll
+    for (int u = 0; u < kBatch; ++u) acc = fmaf(a[u], v[u], acc);
   }
   return acc;
 }
 
-// next = x + (2/3) inv (b - A x); zero: x taken as zero without reading it.
-__device__ void sweep(cg::cluster_group& cluster, float* shared, const TailLevel& l, int rank,
-                      int x, int next, bool zero) {
+// next = x + omega inv (b - A x) on the owned rows.
+__device__ void sweep(const TailLevel& l, int rank, const float* x, float* next) {
   const Rows own = owned(l, rank);
   for (int k = threadIdx.x; k < own.count; k += blockDim.x) {
     const int i = own.base + k;
-    const float b = shared[l.b + k];
-    if (zero) {
-      shared[next + k] = (2.0f / 3.0f) * l.inv[i] * b;
-    } else {
-      const float r = b - l.scale[i] * row_product(cluster, shared, l, x, i);
-      shared[next + k] = shared[x + k] + (2.0f / 3.0f) * l.inv[i] * r;
-    }
+    const float r = __ldcg(l.bg + i) - __ldg(l.scale + i) * row_product(l, x, i);
+    __stcg(next + i, __ldcg(x + i) + kOmega * __ldg(l.inv + i) * r);
   }
 }
 
-__device__ void residual(cg::cluster_group& cluster, float* shared, const TailLevel& l, int rank,
-                         int x, int r) {
+__device__ void residual(const TailLevel& l, int rank, const float* x, float* r) {
   const Rows own = owned(l, rank);
   for (int k = threadIdx.x; k < own.count; k += blockDim.x) {
     const int i = own.base + k;
-    shared[r + k] = shared[l.b + k] - l.scale[i] * row_product(cluster, shared, l, x, i);
+    __stcg(r + i, __ldcg(l.bg + i) - __ldg(l.scale + i) * row_product(l, x, i));
   }
 }
 
-// Coarse b = Kahan sum of the fine residual over each aggregate's members.
-__device__ void restrict_to(cg::cluster_group& cluster, float* shared, const TailLevel& fine,
-                            int r, const TailLevel& coarse, int rank) {
+// Coarse b = Kahan sum of the fine residual over each aggregate's members, in
+// member order; with `zero`, also the coarse zero-start sweep x = omega inv b.
+__device__ void restrict_to(const TailLevel& fine, const float* r, const TailLevel& coarse,
+                            float* coarse_x, bool zero, int rank) {
   const Rows own = owned(coarse, rank);
   for (int k = threadIdx.x; k < own.count; k += blockDim.x) {
     const int g = own.base + k;
     float sum = 0.0f, error = 0.0f;
-    for (int j = fine.offsets[g]; j < fine.offsets[g + 1]; ++j) {
-      const float term = remote(cluster, shared, r, fine.shift, fine.members[j]) - error;
-      const float next = sum + term;
-      error = (next - sum) - term;
-      sum = next;
+    const int end = __ldg(fine.offsets + g + 1);
+    for (int j0 = __ldg(fine.offsets + g); j0 < end; j0 += kBatch) {
+      int m[kBatch];
+#pragma unroll
+      for (int u = 0; u < kBatch; ++u) m[u] = j0 + u < end ? __ldg(fine.members + j0 + u) : -1;
+      float v[kBatch];
+#pragma unroll
+      for (int u = 0; u < kBatch; ++u) v[u] = m[u] >= 0 ? __ldcg(r + m[u]) : 0.0f;
+#pragma unroll
+      for (int u = 0; u < kBatch; ++u) {
+        if (m[u] < 0) break;
+        const float term = v[u] - error;
+        const float next = sum + term;
+        error = (next - sum) - term;
+        sum = next;
+      }
     }
-    shared[coarse.b + k] = sum;
+    __stcg(coarse.bg + g, sum);
+    if (zero) __stcg(coarse_x + g, kOmega * __ldg(coarse.inv + g) * sum);
   }
 }
 
-__device__ void prolong_from(cg::cluster_group& cluster, float* shared, const TailLevel& fine,
-                             int x, const TailLevel& coarse, int coarse_x, int rank) {
+// x += e[aggregate] on the owned rows; e in global memory or, for the dense
+// coarsest, in this CTA's shared memory.
+__device__ void prolong(const TailLevel& fine, float* x, const float* e, bool e_shared, int rank) {
   const Rows own = owned(fine, rank);
   for (int k = threadIdx.x; k < own.count; k += blockDim.x) {
-    const int g = fine.aggregate[own.base + k];
-    if (g >= 0) shared[x + k] += remote(cluster, shared, coarse_x, coarse.shift, g);
+    const int i = own.base + k;
+    const int g = __ldg(fine.aggregate + i);
+    if (g >= 0) __stcg(x + i, __ldcg(x + i) + (e_shared ? e[g] : __ldcg(e + g)));
   }
 }
 
-// x = W b with the dense FP64 inverse: b gathered into this CTA first, then a
-// warp per owned row.
-__device__ void dense_solve(cg::cluster_group& cluster, float* shared, const TailLevel& l,
-                            int rank, const double* W, int x, int gathered) {
-  for (int k = threadIdx.x; k < l.n; k += blockDim.x)
-    shared[gathered + k] = remote(cluster, shared, l.b, l.shift, k);
+// The whole coarsest solution x = W b with the dense FP64 inverse, into this
+// CTA's shared memory (every CTA computes it): b gathered first, then a warp
+// per row.
+__device__ void dense_solve(float* shared, const TailLevel& l, const double* W, int gathered,
+                            int solution) {
+  for (int k = threadIdx.x; k < l.n; k += blockDim.x) shared[gathered + k] = __ldcg(l.bg + k);
   __syncthreads();
-  const Rows own = owned(l, rank);
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, warps = blockDim.x >> 5;
-  for (int k = warp; k < own.count; k += warps) {
-    const double* row = W + static_cast<std::size_t>(own.base + k) * l.n;
+  for (int i = warp; i < l.n; i += warps) {
+    const double* row = W + static_cast<std::size_t>(i) * l.n;
     double acc = 0.0;
     for (int c = lane; c < l.n; c += 32) acc += row[c] * static_cast<double>(shared[gathered + c]);
     for (int d = 16; d > 0; d >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, d);
-    if (lane == 0) shared[x + k] = static_cast<float>(acc);
+    if (lane == 0) shared[solution + i] = static_cast<float>(acc);
   }
+  __syncthreads();
 }
 
 __global__ void __launch_bounds__(kTailThreads)
-    k_tail_cycle(const __grid_constant__ TailPlan p, const float* __restrict__ b_in,
-                 float* __restrict__ x_out, const int* __restrict__ status) {
+    k_tail_cycle(const __grid_constant__ TailPlan p, const int* __restrict__ status) {
   // Uniform across the cluster: nothing else writes status while this runs.
   if (status[0] != 0) return;
   cg::cluster_group cluster = cg::this_cluster();
   extern __shared__ float shared[];
   const int rank = static_cast<int>(cluster.block_rank());
   const int last = p.levels - 1;
-  int x[kMaxTailLevels], spare[kMaxTailLevels];
+  const bool dense = p.dense != nullptr;
+  // Current iterate and spare buffer of each level (uniform across threads).
+  float* x[kMaxTailLevels];
+  float* spare[kMaxTailLevels];
   for (int l = 0; l < p.levels; ++l) {
-    x[l] = p.level[l].x;
-    spare[l] = p.level[l].r;
+    x[l] = p.level[l].xg;
+    spare[l] = p.level[l].rg;
+  }
+  // The first tail level swaps roles (pre - 1) + post times; start so that its
+  // result ends in xg, the buffer the caller reads.
+  if (((p.pre - 1 + p.post) & 1) != 0) {
+    x[0] = p.level[0].rg;
+    spare[0] = p.level[0].xg;
   }
   {
-    const Rows own = owned(p.level[0], rank);
-    for (int k = threadIdx.x; k < own.count; k += blockDim.x)
-      shared[p.level[0].b + k] = b_in[own.base + k];
+    // Zero-start sweep of the first tail level from its right-hand side.
+    const TailLevel& L = p.level[0];
+    const Rows own = owned(L, rank);
+    for (int k = threadIdx.x; k < own.count; k += blockDim.x) {
+      const int i = own.base + k;
+      __stcg(x[0] + i, kOmega * __ldg(L.inv + i) * __ldcg(L.bg + i));
+    }
   }
   cluster.sync();
   for (int l = 0; l < last; ++l) {
     const TailLevel& L = p.level[l];
-    sweep(cluster, shared, L, rank, x[l], x[l], true);
-    cluster.sync();
     for (int s = 1; s < p.pre; ++s) {
-      sweep(cluster, shared, L, rank, x[l], spare[l], false);
+      sweep(L, rank, x[l], spare[l]);
       cluster.sync();
-      const int t = x[l];
+      float* t = x[l];
       x[l] = spare[l];
       spare[l] = t;
     }
-    residual(cluster, shared, L, rank, x[l], spare[l]);
+    residual(L, rank, x[l], spare[l]);
     cluster.sync();
-    restrict_to(cluster, shared, L, spare[l], p.level[l + 1], rank);
+    const bool coarse_sweeps = l + 1 < last || !dense;
+    restrict_to(L, spare[l], p.level[l + 1], x[l + 1], coarse_sweeps, rank);
     cluster.sync();
   }
-  {
-    const TailLevel& C = p.level[last];
-    if (p.dense) {
-      dense_solve(cluster, shared, C, rank, p.dense, x[last], p.gathered);
+  const float* correction = nullptr;  // coarsest solution, when in shared memory
+  if (dense) {
+    dense_solve(shared, p.level[last], p.dense, p.gathered, p.solution);
+    correction = shared + p.solution;
+  } else {
+    // x[last] holds the zero-start sweep (written with the restriction).
+    for (int s = 1; s < p.coarse_sweeps; ++s) {
+      sweep(p.level[last], rank, x[last], spare[last]);
       cluster.sync();
-    } else {
-      sweep(cluster, shared, C, rank, x[last], x[last], true);
-      cluster.sync();
-      for (int s = 1; s < p.coarse_sweeps; ++s) {
-        sweep(cluster, shared, C, rank, x[last], spare[last], false);
-        cluster.sync();
-        const int t = x[last];
-        x[last] = spare[last];
-        spare[last] = t;
-      }
+      float* t = x[last];
+      x[last] = spare[last];
+      spare[last] = t;
     }
   }
   for (int l = last - 1; l >= 0; --l) {
     const TailLevel& L = p.level[l];
-    prolong_from(cluster, shared, L, x[l], p.level[l + 1], x[l + 1], rank);
+    const bool from_shared = l + 1 == last && correction != nullptr;
+    prolong(L, x[l], from_shared ? correction : x[l + 1], from_shared, rank);
     cluster.sync();
     for (int s = 0; s < p.post; ++s) {
-      sweep(cluster, shared, L, rank, x[l], spare[l], false);
-      cluster.sync();
-      const int t = x[l];
+      sweep(L, rank, x[l], spare[l]);
+      // After the last sweep nothing in this launch reads another CTA's rows.
+      if (l > 0 || s + 1 < p.post) cluster.sync();
+      float* t = x[l];
       x[l] = spare[l];
       spare[l] = t;
     }
   }
-  {
-    const Rows own = owned(p.level[0], rank);
-    for (int k = threadIdx.x; k < own.count; k += blockDim.x)
-      x_out[own.base + k] = shared[x[0] + k];
-  }
-  // No CTA leaves while another may still read its shared memory.
-  cluster.sync();
 }
 
 // The attribute is per function, shared by every solver on the device, so it
@@ -262,12 +274,11 @@ bool tail_cluster_fits(int cluster, int smem_bytes) {
   return false;
 }
 
-void tail_cycle(const TailPlan& plan, const float* b, float* x, const int* status,
-                cudaStream_t s) {
+void tail_cycle(const TailPlan& plan, const int* status, cudaStream_t s) {
   ++counter;
   cudaLaunchAttribute attr[1];
   cudaLaunchConfig_t c = config_for(plan, attr, s);
-  cudaLaunchKernelEx(&c, k_tail_cycle, plan, b, x, status);
+  cudaLaunchKernelEx(&c, k_tail_cycle, plan, status);
 }
 
 }  // namespace launch

@@ -152,9 +152,9 @@ Solver::Solver(Kind kind, const CsrView& a, const Options& options,
 
 // The tail starts at the first coarse level with at most 16,384 rows (about a
 // row per thread of a 16-CTA cluster: larger levels run faster spread over
-// every SM) and needs at least two levels. Each level gets three chunks (x, r,
-// b) of 2^shift >= ceil(n / cluster) floats per CTA; the dense coarsest also
-// gets room for its whole right-hand side.
+// every SM) and needs at least two levels. CTA k owns rows
+// [k 2^shift, (k + 1) 2^shift) of each level, 2^shift >= ceil(n / cluster);
+// shared memory holds only the dense coarsest right-hand side and solution.
 void Solver::plan_tail() {
   constexpr int kTailRows = 1 << 14;
   const std::size_t count = levels_.size();
@@ -175,10 +175,10 @@ void Solver::plan_tail() {
     p.coarse_sweeps = options_.coarse_sweeps;
     p.cluster = cluster;
     p.dense = dense(coarsest) ? coarsest.dense_inverse.get() : nullptr;
-    int offset = 0;
     double bytes = 0;
     for (int k = 0; k < p.levels; ++k) {
-      const DevLevel& l = levels_[start + static_cast<std::size_t>(k)];
+      const std::size_t i = start + static_cast<std::size_t>(k);
+      const DevLevel& l = levels_[i];
       auto& t = p.level[k];
       const int per_cta = (l.n + cluster - 1) / cluster;
       int shift = 0;
@@ -195,10 +195,9 @@ void Solver::plan_tail() {
       t.aggregate = last ? nullptr : l.aggregate.get();
       t.offsets = last ? nullptr : l.member_offsets.get();
       t.members = last ? nullptr : l.members.get();
-      t.x = offset;
-      t.r = offset + (1 << shift);
-      t.b = offset + 2 * (1 << shift);
-      offset += 3 * (1 << shift);
+      t.xg = l.xa.get();
+      t.rg = l.ra.get();
+      t.bg = l.b.get();
       const double sweep = 6.0 * l.nnz + 4.0 * (l.n + 1) + 16.0 * l.n;
       if (!last) {
         const double nc = levels_[start + static_cast<std::size_t>(k) + 1].n;
@@ -211,10 +210,10 @@ void Solver::plan_tail() {
       }
     }
     if (p.dense) {
-      p.gathered = offset;
-      offset += coarsest.n;
+      p.gathered = 0;
+      p.solution = coarsest.n;
+      p.smem_bytes = 2 * coarsest.n * static_cast<int>(sizeof(float));
     }
-    p.smem_bytes = offset * static_cast<int>(sizeof(float));
     if (!launch::tail_cluster_fits(cluster, p.smem_bytes)) continue;
     tail_ = p;
     tail_start_ = start;
@@ -356,7 +355,10 @@ void Solver::cycle(std::size_t index, const float* b, float*& x, const int* stat
   // x is not cleared: every first step below writes it without reading it.
   // While status[0] != 0 nothing is written and x is never read.
   if (tail_on_ && index == tail_start_) {
-    launch::tail_cycle(tail_, b, x, status, stream_);
+    // The tail reads its right-hand side from, and leaves its result in, the
+    // level's own b and first buffer, which never change roles.
+    KB2_REQUIRE(b == l.b.get() && x == l.xa.get(), "tail: unexpected level buffers");
+    launch::tail_cycle(tail_, status, stream_);
     tally(tail_bytes_);
     return;
   }
