@@ -115,6 +115,14 @@ void bf16_smooth(int n, const int* rows, const int* cols, const unsigned short* 
 void bf16_residual(int n, const int* rows, const int* cols, const unsigned short* v16,
                    const float* scale, const float* x, const float* b, float* r, const int* status,
                    cudaStream_t s);
+// K-cycle inner step on a BF16 level: q = A p with p.q and w.p (gcr: q.q and
+// w.q) -> scalars[0..3], skipped while status[0] != 0.
+void bf16_spmv_dot2(int n, const int* rows, const int* cols, const unsigned short* v16,
+                    const float* scale, const float* p, const float* w, float* q, bool gcr,
+                    DeviceReducer red, float* scalars, const int* status, cudaStream_t s);
+// inner_first fused with the t.t, b.b reduction -> scalars[4..7].
+void inner_first_dot(int n, const float* b, const float* p, const float* q, float* x, float* t,
+                     float* scalars, const int* status, DeviceReducer red, cudaStream_t s);
 // Dense FP64 Cholesky of an n <= 1024 CSR operator and its explicit inverse
 // (n x n, row-major, into `inverse`; `lower` is n x n scratch); *error = 1 if
 // the operator is not SPD.

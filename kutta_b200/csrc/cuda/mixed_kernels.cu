@@ -40,14 +40,47 @@ __global__ void k_bf16_pack(int n, const int* __restrict__ rows, const float* __
   }
 }
 
-__device__ __forceinline__ float bf16_row(int i, const int* __restrict__ rows,
-                                          const int* __restrict__ cols,
-                                          const unsigned short* __restrict__ v16,
-                                          const float* __restrict__ x) {
+// Coarse rows hold about a dozen entries: four lanes share a row, each taking
+// every fourth entry, so a warp reads eight rows' contiguous segments instead
+// of 32 strided ones, and a row's dependent gathers are a quarter as long.
+constexpr int kLanes = 4;
+constexpr int kRowsPerWarp = 32 / kLanes;
+
+// This lane's share of sum_j a_ij x_j (BF16 values, FP32 accumulation).
+__device__ __forceinline__ float bf16_row_part(int i, int lane, const int* __restrict__ rows,
+                                               const int* __restrict__ cols,
+                                               const unsigned short* __restrict__ v16,
+                                               const float* __restrict__ x) {
   float acc = 0.0f;
   const int end = rows[i + 1];
-  for (int j = rows[i]; j < end; ++j) acc = fmaf(bf(v16[j]), x[cols[j]], acc);
+  for (int j = rows[i] + lane; j < end; j += kLanes) acc = fmaf(bf(v16[j]), x[cols[j]], acc);
   return acc;
+}
+// Sum over the row's four lanes, in lane 0 (every lane of the warp calls it).
+__device__ __forceinline__ float row_total(float v) {
+  v += __shfl_down_sync(0xffffffffu, v, 2, kLanes);
+  v += __shfl_down_sync(0xffffffffu, v, 1, kLanes);
+  return v;
+}
+
+// Visits rows kLanes lanes at a time; the loop bound is uniform across a warp,
+// so every lane reaches the shuffles. body(i, lane, valid).
+template <class Body>
+__device__ __forceinline__ void for_rows(int n, Body body) {
+  const int lane = threadIdx.x & (kLanes - 1);
+  const int warp = static_cast<int>((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+  const int warps = static_cast<int>((gridDim.x * blockDim.x) >> 5);
+  for (int row0 = warp * kRowsPerWarp; row0 < n; row0 += warps * kRowsPerWarp) {
+    const int i = row0 + static_cast<int>((threadIdx.x & 31) / kLanes);
+    body(i, lane, i < n);
+  }
+}
+
+// A reduction's grid stays within the partials buffer (kMaxBlocks blocks).
+inline int lanes_grid(int n, bool reduction) {
+  const long long blocks = (static_cast<long long>(n) * kLanes + kBlock - 1) / kBlock;
+  const long long cap = reduction ? static_cast<long long>(kMaxBlocks) : (1LL << 30);
+  return static_cast<int>(std::max(1LL, std::min(blocks, cap)));
 }
 
 // Damped L1-Jacobi sweep with the BF16 operator (FP32 accumulation).
@@ -58,14 +91,14 @@ __global__ void k_bf16_smooth(int n, const int* __restrict__ rows, const int* __
                               const float* __restrict__ b, const float* __restrict__ inv,
                               float* __restrict__ next, const int* __restrict__ status) {
   if (status[0] != 0) return;
-  ROWS(i, n) {
-    if (kZero) {
-      next[i] = (2.0f / 3.0f) * inv[i] * b[i];
-    } else {
-      const float r = b[i] - scale[i] * bf16_row(i, rows, cols, v16, x);
-      next[i] = x[i] + (2.0f / 3.0f) * inv[i] * r;
-    }
+  if (kZero) {
+    ROWS(i, n) next[i] = (2.0f / 3.0f) * inv[i] * b[i];
+    return;
   }
+  for_rows(n, [&](int i, int lane, bool valid) {
+    const float acc = row_total(valid ? bf16_row_part(i, lane, rows, cols, v16, x) : 0.0f);
+    if (valid && lane == 0) next[i] = x[i] + (2.0f / 3.0f) * inv[i] * (b[i] - scale[i] * acc);
+  });
 }
 
 __global__ void k_bf16_residual(int n, const int* __restrict__ rows, const int* __restrict__ cols,
@@ -74,7 +107,74 @@ __global__ void k_bf16_residual(int n, const int* __restrict__ rows, const int* 
                                 const float* __restrict__ b, float* __restrict__ r,
                                 const int* __restrict__ status) {
   if (status[0] != 0) return;
-  ROWS(i, n) r[i] = b[i] - scale[i] * bf16_row(i, rows, cols, v16, x);
+  for_rows(n, [&](int i, int lane, bool valid) {
+    const float acc = row_total(valid ? bf16_row_part(i, lane, rows, cols, v16, x) : 0.0f);
+    if (valid && lane == 0) r[i] = b[i] - scale[i] * acc;
+  });
+}
+
+// The last block stores the two FP64 totals as (hi, lo) pairs at
+// scalars[offset] and scalars[offset + 2].
+__device__ __forceinline__ void finish_dot2(DeviceReducer red, double a, double b,
+                                            float* scalars, int offset) {
+  __shared__ double shared[32];
+  a = block_sum(a, shared);
+  b = block_sum(b, shared);
+  const Reducer r{red.partials, red.ticket};
+  if (!publish(r, a, b, true)) return;
+  const double total_a = gather(r, 0, shared);
+  const double total_b = gather(r, 1, shared);
+  if (threadIdx.x == 0) {
+    store_pair(scalars, offset, total_a);
+    store_pair(scalars, offset + 2, total_b);
+    *r.ticket = 0;
+  }
+}
+
+// K-cycle inner step on a BF16 level: q = A p and, in the same pass, the two
+// products its step length needs -> scalars[0..3]: p.q and w.p (A-conjugate,
+// SPD) or q.q and w.q (GCR). Skipped while status[0] != 0.
+__global__ void k_bf16_spmv_dot2(int n, const int* __restrict__ rows, const int* __restrict__ cols,
+                                 const unsigned short* __restrict__ v16,
+                                 const float* __restrict__ scale, const float* __restrict__ p,
+                                 const float* __restrict__ w, float* __restrict__ q, bool gcr,
+                                 DeviceReducer red, float* scalars,
+                                 const int* __restrict__ status) {
+  if (status[0] != 0) return;
+  double a = 0.0, b = 0.0;
+  for_rows(n, [&](int i, int lane, bool valid) {
+    const float acc = row_total(valid ? bf16_row_part(i, lane, rows, cols, v16, p) : 0.0f);
+    if (valid && lane == 0) {
+      const float qi = scale[i] * acc;
+      q[i] = qi;
+      const double d = gcr ? static_cast<double>(qi) : static_cast<double>(p[i]);
+      a += d * static_cast<double>(qi);
+      b += static_cast<double>(w[i]) * d;
+    }
+  });
+  finish_dot2(red, a, b, scalars, 0);
+}
+
+// amg_inner_first with the next reduction fused: x = alpha p, t = b - alpha q
+// (or x = p, t = 0 when the level's status is not running), then t.t and b.b
+// -> scalars[4..7]. Skipped (reduction included) while status[0] != 0, as
+// every reader of those slots is.
+__global__ void k_inner_first_dot(int n, const float* __restrict__ b, const float* __restrict__ p,
+                                  const float* __restrict__ q, float* __restrict__ x,
+                                  float* __restrict__ t, float* scalars,
+                                  const int* __restrict__ status, DeviceReducer red) {
+  const bool running = status[0] == 0;
+  const float alpha = kp_float(kp_load(scalars, 8));
+  double tt = 0.0, bb = 0.0;
+  ROWS(i, n) {
+    const float ti = running ? b[i] - alpha * q[i] : 0.0f;
+    x[i] = running ? alpha * p[i] : p[i];
+    t[i] = ti;
+    tt += static_cast<double>(ti) * static_cast<double>(ti);
+    bb += static_cast<double>(b[i]) * static_cast<double>(b[i]);
+  }
+  if (!running) return;
+  finish_dot2(red, tt, bb, scalars, 4);
 }
 
 // Dense FP64 Cholesky of the coarsest operator and its explicit inverse, in one
@@ -196,14 +296,29 @@ void bf16_smooth(int n, const int* rows, const int* cols, const unsigned short* 
   if (zero_start)
     k_bf16_smooth<true><<<rows_grid(n), kBlock, 0, s>>>(n, rows, cols, v16, scale, x, b, inv, next, status);
   else
-    k_bf16_smooth<false><<<rows_grid(n), kBlock, 0, s>>>(n, rows, cols, v16, scale, x, b, inv, next, status);
+    k_bf16_smooth<false><<<lanes_grid(n, false), kBlock, 0, s>>>(n, rows, cols, v16, scale, x, b, inv, next, status);
+}
+void bf16_spmv_dot2(int n, const int* rows, const int* cols, const unsigned short* v16,
+                    const float* scale, const float* p, const float* w, float* q, bool gcr,
+                    DeviceReducer red, float* scalars, const int* status, cudaStream_t s) {
+  if (n <= 0) return;
+  ++counter;
+  k_bf16_spmv_dot2<<<lanes_grid(n, true), kBlock, 0, s>>>(n, rows, cols, v16, scale, p, w, q,
+                                                          gcr, red, scalars, status);
+}
+void inner_first_dot(int n, const float* b, const float* p, const float* q, float* x, float* t,
+                     float* scalars, const int* status, DeviceReducer red, cudaStream_t s) {
+  if (n <= 0) return;
+  ++counter;
+  k_inner_first_dot<<<grid_for(n), kBlock, 0, s>>>(n, b, p, q, x, t, scalars, status, red);
 }
 void bf16_residual(int n, const int* rows, const int* cols, const unsigned short* v16,
                    const float* scale, const float* x, const float* b, float* r, const int* status,
                    cudaStream_t s) {
   if (n <= 0) return;
   ++counter;
-  k_bf16_residual<<<rows_grid(n), kBlock, 0, s>>>(n, rows, cols, v16, scale, x, b, r, status);
+  k_bf16_residual<<<lanes_grid(n, false), kBlock, 0, s>>>(n, rows, cols, v16, scale, x, b, r,
+                                                          status);
 }
 void dense_inverse(int n, const int* rows, const int* cols, const float* vals, double* lower,
                    double* inverse, double* error, cudaStream_t s) {

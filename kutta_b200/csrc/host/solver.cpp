@@ -420,15 +420,31 @@ void Solver::inner(std::size_t index, const int* parent) {
   float *p = l.p.get(), *q = l.q.get(), *t = l.t.get();
   const double spmv_bytes = 8.0 * l.nnz + 4.0 * (n + 1) + 8.0 * n;
 
+  // A BF16 level (mixed precision, SPD) uses its BF16 operator, with the
+  // reductions fused into the kernels that produce their operands.
+  const bool bf16 = l.v16.allocated() && spd;
+  const double bf16_bytes = 6.0 * l.nnz + 4.0 * (n + 1) + 16.0 * n;
+
   cycle(index, l.b.get(), l.z, parent);
   copy(p, l.z, n);
-  launch::spmv(n, rows, cols, vals, p, q, parent, stream_);
-  tally(spmv_bytes);
-  reduce_into(ReduceMode::Dot2, n, spd ? p : q, q, l.b.get(), spd ? p : q, sc, 0, parent);
+  if (bf16) {
+    launch::bf16_spmv_dot2(n, rows, cols, l.v16.get(), l.scale.get(), p, l.b.get(), q, false,
+                           reducer(), sc, parent, stream_);
+    tally(bf16_bytes);
+  } else {
+    launch::spmv(n, rows, cols, vals, p, q, parent, stream_);
+    tally(spmv_bytes);
+    reduce_into(ReduceMode::Dot2, n, spd ? p : q, q, l.b.get(), spd ? p : q, sc, 0, parent);
+  }
   launch::inner_alpha(sc, st, parent, 1, stream_);
-  launch::inner_first(n, l.b.get(), p, q, l.x, t, sc, st, stream_);
-  tally(24.0 * n);
-  reduce_into(ReduceMode::Dot2, n, t, t, l.b.get(), l.b.get(), sc, 4, st);
+  if (bf16) {
+    launch::inner_first_dot(n, l.b.get(), p, q, l.x, t, sc, st, reducer(), stream_);
+    tally(24.0 * n);
+  } else {
+    launch::inner_first(n, l.b.get(), p, q, l.x, t, sc, st, stream_);
+    tally(24.0 * n);
+    reduce_into(ReduceMode::Dot2, n, t, t, l.b.get(), l.b.get(), sc, 4, st);
+  }
   launch::inner_check(sc, st, stream_);
   cycle(index, t, l.z, st);
   if (!spd) {
@@ -438,9 +454,16 @@ void Solver::inner(std::size_t index, const int* parent) {
   reduce_into(ReduceMode::Dot, n, spd ? l.z : l.r, q, nullptr, nullptr, sc, 4, st);
   launch::inner_beta(sc, st, stream_);
   launch::direction(n, l.z, p, sc, st, stream_);
-  launch::spmv(n, rows, cols, vals, p, q, st, stream_);
-  tally(12.0 * n + spmv_bytes);
-  reduce_into(ReduceMode::Dot2, n, spd ? p : q, q, t, spd ? p : q, sc, 0, st);
+  tally(12.0 * n);
+  if (bf16) {
+    launch::bf16_spmv_dot2(n, rows, cols, l.v16.get(), l.scale.get(), p, t, q, false, reducer(),
+                           sc, st, stream_);
+    tally(bf16_bytes);
+  } else {
+    launch::spmv(n, rows, cols, vals, p, q, st, stream_);
+    tally(spmv_bytes);
+    reduce_into(ReduceMode::Dot2, n, spd ? p : q, q, t, spd ? p : q, sc, 0, st);
+  }
   launch::inner_alpha(sc, st, parent, 0, stream_);
   launch::inner_step(n, l.x, p, sc, st, stream_);
   tally(12.0 * n);
