@@ -199,14 +199,19 @@ def run_ours(args, rank, world, local):
         mixed_step()
     clocks = Clocks(local)
     clocks.start()
-    mixed.profile(True)
     launches0 = L.kernel_launches()
     ms, stats = _timed(mixed_step, args.steps, stream, sync)
     launches = L.kernel_launches() - launches0
-    prof = mixed.profile_read()
-    mixed.profile(False)
     clk = clocks.stop()
     ms = max_over_ranks(ms)
+    # The same steps again with profiling on, for the fine-sweep kernel time
+    # and the algorithmic bytes. Profiling brackets individual sweeps with
+    # events, so this pass launches kernels one by one instead of replaying
+    # captured graphs; the sweep kernel itself is the same.
+    mixed.profile(True)
+    prof_ms, _ = _timed(mixed_step, args.steps, stream, sync)
+    prof = mixed.profile_read()
+    mixed.profile(False)
     last = stats[-1]
     true_rel = float(np.linalg.norm(b64 - A @ x64.cpu().numpy()) / last.initial_residual)
 
@@ -285,7 +290,9 @@ def run_ours(args, rank, world, local):
             "roofline": roofline(pprof, plain_ms, max(1, args.plain_steps)),
             "speedup_of_mixed": plain_ms / ms,
         },
-        "roofline": roofline(prof, ms, args.steps),
+        "roofline": dict(roofline(prof, prof_ms, args.steps),
+                         timed_in="profiled pass of the same steps (kernels launched one by one)",
+                         profiled_ms_per_step=prof_ms),
         "e2e": {"value": e2e_ms / world, "unit": UNIT,
                 "h2d_bytes_per_step": 4 * s.nnz + 4 * s.n, "d2h_bytes_per_step": 8 * s.n},
         "gpu_launches": int(launches),

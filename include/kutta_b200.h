@@ -179,6 +179,11 @@ typedef struct {
   int k_cycle_levels;        /* with amg.cycle = K: coarse levels 1..k take the inner
                                 Krylov step, the rest a V-cycle; 0 = every level
                                 (default 1) */
+  int cuda_graphs;           /* default 1: each batch of inner iterations between host
+                                status checks, and each preconditioner application, is
+                                captured once as a CUDA graph and replayed (same kernels,
+                                same results); the solve stream may be the legacy default
+                                stream, capture uses an internal stream */
 } b2_mixed_options;
 
 typedef struct {

@@ -58,6 +58,9 @@ struct Options {  // AmgOptions, src/kutta/linalg/amg.hpp:8-20
   // K-cycle depth: coarse levels 1..k_levels take the inner Krylov step and
   // the levels below them a V-cycle; 0 means every level (the reference).
   int k_levels = 0;
+  // Replay each AMG preconditioner application as a captured CUDA graph (the
+  // same kernels with the same arguments, so the same results).
+  bool graphs = false;
 };
 
 // CsrMatrixHost (src/kutta/linalg/csr.hpp:16-28). val holds float-representable

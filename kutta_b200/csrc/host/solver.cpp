@@ -246,6 +246,8 @@ void Solver::residual(const float* x, const float* b, float* r) {
 
 Solver::~Solver() {
   for (auto e : events_) cudaEventDestroy(e);
+  for (auto& g : graphs_) cudaGraphExecDestroy(g.exec);
+  if (capture_) cudaStreamDestroy(capture_);
 }
 
 void Solver::set_profile(bool on) {
@@ -472,9 +474,81 @@ void Solver::inner(std::size_t index, const int* parent) {
 // Krylov::apply (solver.cpp:197-200) with the AMG (amg.cpp:258-261) or Jacobi
 // (solver.cpp:65-68) preconditioner.
 void Solver::apply(const float* r, float*& z) {
-  if (amg()) cycle(0, r, z, status_.get());
-  else launch::multiply(n_, r, jacobi_inverse_.get(), z, status_.get(), stream_);
+  if (amg() && graphing()) {
+    graphed(r, z, 0, z, [&] { cycle(0, r, z, status_.get()); });
+  } else if (amg()) {
+    cycle(0, r, z, status_.get());
+  } else {
+    launch::multiply(n_, r, jacobi_inverse_.get(), z, status_.get(), stream_);
+  }
   if (nullspace_) project(z, n_, projection_.get());
+}
+
+// Every level's current buffer roles (the ping-pong smoother swaps them).
+std::vector<const float*> Solver::roles(const float* z) const {
+  std::vector<const float*> out{z};
+  for (const auto& l : levels_) {
+    out.push_back(l.x);
+    out.push_back(l.r);
+    out.push_back(l.z);
+  }
+  return out;
+}
+
+// `work` (kernels only, no host waits) as a CUDA graph: captured the first
+// time for this key on an internal stream, then launched on the solve stream.
+// The ping-pong smoother swaps each level's buffers an even number of times
+// per cycle, so the buffer roles after the work equal those before and one
+// capture serves every later call with the same key; if a capture finds
+// otherwise, graphs are turned off for this solver after that capture has been
+// launched once (it is the right work for this call).
+void Solver::graphed(const void* k1, const void* k2, int k3, float* const& tracked,
+                     const std::function<void()>& work) {
+  for (const auto& g : graphs_)
+    if (g.k1 == k1 && g.k2 == k2 && g.k3 == k3) {
+      cuda_check(cudaGraphLaunch(g.exec, stream_), "cudaGraphLaunch");
+      launch::counter += g.launches;
+      tally(g.bytes);
+      return;
+    }
+  if (capture_ == nullptr)
+    cuda_check(cudaStreamCreateWithFlags(&capture_, cudaStreamNonBlocking), "cudaStreamCreate");
+  const auto before = roles(tracked);
+  cudaStream_t solve = stream_;
+  stream_ = capture_;
+  capturing_ = true;
+  const long long launches0 = launch::counter.load();
+  const double bytes0 = prof_.algorithmic_bytes;
+  cudaGraph_t graph = nullptr;
+  cuda_check(cudaStreamBeginCapture(capture_, cudaStreamCaptureModeThreadLocal), "capture");
+  try {
+    work();
+  } catch (...) {
+    cudaStreamEndCapture(capture_, &graph);
+    if (graph) cudaGraphDestroy(graph);
+    stream_ = solve;
+    capturing_ = false;
+    throw;
+  }
+  const cudaError_t ended = cudaStreamEndCapture(capture_, &graph);
+  stream_ = solve;
+  capturing_ = false;
+  cuda_check(ended, "capture");
+  Graph g{k1, k2, k3, nullptr, launch::counter.load() - launches0,
+          prof_.algorithmic_bytes - bytes0};
+  launch::counter -= g.launches;  // counted when launched
+  const cudaError_t made = cudaGraphInstantiate(&g.exec, graph, 0);
+  cudaGraphDestroy(graph);
+  cuda_check(made, "cudaGraphInstantiate");
+  cuda_check(cudaGraphLaunch(g.exec, stream_), "cudaGraphLaunch");
+  launch::counter += g.launches;
+  if (roles(tracked) == before) {
+    graphs_.push_back(g);
+  } else {
+    // Launched in stream order above; CUDA defers the release until it ends.
+    cudaGraphExecDestroy(g.exec);
+    graphs_usable_ = false;
+  }
 }
 
 // Krylov::refresh (solver.cpp:92-95) + Aggregation::refresh (amg.cpp:228-256) or
@@ -595,12 +669,12 @@ void Solver::pcg(float* x, const float* b, const Control& c, double target, Stat
     const int batch = std::min(check_interval, c.max_iter - stats.iterations);
     verified_current_ = false;
     speculated_.reset();
-    for (int j = 0; j < batch; ++j) {
+    auto iterate = [&](int j) {
       launch::spmv_dot(n_, rows0(), cols0(), val_, p_, p_, q_, reducer(), scalars_.get(), 2,
                        status_.get(), Epilogue::PcgAlpha, stream_);
       launch::pcg_step_dot(n_, x, r_, p_, q_, reducer(), scalars_.get(), status_.get(), stream_);
       tally(8.0 * nnz_ + 4.0 * (n_ + 1) + 8.0 * n_ + 24.0 * n_);
-      if (stats.iterations + j + 1 == c.max_iter) continue;
+      if (stats.iterations + j + 1 == c.max_iter) return;
       apply(r_, z_);
       tally((variable() ? 12.0 : 8.0) * n_ + 12.0 * n_);
       if (variable())
@@ -610,7 +684,14 @@ void Solver::pcg(float* x, const float* b, const Control& c, double target, Stat
         launch::reduce_into(ReduceMode::Dot, n_, r_, z_, r_, z_, reducer(), scalars_.get(), 4,
                             status_.get(), true, Epilogue::PcgBeta, stream_);
       launch::direction(n_, z_, p_, scalars_.get(), status_.get(), stream_);
-    }
+    };
+    // A batch of whole iterations between two status polls is one graph.
+    if (amg() && graphing() && stats.iterations + batch < c.max_iter)
+      graphed(x, r_, -batch, z_, [&] {
+        for (int j = 0; j < batch; ++j) iterate(j);
+      });
+    else
+      for (int j = 0; j < batch; ++j) iterate(j);
     const auto state = poll(x, b);
     stats.iterations = state[1];
     if (state[0] == 2) break;

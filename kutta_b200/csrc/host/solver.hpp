@@ -4,6 +4,7 @@
 #pragma once
 
 #include <cmath>
+#include <functional>
 #include <initializer_list>
 #include <memory>
 #include <optional>
@@ -140,6 +141,26 @@ class Solver {
 
   // Preconditioner.
   void apply(const float* r, float*& z);
+  struct Graph {
+    const void* k1;
+    const void* k2;
+    int k3;
+    cudaGraphExec_t exec;
+    long long launches;  // kernels in the graph
+    double bytes;        // their algorithmic bytes
+  };
+  // Whether device work may go through captured graphs now (not while
+  // profiling, whose events sample individual sweeps, nor inside a capture).
+  bool graphing() const {
+    return options_.graphs && graphs_usable_ && !profiling_ && !capturing_;
+  }
+  void graphed(const void* k1, const void* k2, int k3, float* const& tracked,
+               const std::function<void()>& work);
+  std::vector<const float*> roles(const float* z) const;
+  std::vector<Graph> graphs_;
+  bool graphs_usable_ = true;
+  bool capturing_ = false;
+  cudaStream_t capture_ = nullptr;
   // Work queued by cycle/smooth/inner is skipped on the device while
   // status[0] != 0 (the outer solve's status, or a K-cycle level's own).
   void cycle(std::size_t index, const float* b, float*& x, const int* status);

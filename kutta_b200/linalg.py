@@ -435,6 +435,7 @@ class MixedOptions:
     max_refinements: int = 30
     fused_coarse: bool = True
     k_cycle_levels: int = 1
+    cuda_graphs: bool = True
 
 
 @dataclasses.dataclass
@@ -451,7 +452,7 @@ class _MixedOptions(ctypes.Structure):
                 ("dense_rows", ctypes.c_int), ("coarse_bf16", ctypes.c_int),
                 ("inner_rel_tol", ctypes.c_double), ("inner_max_iter", ctypes.c_int),
                 ("max_refinements", ctypes.c_int), ("fused_coarse", ctypes.c_int),
-                ("k_cycle_levels", ctypes.c_int)]
+                ("k_cycle_levels", ctypes.c_int), ("cuda_graphs", ctypes.c_int)]
 
 
 class _MixedStats(ctypes.Structure):
@@ -468,6 +469,7 @@ def _mixed_struct(o: MixedOptions) -> _MixedOptions:
     s.inner_rel_tol, s.inner_max_iter, s.max_refinements = o.inner_rel_tol, o.inner_max_iter, o.max_refinements
     s.fused_coarse = int(o.fused_coarse)
     s.k_cycle_levels = int(o.k_cycle_levels)
+    s.cuda_graphs = int(o.cuda_graphs)
     return s
 
 

@@ -208,3 +208,29 @@ def test_fused_coarse_levels_match_separate_launches(cuda, name, make, amg):
     x64, _ = O.cg64(s, rel_tol=1e-14)
     for xr in (xf, xu):
         assert np.linalg.norm(xr - x64) / np.linalg.norm(x64) < 1e-5
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("k_levels", [1, 0], ids=["k_cycle_level1", "k_cycle_all"])
+def test_cuda_graph_replay_is_bitwise_identical(cuda, k_levels):
+    """Captured-graph replay runs the same kernels with the same arguments as
+    direct launches: equal statistics and a bitwise-equal FP64 solution, over
+    two solves (the second replays graphs captured by the first)."""
+    import torch
+    s = harness.box_system(24, 24, 24, tet=True, seed=14)
+    a = L.upload(s)
+    b = torch.from_numpy(s.b).cuda()
+    out = {}
+    for graphs in (True, False):
+        solver = L.make_mixed_solver(s, L.MixedOptions(cuda_graphs=graphs, k_cycle_levels=k_levels))
+        solver.refresh(a)
+        runs = []
+        for _ in range(2):
+            x = torch.zeros(s.n, dtype=torch.float64, device="cuda")
+            st = solver.solve(a, x, b, L.SolveControl(1e-8, 1e-30, 2000))
+            torch.cuda.synchronize()
+            runs.append((st, x.cpu().numpy()))
+        out[graphs] = runs
+    for (sg, xg), (sd, xd) in zip(out[True], out[False]):
+        assert sg == sd
+        assert np.array_equal(xg.view(np.uint64), xd.view(np.uint64))
