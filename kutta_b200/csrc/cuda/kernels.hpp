@@ -115,6 +115,9 @@ void bf16_smooth(int n, const int* rows, const int* cols, const unsigned short* 
 void bf16_residual(int n, const int* rows, const int* cols, const unsigned short* v16,
                    const float* scale, const float* x, const float* b, float* r, const int* status,
                    cudaStream_t s);
+// Restriction for the mixed V-cycle: plain FP32 sums, four lanes per aggregate.
+void restrict_lanes(int nc, const int* offsets, const int* members, const float* fine,
+                    float* coarse, const int* status, cudaStream_t s);
 // K-cycle inner step on a BF16 level: q = A p with p.q and w.p (gcr: q.q and
 // w.q) -> scalars[0..3], skipped while status[0] != 0.
 void bf16_spmv_dot2(int n, const int* rows, const int* cols, const unsigned short* v16,

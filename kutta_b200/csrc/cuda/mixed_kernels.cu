@@ -46,14 +46,30 @@ __global__ void k_bf16_pack(int n, const int* __restrict__ rows, const float* __
 constexpr int kLanes = 4;
 constexpr int kRowsPerWarp = 32 / kLanes;
 
-// This lane's share of sum_j a_ij x_j (BF16 values, FP32 accumulation).
+// This lane's share of sum_j a_ij x_j (BF16 values, FP32 accumulation). The
+// row is taken in chunks of kLanes * kPerLane entries; a lane issues all its
+// column and value loads of a chunk before any gather, so each warp keeps
+// several independent loads in flight (these levels are latency-bound).
+constexpr int kPerLane = 3;
 __device__ __forceinline__ float bf16_row_part(int i, int lane, const int* __restrict__ rows,
                                                const int* __restrict__ cols,
                                                const unsigned short* __restrict__ v16,
                                                const float* __restrict__ x) {
   float acc = 0.0f;
   const int end = rows[i + 1];
-  for (int j = rows[i] + lane; j < end; j += kLanes) acc = fmaf(bf(v16[j]), x[cols[j]], acc);
+  for (int j0 = rows[i] + lane; j0 < end; j0 += kLanes * kPerLane) {
+    int c[kPerLane];
+    float a[kPerLane];
+#pragma unroll
+    for (int u = 0; u < kPerLane; ++u) {
+      const int j = j0 + u * kLanes;
+      c[u] = j < end ? cols[j] : -1;
+      a[u] = j < end ? bf(v16[j]) : 0.0f;
+    }
+#pragma unroll
+    for (int u = 0; u < kPerLane; ++u)
+      if (c[u] >= 0) acc = fmaf(a[u], x[c[u]], acc);
+  }
   return acc;
 }
 // Sum over the row's four lanes, in lane 0 (every lane of the warp calls it).
@@ -110,6 +126,33 @@ __global__ void k_bf16_residual(int n, const int* __restrict__ rows, const int* 
   for_rows(n, [&](int i, int lane, bool valid) {
     const float acc = row_total(valid ? bf16_row_part(i, lane, rows, cols, v16, x) : 0.0f);
     if (valid && lane == 0) r[i] = b[i] - scale[i] * acc;
+  });
+}
+
+// Coarse b = sum of the fine residual over each aggregate's members, four
+// lanes per aggregate with their member loads batched like the row kernels.
+__global__ void k_restrict_lanes(int nc, const int* __restrict__ offsets,
+                                 const int* __restrict__ members, const float* __restrict__ fine,
+                                 float* __restrict__ coarse, const int* __restrict__ status) {
+  if (status[0] != 0) return;
+  for_rows(nc, [&](int g, int lane, bool valid) {
+    float acc = 0.0f;
+    if (valid) {
+      const int end = offsets[g + 1];
+      for (int j0 = offsets[g] + lane; j0 < end; j0 += kLanes * kPerLane) {
+        int m[kPerLane];
+#pragma unroll
+        for (int u = 0; u < kPerLane; ++u) {
+          const int j = j0 + u * kLanes;
+          m[u] = j < end ? members[j] : -1;
+        }
+#pragma unroll
+        for (int u = 0; u < kPerLane; ++u)
+          if (m[u] >= 0) acc += fine[m[u]];
+      }
+    }
+    acc = row_total(acc);
+    if (valid && lane == 0) coarse[g] = acc;
   });
 }
 
@@ -297,6 +340,13 @@ void bf16_smooth(int n, const int* rows, const int* cols, const unsigned short* 
     k_bf16_smooth<true><<<rows_grid(n), kBlock, 0, s>>>(n, rows, cols, v16, scale, x, b, inv, next, status);
   else
     k_bf16_smooth<false><<<lanes_grid(n, false), kBlock, 0, s>>>(n, rows, cols, v16, scale, x, b, inv, next, status);
+}
+void restrict_lanes(int nc, const int* offsets, const int* members, const float* fine,
+                    float* coarse, const int* status, cudaStream_t s) {
+  if (nc <= 0) return;
+  ++counter;
+  k_restrict_lanes<<<lanes_grid(nc, false), kBlock, 0, s>>>(nc, offsets, members, fine, coarse,
+                                                            status);
 }
 void bf16_spmv_dot2(int n, const int* rows, const int* cols, const unsigned short* v16,
                     const float* scale, const float* p, const float* w, float* q, bool gcr,

@@ -382,8 +382,12 @@ void Solver::cycle(std::size_t index, const float* b, float*& x, const int* stat
     else
       launch::residual(l.n, rows, cols, vals, x, b, l.r, status, stream_);
     auto& c = levels_[index + 1];
-    launch::restrict_(c.n, l.member_offsets.get(), l.members.get(), l.r, c.b.get(), status,
-                      stream_);
+    if (mixed())
+      launch::restrict_lanes(c.n, l.member_offsets.get(), l.members.get(), l.r, c.b.get(), status,
+                             stream_);
+    else
+      launch::restrict_(c.n, l.member_offsets.get(), l.members.get(), l.r, c.b.get(), status,
+                        stream_);
     tally(8.0 * l.nnz + 4.0 * (l.n + 1) + 12.0 * l.n + 4.0 * (c.n + 1) + 8.0 * l.n + 4.0 * c.n);
     if (nullspace_) project(c.b.get(), c.n, c.projection.get());
     if (options_.cycle == Cycle::K && index + 2 < levels_.size() && inner_level(index + 1))
