@@ -129,8 +129,9 @@ void inner_first_dot(int n, const float* b, const float* p, const float* q, floa
 // Dense FP64 Cholesky of an n <= 1024 CSR operator and its explicit inverse
 // (n x n, row-major, into `inverse`; `lower` is n x n scratch); *error = 1 if
 // the operator is not SPD.
+// With `ratio`, also the smallest pivot relative to its diagonal (0 if not SPD).
 void dense_inverse(int n, const int* rows, const int* cols, const float* vals, double* lower,
-                   double* inverse, double* error, cudaStream_t s);
+                   double* inverse, double* error, cudaStream_t s, double* ratio = nullptr);
 // x = inverse * b (FP64 accumulation).
 void dense_solve(int n, const double* inverse, const float* b, float* x, const int* status,
                  cudaStream_t s);

@@ -224,19 +224,28 @@ __global__ void k_inner_first_dot(int n, const float* __restrict__ b, const floa
 // block (n <= 1024). L is n x n row-major scratch and W the n x n inverse, both
 // in global memory (the level is small, so both stay in cache). *error is
 // written at the end: 1 if a pivot was not positive (the operator is not SPD;
-// such a pivot is replaced by 1 so the kernel ends), else 0.
+// such a pivot is replaced by 1 so the kernel ends), else 0. If `ratio` is not
+// null, *ratio is the smallest pivot relative to its row's diagonal (0 if one
+// failed): close to 0 when the operator is nearly singular.
 __global__ void __launch_bounds__(1024)
     k_dense_inverse(int n, const int* __restrict__ rows, const int* __restrict__ cols,
                     const float* __restrict__ vals, double* __restrict__ L,
-                    double* __restrict__ W, double* error) {
+                    double* __restrict__ W, double* error, double* ratio) {
   const int t = threadIdx.x, T = blockDim.x;
   __shared__ int failed;
-  if (t == 0) failed = 0;
+  __shared__ double smallest;
+  __shared__ double diag0[1024];
+  if (t == 0) {
+    failed = 0;
+    smallest = 1.0;
+  }
   for (int k = t; k < n * n; k += T) L[k] = 0.0;
   __syncthreads();
   for (int i = t; i < n; i += T)
-    for (int j = rows[i]; j < rows[i + 1]; ++j)
+    for (int j = rows[i]; j < rows[i + 1]; ++j) {
       if (cols[j] <= i) L[static_cast<std::size_t>(i) * n + cols[j]] = vals[j];
+      if (cols[j] == i) diag0[i] = vals[j];
+    }
   __syncthreads();
   __shared__ double pivot;
   for (int k = 0; k < n; ++k) {
@@ -245,6 +254,8 @@ __global__ void __launch_bounds__(1024)
       if (!(d > 0.0)) {
         failed = 1;
         d = 1.0;
+      } else {
+        smallest = fmin(smallest, d / diag0[k]);
       }
       pivot = sqrt(d);
       L[static_cast<std::size_t>(k) * n + k] = pivot;
@@ -273,7 +284,10 @@ __global__ void __launch_bounds__(1024)
       W[static_cast<std::size_t>(i) * n + j] = s / L[static_cast<std::size_t>(i) * n + i];
     }
   }
-  if (t == 0) *error = failed ? 1.0 : 0.0;
+  if (t == 0) {
+    *error = failed ? 1.0 : 0.0;
+    if (ratio) *ratio = failed ? 0.0 : smallest;
+  }
 }
 
 // x = A^-1 b with the dense FP64 inverse: one warp per row, FP64 accumulation.
@@ -371,11 +385,11 @@ void bf16_residual(int n, const int* rows, const int* cols, const unsigned short
                                                           status);
 }
 void dense_inverse(int n, const int* rows, const int* cols, const float* vals, double* lower,
-                   double* inverse, double* error, cudaStream_t s) {
+                   double* inverse, double* error, cudaStream_t s, double* ratio) {
   if (n <= 0) return;
   ++counter;
   const int threads = std::min(1024, ((n + 31) / 32) * 32);
-  k_dense_inverse<<<1, threads, 0, s>>>(n, rows, cols, vals, lower, inverse, error);
+  k_dense_inverse<<<1, threads, 0, s>>>(n, rows, cols, vals, lower, inverse, error, ratio);
 }
 void dense_solve(int n, const double* inverse, const float* b, float* x, const int* status,
                  cudaStream_t s) {

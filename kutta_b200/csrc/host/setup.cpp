@@ -217,19 +217,30 @@ std::vector<int> pairs(const CsrView& a, double threshold, bool exclude_isolated
     ++next;
   }
   if (!absorb_singletons) return map;
-  // A row left alone joins the pair of its strongest neighbour that belongs to
-  // a pair (rows in row order; aggregates then renumbered in their old order).
+  // A row left alone joins the pair of its strongest strongly connected
+  // neighbour that belongs to a pair; rows in row order, aggregates then
+  // renumbered in their old order. Strongly connected: the pairing criterion
+  // (weight >= threshold * the row's strongest weight) and a coupling of at
+  // least kAbsorbCoupling relative to the two diagonals, |a_ij| >=
+  // 0.01 sqrt(|a_ii a_jj|). The second keeps nearly decoupled cells (a
+  // diagonal orders of magnitude below its neighbours', as in real pressure
+  // matrices) as coarse rows of their own, where the coarse solve resolves the
+  // near-null modes they carry instead of averaging them into a neighbour.
+  constexpr double kAbsorbCoupling = 0.01;
   std::vector<int> size(static_cast<std::size_t>(next), 0);
   for (int g : map)
     if (g >= 0) ++size[g];
   for (int i = 0; i < n; ++i) {
     if (map[i] < 0 || size[map[i]] != 1) continue;
-    neighbours(i);
+    const double strongest = neighbours(i);
+    const double di = std::fabs(a.val[a.diag[i]]);
     int best = -1;
     double weight = 0;
     for (std::size_t k = 0; k < cand_col.size(); ++k) {
       const int g = map[cand_col[k]];
-      if (g >= 0 && g != map[i] && size[g] >= 2 && cand_w[k] > weight) {
+      const double dj = std::fabs(a.val[a.diag[cand_col[k]]]);
+      if (g >= 0 && g != map[i] && size[g] >= 2 && cand_w[k] > weight &&
+          cand_w[k] >= threshold * strongest && cand_w[k] >= kAbsorbCoupling * std::sqrt(di * dj)) {
         best = g;
         weight = cand_w[k];
       }

@@ -140,11 +140,12 @@ Solver::Solver(Kind kind, const CsrView& a, const Options& options,
     }
     // Usable before the first refresh, from the setup values.
     prepare_mixed(s, 0);
-    cuda_check(cudaMemcpyAsync(host_values_.get(), values_.get(), sizeof(double),
+    cuda_check(cudaMemcpyAsync(host_values_.get(), values_.get(), 2 * sizeof(double),
                                cudaMemcpyDeviceToHost, s),
                "setup readback");
     wait(s);
     KB2_REQUIRE(host_values_[0] == 0, "mixed: coarsest operator is not SPD");
+    choose_coarsest(host_values_[1]);
     if (options_.fused_tail && options_.coarse_bf16 && !nullspace_) plan_tail();
   }
   wait(s);
@@ -227,15 +228,32 @@ void Solver::plan_tail() {
 // from the current FP32 coarse values; the dense SPD check lands in values_[0].
 void Solver::prepare_mixed(cudaStream_t s, int slot) {
   double* error = values_.get() + slot;
-  cuda_check(cudaMemsetAsync(error, 0, sizeof(double), s), "memset");
+  cuda_check(cudaMemsetAsync(error, 0, 2 * sizeof(double), s), "memset");
   for (std::size_t i = 1; i < levels_.size(); ++i) {
     auto& l = levels_[i];
     if (l.v16.allocated())
       launch::bf16_pack(l.n, l.row_ptr.get(), l.val.get(), l.v16.get(), l.scale.get(), s);
     if (dense(l))
       launch::dense_inverse(l.n, l.row_ptr.get(), l.col.get(), l.val.get(), l.dense_lower.get(),
-                            l.dense_inverse.get(), error, s);
+                            l.dense_inverse.get(), error, s, error + 1);
   }
+}
+
+// The coarsest level is solved with its dense inverse only when that is
+// well conditioned: a nearly singular operator (smallest relative Cholesky
+// pivot below 1e-6) would multiply the FP32 rounding of the restricted
+// right-hand side by up to the inverse of that pivot along its near-null
+// vector. Such a level is smoothed instead (coarse_sweeps damped sweeps, as the
+// reference treats every coarsest level), leaving those components to the
+// Krylov iteration. Graphs captured under the other choice are dropped.
+void Solver::choose_coarsest(double smallest_pivot) {
+  constexpr double kConditioned = 1e-6;
+  const bool ok = dense(levels_.back()) && smallest_pivot >= kConditioned;
+  if (ok != dense_ok_) {
+    for (auto& g : graphs_) cudaGraphExecDestroy(g.exec);
+    graphs_.clear();
+  }
+  dense_ok_ = ok;
 }
 
 // ---------------------------------------------------------------- primitives --
@@ -360,12 +378,18 @@ void Solver::cycle(std::size_t index, const float* b, float*& x, const int* stat
     // The tail reads its right-hand side from, and leaves its result in, the
     // level's own b and first buffer, which never change roles.
     KB2_REQUIRE(b == l.b.get() && x == l.xa.get(), "tail: unexpected level buffers");
-    launch::tail_cycle(tail_, status, stream_);
+    if (dense_ok_) {
+      launch::tail_cycle(tail_, status, stream_);
+    } else {
+      launch::TailPlan smoothed = tail_;
+      smoothed.dense = nullptr;
+      launch::tail_cycle(smoothed, status, stream_);
+    }
     tally(tail_bytes_);
     return;
   }
   if (index + 1 == levels_.size()) {
-    if (dense(l)) {
+    if (dense(l) && dense_ok_) {
       launch::dense_solve(l.n, l.dense_inverse.get(), b, x, status, stream_);
       tally(8.0 * l.n * l.n + 8.0 * l.n);
     } else if (l.n <= 24) {
@@ -591,7 +615,7 @@ void Solver::refresh(const float* val, cudaStream_t s) {
   const int slots = static_cast<int>(levels_.size());
   if (mixed()) prepare_mixed(s, slots);
   cuda_check(cudaMemcpyAsync(host_values_.get(), values_.get(),
-                             sizeof(double) * (slots + (mixed() ? 1 : 0)), cudaMemcpyDeviceToHost, s),
+                             sizeof(double) * (slots + (mixed() ? 2 : 0)), cudaMemcpyDeviceToHost, s),
              "refresh readback");
   wait(s);
   cuda_check(cudaGetLastError(), "refresh");
@@ -600,7 +624,10 @@ void Solver::refresh(const float* val, cudaStream_t s) {
     KB2_REQUIRE(invalid != 3, "AMG: requires positive diagonals");
     KB2_REQUIRE(invalid <= allowed[i], "AMG: invalid values or zero diagonal");
   }
-  if (mixed()) KB2_REQUIRE(host_values_[slots] == 0, "mixed: coarsest operator is not SPD");
+  if (mixed()) {
+    KB2_REQUIRE(host_values_[slots] == 0, "mixed: coarsest operator is not SPD");
+    choose_coarsest(host_values_[slots + 1]);
+  }
 }
 
 // --------------------------------------------------------------------- Krylov --
@@ -868,7 +895,10 @@ std::string Solver::describe() const {
                   : std::string())
           << (options_.absorb_singletons ? ", singletons absorbed" : "")
           << (options_.coarse_bf16 ? ", BF16 coarse levels" : "")
-          << (dense(levels_.back()) ? ", dense FP64 coarsest" : "");
+          << (dense(levels_.back())
+                  ? (dense_ok_ ? ", dense FP64 coarsest"
+                               : ", nearly singular coarsest smoothed instead of its dense inverse")
+                  : "");
     if (tail_on_)
       out << ", levels " << tail_start_ << "-" << levels_.size() - 1 << " in one "
           << tail_.cluster << "-CTA cluster launch";

@@ -114,6 +114,8 @@ class Solver {
     return options_.k_levels <= 0 || index <= static_cast<std::size_t>(options_.k_levels);
   }
   void prepare_mixed(cudaStream_t s, int error_slot);
+  void choose_coarsest(double smallest_pivot);
+  bool dense_ok_ = false;  // the dense coarsest inverse is used (well conditioned)
   // Cluster-fused tail of the mixed V-cycle: levels >= tail_start_ in one launch.
   void plan_tail();
   bool tail_on_ = false;

@@ -376,29 +376,41 @@ static int* pairs(const hcsr* a, double threshold, int exclude_isolated, int abs
   }
   if (absorb) {
     /* Mixed-precision hierarchy (kutta_b200's own method, no reference
-     * counterpart): an unpaired row joins the pair of its strongest neighbour
-     * that belongs to a pair; rows in order, aggregates renumbered in order. */
+     * counterpart): an unpaired row joins the pair of its strongest strongly
+     * connected neighbour (weight >= threshold * the row's strongest weight
+     * and >= 0.01 sqrt(|a_ii a_jj|)) that belongs to a pair; rows in order,
+     * aggregates renumbered in order. */
     int* size = xcalloc((size_t)(next > 0 ? next : 1), sizeof(int));
     for (int i = 0; i < n; ++i) if (map[i] >= 0) ++size[map[i]];
     for (int i = 0; i < n; ++i) {
       if (map[i] < 0 || size[map[i]] != 1) continue;
       int best = -1;
-      double bw = 0;
-      int out = a->row_ptr[i], in = offsets[i];
-      while (out < a->row_ptr[i + 1] || in < offsets[i + 1]) {
-        int oc = out < a->row_ptr[i + 1] ? a->col[out] : n;
-        int ic = in < offsets[i + 1] ? sources[in] : n;
-        int column = oc < ic ? oc : ic;
-        double w = 0;
-        if (oc == column) w = fabs(a->val[out++]);
-        if (ic == column) {
-          double t = fabs(a->val[find_entry(a, column, i)]);
-          w = w > t ? w : t;
-          ++in;
-        }
-        if (column != i && w != 0) {
-          int g = map[column];
-          if (g >= 0 && g != map[i] && size[g] >= 2 && w > bw) { best = g; bw = w; }
+      double bw = 0, strongest = 0;
+      for (int visit = 0; visit < 2; ++visit) {  /* strongest weight, then the choice */
+        int out = a->row_ptr[i], in = offsets[i];
+        while (out < a->row_ptr[i + 1] || in < offsets[i + 1]) {
+          int oc = out < a->row_ptr[i + 1] ? a->col[out] : n;
+          int ic = in < offsets[i + 1] ? sources[in] : n;
+          int column = oc < ic ? oc : ic;
+          double w = 0;
+          if (oc == column) w = fabs(a->val[out++]);
+          if (ic == column) {
+            double t = fabs(a->val[find_entry(a, column, i)]);
+            w = w > t ? w : t;
+            ++in;
+          }
+          if (column == i || w == 0) continue;
+          if (visit == 0) {
+            if (w > strongest) strongest = w;
+          } else {
+            int g = map[column];
+            double coupling = 0.01 * sqrt(fabs(a->val[a->diag[i]]) * fabs(a->val[a->diag[column]]));
+            if (g >= 0 && g != map[i] && size[g] >= 2 && w > bw && w >= threshold * strongest &&
+                w >= coupling) {
+              best = g;
+              bw = w;
+            }
+          }
         }
       }
       if (best < 0) continue;
