@@ -396,6 +396,150 @@ def profile_once(args):
                       "relative_residual": st.final_residual / st.initial_residual}))
 
 
+def _graded(args, coeff_seed=0):
+    from kutta_b200 import harness
+    return harness.box_system(args.size, args.size, args.size, tet=True, seed=args.seed,
+                              band_layers=10, aspect=1000.0, ratio=1.2, dmin=1e-6, dmax=1.0,
+                              coeff_seed=coeff_seed)
+
+
+def _blend(values, diag, boundary, row_ptr, fresh, keep):
+    """keep * values + (1 - keep) * fresh for the off-diagonal entries (face
+    coefficients are linear in D_f, so this blends the D fields), each
+    diagonal recomputed as the upward-rounded float of its off-diagonal
+    magnitudes plus the blended boundary term (the M-matrix construction)."""
+    import numpy as np
+    out = keep * values + (1.0 - keep) * fresh.val
+    out = out.astype(np.float32).astype(np.float64)
+    bnd = keep * boundary + (1.0 - keep) * fresh.boundary
+    off = np.abs(out)
+    off[diag] = 0.0
+    total = np.add.reduceat(off, row_ptr[:-1]) + bnd
+    d = total.astype(np.float32)
+    d = np.where(d.astype(np.float64) < total, np.nextafter(d, np.float32(np.inf)), d)
+    out[diag] = d.astype(np.float64)
+    return out, bnd
+
+
+def run_sequence(args):
+    """Successive pressure solves as outer iterations produce them: the graded
+    tet mesh, a right-hand side of 16 seeded Fourier modes over the cell
+    centroids whose phases drift 0.01 rad per solve, and D_f blended toward a
+    fresh seeded field with factor 0.7 every 50 solves, refreshing the
+    solvers then. Each solve starts from the previous solution (the learned
+    warm start is not built) and runs to rel_tol relative to its own initial
+    residual. Reports total and per-solve p50/p99 device time for the mixed
+    solve and for the plain FP32 AMG-PCG."""
+    import numpy as np
+    import torch
+    from kutta_b200 import linalg as L
+    torch.cuda.set_device(0)
+    s = _graded(args)
+    values, boundary = s.val.copy(), s.boundary.copy()
+    a = L.upload(s)
+    centroid = torch.from_numpy(s.centroid).cuda()
+    volume = torch.from_numpy(s.volume).cuda()
+    rng = np.random.default_rng(args.seed)
+    k = torch.from_numpy(rng.integers(1, 5, size=(16, 3)) * 2 * np.pi).cuda()
+    amp = torch.from_numpy(rng.normal(size=16)).cuda()
+    phase0 = torch.from_numpy(rng.uniform(0, 2 * np.pi, size=16)).cuda()
+
+    def rhs(t):
+        arg = centroid @ k.T + phase0 + 0.01 * t
+        return ((torch.sin(arg) @ amp) * volume).to(torch.float32)
+
+    control = L.SolveControl(args.rel_tol, 1e-30, args.max_iter)
+    arms = {"mixed": L.make_mixed_solver(s), "plain": L.make_solver(
+        L.SolverKind.AmgPcg, s, L.SolverOptions(structure=L.OperatorStructure.SymmetricMMatrix))}
+    x = {"mixed": torch.zeros(s.n, dtype=torch.float64, device="cuda"),
+         "plain": torch.zeros(s.n, dtype=torch.float32, device="cuda")}
+    times = {name: [] for name in arms}
+    refresh_ms = {name: 0.0 for name in arms}
+    iters = {name: [] for name in arms}
+    conv = {name: 0 for name in arms}
+    for name, solver in arms.items():
+        solver.refresh(a)
+    for t in range(args.solves):
+        if t > 0 and t % 50 == 0:
+            fresh = _graded(args, coeff_seed=1000 + t)
+            values, boundary = _blend(values, s.diag, boundary, s.row_ptr, fresh, 0.7)
+            a.val.copy_(torch.from_numpy(values.astype(np.float32)))
+            for name, solver in arms.items():
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                torch.cuda.synchronize()
+                e0.record()
+                solver.refresh(a)
+                e1.record()
+                torch.cuda.synchronize()
+                refresh_ms[name] += e0.elapsed_time(e1)
+        b = rhs(t)
+        for name, solver in arms.items():
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            torch.cuda.synchronize()
+            e0.record()
+            st = solver.solve(a, x[name], b, control)
+            e1.record()
+            torch.cuda.synchronize()
+            times[name].append(e0.elapsed_time(e1))
+            iters[name].append(st.iterations)
+            conv[name] += int(st.converged)
+    out = {"mode": "sequence", "solves": args.solves, "rel_tol": args.rel_tol,
+           "workload": f"graded_tet{args.size}: {args.size}^3 x 6 tets, 10-layer 1000:1 band at "
+                       f"z=0, D_f log-uniform [1e-6, 1], {s.n} cells, {s.nnz} nonzeros",
+           "warm_start": "previous solution (learned warm start: not built)"}
+    for name, solver in arms.items():
+        ts = sorted(times[name])
+        out[name] = {"method": solver.describe(), "total_ms": sum(ts),
+                     "p50_ms": ts[len(ts) // 2], "p99_ms": ts[min(len(ts) - 1, int(0.99 * len(ts)))],
+                     "refresh_ms_total": refresh_ms[name],
+                     "iterations_mean": float(np.mean(iters[name])),
+                     "converged": f"{conv[name]}/{args.solves}"}
+    return out
+
+
+def run_graded(args):
+    """One refresh + solve from zero to rel_tol on the graded tet matrix (the
+    mixed-precision configuration), mixed against plain, device-timed."""
+    import numpy as np
+    import scipy.sparse as sp
+    import torch
+    from kutta_b200 import linalg as L
+    torch.cuda.set_device(0)
+    s = _graded(args)
+    a = L.upload(s)
+    b = torch.from_numpy(s.b).cuda()
+    A = sp.csr_matrix((s.val, s.col, s.row_ptr), shape=(s.n, s.n))
+    control = L.SolveControl(args.rel_tol, 1e-30, args.max_iter)
+    out = {"mode": "graded", "rel_tol": args.rel_tol,
+           "workload": f"graded_tet{args.size}: {s.n} cells, {s.nnz} nonzeros"}
+    for name in ("mixed", "plain"):
+        if name == "mixed":
+            solver = L.make_mixed_solver(s)
+            x = torch.zeros(s.n, dtype=torch.float64, device="cuda")
+        else:
+            solver = L.make_solver(L.SolverKind.AmgPcg, s, L.SolverOptions(
+                structure=L.OperatorStructure.SymmetricMMatrix))
+            x = torch.zeros(s.n, dtype=torch.float32, device="cuda")
+        best = None
+        for _ in range(max(1, args.steps)):
+            x.zero_()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            torch.cuda.synchronize()
+            e0.record()
+            solver.refresh(a)
+            st = solver.solve(a, x, b, control)
+            e1.record()
+            torch.cuda.synchronize()
+            ms = e0.elapsed_time(e1)
+            best = ms if best is None else min(best, ms)
+        xr = x.cpu().numpy().astype(np.float64)
+        true = float(np.linalg.norm(s.b.astype(np.float64) - A @ xr) / st.initial_residual)
+        out[name] = {"method": solver.describe(), "ms_per_solve": best,
+                     "iterations": st.iterations, "converged": st.converged,
+                     "true_relative_residual_fp64": true}
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -408,13 +552,23 @@ def main():
     ap.add_argument("--plain-steps", type=int, default=3)
     ap.add_argument("--cpu-sample-iters", type=int, default=2)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--mode", default="bench", choices=["bench", "profile"],
-                    help="profile: one refresh + one solve (with --max-iter), for ncu captures")
+    ap.add_argument("--mode", default="bench", choices=["bench", "profile", "sequence", "graded"],
+                    help="profile: one refresh + one solve (with --max-iter), for ncu captures; "
+                         "sequence: successive warm-started solves on the graded mesh; "
+                         "graded: the graded matrix to --rel-tol (default 1e-8)")
     ap.add_argument("--method", default="mixed", choices=["mixed", "plain"])
+    ap.add_argument("--solves", type=int, default=300, help="sequence mode: number of solves")
+    ap.add_argument("--rel-tol", type=float, default=None,
+                    help="sequence / graded modes (defaults 1e-6 / 1e-8)")
     args = ap.parse_args()
     rank, world, local = _dist()
     if args.mode == "profile":
         profile_once(args)
+        return
+    if args.mode in ("sequence", "graded"):
+        if args.rel_tol is None:
+            args.rel_tol = 1e-6 if args.mode == "sequence" else 1e-8
+        print(json.dumps(run_sequence(args) if args.mode == "sequence" else run_graded(args)))
         return
     if args.impl == "reference":
         line = run_reference(args, rank, world)

@@ -31,6 +31,8 @@ typedef struct {
   double* volume; // n, cell volumes
   int* new_to_old;  // n, the renumbering applied (identity when none)
   int faces;        // interior faces
+  double* centroid; // 3n, cell centroids (x, y, z) in the stored order; NULL for poisson
+  double* boundary; // n, the Dirichlet boundary term in each diagonal; NULL for poisson
 } kh_system;
 
 // ---------------------------------------------------------------- random ----
@@ -57,7 +59,7 @@ static float float_up(long double value) {
 void kh_free(kh_system* s) {
   if (!s) return;
   free(s->row_ptr); free(s->col); free(s->diag); free(s->val);
-  free(s->b); free(s->volume); free(s->new_to_old);
+  free(s->b); free(s->volume); free(s->new_to_old); free(s->centroid); free(s->boundary);
   free(s);
 }
 
@@ -498,6 +500,8 @@ static kh_system* assemble(const kh_mesh* m, int renumber, double dmin, double d
   s->diag = (int*)malloc(sizeof(int) * (size_t)n);
   s->b = (float*)malloc(sizeof(float) * (size_t)n);
   s->volume = (double*)malloc(sizeof(double) * (size_t)n);
+  s->centroid = (double*)malloc(sizeof(double) * 3 * (size_t)n);
+  s->boundary = (double*)malloc(sizeof(double) * (size_t)n);
   s->new_to_old = new_to_old;
   // faces per old cell
   int* foff = deg;  // reuse adjacency offsets: same counts per cell
@@ -547,6 +551,10 @@ static kh_system* assemble(const kh_mesh* m, int renumber, double dmin, double d
     }
     s->row_ptr[r + 1] = nnz;
     s->volume[r] = m->volume[c];
+    s->centroid[3 * (size_t)r] = m->centroid[c].x;
+    s->centroid[3 * (size_t)r + 1] = m->centroid[c].y;
+    s->centroid[3 * (size_t)r + 2] = m->centroid[c].z;
+    s->boundary[r] = (double)bnd[c];
     s->b[r] = (float)(normal01(rng) * m->volume[c]);
   }
   free(row); free(fface); free(bnd); free(coef_on); free(coef_no); free(add_o); free(add_n);
@@ -558,14 +566,18 @@ static kh_system* assemble(const kh_mesh* m, int renumber, double dmin, double d
 // system on a jittered nx*ny*nz box, hexahedra (tet = 0) or six tets per hex.
 // band_layers > 0 grades the first layers at z = 0 (first height h/aspect, growth
 // ratio). Returns NULL on invalid sizes.
+// coeff_seed != 0 draws the coefficients (and right-hand side) from a stream of
+// its own, so one mesh can carry several coefficient fields; 0 continues the
+// mesh's stream.
 kh_system* kh_box_system(int nx, int ny, int nz, int tet, double jitter, int band_layers,
                          double aspect, double ratio, double dmin, double dmax,
-                         double convection, int renumber, uint64_t seed) {
+                         double convection, int renumber, uint64_t seed, uint64_t coeff_seed) {
   if (nx < 1 || ny < 1 || nz < 1) return NULL;
   uint64_t rng = seed * 0x2545F4914F6CDD1DULL + 0x1234567ULL;
   kh_mesh m;
   memset(&m, 0, sizeof(m));
   if (build_mesh(&m, nx, ny, nz, tet, jitter, band_layers, aspect, ratio, &rng) != 0) return NULL;
+  if (coeff_seed != 0) rng = coeff_seed * 0x9E3779B97F4A7C15ULL + 0x7654321ULL;
   kh_system* s = assemble(&m, renumber, dmin, dmax, convection, &rng);
   mesh_free(&m);
   return s;

@@ -28,6 +28,7 @@ class _KhSystem(ctypes.Structure):
         ("diag", ctypes.POINTER(ctypes.c_int)), ("val", ctypes.POINTER(ctypes.c_double)),
         ("b", ctypes.POINTER(ctypes.c_float)), ("volume", ctypes.POINTER(ctypes.c_double)),
         ("new_to_old", ctypes.POINTER(ctypes.c_int)), ("faces", ctypes.c_int),
+        ("centroid", ctypes.POINTER(ctypes.c_double)), ("boundary", ctypes.POINTER(ctypes.c_double)),
     ]
 
 
@@ -48,7 +49,8 @@ def _load():
         lib.kh_box_system.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                       ctypes.c_double, ctypes.c_int, ctypes.c_double,
                                       ctypes.c_double, ctypes.c_double, ctypes.c_double,
-                                      ctypes.c_double, ctypes.c_int, ctypes.c_uint64]
+                                      ctypes.c_double, ctypes.c_int, ctypes.c_uint64,
+                                      ctypes.c_uint64]
         lib.kh_free.argtypes = [ctypes.POINTER(_KhSystem)]
         lib.kh_hash.restype = ctypes.c_uint32
         lib.kh_hash.argtypes = [ctypes.c_uint32]
@@ -67,6 +69,8 @@ class HostSystem:
     volume: np.ndarray | None = None
     new_to_old: np.ndarray | None = None
     name: str = ""
+    centroid: np.ndarray | None = None   # float64[n, 3] (box meshes)
+    boundary: np.ndarray | None = None   # float64[n], Dirichlet term in each diagonal
 
     @property
     def n(self) -> int:
@@ -96,6 +100,9 @@ def _take(ptr) -> HostSystem:
         diag=arr(s.diag, n, np.int32), val=arr(s.val, nnz, np.float64),
         b=arr(s.b, n, np.float32), volume=arr(s.volume, n, np.float64),
         new_to_old=arr(s.new_to_old, n, np.int32))
+    if s.centroid:
+        out.centroid = arr(s.centroid, 3 * n, np.float64).reshape(n, 3)
+        out.boundary = arr(s.boundary, n, np.float64)
     _load().kh_free(ptr)
     return out
 
@@ -136,10 +143,12 @@ def random_solution(n: int) -> np.ndarray:
 def box_system(nx: int, ny: int, nz: int, *, tet: bool, seed: int, jitter: float = 0.15,
                band_layers: int = 0, aspect: float = 1000.0, ratio: float = 1.2,
                dmin: float = 1e-3, dmax: float = 1.0, convection: float = 0.0,
-               renumber: bool = True) -> HostSystem:
-    """Finite-volume pressure (or convection-diffusion) system on a jittered box."""
+               renumber: bool = True, coeff_seed: int = 0) -> HostSystem:
+    """Finite-volume pressure (or convection-diffusion) system on a jittered box.
+    `seed` fixes the mesh; a nonzero `coeff_seed` draws the coefficient field
+    and right-hand side from a stream of its own (same mesh, another field)."""
     s = _take(_load().kh_box_system(nx, ny, nz, int(tet), jitter, band_layers, aspect, ratio,
-                                    dmin, dmax, convection, int(renumber), seed))
+                                    dmin, dmax, convection, int(renumber), seed, coeff_seed))
     s.name = (f"{'tet6' if tet else 'hex'}{nx}x{ny}x{nz}-seed{seed}"
               + (f"-band{band_layers}" if band_layers else "")
               + (f"-conv{convection}" if convection > 0 else ""))
