@@ -238,6 +238,33 @@ int b2_mixed_hierarchy_build(int n, int nnz, const int32_t* row_ptr, const int32
                              const int32_t* diag, const double* val,
                              const b2_mixed_options* options, b2_hierarchy** out);
 
+/* ---- Learned preconditioner stage (no reference counterpart) --------------
+ * A message-passing network over the graph of the fine matrix (3 layers,
+ * hidden width 32, FP32; edge features w_ij = -a_ij / sqrt(a_ii a_jj), node
+ * scale 1 / sqrt(a_ii)) mapping a residual r to a correction G(r) ~ A^-1 r.
+ * Trained with b2_gnn_train_step on (matrix, right-hand side, solution)
+ * triples, loss |G(b) - x|^2 / |x|^2, one Adam step per call. Attached to a
+ * mixed solver it runs after each AMG cycle: z = M(r) + G(r - A M(r)). */
+typedef struct b2_gnn b2_gnn;
+int b2_gnn_create(uint64_t seed, b2_gnn** out);
+void b2_gnn_destroy(b2_gnn* g);
+int b2_gnn_parameter_count(void);
+/* Binds the graph of a device CSR matrix (n rows); keep the arrays alive while
+ * bound and bind again after its values change. */
+int b2_gnn_bind(b2_gnn* g, int n, const int32_t* d_row_ptr, const int32_t* d_col,
+                const int32_t* d_diag, const float* d_val, void* stream);
+/* d_z = beta d_z + G(d_r), beta 0 or 1. */
+int b2_gnn_apply(b2_gnn* g, const float* d_r, float* d_z, float beta, void* stream);
+/* One training step on (d_b, d_x) with |x|^2 = x_norm2; *loss before the step. */
+int b2_gnn_train_step(b2_gnn* g, const float* d_b, const float* d_x, double x_norm2,
+                      float learning_rate, float* loss, void* stream);
+int b2_gnn_get_weights(const b2_gnn* g, float* host, size_t count);
+int b2_gnn_set_weights(b2_gnn* g, const float* host, size_t count);
+/* Attaches g (NULL detaches) to a mixed solver; it is bound to the solver's
+ * matrix at once if refreshed, and again at every refresh. g must outlive the
+ * attachment. */
+int b2_mixed_set_learned(b2_mixed* solver, b2_gnn* g);
+
 /* Hierarchy introspection (the captured-hierarchy checks of the reference's
  * tests/linalg/test_solvers.cpp:487-555 read the same data back from launches).
  * Level 0 is the input matrix. Copies are synchronous device-to-host reads on

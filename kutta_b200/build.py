@@ -41,9 +41,11 @@ PRODUCT_CU = {
     "exact_kernels.cu": EXACT,
     "mixed_kernels.cu": [],
     "tail_cycle.cu": [],
+    "learned.cu": [],
     "noalloc.cu": [],
 }
-PRODUCT_CPP = ["host/setup.cpp", "host/solver.cpp", "host/mixed.cpp", "capi.cpp"]
+PRODUCT_CPP = ["host/setup.cpp", "host/solver.cpp", "host/mixed.cpp", "host/learned.cpp",
+               "capi.cpp"]
 
 
 def _hash(paths, extra=""):

@@ -27,6 +27,9 @@ struct b2_hierarchy {
 struct b2_mixed {
   std::unique_ptr<kb2::MixedSolver> s;
 };
+struct b2_gnn {
+  std::unique_ptr<kb2::Gnn> g;
+};
 
 namespace {
 thread_local std::string g_error;
@@ -456,6 +459,68 @@ int b2_mixed_profile(b2_mixed* s, int enable) {
   return guarded([&] {
     KB2_REQUIRE(s && s->s, "solver: null handle");
     s->s->inner().set_profile(enable != 0);
+  });
+}
+
+int b2_gnn_create(uint64_t seed, b2_gnn** out) {
+  return guarded([&] {
+    KB2_REQUIRE(out != nullptr, "learned stage: null output handle");
+    *out = nullptr;
+    *out = new b2_gnn{std::make_unique<kb2::Gnn>(seed)};
+  });
+}
+
+void b2_gnn_destroy(b2_gnn* g) { delete g; }
+
+int b2_gnn_parameter_count(void) { return kb2::Gnn::parameter_count(); }
+
+int b2_gnn_bind(b2_gnn* g, int n, const int32_t* d_row_ptr, const int32_t* d_col,
+                const int32_t* d_diag, const float* d_val, void* stream) {
+  return guarded([&] {
+    KB2_REQUIRE(g && g->g, "learned stage: null handle");
+    g->g->bind(n, d_row_ptr, d_col, d_diag, d_val, as_stream(stream));
+  });
+}
+
+int b2_gnn_apply(b2_gnn* g, const float* d_r, float* d_z, float beta, void* stream) {
+  return guarded([&] {
+    KB2_REQUIRE(g && g->g && d_r && d_z, "learned stage: null argument");
+    KB2_REQUIRE(beta == 0.0f || beta == 1.0f, "learned stage: beta must be 0 or 1");
+    g->g->forward(d_r, d_z, beta, as_stream(stream));
+  });
+}
+
+int b2_gnn_train_step(b2_gnn* g, const float* d_b, const float* d_x, double x_norm2,
+                      float learning_rate, float* loss, void* stream) {
+  return guarded([&] {
+    KB2_REQUIRE(g && g->g && d_b && d_x, "learned stage: null argument");
+    KB2_REQUIRE(learning_rate > 0 && std::isfinite(learning_rate),
+                "learned stage: invalid learning rate");
+    const float l = g->g->train_step(d_b, d_x, x_norm2, learning_rate, as_stream(stream));
+    if (loss) *loss = l;
+  });
+}
+
+int b2_gnn_get_weights(const b2_gnn* g, float* host, size_t count) {
+  return guarded([&] {
+    KB2_REQUIRE(g && g->g && host, "learned stage: null argument");
+    const auto w = g->g->weights();
+    KB2_REQUIRE(count == w.size(), "learned stage: wrong number of weights");
+    std::memcpy(host, w.data(), sizeof(float) * w.size());
+  });
+}
+
+int b2_gnn_set_weights(b2_gnn* g, const float* host, size_t count) {
+  return guarded([&] {
+    KB2_REQUIRE(g && g->g && host, "learned stage: null argument");
+    g->g->set_weights(std::vector<float>(host, host + count));
+  });
+}
+
+int b2_mixed_set_learned(b2_mixed* s, b2_gnn* g) {
+  return guarded([&] {
+    KB2_REQUIRE(s && s->s, "solver: null handle");
+    s->s->inner().set_learned(g ? g->g.get() : nullptr);
   });
 }
 

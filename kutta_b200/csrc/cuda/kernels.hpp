@@ -177,6 +177,34 @@ bool tail_cluster_fits(int cluster, int smem_bytes);
 // while status[0] != 0.
 void tail_cycle(const TailPlan& plan, const int* status, cudaStream_t s);
 
+// ---- learned preconditioner stage (learned.cu) ------------------------------
+// Edge weights w_ij = -a_ij / sqrt(a_ii a_jj) (0 on the diagonal) and node
+// scales 1 / sqrt(a_ii) from the matrix values.
+void gnn_graph(int n, const int* rows, const int* cols, const int* diag, const float* vals,
+               float* edge, float* node_scale, cudaStream_t s);
+// H0 = node_scale * r.
+void gnn_input(int n, const float* r, const float* node_scale, float* H0, cudaStream_t s);
+// M = W H for C <= 32 channels (row-major n x C).
+void gnn_aggregate(int n, int C, const int* rows, const int* cols, const float* edge,
+                   const float* H, float* M, cudaStream_t s);
+// out = relu(Ws H + Wn M + b), Cin -> 32 channels.
+void gnn_dense(int n, int Cin, const float* H, const float* M, const float* Ws, const float* Wn,
+               const float* bias, float* out, cudaStream_t s);
+// z = beta z + node_scale * (H wo).
+void gnn_output(int n, const float* H, const float* wo, const float* node_scale, float* z,
+                float beta, cudaStream_t s);
+// dz = 2 (z - x) inv_norm2; loss += |z - x|^2 inv_norm2 (atomic).
+void gnn_loss(int n, const float* z, const float* x, float inv_norm2, float* dz, float* loss,
+              cudaStream_t s);
+void gnn_output_back(int n, const float* H, const float* wo, const float* node_scale,
+                     const float* dz, float* dH, float* dwo, cudaStream_t s);
+void gnn_dense_back(int n, int Cin, const float* H, const float* M, const float* out,
+                    const float* dOut, const float* Ws, const float* Wn, float* dH, float* dM,
+                    float* dWs, float* dWn, float* db, cudaStream_t s);
+void gnn_add(std::size_t count, const float* a, const float* b, float* out, cudaStream_t s);
+void gnn_adam(int count, float* w, const float* g, float* m, float* v, float lr, float beta1,
+              float beta2, float eps, float correction1, float correction2, cudaStream_t s);
+
 // ---- single-thread scalar kernels -------------------------------------------
 void solver_limits(float* scalars, float th, float tl, float dh, float dl, cudaStream_t s);
 void solver_reset(float* scalars, int* status, int iterations, cudaStream_t s);

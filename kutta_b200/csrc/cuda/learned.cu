@@ -1,0 +1,305 @@
+// Learned preconditioner stage (no reference counterpart): a small
+// message-passing network over the matrix graph (the cell-face graph of the
+// pressure operator), its backward pass and an Adam step, all in FP32.
+//
+// Graph features come from the matrix alone (the solver sees no geometry):
+// edge weight w_ij = -a_ij / sqrt(a_ii a_jj), node scale s_i = 1 / sqrt(a_ii).
+// Layer l maps H (n x Cin) to H' (n x 32):
+//   M = W H  (M_i = sum_j w_ij H_j),   H'_i = relu(Ws H_i + Wn M_i + b);
+// the output is z_i = s_i (wo . H3_i). Since w is symmetric, the backward of
+// the aggregation is the aggregation itself.
+//
+// Activations are row-major n x C; a warp handles one row with lane = output
+// channel (C <= 32), so a row of H is one 128-byte read.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+
+#include "common.cuh"
+#include "kernels.hpp"
+
+namespace kb2 {
+namespace {
+using namespace dev;
+
+constexpr int kHidden = 32;
+
+#define ROWS(i, n) \
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < (n); i += gridDim.x * blockDim.x)
+
+// Warp-per-row loop (uniform per warp).
+#define WARP_ROWS(i, n)                                                                \
+  for (int i = static_cast<int>((blockIdx.x * blockDim.x + threadIdx.x) >> 5); i < (n); \
+       i += static_cast<int>((gridDim.x * blockDim.x) >> 5))
+
+__global__ void k_gnn_graph(int n, const int* __restrict__ rows, const int* __restrict__ cols,
+                            const int* __restrict__ diag, const float* __restrict__ vals,
+                            float* __restrict__ edge, float* __restrict__ node_scale) {
+  ROWS(i, n) {
+    const float di = vals[diag[i]];
+    node_scale[i] = di > 0.0f ? rsqrtf(di) : 0.0f;
+    for (int j = rows[i]; j < rows[i + 1]; ++j) {
+      const int c = cols[j];
+      const float dc = vals[diag[c]];
+      edge[j] = (c == i || di <= 0.0f || dc <= 0.0f) ? 0.0f : -vals[j] * rsqrtf(di * dc);
+    }
+  }
+}
+
+// M = W H (C channels).
+__global__ void k_gnn_aggregate(int n, int C, const int* __restrict__ rows,
+                                const int* __restrict__ cols, const float* __restrict__ edge,
+                                const float* __restrict__ H, float* __restrict__ M) {
+  const int lane = threadIdx.x & 31;
+  WARP_ROWS(i, n) {
+    float acc = 0.0f;
+    const int end = rows[i + 1];
+    for (int j = rows[i]; j < end; ++j) {
+      const float w = edge[j];
+      if (lane < C && w != 0.0f) acc = fmaf(w, H[static_cast<std::size_t>(cols[j]) * C + lane], acc);
+    }
+    if (lane < C) M[static_cast<std::size_t>(i) * C + lane] = acc;
+  }
+}
+
+// H'_i = relu(Ws H_i + Wn M_i + b): weights [Cout=32][Cin] in shared memory,
+// lane = output channel; the row's inputs are broadcast by shuffles.
+__global__ void k_gnn_dense(int n, int Cin, const float* __restrict__ H,
+                            const float* __restrict__ M, const float* __restrict__ Ws,
+                            const float* __restrict__ Wn, const float* __restrict__ bias,
+                            float* __restrict__ out) {
+  __shared__ float ws[kHidden * kHidden], wn[kHidden * kHidden], bs[kHidden];
+  for (int k = threadIdx.x; k < kHidden * Cin; k += blockDim.x) {
+    ws[k] = Ws[k];
+    wn[k] = Wn[k];
+  }
+  if (threadIdx.x < kHidden) bs[threadIdx.x] = bias[threadIdx.x];
+  __syncthreads();
+  const int lane = threadIdx.x & 31;
+  WARP_ROWS(i, n) {
+    const float h = lane < Cin ? H[static_cast<std::size_t>(i) * Cin + lane] : 0.0f;
+    const float m = lane < Cin ? M[static_cast<std::size_t>(i) * Cin + lane] : 0.0f;
+    float acc = bs[lane];
+    for (int k = 0; k < Cin; ++k) {
+      const float hk = __shfl_sync(0xffffffffu, h, k);
+      const float mk = __shfl_sync(0xffffffffu, m, k);
+      acc = fmaf(ws[lane * Cin + k], hk, acc);
+      acc = fmaf(wn[lane * Cin + k], mk, acc);
+    }
+    out[static_cast<std::size_t>(i) * kHidden + lane] = fmaxf(acc, 0.0f);
+  }
+}
+
+// z_i = s_i (wo . H_i).
+__global__ void k_gnn_output(int n, const float* __restrict__ H, const float* __restrict__ wo,
+                             const float* __restrict__ node_scale, float* __restrict__ z,
+                             float beta) {
+  const int lane = threadIdx.x & 31;
+  const float w = wo[lane];
+  WARP_ROWS(i, n) {
+    float v = w * H[static_cast<std::size_t>(i) * kHidden + lane];
+    for (int d = 16; d > 0; d >>= 1) v += __shfl_down_sync(0xffffffffu, v, d);
+    if (lane == 0) z[i] = (beta != 0.0f ? beta * z[i] : 0.0f) + node_scale[i] * v;
+  }
+}
+
+// Input layer features: H0_i = s_i r_i.
+__global__ void k_gnn_input(int n, const float* __restrict__ r, const float* __restrict__ node_scale,
+                            float* __restrict__ H0) {
+  ROWS(i, n) H0[i] = node_scale[i] * r[i];
+}
+
+// ---- training -------------------------------------------------------------
+// Loss: |z - x|^2 / |x|^2 (x the solver's solution). dz = 2 (z - x) / |x|^2;
+// the loss itself accumulated (atomically) into loss[0].
+__global__ void k_gnn_loss(int n, const float* __restrict__ z, const float* __restrict__ x,
+                           float inv_norm2, float* __restrict__ dz, float* loss) {
+  float acc = 0.0f;
+  ROWS(i, n) {
+    const float d = z[i] - x[i];
+    dz[i] = 2.0f * d * inv_norm2;
+    acc += d * d;
+  }
+  for (int d = 16; d > 0; d >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, d);
+  if ((threadIdx.x & 31) == 0) atomicAdd(loss, acc * inv_norm2);
+}
+
+// Output backward: dH_i = dz_i s_i wo, dwo += sum_i dz_i s_i H_i.
+__global__ void k_gnn_output_back(int n, const float* __restrict__ H, const float* __restrict__ wo,
+                                  const float* __restrict__ node_scale,
+                                  const float* __restrict__ dz, float* __restrict__ dH,
+                                  float* __restrict__ dwo) {
+  const int lane = threadIdx.x & 31;
+  const float w = wo[lane];
+  float g = 0.0f;
+  WARP_ROWS(i, n) {
+    const float t = dz[i] * node_scale[i];
+    const std::size_t k = static_cast<std::size_t>(i) * kHidden + lane;
+    dH[k] = t * w;
+    g = fmaf(t, H[k], g);
+  }
+  atomicAdd(dwo + lane, g);
+}
+
+// Dense layer backward. G = dOut * (out > 0); dH_i = Ws^T G_i, dM_i = Wn^T G_i;
+// dWs += G_i H_i^T, dWn += G_i M_i^T, db += G_i (per-warp sums, then atomics).
+__global__ void k_gnn_dense_back(int n, int Cin, const float* __restrict__ H,
+                                 const float* __restrict__ M, const float* __restrict__ out,
+                                 const float* __restrict__ dOut, const float* __restrict__ Ws,
+                                 const float* __restrict__ Wn, float* __restrict__ dH,
+                                 float* __restrict__ dM, float* __restrict__ dWs,
+                                 float* __restrict__ dWn, float* __restrict__ db) {
+  __shared__ float ws[kHidden * kHidden], wn[kHidden * kHidden];
+  __shared__ float gws[kHidden * kHidden], gwn[kHidden * kHidden], gb[kHidden];
+  for (int k = threadIdx.x; k < kHidden * Cin; k += blockDim.x) {
+    ws[k] = Ws[k];
+    wn[k] = Wn[k];
+    gws[k] = 0.0f;
+    gwn[k] = 0.0f;
+  }
+  if (threadIdx.x < kHidden) gb[threadIdx.x] = 0.0f;
+  __syncthreads();
+  const int lane = threadIdx.x & 31;
+  // Per-lane accumulators for this lane's output channel c = lane.
+  float aws[kHidden], awn[kHidden];
+#pragma unroll
+  for (int k = 0; k < kHidden; ++k) aws[k] = awn[k] = 0.0f;
+  float ab = 0.0f;
+  WARP_ROWS(i, n) {
+    const std::size_t row = static_cast<std::size_t>(i);
+    const float o = out[row * kHidden + lane];
+    const float g = o > 0.0f ? dOut[row * kHidden + lane] : 0.0f;  // channel c = lane
+    const float h = lane < Cin ? H[row * Cin + lane] : 0.0f;
+    const float m = lane < Cin ? M[row * Cin + lane] : 0.0f;
+    ab += g;
+    // dH_i[k] = sum_c Ws[c][k] g_c; lane k gathers over c by shuffles.
+    float dh = 0.0f, dm = 0.0f;
+#pragma unroll
+    for (int c = 0; c < kHidden; ++c) {
+      const float gc = __shfl_sync(0xffffffffu, g, c);
+      if (lane < Cin) {
+        dh = fmaf(ws[c * Cin + lane], gc, dh);
+        dm = fmaf(wn[c * Cin + lane], gc, dm);
+      }
+    }
+    if (lane < Cin) {
+      dH[row * Cin + lane] = dh;
+      dM[row * Cin + lane] = dm;
+    }
+#pragma unroll
+    for (int k = 0; k < kHidden; ++k) {
+      if (k < Cin) {
+        aws[k] = fmaf(g, __shfl_sync(0xffffffffu, h, k), aws[k]);
+        awn[k] = fmaf(g, __shfl_sync(0xffffffffu, m, k), awn[k]);
+      }
+    }
+  }
+#pragma unroll
+  for (int k = 0; k < kHidden; ++k)
+    if (k < Cin) {
+      atomicAdd(&gws[lane * Cin + k], aws[k]);
+      atomicAdd(&gwn[lane * Cin + k], awn[k]);
+    }
+  atomicAdd(&gb[lane], ab);
+  __syncthreads();
+  for (int k = threadIdx.x; k < kHidden * Cin; k += blockDim.x) {
+    atomicAdd(dWs + k, gws[k]);
+    atomicAdd(dWn + k, gwn[k]);
+  }
+  if (threadIdx.x < kHidden) atomicAdd(db + threadIdx.x, gb[threadIdx.x]);
+}
+
+// out = a + b (elementwise).
+__global__ void k_gnn_add(std::size_t count, const float* __restrict__ a,
+                          const float* __restrict__ b, float* __restrict__ out) {
+  for (std::size_t k = blockIdx.x * blockDim.x + threadIdx.x; k < count;
+       k += static_cast<std::size_t>(gridDim.x) * blockDim.x)
+    out[k] = a[k] + b[k];
+}
+
+// Adam with bias correction (step t >= 1).
+__global__ void k_gnn_adam(int count, float* __restrict__ w, const float* __restrict__ g,
+                           float* __restrict__ m, float* __restrict__ v, float lr, float beta1,
+                           float beta2, float eps, float correction1, float correction2) {
+  ROWS(k, count) {
+    const float gk = g[k];
+    m[k] = beta1 * m[k] + (1.0f - beta1) * gk;
+    v[k] = beta2 * v[k] + (1.0f - beta2) * gk * gk;
+    w[k] -= lr * (m[k] / correction1) / (sqrtf(v[k] / correction2) + eps);
+  }
+}
+
+int warp_grid(int n) {
+  const long long blocks = (static_cast<long long>(n) * 32 + kBlock - 1) / kBlock;
+  return static_cast<int>(std::max(1LL, std::min(blocks, static_cast<long long>(kMaxBlocks))));
+}
+
+}  // namespace
+
+namespace launch {
+
+void gnn_graph(int n, const int* rows, const int* cols, const int* diag, const float* vals,
+               float* edge, float* node_scale, cudaStream_t s) {
+  if (n <= 0) return;
+  ++counter;
+  k_gnn_graph<<<grid_for(n), kBlock, 0, s>>>(n, rows, cols, diag, vals, edge, node_scale);
+}
+void gnn_input(int n, const float* r, const float* node_scale, float* H0, cudaStream_t s) {
+  if (n <= 0) return;
+  ++counter;
+  k_gnn_input<<<grid_for(n), kBlock, 0, s>>>(n, r, node_scale, H0);
+}
+void gnn_aggregate(int n, int C, const int* rows, const int* cols, const float* edge,
+                   const float* H, float* M, cudaStream_t s) {
+  if (n <= 0) return;
+  ++counter;
+  k_gnn_aggregate<<<warp_grid(n), kBlock, 0, s>>>(n, C, rows, cols, edge, H, M);
+}
+void gnn_dense(int n, int Cin, const float* H, const float* M, const float* Ws, const float* Wn,
+               const float* bias, float* out, cudaStream_t s) {
+  if (n <= 0) return;
+  ++counter;
+  k_gnn_dense<<<warp_grid(n), kBlock, 0, s>>>(n, Cin, H, M, Ws, Wn, bias, out);
+}
+void gnn_output(int n, const float* H, const float* wo, const float* node_scale, float* z,
+                float beta, cudaStream_t s) {
+  if (n <= 0) return;
+  ++counter;
+  k_gnn_output<<<warp_grid(n), kBlock, 0, s>>>(n, H, wo, node_scale, z, beta);
+}
+void gnn_loss(int n, const float* z, const float* x, float inv_norm2, float* dz, float* loss,
+              cudaStream_t s) {
+  if (n <= 0) return;
+  ++counter;
+  k_gnn_loss<<<grid_for(n), kBlock, 0, s>>>(n, z, x, inv_norm2, dz, loss);
+}
+void gnn_output_back(int n, const float* H, const float* wo, const float* node_scale,
+                     const float* dz, float* dH, float* dwo, cudaStream_t s) {
+  if (n <= 0) return;
+  ++counter;
+  k_gnn_output_back<<<warp_grid(n), kBlock, 0, s>>>(n, H, wo, node_scale, dz, dH, dwo);
+}
+void gnn_dense_back(int n, int Cin, const float* H, const float* M, const float* out,
+                    const float* dOut, const float* Ws, const float* Wn, float* dH, float* dM,
+                    float* dWs, float* dWn, float* db, cudaStream_t s) {
+  if (n <= 0) return;
+  ++counter;
+  k_gnn_dense_back<<<warp_grid(n), kBlock, 0, s>>>(n, Cin, H, M, out, dOut, Ws, Wn, dH, dM, dWs,
+                                                   dWn, db);
+}
+void gnn_add(std::size_t count, const float* a, const float* b, float* out, cudaStream_t s) {
+  if (count == 0) return;
+  ++counter;
+  const int blocks = static_cast<int>(std::min<std::size_t>((count + kBlock - 1) / kBlock, kMaxBlocks));
+  k_gnn_add<<<blocks, kBlock, 0, s>>>(count, a, b, out);
+}
+void gnn_adam(int count, float* w, const float* g, float* m, float* v, float lr, float beta1,
+              float beta2, float eps, float correction1, float correction2, cudaStream_t s) {
+  if (count <= 0) return;
+  ++counter;
+  k_gnn_adam<<<grid_for(count), kBlock, 0, s>>>(count, w, g, m, v, lr, beta1, beta2, eps,
+                                                correction1, correction2);
+}
+
+}  // namespace launch
+}  // namespace kb2

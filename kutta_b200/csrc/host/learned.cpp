@@ -1,0 +1,154 @@
+// Learned preconditioner stage: parameters, activations, forward, training.
+#include "learned.hpp"
+
+#include <cmath>
+
+#include "../cuda/kernels.hpp"
+
+namespace kb2 {
+
+namespace {
+std::uint64_t mix(std::uint64_t& state) {
+  std::uint64_t z = (state += 0x9e3779b97f4a7c15ULL);
+  z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ULL;
+  z = (z ^ (z >> 27)) * 0x94d049bb133111ebULL;
+  return z ^ (z >> 31);
+}
+double uniform(std::uint64_t& state) { return static_cast<double>(mix(state) >> 11) * 0x1.0p-53; }
+
+int cin(int layer) { return layer == 0 ? 1 : Gnn::kHidden; }
+}  // namespace
+
+int Gnn::parameter_count() {
+  int count = kHidden;  // wo
+  for (int l = 0; l < kLayers; ++l) count += 2 * kHidden * cin(l) + kHidden;
+  return count;
+}
+
+Gnn::Slices Gnn::slices(float* base) const {
+  Slices s{};
+  float* p = base;
+  for (int l = 0; l < kLayers; ++l) {
+    s.ws[l] = p;
+    p += kHidden * cin(l);
+    s.wn[l] = p;
+    p += kHidden * cin(l);
+    s.b[l] = p;
+    p += kHidden;
+  }
+  s.wo = p;
+  return s;
+}
+
+// Uniform Glorot-style initialisation (fan-in 2 Cin for the two halves of a
+// layer), zero biases, small output weights.
+Gnn::Gnn(std::uint64_t seed) {
+  const int count = parameter_count();
+  std::vector<float> w(static_cast<std::size_t>(count), 0.0f);
+  std::uint64_t state = seed * 0x2545F4914F6CDD1DULL + 1;
+  std::size_t k = 0;
+  for (int l = 0; l < kLayers; ++l) {
+    const double limit = std::sqrt(6.0 / (2.0 * cin(l) + kHidden));
+    for (int half = 0; half < 2; ++half)
+      for (int e = 0; e < kHidden * cin(l); ++e)
+        w[k++] = static_cast<float>((2.0 * uniform(state) - 1.0) * limit);
+    k += kHidden;  // biases stay 0
+  }
+  for (int c = 0; c < kHidden; ++c) w[k++] = static_cast<float>((2.0 * uniform(state) - 1.0) * 0.1);
+  params_.upload(w, nullptr);
+  grads_.reset(static_cast<std::size_t>(count));
+  m_.reset(static_cast<std::size_t>(count));
+  v_.reset(static_cast<std::size_t>(count));
+  cuda_check(cudaMemset(m_.get(), 0, sizeof(float) * count), "memset");
+  cuda_check(cudaMemset(v_.get(), 0, sizeof(float) * count), "memset");
+  loss_.reset(1);
+}
+
+void Gnn::bind(int n, const int* rows, const int* cols, const int* diag, const float* vals,
+               cudaStream_t s) {
+  KB2_REQUIRE(n > 0 && rows && cols && diag && vals, "learned stage: invalid matrix");
+  if (n != n_) {
+    const auto rows_n = static_cast<std::size_t>(n);
+    const auto wide = rows_n * kHidden;
+    h_[0].reset(rows_n);
+    for (int l = 1; l <= kLayers; ++l) h_[l].reset(wide);
+    m_agg_[0].reset(rows_n);
+    for (int l = 1; l < kLayers; ++l) m_agg_[l].reset(wide);
+    dz_.reset(rows_n);
+    z_.reset(rows_n);
+    dh_.reset(wide);
+    dhs_.reset(wide);
+    dm_.reset(wide);
+    dagg_.reset(wide);
+    scale_.reset(rows_n);
+  }
+  int nnz = 0;
+  cuda_check(cudaMemcpy(&nnz, rows + n, sizeof(int), cudaMemcpyDeviceToHost), "learned stage");
+  if (edge_.size() != static_cast<std::size_t>(nnz)) edge_.reset(static_cast<std::size_t>(nnz));
+  n_ = n;
+  rows_ = rows;
+  cols_ = cols;
+  launch::gnn_graph(n, rows, cols, diag, vals, edge_.get(), scale_.get(), s);
+}
+
+void Gnn::forward(const float* r, float* z, float beta, cudaStream_t s) {
+  KB2_REQUIRE(n_ > 0, "learned stage: no matrix bound");
+  const Slices p = slices(params_.get());
+  launch::gnn_input(n_, r, scale_.get(), h_[0].get(), s);
+  for (int l = 0; l < kLayers; ++l) {
+    launch::gnn_aggregate(n_, cin(l), rows_, cols_, edge_.get(), h_[l].get(), m_agg_[l].get(), s);
+    launch::gnn_dense(n_, cin(l), h_[l].get(), m_agg_[l].get(), p.ws[l], p.wn[l], p.b[l],
+                      h_[l + 1].get(), s);
+  }
+  launch::gnn_output(n_, h_[kLayers].get(), p.wo, scale_.get(), z, beta, s);
+}
+
+float Gnn::train_step(const float* b, const float* x, double x_norm2, float lr, cudaStream_t s) {
+  KB2_REQUIRE(x_norm2 > 0 && std::isfinite(x_norm2), "learned stage: invalid target norm");
+  const int count = parameter_count();
+  forward(b, z_.get(), 0.0f, s);
+  cuda_check(cudaMemsetAsync(grads_.get(), 0, sizeof(float) * count, s), "memset");
+  cuda_check(cudaMemsetAsync(loss_.get(), 0, sizeof(float), s), "memset");
+  const Slices p = slices(params_.get());
+  const Slices g = slices(grads_.get());
+  launch::gnn_loss(n_, z_.get(), x, static_cast<float>(1.0 / x_norm2), dz_.get(), loss_.get(), s);
+  launch::gnn_output_back(n_, h_[kLayers].get(), p.wo, scale_.get(), dz_.get(), dh_.get(), g.wo, s);
+  for (int l = kLayers - 1; l >= 0; --l) {
+    launch::gnn_dense_back(n_, cin(l), h_[l].get(), m_agg_[l].get(), h_[l + 1].get(), dh_.get(),
+                           p.ws[l], p.wn[l], dhs_.get(), dm_.get(), g.ws[l], g.wn[l], g.b[l], s);
+    if (l > 0) {
+      // dL/dh[l] = Ws^T G + W^T (Wn^T G); W is symmetric.
+      launch::gnn_aggregate(n_, cin(l), rows_, cols_, edge_.get(), dm_.get(), dagg_.get(), s);
+      launch::gnn_add(static_cast<std::size_t>(n_) * cin(l), dhs_.get(), dagg_.get(), dh_.get(), s);
+    }
+  }
+  ++step_;
+  const float beta1 = 0.9f, beta2 = 0.999f;
+  launch::gnn_adam(count, params_.get(), grads_.get(), m_.get(), v_.get(), lr, beta1, beta2, 1e-8f,
+                   1.0f - std::pow(beta1, static_cast<float>(step_)),
+                   1.0f - std::pow(beta2, static_cast<float>(step_)), s);
+  float loss = 0;
+  cuda_check(cudaMemcpyAsync(&loss, loss_.get(), sizeof(float), cudaMemcpyDeviceToHost, s),
+             "loss readback");
+  wait(s);
+  return loss;
+}
+
+std::vector<float> Gnn::weights() const {
+  std::vector<float> w(static_cast<std::size_t>(parameter_count()));
+  cuda_check(cudaMemcpy(w.data(), params_.get(), sizeof(float) * w.size(), cudaMemcpyDeviceToHost),
+             "weights");
+  return w;
+}
+
+void Gnn::set_weights(const std::vector<float>& w) {
+  KB2_REQUIRE(w.size() == static_cast<std::size_t>(parameter_count()),
+              "learned stage: wrong number of weights");
+  cuda_check(cudaMemcpy(params_.get(), w.data(), sizeof(float) * w.size(), cudaMemcpyHostToDevice),
+             "weights");
+  step_ = 0;
+  cuda_check(cudaMemset(m_.get(), 0, sizeof(float) * w.size()), "memset");
+  cuda_check(cudaMemset(v_.get(), 0, sizeof(float) * w.size()), "memset");
+}
+
+}  // namespace kb2

@@ -503,13 +503,38 @@ void Solver::inner(std::size_t index, const int* parent) {
 // (solver.cpp:65-68) preconditioner.
 void Solver::apply(const float* r, float*& z) {
   if (amg() && graphing()) {
-    graphed(r, z, 0, z, [&] { cycle(0, r, z, status_.get()); });
+    graphed(r, z, 0, z, [&] { precondition(r, z); });
   } else if (amg()) {
-    cycle(0, r, z, status_.get());
+    precondition(r, z);
   } else {
     launch::multiply(n_, r, jacobi_inverse_.get(), z, status_.get(), stream_);
   }
   if (nullspace_) project(z, n_, projection_.get());
+}
+
+// The AMG cycle, then, with a learned stage attached, its correction of what
+// the cycle left: z += G(r - A z) (a variable preconditioner, so the Krylov
+// driver must be the flexible one, as it is for the mixed solve).
+void Solver::precondition(const float* r, float*& z) {
+  cycle(0, r, z, status_.get());
+  if (learned_ != nullptr) {
+    launch::residual(n_, rows0(), cols0(), val_, z, r, learned_residual_.get(), status_.get(),
+                     stream_);
+    tally(8.0 * nnz_ + 4.0 * (n_ + 1) + 12.0 * n_);
+    learned_->forward(learned_residual_.get(), z, 1.0f, stream_);
+  }
+}
+
+void Solver::set_learned(Gnn* g) {
+  KB2_REQUIRE(g == nullptr || (amg() && variable()),
+              "learned stage: needs an AMG solver with the flexible Krylov driver");
+  for (auto& graph : graphs_) cudaGraphExecDestroy(graph.exec);
+  graphs_.clear();
+  learned_ = g;
+  if (g != nullptr) {
+    if (!learned_residual_.allocated()) learned_residual_.reset(static_cast<std::size_t>(n_));
+    if (val_ != nullptr) g->bind(n_, rows0(), cols0(), levels_[0].diag.get(), val_, stream_);
+  }
 }
 
 // Every level's current buffer roles (the ping-pong smoother swaps them).
@@ -628,6 +653,8 @@ void Solver::refresh(const float* val, cudaStream_t s) {
     KB2_REQUIRE(host_values_[slots] == 0, "mixed: coarsest operator is not SPD");
     choose_coarsest(host_values_[slots + 1]);
   }
+  // The learned stage's edge weights follow the values.
+  if (learned_ != nullptr) learned_->bind(n_, rows0(), cols0(), levels_[0].diag.get(), val, s);
 }
 
 // --------------------------------------------------------------------- Krylov --
@@ -902,6 +929,7 @@ std::string Solver::describe() const {
     if (tail_on_)
       out << ", levels " << tail_start_ << "-" << levels_.size() - 1 << " in one "
           << tail_.cluster << "-CTA cluster launch";
+    if (learned_ != nullptr) out << ", learned stage";
     if (mixed()) out << ")";
   } else {
     out << "Jacobi";

@@ -13,6 +13,7 @@
 
 #include "../cuda/kernels.hpp"
 #include "device.hpp"
+#include "learned.hpp"
 #include "setup.hpp"
 
 namespace kb2 {
@@ -143,6 +144,16 @@ class Solver {
 
   // Preconditioner.
   void apply(const float* r, float*& z);
+  void precondition(const float* r, float*& z);
+  Gnn* learned_ = nullptr;  // optional learned stage (not owned)
+  DArray<float> learned_residual_;
+
+ public:
+  // Attaches (or, with null, detaches) a learned correction after each AMG
+  // cycle; the network must outlive its attachment.
+  void set_learned(Gnn* g);
+
+ private:
   struct Graph {
     const void* k1;
     const void* k2;

@@ -180,6 +180,15 @@ _SIGNATURES = {
     "b2_mixed_hierarchy_build": (_I, [_I, _I, _P, _P, _P, _P, _P, _P]),
     "b2_dense_inverse": (_I, [_I, _P, _P, _P, _P, _P, _P]),
     "b2_dense_inverse_noalloc": (_I, [_I, _P, _P, _P, _P, _P, _P]),
+    "b2_gnn_create": (_I, [ctypes.c_uint64, _P]),
+    "b2_gnn_destroy": (None, [_P]),
+    "b2_gnn_parameter_count": (_I, []),
+    "b2_gnn_bind": (_I, [_P, _I, _P, _P, _P, _P, _P]),
+    "b2_gnn_apply": (_I, [_P, _P, _P, ctypes.c_float, _P]),
+    "b2_gnn_train_step": (_I, [_P, _P, _P, ctypes.c_double, ctypes.c_float, _P, _P]),
+    "b2_gnn_get_weights": (_I, [_P, _P, ctypes.c_size_t]),
+    "b2_gnn_set_weights": (_I, [_P, _P, ctypes.c_size_t]),
+    "b2_mixed_set_learned": (_I, [_P, _P]),
     "b2_mixed_profile": (_I, [_P, _I]),
     "b2_mixed_profile_read": (_I, [_P, _P]),
 }
@@ -518,9 +527,61 @@ class MixedSolver:
         _check(_load().b2_mixed_profile_read(self._handle, ctypes.byref(p)))
         return {f: getattr(p, f) for f, _ in _Profile._fields_}
 
+    def set_learned(self, stage: "LearnedStage | None") -> None:
+        """Attaches a learned correction after each AMG cycle (None detaches);
+        the stage must stay alive while attached."""
+        self._learned = stage
+        _check(_load().b2_mixed_set_learned(self._handle, stage._handle if stage else None))
+
     def __del__(self):
         if getattr(self, "_handle", None) and _lib is not None:
             _lib.b2_mixed_destroy(self._handle)
+            self._handle = None
+
+
+class LearnedStage:
+    """b2_gnn: the learned preconditioner stage (no reference counterpart), a
+    3-layer message-passing network of width 32 over the matrix graph, mapping
+    a residual r to a correction G(r) ~ A^-1 r; trained with hand-written CUDA
+    forward, backward and Adam kernels."""
+
+    def __init__(self, seed: int = 1):
+        handle = ctypes.c_void_p()
+        _check(_load().b2_gnn_create(seed, ctypes.byref(handle)))
+        self._handle = handle
+
+    @staticmethod
+    def parameter_count() -> int:
+        return int(_load().b2_gnn_parameter_count())
+
+    def bind(self, a: CsrMatrix) -> None:
+        self._bound = a
+        _check(_load().b2_gnn_bind(self._handle, a.n_rows, _tptr(a.row_ptr), _tptr(a.col),
+                                   _tptr(a.diag), _tptr(a.val), _stream()))
+
+    def apply(self, r, z, beta: float = 0.0) -> None:
+        _check(_load().b2_gnn_apply(self._handle, _tptr(r), _tptr(z), beta, _stream()))
+
+    def train_step(self, b, x, learning_rate: float = 1e-3) -> float:
+        """One Adam step on |G(b) - x|^2 / |x|^2 for the bound matrix; returns the loss."""
+        x_norm2 = float((x.double() ** 2).sum())
+        loss = ctypes.c_float()
+        _check(_load().b2_gnn_train_step(self._handle, _tptr(b), _tptr(x), x_norm2,
+                                         learning_rate, ctypes.byref(loss), _stream()))
+        return float(loss.value)
+
+    def weights(self) -> np.ndarray:
+        w = np.empty(self.parameter_count(), np.float32)
+        _check(_load().b2_gnn_get_weights(self._handle, _ptr(w), w.size))
+        return w
+
+    def set_weights(self, w: np.ndarray) -> None:
+        w = np.ascontiguousarray(w, np.float32)
+        _check(_load().b2_gnn_set_weights(self._handle, _ptr(w), w.size))
+
+    def __del__(self):
+        if getattr(self, "_handle", None) and _lib is not None:
+            _lib.b2_gnn_destroy(self._handle)
             self._handle = None
 
 
