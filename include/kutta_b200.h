@@ -244,7 +244,9 @@ int b2_mixed_hierarchy_build(int n, int nnz, const int32_t* row_ptr, const int32
  * scale 1 / sqrt(a_ii)) mapping a residual r to a correction G(r) ~ A^-1 r.
  * Trained with b2_gnn_train_step on (matrix, right-hand side, solution)
  * triples, loss |G(b) - x|^2 / |x|^2, one Adam step per call. Attached to a
- * mixed solver it runs after each AMG cycle: z = M(r) + G(r - A M(r)). */
+ * mixed solver it runs after each AMG cycle: with z = M(r), t = r - A z and
+ * c = G(t), z += alpha c for the energy-minimising alpha = max(0, c.t / c.Ac),
+ * so the stage never makes the error larger in the A-norm. */
 typedef struct b2_gnn b2_gnn;
 int b2_gnn_create(uint64_t seed, b2_gnn** out);
 void b2_gnn_destroy(b2_gnn* g);

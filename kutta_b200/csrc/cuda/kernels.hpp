@@ -202,6 +202,8 @@ void gnn_dense_back(int n, int Cin, const float* H, const float* M, const float*
                     const float* dOut, const float* Ws, const float* Wn, float* dH, float* dM,
                     float* dWs, float* dWn, float* db, cudaStream_t s);
 void gnn_add(std::size_t count, const float* a, const float* b, float* out, cudaStream_t s);
+// z += max(0, dots[0] / dots[1]) c.
+void gnn_step(int n, float* z, const float* c, const double* dots, cudaStream_t s);
 void gnn_adam(int count, float* w, const float* g, float* m, float* v, float lr, float beta1,
               float beta2, float eps, float correction1, float correction2, cudaStream_t s);
 

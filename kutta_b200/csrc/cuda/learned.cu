@@ -217,6 +217,16 @@ __global__ void k_gnn_add(std::size_t count, const float* __restrict__ a,
     out[k] = a[k] + b[k];
 }
 
+// z += alpha c with alpha = max(0, dots[0] / dots[1]) (dots = c.t, c.A c in
+// FP64): the step along c that minimises the A-norm of the error, never
+// negative.
+__global__ void k_gnn_step(int n, float* __restrict__ z, const float* __restrict__ c,
+                           const double* __restrict__ dots) {
+  const double den = dots[1];
+  const float alpha = den > 0.0 && dots[0] > 0.0 ? static_cast<float>(dots[0] / den) : 0.0f;
+  ROWS(i, n) z[i] = fmaf(alpha, c[i], z[i]);
+}
+
 // Adam with bias correction (step t >= 1).
 __global__ void k_gnn_adam(int count, float* __restrict__ w, const float* __restrict__ g,
                            float* __restrict__ m, float* __restrict__ v, float lr, float beta1,
@@ -292,6 +302,11 @@ void gnn_add(std::size_t count, const float* a, const float* b, float* out, cuda
   ++counter;
   const int blocks = static_cast<int>(std::min<std::size_t>((count + kBlock - 1) / kBlock, kMaxBlocks));
   k_gnn_add<<<blocks, kBlock, 0, s>>>(count, a, b, out);
+}
+void gnn_step(int n, float* z, const float* c, const double* dots, cudaStream_t s) {
+  if (n <= 0) return;
+  ++counter;
+  k_gnn_step<<<grid_for(n), kBlock, 0, s>>>(n, z, c, dots);
 }
 void gnn_adam(int count, float* w, const float* g, float* m, float* v, float lr, float beta1,
               float beta2, float eps, float correction1, float correction2, cudaStream_t s) {

@@ -414,12 +414,33 @@ static int* rcm(int n, const int* off, const int* adj) {
 // fluxes of u = curl(sum of 8 seeded Fourier modes of a vector potential),
 // normalised to |u|~1, plus diffusion nu = `convection` * |A|/|d|, with the
 // diagonal divided by the under-relaxation factor 0.7.
+// field_sigma > 0 replaces the per-cell log-uniform D by a smooth log-normal
+// field D = exp(field_sigma g(x_c)), g a unit-variance Gaussian random field
+// with correlation length field_corr, drawn as 64 random Fourier features:
+// g(x) = sqrt(2/64) sum_q cos(w_q . x + p_q), w_q ~ N(0, I / corr^2).
 static kh_system* assemble(const kh_mesh* m, int renumber, double dmin, double dmax,
-                           double convection, uint64_t* rng) {
+                           double convection, double field_sigma, double field_corr,
+                           uint64_t* rng) {
   const int n = m->cells;
   double* D = (double*)malloc(sizeof(double) * (size_t)n);
-  const double l0 = log(dmin), l1 = log(dmax);
-  for (int c = 0; c < n; ++c) D[c] = exp(l0 + (l1 - l0) * uniform01(rng));
+  if (field_sigma > 0) {
+    enum { kFeatures = 64 };
+    double w[kFeatures][3], p[kFeatures];
+    for (int q = 0; q < kFeatures; ++q) {
+      for (int d = 0; d < 3; ++d) w[q][d] = normal01(rng) / field_corr;
+      p[q] = 6.283185307179586 * uniform01(rng);
+    }
+    const double norm = sqrt(2.0 / kFeatures);
+    for (int c = 0; c < n; ++c) {
+      const v3 x = m->centroid[c];
+      double g = 0;
+      for (int q = 0; q < kFeatures; ++q) g += cos(w[q][0] * x.x + w[q][1] * x.y + w[q][2] * x.z + p[q]);
+      D[c] = exp(field_sigma * norm * g);
+    }
+  } else {
+    const double l0 = log(dmin), l1 = log(dmax);
+    for (int c = 0; c < n; ++c) D[c] = exp(l0 + (l1 - l0) * uniform01(rng));
+  }
   // Fourier modes of the vector potential for the convective twin.
   double mk[8][3], ma[8][3], mp[8];
   for (int q = 0; q < 8; ++q) {
@@ -571,14 +592,15 @@ static kh_system* assemble(const kh_mesh* m, int renumber, double dmin, double d
 // mesh's stream.
 kh_system* kh_box_system(int nx, int ny, int nz, int tet, double jitter, int band_layers,
                          double aspect, double ratio, double dmin, double dmax,
-                         double convection, int renumber, uint64_t seed, uint64_t coeff_seed) {
+                         double convection, int renumber, uint64_t seed, uint64_t coeff_seed,
+                         double field_sigma, double field_corr) {
   if (nx < 1 || ny < 1 || nz < 1) return NULL;
   uint64_t rng = seed * 0x2545F4914F6CDD1DULL + 0x1234567ULL;
   kh_mesh m;
   memset(&m, 0, sizeof(m));
   if (build_mesh(&m, nx, ny, nz, tet, jitter, band_layers, aspect, ratio, &rng) != 0) return NULL;
   if (coeff_seed != 0) rng = coeff_seed * 0x9E3779B97F4A7C15ULL + 0x7654321ULL;
-  kh_system* s = assemble(&m, renumber, dmin, dmax, convection, &rng);
+  kh_system* s = assemble(&m, renumber, dmin, dmax, convection, field_sigma, field_corr, &rng);
   mesh_free(&m);
   return s;
 }

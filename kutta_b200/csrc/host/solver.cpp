@@ -513,15 +513,24 @@ void Solver::apply(const float* r, float*& z) {
 }
 
 // The AMG cycle, then, with a learned stage attached, its correction of what
-// the cycle left: z += G(r - A z) (a variable preconditioner, so the Krylov
-// driver must be the flexible one, as it is for the mixed solve).
+// the cycle left: c = G(t) for t = r - A z, added as z += alpha c with the
+// energy-minimising alpha = max(0, c.t / c.A c), so a poor network cannot
+// make the error larger in the A-norm. The result is a variable
+// preconditioner, so the Krylov driver must be the flexible one, as it is for
+// the mixed solve.
 void Solver::precondition(const float* r, float*& z) {
   cycle(0, r, z, status_.get());
   if (learned_ != nullptr) {
-    launch::residual(n_, rows0(), cols0(), val_, z, r, learned_residual_.get(), status_.get(),
-                     stream_);
-    tally(8.0 * nnz_ + 4.0 * (n_ + 1) + 12.0 * n_);
-    learned_->forward(learned_residual_.get(), z, 1.0f, stream_);
+    float* t = learned_residual_.get();
+    float* c = learned_correction_.get();
+    float* q = learned_product_.get();
+    launch::residual(n_, rows0(), cols0(), val_, z, r, t, status_.get(), stream_);
+    learned_->forward(t, c, 0.0f, stream_);
+    launch::spmv(n_, rows0(), cols0(), val_, c, q, status_.get(), stream_);
+    launch::reduce_value(ReduceMode::Dot, n_, c, t, reducer(), learned_dots_.get(), 0, stream_);
+    launch::reduce_value(ReduceMode::Dot, n_, c, q, reducer(), learned_dots_.get(), 1, stream_);
+    launch::gnn_step(n_, z, c, learned_dots_.get(), stream_);
+    tally(2.0 * (8.0 * nnz_ + 4.0 * (n_ + 1) + 8.0 * n_) + 4.0 * n_ + 16.0 * n_ + 12.0 * n_);
   }
 }
 
@@ -532,7 +541,12 @@ void Solver::set_learned(Gnn* g) {
   graphs_.clear();
   learned_ = g;
   if (g != nullptr) {
-    if (!learned_residual_.allocated()) learned_residual_.reset(static_cast<std::size_t>(n_));
+    if (!learned_residual_.allocated()) {
+      learned_residual_.reset(static_cast<std::size_t>(n_));
+      learned_correction_.reset(static_cast<std::size_t>(n_));
+      learned_product_.reset(static_cast<std::size_t>(n_));
+      learned_dots_.reset(2);
+    }
     if (val_ != nullptr) g->bind(n_, rows0(), cols0(), levels_[0].diag.get(), val_, stream_);
   }
 }

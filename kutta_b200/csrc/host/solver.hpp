@@ -146,7 +146,8 @@ class Solver {
   void apply(const float* r, float*& z);
   void precondition(const float* r, float*& z);
   Gnn* learned_ = nullptr;  // optional learned stage (not owned)
-  DArray<float> learned_residual_;
+  DArray<float> learned_residual_, learned_correction_, learned_product_;
+  DArray<double> learned_dots_;
 
  public:
   // Attaches (or, with null, detaches) a learned correction after each AMG

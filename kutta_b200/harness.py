@@ -50,7 +50,7 @@ def _load():
                                       ctypes.c_double, ctypes.c_int, ctypes.c_double,
                                       ctypes.c_double, ctypes.c_double, ctypes.c_double,
                                       ctypes.c_double, ctypes.c_int, ctypes.c_uint64,
-                                      ctypes.c_uint64]
+                                      ctypes.c_uint64, ctypes.c_double, ctypes.c_double]
         lib.kh_free.argtypes = [ctypes.POINTER(_KhSystem)]
         lib.kh_hash.restype = ctypes.c_uint32
         lib.kh_hash.argtypes = [ctypes.c_uint32]
@@ -143,12 +143,17 @@ def random_solution(n: int) -> np.ndarray:
 def box_system(nx: int, ny: int, nz: int, *, tet: bool, seed: int, jitter: float = 0.15,
                band_layers: int = 0, aspect: float = 1000.0, ratio: float = 1.2,
                dmin: float = 1e-3, dmax: float = 1.0, convection: float = 0.0,
-               renumber: bool = True, coeff_seed: int = 0) -> HostSystem:
+               renumber: bool = True, coeff_seed: int = 0, field_sigma: float = 0.0,
+               field_corr: float = 0.1) -> HostSystem:
     """Finite-volume pressure (or convection-diffusion) system on a jittered box.
     `seed` fixes the mesh; a nonzero `coeff_seed` draws the coefficient field
-    and right-hand side from a stream of its own (same mesh, another field)."""
+    and right-hand side from a stream of its own (same mesh, another field).
+    field_sigma > 0: D = exp(field_sigma g) for a smooth unit-variance Gaussian
+    field g of correlation length field_corr, instead of per-cell log-uniform
+    D in [dmin, dmax]."""
     s = _take(_load().kh_box_system(nx, ny, nz, int(tet), jitter, band_layers, aspect, ratio,
-                                    dmin, dmax, convection, int(renumber), seed, coeff_seed))
+                                    dmin, dmax, convection, int(renumber), seed, coeff_seed,
+                                    field_sigma, field_corr))
     s.name = (f"{'tet6' if tet else 'hex'}{nx}x{ny}x{nz}-seed{seed}"
               + (f"-band{band_layers}" if band_layers else "")
               + (f"-conv{convection}" if convection > 0 else ""))
