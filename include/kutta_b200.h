@@ -240,13 +240,13 @@ int b2_mixed_hierarchy_build(int n, int nnz, const int32_t* row_ptr, const int32
 
 /* ---- Learned preconditioner stage (no reference counterpart) --------------
  * A message-passing network over the graph of the fine matrix (3 layers,
- * hidden width 32, FP32; edge features w_ij = -a_ij / sqrt(a_ii a_jj), node
- * scale 1 / sqrt(a_ii)) mapping a residual r to a correction G(r) ~ A^-1 r.
- * Trained with b2_gnn_train_step on (matrix, right-hand side, solution)
- * triples, loss |G(b) - x|^2 / |x|^2, one Adam step per call. Attached to a
- * mixed solver it runs after each AMG cycle: with z = M(r), t = r - A z and
- * c = G(t), z += alpha c for the energy-minimising alpha = max(0, c.t / c.Ac),
- * so the stage never makes the error larger in the A-norm. */
+ * hidden width 32; edge features w_ij = -a_ij / sqrt(a_ii a_jj), node scale
+ * 1 / sqrt(a_ii)) mapping a residual r to a correction direction G(r). The
+ * input is normalised by its RMS and the output scaled back, so
+ * G(lambda r) = lambda G(r) for lambda > 0. Trained with b2_gnn_train_step on
+ * (residual t, error e) pairs with A e = t, one Adam step per call, on the
+ * energy loss 1 - (c.t)^2 / ((c.Ac)(t.e)) for c = G(t): the fraction of the
+ * error's A-energy left after the best step along c. */
 typedef struct b2_gnn b2_gnn;
 int b2_gnn_create(uint64_t seed, b2_gnn** out);
 void b2_gnn_destroy(b2_gnn* g);
@@ -255,17 +255,33 @@ int b2_gnn_parameter_count(void);
  * bound and bind again after its values change. */
 int b2_gnn_bind(b2_gnn* g, int n, const int32_t* d_row_ptr, const int32_t* d_col,
                 const int32_t* d_diag, const float* d_val, void* stream);
-/* d_z = beta d_z + G(d_r), beta 0 or 1. */
+/* d_z = beta d_z + G(d_r), beta 0 or 1: the tensor-core forward (BF16
+ * operands, FP32 accumulation); waits for the stream to report a device
+ * fault of the stage. */
 int b2_gnn_apply(b2_gnn* g, const float* d_r, float* d_z, float beta, void* stream);
-/* One training step on (d_b, d_x) with |x|^2 = x_norm2; *loss before the step. */
-int b2_gnn_train_step(b2_gnn* g, const float* d_b, const float* d_x, double x_norm2,
-                      float learning_rate, float* loss, void* stream);
+/* One training step on (d_t, d_e), A e = t for the bound matrix; *loss is the
+ * energy loss before the step. */
+int b2_gnn_train_step(b2_gnn* g, const float* d_t, const float* d_e, float learning_rate,
+                      float* loss, void* stream);
 int b2_gnn_get_weights(const b2_gnn* g, float* host, size_t count);
 int b2_gnn_set_weights(b2_gnn* g, const float* host, size_t count);
 /* Attaches g (NULL detaches) to a mixed solver; it is bound to the solver's
  * matrix at once if refreshed, and again at every refresh. g must outlive the
- * attachment. */
-int b2_mixed_set_learned(b2_mixed* solver, b2_gnn* g);
+ * attachment. `mode` is a bit set:
+ *   B2_LEARNED_CYCLE: after each AMG cycle, with z = M(r), t = r - A z and
+ *     c = G(t), z += alpha c for the energy-minimising alpha =
+ *     max(0, c.t / c.Ac), so the stage never makes the error larger in the
+ *     A-norm (the flexible inner PCG absorbs the variable preconditioner);
+ *   B2_LEARNED_WARM_START: before the refinement loop, the initial guess x0
+ *     takes the same safeguarded step along G(b - A x0). */
+#define B2_LEARNED_CYCLE 1
+#define B2_LEARNED_WARM_START 2
+int b2_mixed_set_learned(b2_mixed* solver, b2_gnn* g, int mode);
+/* One application of the mixed solver's preconditioner (the AMG cycle, and
+ * the learned stage when attached in B2_LEARNED_CYCLE mode) to d_r, into d_z,
+ * with the values d_val the solver was refreshed with. */
+int b2_mixed_precondition(b2_mixed* solver, const float* d_val, const float* d_r, float* d_z,
+                          void* stream);
 
 /* Hierarchy introspection (the captured-hierarchy checks of the reference's
  * tests/linalg/test_solvers.cpp:487-555 read the same data back from launches).

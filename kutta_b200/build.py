@@ -42,6 +42,7 @@ PRODUCT_CU = {
     "mixed_kernels.cu": [],
     "tail_cycle.cu": [],
     "learned.cu": [],
+    "learned_tc.cu": [],
     "noalloc.cu": [],
 }
 PRODUCT_CPP = ["host/setup.cpp", "host/solver.cpp", "host/mixed.cpp", "host/learned.cpp",

@@ -12,6 +12,10 @@
 #include "cuda/kernels.hpp"
 #include "host/mixed.hpp"
 #include "host/setup.hpp"
+
+static_assert(B2_LEARNED_CYCLE == kb2::Solver::kLearnedCycle &&
+                  B2_LEARNED_WARM_START == kb2::Solver::kLearnedWarmStart,
+              "learned-stage mode bits");
 #include "host/solver.hpp"
 
 struct b2_workspace {
@@ -487,16 +491,17 @@ int b2_gnn_apply(b2_gnn* g, const float* d_r, float* d_z, float beta, void* stre
     KB2_REQUIRE(g && g->g && d_r && d_z, "learned stage: null argument");
     KB2_REQUIRE(beta == 0.0f || beta == 1.0f, "learned stage: beta must be 0 or 1");
     g->g->forward(d_r, d_z, beta, as_stream(stream));
+    g->g->check(as_stream(stream));
   });
 }
 
-int b2_gnn_train_step(b2_gnn* g, const float* d_b, const float* d_x, double x_norm2,
-                      float learning_rate, float* loss, void* stream) {
+int b2_gnn_train_step(b2_gnn* g, const float* d_t, const float* d_e, float learning_rate,
+                      float* loss, void* stream) {
   return guarded([&] {
-    KB2_REQUIRE(g && g->g && d_b && d_x, "learned stage: null argument");
+    KB2_REQUIRE(g && g->g && d_t && d_e, "learned stage: null argument");
     KB2_REQUIRE(learning_rate > 0 && std::isfinite(learning_rate),
                 "learned stage: invalid learning rate");
-    const float l = g->g->train_step(d_b, d_x, x_norm2, learning_rate, as_stream(stream));
+    const float l = g->g->train_step(d_t, d_e, learning_rate, as_stream(stream));
     if (loss) *loss = l;
   });
 }
@@ -517,10 +522,18 @@ int b2_gnn_set_weights(b2_gnn* g, const float* host, size_t count) {
   });
 }
 
-int b2_mixed_set_learned(b2_mixed* s, b2_gnn* g) {
+int b2_mixed_set_learned(b2_mixed* s, b2_gnn* g, int mode) {
   return guarded([&] {
     KB2_REQUIRE(s && s->s, "solver: null handle");
-    s->s->inner().set_learned(g ? g->g.get() : nullptr);
+    s->s->inner().set_learned(g ? g->g.get() : nullptr, mode);
+  });
+}
+
+int b2_mixed_precondition(b2_mixed* s, const float* d_val, const float* d_r, float* d_z,
+                          void* stream) {
+  return guarded([&] {
+    KB2_REQUIRE(s && s->s && d_val, "solver: null argument");
+    s->s->inner().precondition_into(d_val, d_r, d_z, as_stream(stream));
   });
 }
 

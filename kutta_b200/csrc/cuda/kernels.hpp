@@ -178,34 +178,55 @@ bool tail_cluster_fits(int cluster, int smem_bytes);
 void tail_cycle(const TailPlan& plan, const int* status, cudaStream_t s);
 
 // ---- learned preconditioner stage (learned.cu) ------------------------------
-// Edge weights w_ij = -a_ij / sqrt(a_ii a_jj) (0 on the diagonal) and node
-// scales 1 / sqrt(a_ii) from the matrix values.
+// Edge weights w_ij = -a_ij / sqrt(a_ii a_jj) (0 on the diagonal), lift_ij =
+// w_ij / sqrt(a_jj) and node scales 1 / sqrt(a_ii) from the matrix values.
 void gnn_graph(int n, const int* rows, const int* cols, const int* diag, const float* vals,
-               float* edge, float* node_scale, cudaStream_t s);
-// H0 = node_scale * r.
+               float* edge, float* lift, float* node_scale, cudaStream_t s);
+// H0 = node_scale * r; then H0 /= rho, rho = sqrt(sum2[0] / n) (the RMS of
+// H0, reduced on the device in between).
 void gnn_input(int n, const float* r, const float* node_scale, float* H0, cudaStream_t s);
+void gnn_normalize(int n, float* H0, const double* sum2, cudaStream_t s);
 // M = W H for C <= 32 channels (row-major n x C).
 void gnn_aggregate(int n, int C, const int* rows, const int* cols, const float* edge,
                    const float* H, float* M, cudaStream_t s);
 // out = relu(Ws H + Wn M + b), Cin -> 32 channels.
 void gnn_dense(int n, int Cin, const float* H, const float* M, const float* Ws, const float* Wn,
                const float* bias, float* out, cudaStream_t s);
-// z = beta z + node_scale * (H wo).
-void gnn_output(int n, const float* H, const float* wo, const float* node_scale, float* z,
-                float beta, cudaStream_t s);
-// dz = 2 (z - x) inv_norm2; loss += |z - x|^2 inv_norm2 (atomic).
-void gnn_loss(int n, const float* z, const float* x, float inv_norm2, float* dz, float* loss,
-              cudaStream_t s);
+// z = beta z + rho node_scale * (H wo).
+void gnn_output(int n, const float* H, const float* wo, const float* node_scale,
+                const double* sum2, float* z, float beta, cudaStream_t s);
+// Energy loss 1 - P^2 / (Q E) of a correction c for t = A e, dots = {P = c.t,
+// Q = c.Ac, E = t.e}, q = A c: dz = dL/dc, loss[0] = L.
+void gnn_energy(int n, const float* t, const float* q, const double* dots, float* dz, float* loss,
+                cudaStream_t s);
 void gnn_output_back(int n, const float* H, const float* wo, const float* node_scale,
-                     const float* dz, float* dH, float* dwo, cudaStream_t s);
+                     const double* sum2, const float* dz, float* dH, float* dwo, cudaStream_t s);
 void gnn_dense_back(int n, int Cin, const float* H, const float* M, const float* out,
                     const float* dOut, const float* Ws, const float* Wn, float* dH, float* dM,
                     float* dWs, float* dWn, float* db, cudaStream_t s);
 void gnn_add(std::size_t count, const float* a, const float* b, float* out, cudaStream_t s);
 // z += max(0, dots[0] / dots[1]) c.
 void gnn_step(int n, float* z, const float* c, const double* dots, cudaStream_t s);
+void gnn_step64(int n, double* x, const float* c, const double* dots, cudaStream_t s);
 void gnn_adam(int count, float* w, const float* g, float* m, float* v, float lr, float beta1,
               float beta2, float eps, float correction1, float correction2, cudaStream_t s);
+
+// Tensor-core forward (learned_tc.cu). lift: uv = (s t, sum_j lift_ij t_j),
+// sum2[0] = |s t|^2 (fixed-order reduction). layer_a: BF16 rows hout (n x 32)
+// = relu([H1 | W H1] [Ws | Wn]^T + b), H1 from uv and the first layer's
+// (ws1, wn1, b1) = first[0..95]. layer_b: z = beta z + rho s (wo .
+// relu([H | W H] [Ws | Wn]^T + b)) for the BF16 rows hin. A CTA whose MMA
+// does not complete sets fault[0] and returns.
+void gnn_lift(int n, const int* rows, const int* cols, const float* lift, const float* t,
+              const float* node_scale, float2* uv, DeviceReducer red, double* sum2,
+              cudaStream_t s);
+void gnn_layer_a(int n, const int* rows, const int* cols, const float* edge, const float2* uv,
+                 const float* first, const float* ws, const float* wn, const float* bias,
+                 const double* sum2, unsigned short* hout, int* fault, cudaStream_t s);
+void gnn_layer_b(int n, const int* rows, const int* cols, const float* edge,
+                 const unsigned short* hin, const float* ws, const float* wn, const float* bias,
+                 const float* wo, const float* node_scale, const double* sum2, float* z,
+                 float beta, int* fault, cudaStream_t s);
 
 // ---- single-thread scalar kernels -------------------------------------------
 void solver_limits(float* scalars, float th, float tl, float dh, float dl, cudaStream_t s);

@@ -32,16 +32,21 @@ constexpr int kHidden = 32;
   for (int i = static_cast<int>((blockIdx.x * blockDim.x + threadIdx.x) >> 5); i < (n); \
        i += static_cast<int>((gridDim.x * blockDim.x) >> 5))
 
+// Also lift_ij = w_ij s_j, the input aggregation weight of the tensor-core
+// forward (which aggregates t rather than s t).
 __global__ void k_gnn_graph(int n, const int* __restrict__ rows, const int* __restrict__ cols,
                             const int* __restrict__ diag, const float* __restrict__ vals,
-                            float* __restrict__ edge, float* __restrict__ node_scale) {
+                            float* __restrict__ edge, float* __restrict__ lift,
+                            float* __restrict__ node_scale) {
   ROWS(i, n) {
     const float di = vals[diag[i]];
     node_scale[i] = di > 0.0f ? rsqrtf(di) : 0.0f;
     for (int j = rows[i]; j < rows[i + 1]; ++j) {
       const int c = cols[j];
       const float dc = vals[diag[c]];
-      edge[j] = (c == i || di <= 0.0f || dc <= 0.0f) ? 0.0f : -vals[j] * rsqrtf(di * dc);
+      const float w = (c == i || di <= 0.0f || dc <= 0.0f) ? 0.0f : -vals[j] * rsqrtf(di * dc);
+      edge[j] = w;
+      lift[j] = dc > 0.0f ? w * rsqrtf(dc) : 0.0f;
     }
   }
 }
@@ -62,16 +67,18 @@ __global__ void k_gnn_aggregate(int n, int C, const int* __restrict__ rows,
   }
 }
 
-// H'_i = relu(Ws H_i + Wn M_i + b): weights [Cout=32][Cin] in shared memory,
-// lane = output channel; the row's inputs are broadcast by shuffles.
+// H'_i = relu(Ws H_i + Wn M_i + b): weights [Cout=32][Cin] held transposed in
+// shared memory (lane = output channel reads consecutive words, no bank
+// conflicts); the row's inputs are broadcast by shuffles.
 __global__ void k_gnn_dense(int n, int Cin, const float* __restrict__ H,
                             const float* __restrict__ M, const float* __restrict__ Ws,
                             const float* __restrict__ Wn, const float* __restrict__ bias,
                             float* __restrict__ out) {
   __shared__ float ws[kHidden * kHidden], wn[kHidden * kHidden], bs[kHidden];
   for (int k = threadIdx.x; k < kHidden * Cin; k += blockDim.x) {
-    ws[k] = Ws[k];
-    wn[k] = Wn[k];
+    const int c = k / Cin, j = k % Cin;  // Ws[c][j] -> ws[j][c]
+    ws[j * kHidden + c] = Ws[k];
+    wn[j * kHidden + c] = Wn[k];
   }
   if (threadIdx.x < kHidden) bs[threadIdx.x] = bias[threadIdx.x];
   __syncthreads();
@@ -83,57 +90,78 @@ __global__ void k_gnn_dense(int n, int Cin, const float* __restrict__ H,
     for (int k = 0; k < Cin; ++k) {
       const float hk = __shfl_sync(0xffffffffu, h, k);
       const float mk = __shfl_sync(0xffffffffu, m, k);
-      acc = fmaf(ws[lane * Cin + k], hk, acc);
-      acc = fmaf(wn[lane * Cin + k], mk, acc);
+      acc = fmaf(ws[k * kHidden + lane], hk, acc);
+      acc = fmaf(wn[k * kHidden + lane], mk, acc);
     }
     out[static_cast<std::size_t>(i) * kHidden + lane] = fmaxf(acc, 0.0f);
   }
 }
 
-// z_i = s_i (wo . H_i).
+// RMS of the input features from their sum of squares (FP64, reduced on the
+// device); 0 for a zero input.
+__device__ __forceinline__ double input_rms(int n, const double* sum2) {
+  const double m = sum2[0] / static_cast<double>(n);
+  return m > 0.0 ? sqrt(m) : 0.0;
+}
+
+// z_i = rho s_i (wo . H_i), rho the input RMS: with the input normalised by rho
+// the network is positively homogeneous, G(lambda r) = lambda G(r).
 __global__ void k_gnn_output(int n, const float* __restrict__ H, const float* __restrict__ wo,
-                             const float* __restrict__ node_scale, float* __restrict__ z,
-                             float beta) {
+                             const float* __restrict__ node_scale, const double* __restrict__ sum2,
+                             float* __restrict__ z, float beta) {
   const int lane = threadIdx.x & 31;
   const float w = wo[lane];
+  const float rho = static_cast<float>(input_rms(n, sum2));
   WARP_ROWS(i, n) {
     float v = w * H[static_cast<std::size_t>(i) * kHidden + lane];
     for (int d = 16; d > 0; d >>= 1) v += __shfl_down_sync(0xffffffffu, v, d);
-    if (lane == 0) z[i] = (beta != 0.0f ? beta * z[i] : 0.0f) + node_scale[i] * v;
+    if (lane == 0) z[i] = (beta != 0.0f ? beta * z[i] : 0.0f) + rho * node_scale[i] * v;
   }
 }
 
-// Input layer features: H0_i = s_i r_i.
+// Input features before normalisation: H0_i = s_i r_i.
 __global__ void k_gnn_input(int n, const float* __restrict__ r, const float* __restrict__ node_scale,
                             float* __restrict__ H0) {
   ROWS(i, n) H0[i] = node_scale[i] * r[i];
 }
 
-// ---- training -------------------------------------------------------------
-// Loss: |z - x|^2 / |x|^2 (x the solver's solution). dz = 2 (z - x) / |x|^2;
-// the loss itself accumulated (atomically) into loss[0].
-__global__ void k_gnn_loss(int n, const float* __restrict__ z, const float* __restrict__ x,
-                           float inv_norm2, float* __restrict__ dz, float* loss) {
-  float acc = 0.0f;
-  ROWS(i, n) {
-    const float d = z[i] - x[i];
-    dz[i] = 2.0f * d * inv_norm2;
-    acc += d * d;
-  }
-  for (int d = 16; d > 0; d >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, d);
-  if ((threadIdx.x & 31) == 0) atomicAdd(loss, acc * inv_norm2);
+// H0 /= rho (the RMS of H0), so the network sees unit-RMS features whatever
+// the residual's magnitude.
+__global__ void k_gnn_normalize(int n, float* __restrict__ H0, const double* __restrict__ sum2) {
+  const double rho = input_rms(n, sum2);
+  const float inv = rho > 0.0 ? static_cast<float>(1.0 / rho) : 0.0f;
+  ROWS(i, n) H0[i] *= inv;
 }
 
-// Output backward: dH_i = dz_i s_i wo, dwo += sum_i dz_i s_i H_i.
+// ---- training -------------------------------------------------------------
+// Energy loss of a correction c for the residual t = A e:
+//   L = 1 - (c.t)^2 / ((c.Ac)(t.e)),
+// the fraction of the error's A-energy left after the best step along c
+// (alpha = c.t / c.Ac). dots = {c.t, c.Ac, t.e} in FP64; q = A c.
+//   dL/dc = -(2P / (Q E)) t + (2P^2 / (Q^2 E)) q    (P, Q, E = dots).
+// Zero gradient and L = 1 when c.Ac or t.e is not positive.
+__global__ void k_gnn_energy(int n, const float* __restrict__ t, const float* __restrict__ q,
+                             const double* __restrict__ dots, float* __restrict__ dz,
+                             float* __restrict__ loss) {
+  const double P = dots[0], Q = dots[1], E = dots[2];
+  const bool ok = Q > 0.0 && E > 0.0;
+  const float gt = ok ? static_cast<float>(-2.0 * P / (Q * E)) : 0.0f;
+  const float gq = ok ? static_cast<float>(2.0 * P * P / (Q * Q * E)) : 0.0f;
+  if (blockIdx.x == 0 && threadIdx.x == 0) *loss = ok ? static_cast<float>(1.0 - P * P / (Q * E)) : 1.0f;
+  ROWS(i, n) dz[i] = fmaf(gt, t[i], gq * q[i]);
+}
+
+// Output backward: dH_i = dz_i rho s_i wo, dwo += sum_i dz_i rho s_i H_i.
 __global__ void k_gnn_output_back(int n, const float* __restrict__ H, const float* __restrict__ wo,
                                   const float* __restrict__ node_scale,
-                                  const float* __restrict__ dz, float* __restrict__ dH,
-                                  float* __restrict__ dwo) {
+                                  const double* __restrict__ sum2, const float* __restrict__ dz,
+                                  float* __restrict__ dH, float* __restrict__ dwo) {
   const int lane = threadIdx.x & 31;
   const float w = wo[lane];
+  const float rho = static_cast<float>(input_rms(n, sum2));
   float g = 0.0f;
   WARP_ROWS(i, n) {
-    const float t = dz[i] * node_scale[i];
+    const float t = dz[i] * rho * node_scale[i];
     const std::size_t k = static_cast<std::size_t>(i) * kHidden + lane;
     dH[k] = t * w;
     g = fmaf(t, H[k], g);
@@ -227,6 +255,14 @@ __global__ void k_gnn_step(int n, float* __restrict__ z, const float* __restrict
   ROWS(i, n) z[i] = fmaf(alpha, c[i], z[i]);
 }
 
+// The same step on an FP64 vector (the warm start of the mixed solve).
+__global__ void k_gnn_step64(int n, double* __restrict__ x, const float* __restrict__ c,
+                             const double* __restrict__ dots) {
+  const double den = dots[1];
+  const double alpha = den > 0.0 && dots[0] > 0.0 ? dots[0] / den : 0.0;
+  ROWS(i, n) x[i] += alpha * static_cast<double>(c[i]);
+}
+
 // Adam with bias correction (step t >= 1).
 __global__ void k_gnn_adam(int count, float* __restrict__ w, const float* __restrict__ g,
                            float* __restrict__ m, float* __restrict__ v, float lr, float beta1,
@@ -249,15 +285,20 @@ int warp_grid(int n) {
 namespace launch {
 
 void gnn_graph(int n, const int* rows, const int* cols, const int* diag, const float* vals,
-               float* edge, float* node_scale, cudaStream_t s) {
+               float* edge, float* lift, float* node_scale, cudaStream_t s) {
   if (n <= 0) return;
   ++counter;
-  k_gnn_graph<<<grid_for(n), kBlock, 0, s>>>(n, rows, cols, diag, vals, edge, node_scale);
+  k_gnn_graph<<<grid_for(n), kBlock, 0, s>>>(n, rows, cols, diag, vals, edge, lift, node_scale);
 }
 void gnn_input(int n, const float* r, const float* node_scale, float* H0, cudaStream_t s) {
   if (n <= 0) return;
   ++counter;
   k_gnn_input<<<grid_for(n), kBlock, 0, s>>>(n, r, node_scale, H0);
+}
+void gnn_normalize(int n, float* H0, const double* sum2, cudaStream_t s) {
+  if (n <= 0) return;
+  ++counter;
+  k_gnn_normalize<<<grid_for(n), kBlock, 0, s>>>(n, H0, sum2);
 }
 void gnn_aggregate(int n, int C, const int* rows, const int* cols, const float* edge,
                    const float* H, float* M, cudaStream_t s) {
@@ -271,23 +312,23 @@ void gnn_dense(int n, int Cin, const float* H, const float* M, const float* Ws, 
   ++counter;
   k_gnn_dense<<<warp_grid(n), kBlock, 0, s>>>(n, Cin, H, M, Ws, Wn, bias, out);
 }
-void gnn_output(int n, const float* H, const float* wo, const float* node_scale, float* z,
-                float beta, cudaStream_t s) {
+void gnn_output(int n, const float* H, const float* wo, const float* node_scale,
+                const double* sum2, float* z, float beta, cudaStream_t s) {
   if (n <= 0) return;
   ++counter;
-  k_gnn_output<<<warp_grid(n), kBlock, 0, s>>>(n, H, wo, node_scale, z, beta);
+  k_gnn_output<<<warp_grid(n), kBlock, 0, s>>>(n, H, wo, node_scale, sum2, z, beta);
 }
-void gnn_loss(int n, const float* z, const float* x, float inv_norm2, float* dz, float* loss,
-              cudaStream_t s) {
+void gnn_energy(int n, const float* t, const float* q, const double* dots, float* dz, float* loss,
+                cudaStream_t s) {
   if (n <= 0) return;
   ++counter;
-  k_gnn_loss<<<grid_for(n), kBlock, 0, s>>>(n, z, x, inv_norm2, dz, loss);
+  k_gnn_energy<<<grid_for(n), kBlock, 0, s>>>(n, t, q, dots, dz, loss);
 }
 void gnn_output_back(int n, const float* H, const float* wo, const float* node_scale,
-                     const float* dz, float* dH, float* dwo, cudaStream_t s) {
+                     const double* sum2, const float* dz, float* dH, float* dwo, cudaStream_t s) {
   if (n <= 0) return;
   ++counter;
-  k_gnn_output_back<<<warp_grid(n), kBlock, 0, s>>>(n, H, wo, node_scale, dz, dH, dwo);
+  k_gnn_output_back<<<warp_grid(n), kBlock, 0, s>>>(n, H, wo, node_scale, sum2, dz, dH, dwo);
 }
 void gnn_dense_back(int n, int Cin, const float* H, const float* M, const float* out,
                     const float* dOut, const float* Ws, const float* Wn, float* dH, float* dM,
@@ -307,6 +348,11 @@ void gnn_step(int n, float* z, const float* c, const double* dots, cudaStream_t 
   if (n <= 0) return;
   ++counter;
   k_gnn_step<<<grid_for(n), kBlock, 0, s>>>(n, z, c, dots);
+}
+void gnn_step64(int n, double* x, const float* c, const double* dots, cudaStream_t s) {
+  if (n <= 0) return;
+  ++counter;
+  k_gnn_step64<<<grid_for(n), kBlock, 0, s>>>(n, x, c, dots);
 }
 void gnn_adam(int count, float* w, const float* g, float* m, float* v, float lr, float beta1,
               float beta2, float eps, float correction1, float correction2, cudaStream_t s) {

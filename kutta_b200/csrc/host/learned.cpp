@@ -4,6 +4,7 @@
 #include <cmath>
 
 #include "../cuda/kernels.hpp"
+#include "setup.hpp"
 
 namespace kb2 {
 
@@ -62,6 +63,12 @@ Gnn::Gnn(std::uint64_t seed) {
   cuda_check(cudaMemset(m_.get(), 0, sizeof(float) * count), "memset");
   cuda_check(cudaMemset(v_.get(), 0, sizeof(float) * count), "memset");
   loss_.reset(1);
+  partials_.reset(kReducePartials);
+  ticket_.reset(1);
+  cuda_check(cudaMemset(ticket_.get(), 0, sizeof(unsigned)), "memset");
+  sums_.reset(4);
+  fault_.reset(1);
+  cuda_check(cudaMemset(fault_.get(), 0, sizeof(int)), "memset");
 }
 
 void Gnn::bind(int n, const int* rows, const int* cols, const int* diag, const float* vals,
@@ -76,43 +83,83 @@ void Gnn::bind(int n, const int* rows, const int* cols, const int* diag, const f
     for (int l = 1; l < kLayers; ++l) m_agg_[l].reset(wide);
     dz_.reset(rows_n);
     z_.reset(rows_n);
+    q_.reset(rows_n);
     dh_.reset(wide);
     dhs_.reset(wide);
     dm_.reset(wide);
     dagg_.reset(wide);
     scale_.reset(rows_n);
+    uv_.reset(2 * rows_n);
+    h2_.reset(wide);
   }
   int nnz = 0;
   cuda_check(cudaMemcpy(&nnz, rows + n, sizeof(int), cudaMemcpyDeviceToHost), "learned stage");
-  if (edge_.size() != static_cast<std::size_t>(nnz)) edge_.reset(static_cast<std::size_t>(nnz));
+  if (edge_.size() != static_cast<std::size_t>(nnz)) {
+    edge_.reset(static_cast<std::size_t>(nnz));
+    lift_.reset(static_cast<std::size_t>(nnz));
+  }
   n_ = n;
   rows_ = rows;
   cols_ = cols;
-  launch::gnn_graph(n, rows, cols, diag, vals, edge_.get(), scale_.get(), s);
+  vals_ = vals;
+  launch::gnn_graph(n, rows, cols, diag, vals, edge_.get(), lift_.get(), scale_.get(), s);
 }
 
 void Gnn::forward(const float* r, float* z, float beta, cudaStream_t s) {
   KB2_REQUIRE(n_ > 0, "learned stage: no matrix bound");
   const Slices p = slices(params_.get());
+  float2* uv = reinterpret_cast<float2*>(uv_.get());
+  launch::gnn_lift(n_, rows_, cols_, lift_.get(), r, scale_.get(), uv,
+                   DeviceReducer{partials_.get(), ticket_.get()}, sums_.get(), s);
+  launch::gnn_layer_a(n_, rows_, cols_, edge_.get(), uv, params_.get(), p.ws[1], p.wn[1], p.b[1],
+                      sums_.get(), h2_.get(), fault_.get(), s);
+  launch::gnn_layer_b(n_, rows_, cols_, edge_.get(), h2_.get(), p.ws[2], p.wn[2], p.b[2], p.wo,
+                      scale_.get(), sums_.get(), z, beta, fault_.get(), s);
+}
+
+void Gnn::check(cudaStream_t s) {
+  int fault = 0;
+  cuda_check(cudaMemcpyAsync(&fault, fault_.get(), sizeof(int), cudaMemcpyDeviceToHost, s),
+             "learned stage fault readback");
+  wait(s);
+  if (fault != 0) {
+    cuda_check(cudaMemsetAsync(fault_.get(), 0, sizeof(int), s), "memset");
+    throw TimeoutError("learned stage: a tensor-core tile did not complete");
+  }
+}
+
+void Gnn::forward32(const float* r, float* z, cudaStream_t s) {
+  KB2_REQUIRE(n_ > 0, "learned stage: no matrix bound");
+  const Slices p = slices(params_.get());
   launch::gnn_input(n_, r, scale_.get(), h_[0].get(), s);
+  launch::reduce_value(ReduceMode::Dot, n_, h_[0].get(), h_[0].get(),
+                       DeviceReducer{partials_.get(), ticket_.get()}, sums_.get(), 0, s);
+  launch::gnn_normalize(n_, h_[0].get(), sums_.get(), s);
   for (int l = 0; l < kLayers; ++l) {
     launch::gnn_aggregate(n_, cin(l), rows_, cols_, edge_.get(), h_[l].get(), m_agg_[l].get(), s);
     launch::gnn_dense(n_, cin(l), h_[l].get(), m_agg_[l].get(), p.ws[l], p.wn[l], p.b[l],
                       h_[l + 1].get(), s);
   }
-  launch::gnn_output(n_, h_[kLayers].get(), p.wo, scale_.get(), z, beta, s);
+  launch::gnn_output(n_, h_[kLayers].get(), p.wo, scale_.get(), sums_.get(), z, 0.0f, s);
 }
 
-float Gnn::train_step(const float* b, const float* x, double x_norm2, float lr, cudaStream_t s) {
-  KB2_REQUIRE(x_norm2 > 0 && std::isfinite(x_norm2), "learned stage: invalid target norm");
+float Gnn::train_step(const float* t, const float* e, float lr, cudaStream_t s) {
+  KB2_REQUIRE(n_ > 0, "learned stage: no matrix bound");
+  KB2_REQUIRE(t != nullptr && e != nullptr, "learned stage: null training vector");
   const int count = parameter_count();
-  forward(b, z_.get(), 0.0f, s);
+  const DeviceReducer red{partials_.get(), ticket_.get()};
+  float* c = z_.get();
+  forward32(t, c, s);
+  launch::spmv(n_, rows_, cols_, vals_, c, q_.get(), nullptr, s);
+  launch::reduce_value(ReduceMode::Dot, n_, c, t, red, sums_.get(), 1, s);
+  launch::reduce_value(ReduceMode::Dot, n_, c, q_.get(), red, sums_.get(), 2, s);
+  launch::reduce_value(ReduceMode::Dot, n_, t, e, red, sums_.get(), 3, s);
   cuda_check(cudaMemsetAsync(grads_.get(), 0, sizeof(float) * count, s), "memset");
-  cuda_check(cudaMemsetAsync(loss_.get(), 0, sizeof(float), s), "memset");
   const Slices p = slices(params_.get());
   const Slices g = slices(grads_.get());
-  launch::gnn_loss(n_, z_.get(), x, static_cast<float>(1.0 / x_norm2), dz_.get(), loss_.get(), s);
-  launch::gnn_output_back(n_, h_[kLayers].get(), p.wo, scale_.get(), dz_.get(), dh_.get(), g.wo, s);
+  launch::gnn_energy(n_, t, q_.get(), sums_.get() + 1, dz_.get(), loss_.get(), s);
+  launch::gnn_output_back(n_, h_[kLayers].get(), p.wo, scale_.get(), sums_.get(), dz_.get(),
+                          dh_.get(), g.wo, s);
   for (int l = kLayers - 1; l >= 0; --l) {
     launch::gnn_dense_back(n_, cin(l), h_[l].get(), m_agg_[l].get(), h_[l + 1].get(), dh_.get(),
                            p.ws[l], p.wn[l], dhs_.get(), dm_.get(), g.ws[l], g.wn[l], g.b[l], s);

@@ -1,9 +1,12 @@
 // The learned preconditioner stage (no reference counterpart): a 3-layer
 // message-passing network, hidden width 32, over the graph of the fine matrix,
-// mapping a residual r to an approximate correction G(r) ~ A^-1 r. It is
-// trained on (matrix, right-hand side, solution) triples produced by the
-// solvers themselves, with the loss |G(b) - x|^2 / |x|^2, and used inside the
-// mixed solve's flexible PCG as z = M_amg(r) + G(r - A M_amg(r)).
+// mapping a residual r to a correction direction G(r) (positively homogeneous:
+// the input is normalised by its RMS and the output scaled back). It is used
+// inside the mixed solve's flexible PCG as z = M(r) + alpha G(t), t = r - A M(r)
+// and alpha the energy-optimal step, and as a warm-start correction. Training
+// takes (residual t, error e) pairs with A e = t, made by the solvers
+// themselves, and minimises the fraction of the error's A-energy that the best
+// step along G(t) leaves: 1 - (c.t)^2 / ((c.Ac)(t.e)), c = G(t).
 #pragma once
 
 #include <cstdint>
@@ -26,10 +29,15 @@ class Gnn {
   // arrays must stay valid while bound; call again after values change.
   void bind(int n, const int* rows, const int* cols, const int* diag, const float* vals,
             cudaStream_t s);
-  // z = beta z + G(r) (beta 0 or 1), kernels only.
+  // z = beta z + G(r) (beta 0 or 1), kernels only: the tensor-core forward
+  // (BF16 operands, FP32 accumulation) of learned_tc.cu.
   void forward(const float* r, float* z, float beta, cudaStream_t s);
-  // One Adam step on |G(b) - x|^2 / x_norm2; returns that loss (host wait).
-  float train_step(const float* b, const float* x, double x_norm2, float lr, cudaStream_t s);
+  // Throws TimeoutError if a tensor-core launch recorded an MMA that did not
+  // complete (host wait on s).
+  void check(cudaStream_t s);
+  // One Adam step on the energy loss of G(t) for A e = t (the bound matrix);
+  // returns that loss before the step (host wait).
+  float train_step(const float* t, const float* e, float lr, cudaStream_t s);
   std::vector<float> weights() const;
   void set_weights(const std::vector<float>& w);
   int rows() const { return n_; }
@@ -39,14 +47,24 @@ class Gnn {
     float *ws[kLayers], *wn[kLayers], *b[kLayers], *wo;
   };
   Slices slices(float* base) const;
+  // The FP32 forward of learned.cu, keeping every layer's activations for
+  // the backward pass of training.
+  void forward32(const float* r, float* z, cudaStream_t s);
   int n_ = 0;
   const int* rows_ = nullptr;
   const int* cols_ = nullptr;
+  const float* vals_ = nullptr;
+  DArray<double> partials_;
+  DArray<unsigned> ticket_;
+  DArray<double> sums_;  // [0] input sum of squares; [1..3] energy-loss dots
   DArray<float> params_, grads_, m_, v_, loss_;
-  DArray<float> edge_, scale_;
+  DArray<float> edge_, lift_, scale_;
+  DArray<float> uv_;             // (u, v) pairs of the tensor-core forward
+  DArray<unsigned short> h2_;    // its BF16 hidden rows (n x 32)
+  DArray<int> fault_;
   // h[0] = input (n), h[l] = layer l output (n x 32); m[l] = aggregation of h[l].
   DArray<float> h_[kLayers + 1], m_agg_[kLayers];
-  DArray<float> dz_, z_, dh_, dhs_, dm_, dagg_;
+  DArray<float> dz_, z_, q_, dh_, dhs_, dm_, dagg_;
   int step_ = 0;
 };
 

@@ -47,6 +47,12 @@ MixedStats MixedSolver::solve(const float* val, double* x, const float* b, const
   if (!std::isfinite(r)) throw NonfiniteError("solve: nonfinite input vector");
   st.initial_residual = st.final_residual = r;
   const double target = std::max(c.abs_tol, c.rel_tol * r);
+  if (r > target && (inner_.learned_mode() & Solver::kLearnedWarmStart)) {
+    // The learned warm start: one safeguarded step along G(b - A x0); the
+    // tolerance stays relative to the residual of the caller's x0.
+    inner_.learned_warm_start(val, rf_.get(), x, s);
+    r = residual(val, x, b, s);
+  }
   int stalled = 0;
   while (r > target && st.refinements < o_.max_refinements && st.iterations < c.max_iter) {
     cuda_check(cudaMemsetAsync(e_.get(), 0, sizeof(float) * static_cast<std::size_t>(n_), s),
@@ -68,6 +74,7 @@ MixedStats MixedSolver::solve(const float* val, double* x, const float* b, const
     r = next;
     if (!std::isfinite(r) || stalled >= 2) break;
   }
+  inner_.check_learned(s);
   st.final_residual = r;
   st.converged = std::isfinite(r) && r <= target;
   return st;

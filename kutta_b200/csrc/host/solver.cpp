@@ -520,26 +520,58 @@ void Solver::apply(const float* r, float*& z) {
 // the mixed solve.
 void Solver::precondition(const float* r, float*& z) {
   cycle(0, r, z, status_.get());
-  if (learned_ != nullptr) {
+  if (learned_ != nullptr && (learned_mode_ & kLearnedCycle)) {
     float* t = learned_residual_.get();
-    float* c = learned_correction_.get();
-    float* q = learned_product_.get();
     launch::residual(n_, rows0(), cols0(), val_, z, r, t, status_.get(), stream_);
-    learned_->forward(t, c, 0.0f, stream_);
-    launch::spmv(n_, rows0(), cols0(), val_, c, q, status_.get(), stream_);
-    launch::reduce_value(ReduceMode::Dot, n_, c, t, reducer(), learned_dots_.get(), 0, stream_);
-    launch::reduce_value(ReduceMode::Dot, n_, c, q, reducer(), learned_dots_.get(), 1, stream_);
-    launch::gnn_step(n_, z, c, learned_dots_.get(), stream_);
-    tally(2.0 * (8.0 * nnz_ + 4.0 * (n_ + 1) + 8.0 * n_) + 4.0 * n_ + 16.0 * n_ + 12.0 * n_);
+    learned_direction(t);
+    launch::gnn_step(n_, z, learned_correction_.get(), learned_dots_.get(), stream_);
+    tally(8.0 * nnz_ + 4.0 * (n_ + 1) + 12.0 * n_ + 12.0 * n_);
   }
 }
 
-void Solver::set_learned(Gnn* g) {
+void Solver::learned_direction(const float* t) {
+  float* c = learned_correction_.get();
+  float* q = learned_product_.get();
+  learned_->forward(t, c, 0.0f, stream_);
+  launch::spmv(n_, rows0(), cols0(), val_, c, q, status_.get(), stream_);
+  launch::reduce_value(ReduceMode::Dot, n_, c, t, reducer(), learned_dots_.get(), 0, stream_);
+  launch::reduce_value(ReduceMode::Dot, n_, c, q, reducer(), learned_dots_.get(), 1, stream_);
+  tally(8.0 * nnz_ + 4.0 * (n_ + 1) + 8.0 * n_ + 16.0 * n_);
+}
+
+void Solver::learned_warm_start(const float* val, const float* r, double* x, cudaStream_t s) {
+  if (learned_ == nullptr || !(learned_mode_ & kLearnedWarmStart)) return;
+  stream_ = s;
+  val_ = val;
+  reset(0);
+  learned_direction(r);
+  launch::gnn_step64(n_, x, learned_correction_.get(), learned_dots_.get(), stream_);
+  tally(20.0 * n_);
+}
+
+void Solver::precondition_into(const float* val, const float* r, float* z, cudaStream_t s) {
+  KB2_REQUIRE(amg(), "precondition: needs an AMG solver");
+  KB2_REQUIRE(n_ == 0 || (r != nullptr && z != nullptr && r != z),
+              "precondition: null or aliased vector");
+  if (n_ == 0) return;
+  stream_ = s;
+  val_ = val;
+  reset(0);
+  precondition(r, z_);
+  if (nullspace_) project(z_, n_, projection_.get());
+  copy(z, z_, n_);
+  check_learned(s);
+}
+
+void Solver::set_learned(Gnn* g, int mode) {
   KB2_REQUIRE(g == nullptr || (amg() && variable()),
               "learned stage: needs an AMG solver with the flexible Krylov driver");
+  KB2_REQUIRE(g == nullptr || (mode >= 1 && mode <= (kLearnedCycle | kLearnedWarmStart)),
+              "learned stage: mode must be a nonempty set of cycle and warm start");
   for (auto& graph : graphs_) cudaGraphExecDestroy(graph.exec);
   graphs_.clear();
   learned_ = g;
+  learned_mode_ = g != nullptr ? mode : 0;
   if (g != nullptr) {
     if (!learned_residual_.allocated()) {
       learned_residual_.reset(static_cast<std::size_t>(n_));
@@ -943,7 +975,8 @@ std::string Solver::describe() const {
     if (tail_on_)
       out << ", levels " << tail_start_ << "-" << levels_.size() - 1 << " in one "
           << tail_.cluster << "-CTA cluster launch";
-    if (learned_ != nullptr) out << ", learned stage";
+    if (learned_mode_ & kLearnedCycle) out << ", learned stage";
+    if (learned_mode_ & kLearnedWarmStart) out << ", learned warm start";
     if (mixed()) out << ")";
   } else {
     out << "Jacobi";

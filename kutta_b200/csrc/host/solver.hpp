@@ -145,14 +145,31 @@ class Solver {
   // Preconditioner.
   void apply(const float* r, float*& z);
   void precondition(const float* r, float*& z);
+  // c = G(t), q = A c and the dots {c.t, c.Ac} for the safeguarded step.
+  void learned_direction(const float* t);
   Gnn* learned_ = nullptr;  // optional learned stage (not owned)
+  int learned_mode_ = 0;    // kLearnedCycle | kLearnedWarmStart
   DArray<float> learned_residual_, learned_correction_, learned_product_;
   DArray<double> learned_dots_;
 
  public:
-  // Attaches (or, with null, detaches) a learned correction after each AMG
-  // cycle; the network must outlive its attachment.
-  void set_learned(Gnn* g);
+  static constexpr int kLearnedCycle = 1, kLearnedWarmStart = 2;
+  // Attaches (or, with null, detaches) a learned stage: after each AMG cycle
+  // (kLearnedCycle) and/or as a warm-start step (kLearnedWarmStart). The
+  // network must outlive its attachment.
+  void set_learned(Gnn* g, int mode);
+  int learned_mode() const { return learned_ != nullptr ? learned_mode_ : 0; }
+  // x += alpha G(r) in FP64 for the residual r = b - A x, alpha =
+  // max(0, c.t / c.Ac): the learned warm start (a no-op unless attached in
+  // kLearnedWarmStart mode).
+  void learned_warm_start(const float* val, const float* r, double* x, cudaStream_t s);
+  // One application of the preconditioner (the cycle, and the learned stage in
+  // kLearnedCycle mode) to r, into z.
+  void precondition_into(const float* val, const float* r, float* z, cudaStream_t s);
+  // Throws TimeoutError if the attached stage recorded a device fault.
+  void check_learned(cudaStream_t s) {
+    if (learned_ != nullptr) learned_->check(s);
+  }
 
  private:
   struct Graph {

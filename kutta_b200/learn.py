@@ -3,23 +3,28 @@
 Training data: seeded 64^3 jittered hex meshes of the unit cube with smooth
 log-normal D_f (sigma 1.5, correlation length 0.1), right-hand sides of 16
 seeded Fourier modes over the cell centroids plus 10 % white noise (scaled by
-cell volume), and their solutions computed by the mixed solve itself to
-relative 1e-8 (FP64, rounded to float): (matrix, right-hand side, solution)
-triples. Training runs the CUDA forward, backward and Adam kernels
-(b2_gnn_train_step) over the triples, cycling through them in a seeded random
-order.
+cell volume), and their solutions x computed by the mixed solve itself to
+relative 1e-8 in FP64. Each (matrix, b, x) triple yields the pairs the stage
+sees inside the solve: for a residual r of an iterate x_k (x_k = 0, and x_k
+from a solve to relative 1e-3), z = M(r) is one application of the AMG
+preconditioner, t = r - A z what it leaves and e = (x - x_k) - z the error with
+A e = t. Training runs the CUDA forward, backward and Adam kernels
+(b2_gnn_train_step) over the pairs in a seeded random order, on the energy loss
+1 - (c.t)^2 / ((c.Ac)(t.e)) for c = G(t): the fraction of the error's A-energy
+that the best step along c leaves.
 
 Evaluation: unseen 128^3 seeds of the same family, the mixed solve to
 relative 1e-6 with and without the stage attached, and the plain FP32
-AMG-PCG, device-timed.
+AMG-PCG, device-timed; the held-out energy loss on the same kind of pairs.
 
-    python -m kutta_b200.learn --out weights.npy [--systems 48] [--steps 4000]
+    python -m kutta_b200.learn --out weights.npy [--systems 250] [--rhs 8] [--steps 20000]
 """
 from __future__ import annotations
 
 import argparse
 import json
 import pathlib
+import sys
 import time
 
 import numpy as np
@@ -48,8 +53,36 @@ def system(n_side: int, seed: int) -> harness.HostSystem:
                               field_sigma=FIELD_SIGMA, field_corr=FIELD_CORR)
 
 
+def _csr64(s: harness.HostSystem):
+    import torch
+    return torch.sparse_csr_tensor(torch.from_numpy(s.row_ptr.astype(np.int64)),
+                                   torch.from_numpy(s.col.astype(np.int64)),
+                                   torch.from_numpy(s.val.astype(np.float64)),
+                                   (s.n, s.n)).cuda()
+
+
+def pairs(s: harness.HostSystem, a: L.CsrMatrix, solver: L.MixedSolver, b, x):
+    """(t, e) pairs with A e = t from the solution x of A x = b: the residual
+    of x_k = 0 and of a solve to relative 1e-3, each after one application of
+    the preconditioner."""
+    import torch
+    A = _csr64(s)
+    out = []
+    xk = torch.zeros(s.n, dtype=torch.float64, device="cuda")
+    for tol in (None, 1e-3):
+        if tol is not None:
+            solver.solve(a, xk, b, L.SolveControl(tol, 1e-30, 3000))
+        r = (b.double() - A @ xk).float()
+        z = torch.zeros(s.n, dtype=torch.float32, device="cuda")
+        solver.precondition(a, r, z)
+        t = r.double() - A @ z.double()
+        e = (x - xk) - z.double()
+        out.append((t.float(), e.float()))
+    return out
+
+
 def training_set(count: int, n_side: int, rhs_per_system: int, seed0: int):
-    """[(device matrix, b, x)] with x the mixed solve's solution of A x = b."""
+    """[(device matrix, t, e)] from `count` systems x `rhs_per_system` solves."""
     import torch
     rng = np.random.default_rng(seed0)
     data = []
@@ -63,25 +96,43 @@ def training_set(count: int, n_side: int, rhs_per_system: int, seed0: int):
             x = torch.zeros(s.n, dtype=torch.float64, device="cuda")
             st = solver.solve(a, x, b, L.SolveControl(1e-8, 1e-30, 3000))
             if st.converged:
-                data.append((a, b, x.float()))
+                data.extend((a, t, e) for t, e in pairs(s, a, solver, b, x))
         del solver
     return data
 
 
 def train(stage: L.LearnedStage, data, steps: int, learning_rate: float, seed: int = 0):
     rng = np.random.default_rng(seed)
-    order = rng.permutation(len(data))
+    order = np.concatenate([rng.permutation(len(data))
+                            for _ in range(steps // max(1, len(data)) + 1)])
     bound = None
     losses = []
     for step in range(steps):
-        a, b, x = data[order[step % len(order)]]
+        a, t, e = data[order[step]]
         if bound is not a:
             stage.bind(a)
             bound = a
         # Cosine decay to a tenth of the rate.
         lr = learning_rate * (0.1 + 0.9 * 0.5 * (1.0 + np.cos(np.pi * step / steps)))
-        losses.append(stage.train_step(b, x, learning_rate=float(lr)))
+        losses.append(stage.train_step(t, e, learning_rate=float(lr)))
+        if (step + 1) % 1000 == 0:
+            print(f"step {step + 1}: energy loss {np.mean(losses[-1000:]):.4f}", file=sys.stderr,
+                  flush=True)
     return losses
+
+
+def held_out_loss(stage: L.LearnedStage, data) -> float:
+    """Mean energy loss over pairs, measured as a training step with a
+    negligible rate on a copy of the weights (the weights are restored)."""
+    w = stage.weights()
+    bound, losses = None, []
+    for a, t, e in data:
+        if bound is not a:
+            stage.bind(a)
+            bound = a
+        losses.append(stage.train_step(t, e, learning_rate=1e-30))
+        stage.set_weights(w)
+    return float(np.mean(losses))
 
 
 def evaluate(stage: L.LearnedStage | None, n_side: int, seeds, rel_tol: float = 1e-6) -> dict:
@@ -104,10 +155,10 @@ def evaluate(stage: L.LearnedStage | None, n_side: int, seeds, rel_tol: float = 
                 x = torch.zeros(s.n, dtype=torch.float32, device="cuda")
             else:
                 solver = L.make_mixed_solver(s)
-                if g is not None:
-                    solver.set_learned(g)
                 x = torch.zeros(s.n, dtype=torch.float64, device="cuda")
             solver.refresh(a)
+            if g is not None:
+                solver.set_learned(g, L.LEARNED_CYCLE)
             best, st = None, None
             for _ in range(3):
                 x.zero_()
@@ -122,7 +173,11 @@ def evaluate(stage: L.LearnedStage | None, n_side: int, seeds, rel_tol: float = 
             row[name] = {"ms": best, "iterations": st.iterations, "converged": bool(st.converged),
                          "relative_residual": st.final_residual / st.initial_residual}
             if g is not None:
+                x_true = torch.zeros(s.n, dtype=torch.float64, device="cuda")
                 solver.set_learned(None)
+                solver.solve(a, x_true, b, L.SolveControl(1e-8, 1e-30, 3000))
+                row["held_out_energy_loss"] = held_out_loss(g, [(a, t, e) for t, e in
+                                                                pairs(s, a, solver, b, x_true)])
             del solver
         results.append(row)
     return {"rel_tol": rel_tol, "mesh": f"{n_side}^3 jittered hex, smooth log-normal D_f "
@@ -133,10 +188,10 @@ def evaluate(stage: L.LearnedStage | None, n_side: int, seeds, rel_tol: float = 
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--out", required=True, help="weights file (.npy) to write")
-    ap.add_argument("--systems", type=int, default=48)
-    ap.add_argument("--rhs", type=int, default=4)
+    ap.add_argument("--systems", type=int, default=250)
+    ap.add_argument("--rhs", type=int, default=8)
     ap.add_argument("--n", type=int, default=64)
-    ap.add_argument("--steps", type=int, default=4000)
+    ap.add_argument("--steps", type=int, default=20000)
     ap.add_argument("--lr", type=float, default=2e-3)
     ap.add_argument("--seed", type=int, default=1000)
     ap.add_argument("--eval-n", type=int, default=128)
@@ -149,7 +204,7 @@ def main():
     losses = train(stage, data, args.steps, args.lr)
     t2 = time.time()
     np.save(args.out, stage.weights())
-    report = {"triples": len(data), "data_s": t1 - t0, "train_s": t2 - t1,
+    report = {"pairs": len(data), "solutions": len(data) // 2, "data_s": t1 - t0, "train_s": t2 - t1,
               "loss_first": float(np.mean(losses[:50])), "loss_last": float(np.mean(losses[-50:])),
               "evaluation": evaluate(stage, args.eval_n,
                                      [args.seed + 10_000 + k for k in range(args.eval_seeds)])}

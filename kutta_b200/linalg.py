@@ -185,10 +185,11 @@ _SIGNATURES = {
     "b2_gnn_parameter_count": (_I, []),
     "b2_gnn_bind": (_I, [_P, _I, _P, _P, _P, _P, _P]),
     "b2_gnn_apply": (_I, [_P, _P, _P, ctypes.c_float, _P]),
-    "b2_gnn_train_step": (_I, [_P, _P, _P, ctypes.c_double, ctypes.c_float, _P, _P]),
+    "b2_gnn_train_step": (_I, [_P, _P, _P, ctypes.c_float, _P, _P]),
     "b2_gnn_get_weights": (_I, [_P, _P, ctypes.c_size_t]),
     "b2_gnn_set_weights": (_I, [_P, _P, ctypes.c_size_t]),
-    "b2_mixed_set_learned": (_I, [_P, _P]),
+    "b2_mixed_set_learned": (_I, [_P, _P, _I]),
+    "b2_mixed_precondition": (_I, [_P, _P, _P, _P, _P]),
     "b2_mixed_profile": (_I, [_P, _I]),
     "b2_mixed_profile_read": (_I, [_P, _P]),
 }
@@ -482,6 +483,11 @@ def _mixed_struct(o: MixedOptions) -> _MixedOptions:
     return s
 
 
+# b2_mixed_set_learned mode bits.
+LEARNED_CYCLE = 1
+LEARNED_WARM_START = 2
+
+
 class MixedSolver:
     """FP64 iterative refinement around the FP32 AMG-PCG with BF16 coarse
     levels and a dense FP64 coarsest solve; the solution is FP64."""
@@ -527,11 +533,18 @@ class MixedSolver:
         _check(_load().b2_mixed_profile_read(self._handle, ctypes.byref(p)))
         return {f: getattr(p, f) for f, _ in _Profile._fields_}
 
-    def set_learned(self, stage: "LearnedStage | None") -> None:
-        """Attaches a learned correction after each AMG cycle (None detaches);
-        the stage must stay alive while attached."""
+    def set_learned(self, stage: "LearnedStage | None", mode: int = LEARNED_CYCLE) -> None:
+        """Attaches a learned stage (None detaches): after each AMG cycle
+        (LEARNED_CYCLE) and/or as a warm-start step (LEARNED_WARM_START); the
+        stage must stay alive while attached."""
         self._learned = stage
-        _check(_load().b2_mixed_set_learned(self._handle, stage._handle if stage else None))
+        _check(_load().b2_mixed_set_learned(self._handle, stage._handle if stage else None,
+                                            int(mode) if stage else 0))
+
+    def precondition(self, a: CsrMatrix, r, z) -> None:
+        """z = M(r): one application of the preconditioner (float32 tensors)."""
+        _check(_load().b2_mixed_precondition(self._handle, _tptr(a.val), _tptr(r), _tptr(z),
+                                             _stream()))
 
     def __del__(self):
         if getattr(self, "_handle", None) and _lib is not None:
@@ -542,8 +555,9 @@ class MixedSolver:
 class LearnedStage:
     """b2_gnn: the learned preconditioner stage (no reference counterpart), a
     3-layer message-passing network of width 32 over the matrix graph, mapping
-    a residual r to a correction G(r) ~ A^-1 r; trained with hand-written CUDA
-    forward, backward and Adam kernels."""
+    a residual r to a correction direction G(r) (G(lambda r) = lambda G(r));
+    trained with hand-written CUDA forward, backward and Adam kernels on the
+    energy loss of (residual, error) pairs."""
 
     def __init__(self, seed: int = 1):
         handle = ctypes.c_void_p()
@@ -562,12 +576,12 @@ class LearnedStage:
     def apply(self, r, z, beta: float = 0.0) -> None:
         _check(_load().b2_gnn_apply(self._handle, _tptr(r), _tptr(z), beta, _stream()))
 
-    def train_step(self, b, x, learning_rate: float = 1e-3) -> float:
-        """One Adam step on |G(b) - x|^2 / |x|^2 for the bound matrix; returns the loss."""
-        x_norm2 = float((x.double() ** 2).sum())
+    def train_step(self, t, e, learning_rate: float = 1e-3) -> float:
+        """One Adam step on the energy loss 1 - (c.t)^2 / ((c.Ac)(t.e)), c = G(t),
+        for A e = t with the bound matrix; returns the loss before the step."""
         loss = ctypes.c_float()
-        _check(_load().b2_gnn_train_step(self._handle, _tptr(b), _tptr(x), x_norm2,
-                                         learning_rate, ctypes.byref(loss), _stream()))
+        _check(_load().b2_gnn_train_step(self._handle, _tptr(t), _tptr(e), learning_rate,
+                                         ctypes.byref(loss), _stream()))
         return float(loss.value)
 
     def weights(self) -> np.ndarray:
