@@ -235,6 +235,24 @@ def run_ours(args, rank, world, local):
     e2e_ms, _ = _timed(e2e_step, args.steps, stream, sync)
     e2e_ms = max_over_ranks(e2e_ms)
 
+    # ---- the same solver with the trained learned stage after each cycle ----
+    from kutta_b200 import learn
+    stage = learn.trained_stage()
+    mixed.set_learned(stage, L.LEARNED_CYCLE)
+    mixed_step()
+    learned_ms, lstats = _timed(mixed_step, max(1, min(args.steps, 5)), stream, sync)
+    learned_ms = max_over_ranks(learned_ms)
+    mixed.set_learned(None)
+    llast = lstats[-1]
+    learned_line = {
+        "method": "as method, plus the learned stage (packaged trained weights, tensor-core "
+                  "forward) after each cycle: z += alpha G(r - A z), energy-optimal alpha",
+        "ms_per_solve": learned_ms, "iterations": llast.iterations,
+        "converged": llast.converged,
+        "relative_residual": llast.final_residual / llast.initial_residual,
+        "steps": max(1, min(args.steps, 5)),
+    }
+
     # ---- plain FP32 AMG-PCG: the reference's method on the same GPU ----
     t0 = time.perf_counter()
     plain = L.make_solver(L.SolverKind.AmgPcg, s,
@@ -276,7 +294,8 @@ def run_ours(args, rank, world, local):
         "dtype": "f32 operator, bf16 coarse levels, f64 refinement/reductions/coarsest",
         "data": "synthetic (seeded FV pressure matrix; no dataset)",
         "config": _config(args, s, world),
-        "method": mixed.describe() + " (learned stage: not built)",
+        "method": mixed.describe(),
+        "learned_mixed": learned_line,
         "refinements": last.refinements, "iterations": last.iterations,
         "converged": last.converged,
         "relative_residual": last.final_residual / last.initial_residual,
@@ -426,10 +445,12 @@ def run_sequence(args):
     tet mesh, a right-hand side of 16 seeded Fourier modes over the cell
     centroids whose phases drift 0.01 rad per solve, and D_f blended toward a
     fresh seeded field with factor 0.7 every 50 solves, refreshing the
-    solvers then. Each solve starts from the previous solution (the learned
-    warm start is not built) and runs to rel_tol relative to its own initial
-    residual. Reports total and per-solve p50/p99 device time for the mixed
-    solve and for the plain FP32 AMG-PCG."""
+    solvers then. Each solve starts from the previous solution and runs to
+    rel_tol relative to its own initial residual; the learned+mixed arm first
+    corrects that start by the learned warm start (one safeguarded step along
+    G(b - A x_prev), packaged trained weights). Reports total and per-solve
+    p50/p99 device time for the mixed solve with and without the learned warm
+    start and for the plain FP32 AMG-PCG."""
     import numpy as np
     import torch
     from kutta_b200 import linalg as L
@@ -449,9 +470,13 @@ def run_sequence(args):
         return ((torch.sin(arg) @ amp) * volume).to(torch.float32)
 
     control = L.SolveControl(args.rel_tol, 1e-30, args.max_iter)
-    arms = {"mixed": L.make_mixed_solver(s), "plain": L.make_solver(
-        L.SolverKind.AmgPcg, s, L.SolverOptions(structure=L.OperatorStructure.SymmetricMMatrix))}
+    from kutta_b200 import learn
+    stage = learn.trained_stage()
+    arms = {"mixed": L.make_mixed_solver(s), "learned+mixed": L.make_mixed_solver(s),
+            "plain": L.make_solver(L.SolverKind.AmgPcg, s, L.SolverOptions(
+                structure=L.OperatorStructure.SymmetricMMatrix))}
     x = {"mixed": torch.zeros(s.n, dtype=torch.float64, device="cuda"),
+         "learned+mixed": torch.zeros(s.n, dtype=torch.float64, device="cuda"),
          "plain": torch.zeros(s.n, dtype=torch.float32, device="cuda")}
     times = {name: [] for name in arms}
     refresh_ms = {name: 0.0 for name in arms}
@@ -459,6 +484,7 @@ def run_sequence(args):
     conv = {name: 0 for name in arms}
     for name, solver in arms.items():
         solver.refresh(a)
+    arms["learned+mixed"].set_learned(stage, L.LEARNED_WARM_START)
     for t in range(args.solves):
         if t > 0 and t % 50 == 0:
             fresh = _graded(args, coeff_seed=1000 + t)
@@ -486,7 +512,8 @@ def run_sequence(args):
     out = {"mode": "sequence", "solves": args.solves, "rel_tol": args.rel_tol,
            "workload": f"graded_tet{args.size}: {args.size}^3 x 6 tets, 10-layer 1000:1 band at "
                        f"z=0, D_f log-uniform [1e-6, 1], {s.n} cells, {s.nnz} nonzeros",
-           "warm_start": "previous solution (learned warm start: not built)"}
+           "warm_start": "previous solution; learned+mixed: previous solution corrected by "
+                         "the learned warm start"}
     for name, solver in arms.items():
         ts = sorted(times[name])
         out[name] = {"method": solver.describe(), "total_ms": sum(ts),

@@ -47,6 +47,11 @@ constexpr int kTcSmem = 1024 + kTileBytes + kWeightBytes + kMiscFloats * 4 + 16;
 constexpr int kTcPerSm = 4;
 constexpr long long kSpinLimit = 1LL << 22;     // mbarrier polls before giving up
 constexpr uint32_t kTmemColumns = 32;
+// Neighbours whose loads are issued together: all of a tet or hex row for the
+// lifted pairs (8 bytes each), half of it for the 64-byte BF16 rows, whose
+// registers would otherwise spill.
+template <bool kLift>
+constexpr int kBatch = kLift ? 8 : 4;
 
 // Instruction descriptor of tcgen05.mma kind::f16: FP32 accumulator (bits
 // 4-5 = 1), BF16 A and B (bits 7-9 and 10-12 = 1), both K-major (bits 15 and
@@ -83,6 +88,18 @@ __device__ __forceinline__ uint32_t pack_bf16(float lo, float hi) {
 }
 __device__ __forceinline__ float bf16_lo(uint32_t w) { return __uint_as_float(w << 16); }
 __device__ __forceinline__ float bf16_hi(uint32_t w) { return __uint_as_float(w & 0xFFFF0000u); }
+
+// m[0..7] += w * (8 BF16 values of q).
+__device__ __forceinline__ void accumulate8(float w, uint4 q, float* m) {
+  m[0] = fmaf(w, bf16_lo(q.x), m[0]);
+  m[1] = fmaf(w, bf16_hi(q.x), m[1]);
+  m[2] = fmaf(w, bf16_lo(q.y), m[2]);
+  m[3] = fmaf(w, bf16_hi(q.y), m[3]);
+  m[4] = fmaf(w, bf16_lo(q.z), m[4]);
+  m[5] = fmaf(w, bf16_hi(q.z), m[5]);
+  m[6] = fmaf(w, bf16_lo(q.w), m[6]);
+  m[7] = fmaf(w, bf16_hi(q.w), m[7]);
+}
 
 __device__ __forceinline__ uint4 pack8(const float* v) {
   return make_uint4(pack_bf16(v[0], v[1]), pack_bf16(v[2], v[3]), pack_bf16(v[4], v[5]),
@@ -202,7 +219,7 @@ __global__ void k_gnn_lift(int n, const int* __restrict__ rows, const int* __res
 // kLift: the input is the lifted pair uv (layer A, output BF16 rows hout);
 // otherwise the BF16 rows hin (layer B, output z).
 template <bool kLift>
-__global__ void __launch_bounds__(kTcThreads)
+__global__ void __launch_bounds__(kTcThreads, kLift ? 2 : 4)
     k_gnn_layer_tc(int n, const int* __restrict__ rows, const int* __restrict__ cols,
                    const float* __restrict__ edge, const float2* __restrict__ uv,
                    const uint4* __restrict__ hin, const float* __restrict__ first,
@@ -274,21 +291,21 @@ __global__ void __launch_bounds__(kTcThreads)
           h[k] = fmaxf(fmaf(ws1[c0 + k], u, fmaf(wn1[c0 + k], v, b1[c0 + k])), 0.0f);
         own[0] = pack8(h);
         own[1] = pack8(h + 8);
-        for (int j0 = start; j0 < end; j0 += 4) {
-          int cc[4];
-          float ww[4];
-          float2 q[4];
+        for (int j0 = start; j0 < end; j0 += kBatch<kLift>) {
+          int cc[kBatch<kLift>];
+          float ww[kBatch<kLift>];
+          float2 q[kBatch<kLift>];
 #pragma unroll
-          for (int k = 0; k < 4; ++k) {
+          for (int k = 0; k < kBatch<kLift>; ++k) {
             const int j = j0 + k;
             cc[k] = j < end ? cols[j] : i;
             ww[k] = j < end ? edge[j] : 0.0f;
           }
 #pragma unroll
-          for (int k = 0; k < 4; ++k)
+          for (int k = 0; k < kBatch<kLift>; ++k)
             q[k] = (cc[k] != i && ww[k] != 0.0f) ? uv[cc[k]] : make_float2(0.0f, 0.0f);
 #pragma unroll
-          for (int k = 0; k < 4; ++k) {
+          for (int k = 0; k < kBatch<kLift>; ++k) {
             if (cc[k] == i || ww[k] == 0.0f) continue;
             const float uj = q[k].x * inv_rho, vj = q[k].y * inv_rho;
 #pragma unroll
@@ -301,18 +318,18 @@ __global__ void __launch_bounds__(kTcThreads)
         const uint4* self = hin + static_cast<std::size_t>(i) * 4 + half * 2;
         own[0] = __ldg(self);
         own[1] = __ldg(self + 1);
-        for (int j0 = start; j0 < end; j0 += 4) {
-          int cc[4];
-          float ww[4];
-          uint4 qa[4], qb[4];
+        for (int j0 = start; j0 < end; j0 += kBatch<kLift>) {
+          int cc[kBatch<kLift>];
+          float ww[kBatch<kLift>];
+          uint4 qa[kBatch<kLift>], qb[kBatch<kLift>];
 #pragma unroll
-          for (int k = 0; k < 4; ++k) {
+          for (int k = 0; k < kBatch<kLift>; ++k) {
             const int j = j0 + k;
             cc[k] = j < end ? cols[j] : i;
             ww[k] = j < end ? edge[j] : 0.0f;
           }
 #pragma unroll
-          for (int k = 0; k < 4; ++k) {
+          for (int k = 0; k < kBatch<kLift>; ++k) {
             if (cc[k] != i && ww[k] != 0.0f) {
               const uint4* nb = hin + static_cast<std::size_t>(cc[k]) * 4 + half * 2;
               qa[k] = __ldg(nb);
@@ -323,15 +340,10 @@ __global__ void __launch_bounds__(kTcThreads)
             }
           }
 #pragma unroll
-          for (int k = 0; k < 4; ++k) {
+          for (int k = 0; k < kBatch<kLift>; ++k) {
             const float w = (cc[k] != i) ? ww[k] : 0.0f;
-            const uint32_t words[8] = {qa[k].x, qa[k].y, qa[k].z, qa[k].w,
-                                       qb[k].x, qb[k].y, qb[k].z, qb[k].w};
-#pragma unroll
-            for (int e = 0; e < 8; ++e) {
-              m[2 * e] = fmaf(w, bf16_lo(words[e]), m[2 * e]);
-              m[2 * e + 1] = fmaf(w, bf16_hi(words[e]), m[2 * e + 1]);
-            }
+            accumulate8(w, qa[k], m);
+            accumulate8(w, qb[k], m + 8);
           }
         }
       }

@@ -18,6 +18,7 @@ relative 1e-6 with and without the stage attached, and the plain FP32
 AMG-PCG, device-timed; the held-out energy loss on the same kind of pairs.
 
     python -m kutta_b200.learn --out weights.npy [--systems 250] [--rhs 8] [--steps 20000]
+    python -m kutta_b200.learn --time-forward 128
 """
 from __future__ import annotations
 
@@ -185,9 +186,45 @@ def evaluate(stage: L.LearnedStage | None, n_side: int, seeds, rel_tol: float = 
             "results": results}
 
 
+WEIGHTS = pathlib.Path(__file__).resolve().parent / "data" / "learned_stage.npy"
+
+
+def trained_stage() -> L.LearnedStage:
+    """The stage with the packaged weights (data/learned_stage.npy, written by
+    this module's training run; data/learned_stage.json records the command
+    and its report)."""
+    g = L.LearnedStage(seed=1)
+    g.set_weights(np.load(WEIGHTS))
+    return g
+
+
+def time_forward(n_side: int, repeats: int = 10) -> dict:
+    """Device time of one tensor-core forward of an (untrained) stage on the
+    n^3 evaluation mesh, averaged over `repeats` applications."""
+    import torch
+    s = system(n_side, 5)
+    a = L.upload(s)
+    g = L.LearnedStage(seed=1)
+    g.bind(a)
+    r = torch.from_numpy(fourier_rhs(s, np.random.default_rng(5))).cuda()
+    z = torch.zeros(s.n, device="cuda")
+    for _ in range(3):
+        g.apply(r, z)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record()
+    for _ in range(repeats):
+        g.apply(r, z)
+    e1.record()
+    torch.cuda.synchronize()
+    return {"n": s.n, "nnz": int(s.row_ptr[-1]), "forward_ms": e0.elapsed_time(e1) / repeats}
+
+
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--out", required=True, help="weights file (.npy) to write")
+    ap.add_argument("--out", help="weights file (.npy) to write")
+    ap.add_argument("--time-forward", type=int, metavar="N",
+                    help="only time the forward on the N^3 mesh and exit")
     ap.add_argument("--systems", type=int, default=250)
     ap.add_argument("--rhs", type=int, default=8)
     ap.add_argument("--n", type=int, default=64)
@@ -197,6 +234,11 @@ def main():
     ap.add_argument("--eval-n", type=int, default=128)
     ap.add_argument("--eval-seeds", type=int, default=2)
     args = ap.parse_args()
+    if args.time_forward:
+        print(json.dumps(time_forward(args.time_forward)))
+        return
+    if not args.out:
+        ap.error("--out is required for training")
     t0 = time.time()
     data = training_set(args.systems, args.n, args.rhs, args.seed)
     t1 = time.time()
