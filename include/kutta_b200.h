@@ -49,6 +49,11 @@ typedef enum {
 typedef enum { B2_NULLSPACE_NONE = 0, B2_NULLSPACE_CONSTANT = 1 } b2_nullspace;
 typedef enum { B2_STRUCTURE_GENERAL = 0, B2_STRUCTURE_SYMMETRIC_M_MATRIX = 1 } b2_structure;
 typedef enum { B2_CYCLE_V = 0, B2_CYCLE_K = 1 } b2_cycle;
+/* Where the AMG hierarchy is built (no reference counterpart; the results are
+ * the same bit for bit). B2_SETUP_DEVICE runs the pairing, coarsening and
+ * Galerkin product on the GPU when the pattern is structurally symmetric, and
+ * falls back to the host setup otherwise. */
+typedef enum { B2_SETUP_HOST = 0, B2_SETUP_DEVICE = 1 } b2_setup;
 
 typedef struct b2_workspace b2_workspace;
 typedef struct b2_solver b2_solver;
@@ -68,6 +73,7 @@ typedef struct {
   int nullspace;           /* b2_nullspace; default none */
   int structure;           /* b2_structure; default general */
   b2_workspace* workspace; /* KrylovWorkspace (solver.hpp:47-64) or NULL */
+  int setup;               /* b2_setup; default device */
 } b2_options;
 
 /* SolveControl, solver.hpp:18-23. */
@@ -291,6 +297,14 @@ int b2_solver_levels(const b2_solver* solver);
 int b2_solver_level_shape(const b2_solver* solver, int level, int* n, int* nnz);
 int b2_solver_level_copy(const b2_solver* solver, int level, int32_t* row_ptr, int32_t* col,
                          float* val, float* inverse_l1, int32_t* aggregate, void* stream);
+/* The level's diagonal positions diag[n] and its transfer to level + 1 (none
+ * on the coarsest): member_offsets[n_c + 1], members (at most n), entry_offsets
+ * [nnz_c + 1] and entries (at most nnz), the last two the Galerkin entry map
+ * (coarse entry e sums the level's entries entries[entry_offsets[e] ..
+ * entry_offsets[e+1])). Synchronous reads on `stream`; any pointer may be NULL. */
+int b2_solver_level_transfer(const b2_solver* solver, int level, int32_t* diag,
+                             int32_t* member_offsets, int32_t* members, int32_t* entry_offsets,
+                             int32_t* entries, void* stream);
 
 /* Host-only AMG setup (no GPU needed): the aggregation hierarchy that
  * b2_solver_create builds (Aggregation ctor, amg.cpp:200-226: pairs :25-75,

@@ -43,10 +43,11 @@ PRODUCT_CU = {
     "tail_cycle.cu": [],
     "learned.cu": [],
     "learned_tc.cu": [],
+    "setup_kernels.cu": EXACT,
     "noalloc.cu": [],
 }
-PRODUCT_CPP = ["host/setup.cpp", "host/solver.cpp", "host/mixed.cpp", "host/learned.cpp",
-               "capi.cpp"]
+PRODUCT_CPP = ["host/setup.cpp", "host/solver.cpp", "host/device_setup.cpp", "host/mixed.cpp",
+               "host/learned.cpp", "capi.cpp"]
 
 
 def _hash(paths, extra=""):

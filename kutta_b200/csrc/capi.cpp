@@ -82,6 +82,8 @@ kb2::Options to_options(const b2_options* o) {
   KB2_REQUIRE(o->structure == B2_STRUCTURE_GENERAL || o->structure == B2_STRUCTURE_SYMMETRIC_M_MATRIX,
               "AMG: invalid operator structure");
   r.m_matrix = o->structure == B2_STRUCTURE_SYMMETRIC_M_MATRIX;
+  KB2_REQUIRE(o->setup == B2_SETUP_HOST || o->setup == B2_SETUP_DEVICE, "AMG: invalid setup option");
+  r.device_setup = o->setup == B2_SETUP_DEVICE;
   return r;
 }
 
@@ -123,6 +125,7 @@ void b2_options_default(b2_options* o) {
   o->nullspace = B2_NULLSPACE_NONE;
   o->structure = B2_STRUCTURE_GENERAL;
   o->workspace = nullptr;
+  o->setup = B2_SETUP_DEVICE;
 }
 
 void b2_control_default(b2_control* c) {
@@ -160,10 +163,11 @@ int b2_solver_create(int kind, int n, int nnz, const int32_t* row_ptr, const int
       o = to_options(options);
     } else if (options) {
       // make_solver: AMG defaults with only nullspace and structure taken over
-      // (amg.cpp:388-396).
+      // (amg.cpp:388-396), and where the hierarchy is built.
       const auto given = to_options(options);
       o.nullspace = given.nullspace;
       o.m_matrix = given.m_matrix;
+      o.device_setup = given.device_setup;
     }
     std::shared_ptr<kb2::Workspace> ws = options && options->workspace ? options->workspace->w : nullptr;
     if (k == kb2::Kind::AmgPcg || k == kb2::Kind::AmgBicgstab) {
@@ -299,6 +303,31 @@ int b2_solver_level_copy(const b2_solver* s, int level, int32_t* row_ptr, int32_
     if (l.l1.allocated()) get(inverse_l1, l.l1.get(), sizeof(float) * static_cast<std::size_t>(l.n));
     if (l.aggregate.allocated())
       get(aggregate, l.aggregate.get(), sizeof(int) * static_cast<std::size_t>(l.n));
+    kb2::wait(st);
+  });
+}
+
+int b2_solver_level_transfer(const b2_solver* s, int level, int32_t* diag, int32_t* member_offsets,
+                             int32_t* members, int32_t* entry_offsets, int32_t* entries,
+                             void* stream) {
+  return guarded([&] {
+    KB2_REQUIRE(s && s->s && level >= 0 && level < s->s->levels(), "level out of range");
+    const auto& l = s->s->level(level);
+    const auto st = as_stream(stream);
+    auto get = [&](void* dst, const kb2::DArray<int>& src, std::size_t count) {
+      if (dst && src.allocated() && count)
+        kb2::cuda_check(cudaMemcpyAsync(dst, src.get(), sizeof(int) * count,
+                                        cudaMemcpyDeviceToHost, st),
+                        "level copy");
+    };
+    get(diag, l.diag, static_cast<std::size_t>(l.n));
+    if (level + 1 < s->s->levels()) {
+      const auto& c = s->s->level(level + 1);
+      get(member_offsets, l.member_offsets, static_cast<std::size_t>(c.n) + 1);
+      get(members, l.members, l.members.size());
+      get(entry_offsets, l.entry_offsets, static_cast<std::size_t>(c.nnz) + 1);
+      get(entries, l.entries, l.entries.size());
+    }
     kb2::wait(st);
   });
 }

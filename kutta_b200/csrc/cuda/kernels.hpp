@@ -228,6 +228,46 @@ void gnn_layer_b(int n, const int* rows, const int* cols, const float* edge,
                  const float* wo, const float* node_scale, const double* sum2, float* z,
                  float beta, int* fault, cudaStream_t s);
 
+// ---- AMG setup on the device (setup_kernels.cu) -----------------------------
+// out[0..n] = exclusive scan of in[0..n) (out[n] = total); block_sums holds
+// scan_scratch(n) ints.
+void exclusive_scan(int n, const int* in, int* out, int* block_sums, cudaStream_t s);
+int scan_scratch(int n);
+// flag[0] = 1 if some entry (i, j) has no entry (j, i).
+void pattern_symmetric(int n, const int* rows, const int* cols, int* flag, cudaStream_t s);
+// Pairing: candidate counts and initial states, preference lists (keys is
+// scratch of the same length), and one Jacobi sweep of the greedy pass
+// (owner: n ints of scratch; changed[0] = 1 if a row's state moved).
+void pair_count(int n, const int* rows, const int* cols, const float* vals, double threshold,
+                int exclude_isolated, int* count, int* state, cudaStream_t s);
+void pair_fill(int n, const int* rows, const int* cols, const float* vals, double threshold,
+               const int* offsets, unsigned long long* keys, int* pref, cudaStream_t s);
+void pair_sweep(int n, const int* offsets, const int* pref, int* owner, const int* state,
+                int* next, int* changed, cudaStream_t s);
+void pair_leaders(int n, const int* state, int* flag, cudaStream_t s);
+void pair_assign(int n, const int* state, const int* owner, const int* id, int* aggregate,
+                 cudaStream_t s);
+// Singleton absorption (mixed hierarchy): sizes, one Jacobi sweep, used marks.
+void aggregate_sizes(int n, const int* aggregate, int* size, cudaStream_t s);
+void absorb_sweep(int n, const int* rows, const int* cols, const int* diag, const float* vals,
+                  double threshold, double coupling, const int* map0, const int* size0,
+                  const int* cur, int* next, int* changed, cudaStream_t s);
+void mark_used(int n, const int* aggregate, int* used, cudaStream_t s);
+// map[i] = table[map[i]] where map[i] >= 0.
+void compose(int n, int* map, const int* table, cudaStream_t s);
+// Coarse pattern and entry map of an aggregation.
+void coarsen_count(int n, const int* rows, const int* cols, const int* aggregate, int* size,
+                   int* triples, cudaStream_t s);
+void place_members(int n, const int* aggregate, const int* offsets, int* cursor, int* members,
+                   cudaStream_t s);
+void sort_members(int nc, const int* offsets, int* members, cudaStream_t s);
+void coarsen_triples(int nc, const int* rows, const int* cols, const int* aggregate,
+                     const int* member_offsets, const int* members, const int* triple_offsets,
+                     int m_matrix, int4* triples, int* unique, cudaStream_t s);
+void coarsen_fill(int nc, const int* triple_offsets, const int4* triples, const int* coarse_rows,
+                  int* coarse_cols, int* coarse_diag, int* entry_offsets, int* entries,
+                  cudaStream_t s);
+
 // ---- single-thread scalar kernels -------------------------------------------
 void solver_limits(float* scalars, float th, float tl, float dh, float dl, cudaStream_t s);
 void solver_reset(float* scalars, int* status, int iterations, cudaStream_t s);

@@ -61,6 +61,9 @@ struct Options {  // AmgOptions, src/kutta/linalg/amg.hpp:8-20
   // Replay each AMG preconditioner application as a captured CUDA graph (the
   // same kernels with the same arguments, so the same results).
   bool graphs = false;
+  // Build the hierarchy on the device (same aggregates, patterns and values as
+  // the host setup) when the pattern is structurally symmetric.
+  bool device_setup = true;
 };
 
 // CsrMatrixHost (src/kutta/linalg/csr.hpp:16-28). val holds float-representable

@@ -45,7 +45,10 @@ Solver::Solver(Kind kind, const CsrView& a, const Options& options,
     l.diag.reset(static_cast<std::size_t>(a.n));
     l.diag.upload(a.diag, static_cast<std::size_t>(a.n), s);
   }
-  if (amg()) {
+  if (amg() && options_.device_setup && device_pattern_symmetric(s)) {
+    // Aggregation ctor (amg.cpp:200-226) on the device.
+    build_device_levels(a, s);
+  } else if (amg()) {
     // Aggregation ctor (amg.cpp:200-226): host hierarchy, then uploads.
     const Hierarchy h = build_hierarchy(a, options_);
     complexity_ = h.complexity;
@@ -67,9 +70,6 @@ Solver::Solver(Kind kind, const CsrView& a, const Options& options,
       }
       auto& l = levels_.back();
       l.l1.upload(h.levels[i].l1, s);
-      l.ra.reset(static_cast<std::size_t>(l.n));
-      l.r = l.ra.get();
-      if (nullspace_) l.projection.reset(2);
       const auto& t = h.levels[i].transfer;
       if (i + 1 < h.levels.size()) {
         l.aggregate.upload(t.aggregate, s);
@@ -78,6 +78,13 @@ Solver::Solver(Kind kind, const CsrView& a, const Options& options,
         l.entry_offsets.upload(t.entry_offsets, s);
         l.entries.upload(t.entries, s);
       }
+    }
+  }
+  if (amg()) {
+    for (auto& l : levels_) {
+      l.ra.reset(static_cast<std::size_t>(l.n));
+      l.r = l.ra.get();
+      if (nullspace_) l.projection.reset(2);
     }
     // K-cycle work vectors on the levels reached through inner() (Level ctor,
     // amg.cpp:179-195): every coarse level but the coarsest.

@@ -114,6 +114,11 @@ class Solver {
   bool inner_level(std::size_t index) const {
     return options_.k_levels <= 0 || index <= static_cast<std::size_t>(options_.k_levels);
   }
+  // The hierarchy built on the device (device_setup.cpp) when the options ask
+  // for it and the pattern is structurally symmetric; the host setup else.
+  bool device_pattern_symmetric(cudaStream_t s);
+  void build_device_levels(const CsrView& a, cudaStream_t s);
+  bool device_setup_ = false;
   void prepare_mixed(cudaStream_t s, int error_slot);
   void choose_coarsest(double smallest_pivot);
   bool dense_ok_ = false;  // the dense coarsest inverse is used (well conditioned)

@@ -96,11 +96,18 @@ class KrylovWorkspace:  # solver.hpp:47-64
             self._handle = None
 
 
+class Setup(enum.IntEnum):
+    """b2_setup: where the AMG hierarchy is built (the same results either way)."""
+    Host = 0
+    Device = 1
+
+
 @dataclasses.dataclass
 class SolverOptions:  # solver.hpp:66-72
     nullspace: NullSpace = NullSpace.None_
     structure: OperatorStructure = OperatorStructure.General
     workspace: KrylovWorkspace | None = None
+    setup: Setup = Setup.Device
 
 
 @dataclasses.dataclass
@@ -116,6 +123,7 @@ class AmgOptions:  # amg.hpp:8-20
     nullspace: NullSpace = NullSpace.None_
     structure: OperatorStructure = OperatorStructure.General
     workspace: KrylovWorkspace | None = None
+    setup: Setup = Setup.Device
 
 
 class _Options(ctypes.Structure):
@@ -124,7 +132,7 @@ class _Options(ctypes.Structure):
                 ("coarse_rows", ctypes.c_int), ("max_levels", ctypes.c_int),
                 ("aggregation_passes", ctypes.c_int), ("strength_threshold", ctypes.c_double),
                 ("nullspace", ctypes.c_int), ("structure", ctypes.c_int),
-                ("workspace", ctypes.c_void_p)]
+                ("workspace", ctypes.c_void_p), ("setup", ctypes.c_int)]
 
 
 class _Control(ctypes.Structure):
@@ -166,6 +174,7 @@ _SIGNATURES = {
     "b2_solver_levels": (_I, [_P]),
     "b2_solver_level_shape": (_I, [_P, _I, _P, _P]),
     "b2_solver_level_copy": (_I, [_P, _I, _P, _P, _P, _P, _P, _P]),
+    "b2_solver_level_transfer": (_I, [_P, _I, _P, _P, _P, _P, _P, _P]),
     "b2_hierarchy_build": (_I, [_I, _I, _P, _P, _P, _P, _P, _I, _P]),
     "b2_hierarchy_levels": (_I, [_P]),
     "b2_hierarchy_level_shape": (_I, [_P, _I, _P, _P]),
@@ -311,6 +320,7 @@ def _options_struct(o, use_amg: bool) -> _Options:
     if o is not None:
         s.nullspace, s.structure = int(o.nullspace), int(o.structure)
         s.workspace = o.workspace._handle if o.workspace is not None else None
+        s.setup = int(o.setup)
     return s
 
 
@@ -383,6 +393,30 @@ class LinearSolver:
                                             _ptr(l1), _ptr(ag), _stream()))
             out.append((n.value, rp, cl, vl, l1, ag))
         return out
+
+    def level_transfer(self, level: int) -> dict:
+        """Level `level`'s diagonal positions and its transfer to level + 1
+        (member_offsets, members, entry_offsets, entries; empty on the coarsest)."""
+        lib = _load()
+        count = lib.b2_solver_levels(self._handle)
+        n, nnz = ctypes.c_int(), ctypes.c_int()
+        _check(lib.b2_solver_level_shape(self._handle, level, ctypes.byref(n), ctypes.byref(nnz)))
+        nc, nnz_c = ctypes.c_int(0), ctypes.c_int(0)
+        if level + 1 < count:
+            _check(lib.b2_solver_level_shape(self._handle, level + 1, ctypes.byref(nc),
+                                             ctypes.byref(nnz_c)))
+        diag = np.zeros(n.value, np.int32)
+        offsets = np.zeros(nc.value + 1, np.int32)
+        members = np.full(n.value, -1, np.int32)
+        entry_offsets = np.zeros(nnz_c.value + 1, np.int32)
+        entries = np.full(nnz.value, -1, np.int32)
+        _check(lib.b2_solver_level_transfer(self._handle, level, _ptr(diag), _ptr(offsets),
+                                            _ptr(members), _ptr(entry_offsets), _ptr(entries),
+                                            _stream()))
+        if level + 1 >= count:
+            return {"diag": diag}
+        return {"diag": diag, "member_offsets": offsets, "members": members[:offsets[-1]],
+                "entry_offsets": entry_offsets, "entries": entries[:entry_offsets[-1]]}
 
     def __del__(self):
         if getattr(self, "_handle", None) and _lib is not None:
