@@ -567,6 +567,116 @@ def run_graded(args):
     return out
 
 
+def run_transport(args):
+    """The non-symmetric twin of the pressure matrix (upwind convection by a
+    divergence-free velocity plus nu = 1e-3 diffusion, diagonal under-relaxation
+    0.7, on the same tet mesh): refresh + solve from zero to rel_tol with the
+    reference's AMG-BiCGStab (make_solver defaults: V(5,5)) and BiCGStab-Jacobi,
+    device-timed, with the FP64 true residual."""
+    import numpy as np
+    import scipy.sparse as sp
+    import torch
+    from kutta_b200 import harness
+    from kutta_b200 import linalg as L
+    torch.cuda.set_device(0)
+    s = harness.convection_tet96(seed=args.seed, n=args.size)
+    a = L.upload(s)
+    b = torch.from_numpy(s.b).cuda()
+    A = sp.csr_matrix((s.val, s.col, s.row_ptr), shape=(s.n, s.n))
+    control = L.SolveControl(args.rel_tol, 1e-12, args.max_iter)
+    out = {"mode": "transport", "rel_tol": args.rel_tol,
+           "workload": f"convection_tet{args.size}: {s.n} cells, {s.nnz} nonzeros"}
+    for name, kind in (("amg_bicgstab", L.SolverKind.AmgBicgstab),
+                       ("bicgstab_jacobi", L.SolverKind.BicgstabJacobi)):
+        t0 = time.perf_counter()
+        solver = L.make_solver(kind, s, L.SolverOptions())
+        setup = time.perf_counter() - t0
+        x = torch.zeros(s.n, dtype=torch.float32, device="cuda")
+        best = None
+        for _ in range(max(1, args.steps)):
+            x.zero_()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            torch.cuda.synchronize()
+            e0.record()
+            solver.refresh(a)
+            st = solver.solve(a, x, b, control)
+            e1.record()
+            torch.cuda.synchronize()
+            ms = e0.elapsed_time(e1)
+            best = ms if best is None else min(best, ms)
+        xr = x.cpu().numpy().astype(np.float64)
+        true = float(np.linalg.norm(s.b.astype(np.float64) - A @ xr) / st.initial_residual)
+        out[name] = {"method": solver.describe(), "ms_per_solve": best, "setup_s": setup,
+                     "iterations": st.iterations, "converged": st.converged,
+                     "true_relative_residual_fp64": true}
+    return out
+
+
+def run_outer(args):
+    """The steps on either side of the pressure solve in the steady solver's
+    outer iteration (src/kutta/fv/steady_solver.cpp:1334-1366), on the
+    headline mesh with synthetic face data (harness.fv_faces): the pressure
+    assembly fused with the mixed solver's refresh against the assembly
+    kernel followed by a separate refresh, and the flux and velocity
+    corrections. Device-timed over --steps; algorithmic bytes per launch of
+    the fused kernel for its HBM fraction."""
+    import numpy as np
+    import torch
+    from kutta_b200 import harness
+    from kutta_b200 import linalg as L
+    torch.cuda.set_device(0)
+    s = harness.pressure_tet96(seed=args.seed, n=args.size)
+    c = harness.fv_faces(s.row_ptr, s.col, s.diag, seed=args.seed)
+    t = lambda a: torch.from_numpy(np.ascontiguousarray(a)).cuda()  # noqa: E731
+    fv = L.FvPressure(t(c.offsets), t(c.faces), t(c.sign), t(c.adjacent), t(c.entry),
+                      t(c.coefficient), t(c.flux), -1)
+    a = L.upload(s)
+    rhs = torch.zeros(s.n, device="cuda")
+    mixed = L.make_mixed_solver(s)
+    rng = np.random.default_rng(args.seed)
+    correction = t(rng.normal(size=s.n).astype(np.float32))
+    flux = t(c.flux.copy())
+    owner, neighbour, coefficient = t(c.owner), t(c.neighbour), t(c.coefficient)
+    cells = [t(rng.uniform(0.5, 1.5, s.n).astype(np.float32)) for _ in range(3)]
+    grads = [t(rng.normal(size=s.n).astype(np.float32)) for _ in range(3)]
+    fields = [torch.zeros(s.n, device="cuda") for _ in range(4)]
+
+    def timed(fn):
+        for _ in range(args.warmup):
+            fn()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record()
+        for _ in range(args.steps):
+            fn()
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / args.steps
+
+    fused_ms = timed(lambda: mixed.assemble_refresh(a, fv, rhs))
+    separate_ms = timed(lambda: (L.fv_pressure_assemble(a, fv, rhs), mixed.refresh(a)))
+    assemble_ms = timed(lambda: L.fv_pressure_assemble(a, fv, rhs))
+    flux_ms = timed(lambda: L.fv_correct_flux(owner, neighbour, correction, coefficient, flux,
+                                              c.internal))
+    velocity_ms = timed(lambda: L.fv_correct_velocity(*cells, *grads, correction, *fields, 0.3))
+    slots = len(c.faces)
+    # offsets, four ints/floats per slot, gathered coefficient and flux per
+    # slot, values written and re-read for the diagonal sum, rows and diag,
+    # rhs; the L1 diagonal written by the fused form.
+    assemble_bytes = 4 * (s.n + 1) + 16 * slots + 8 * slots + 8 * s.nnz + 8 * (s.n + 1) + 4 * s.n
+    peak, kind = _peaks()
+    return {"mode": "outer", "workload": f"pressure_tet{args.size}: {s.n} cells, {s.nnz} nonzeros, "
+                                         f"{c.n_faces} faces ({c.internal} internal), {slots} "
+                                         "cell-face slots",
+            "assemble_refresh_fused_ms": fused_ms, "assemble_then_refresh_ms": separate_ms,
+            "assemble_ms": assemble_ms, "correct_flux_ms": flux_ms,
+            "correct_velocity_ms": velocity_ms,
+            "assemble_algorithmic_bytes": assemble_bytes,
+            "assemble_gbs": assemble_bytes / (assemble_ms * 1e-3) / 1e9,
+            "assemble_frac_of_hbm": assemble_bytes / (assemble_ms * 1e-3) / 1e9 / peak,
+            "peak_source": kind, "steps": args.steps}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -579,10 +689,14 @@ def main():
     ap.add_argument("--plain-steps", type=int, default=3)
     ap.add_argument("--cpu-sample-iters", type=int, default=2)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--mode", default="bench", choices=["bench", "profile", "sequence", "graded"],
+    ap.add_argument("--mode", default="bench",
+                    choices=["bench", "profile", "sequence", "graded", "transport", "outer"],
                     help="profile: one refresh + one solve (with --max-iter), for ncu captures; "
                          "sequence: successive warm-started solves on the graded mesh; "
-                         "graded: the graded matrix to --rel-tol (default 1e-8)")
+                         "graded: the graded matrix to --rel-tol (default 1e-8); "
+                         "transport: the non-symmetric twin with AMG-BiCGStab and "
+                         "BiCGStab-Jacobi (default 1e-6); outer: the pressure assembly fused "
+                         "with the refresh, and the flux/velocity corrections")
     ap.add_argument("--method", default="mixed", choices=["mixed", "plain"])
     ap.add_argument("--solves", type=int, default=300, help="sequence mode: number of solves")
     ap.add_argument("--rel-tol", type=float, default=None,
@@ -592,10 +706,12 @@ def main():
     if args.mode == "profile":
         profile_once(args)
         return
-    if args.mode in ("sequence", "graded"):
+    if args.mode in ("sequence", "graded", "transport", "outer"):
         if args.rel_tol is None:
-            args.rel_tol = 1e-6 if args.mode == "sequence" else 1e-8
-        print(json.dumps(run_sequence(args) if args.mode == "sequence" else run_graded(args)))
+            args.rel_tol = 1e-8 if args.mode == "graded" else 1e-6
+        run = {"sequence": run_sequence, "graded": run_graded, "transport": run_transport,
+               "outer": run_outer}
+        print(json.dumps(run[args.mode](args)))
         return
     if args.impl == "reference":
         line = run_reference(args, rank, world)

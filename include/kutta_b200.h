@@ -289,6 +289,47 @@ int b2_mixed_set_learned(b2_mixed* solver, b2_gnn* g, int mode);
 int b2_mixed_precondition(b2_mixed* solver, const float* d_val, const float* d_r, float* d_z,
                           void* stream);
 
+/* ---- Finite-volume steps around the pressure solve --------------------------
+ * The reference's kernels on either side of the solve, same arguments and
+ * the same float results bit for bit (src/kutta/kernels/fv_flow.kern.h:
+ * 164-201; called at src/kutta/fv/steady_solver.cpp:1334, 1345, 1364). All
+ * arrays are device pointers; cell-face slots run over offsets[n_cells].
+ *   fv_pressure_assemble: row i of the pressure-correction matrix (values in
+ *     the CSR pattern rows/diag, entry[j] the position of (i, adjacent[j]))
+ *     and rhs[i], from per-face coefficients and mass fluxes; `reference` is
+ *     an eliminated cell (unit row, column removed) or -1.
+ *   fv_correct_flux: flux[f] += coefficient[f] (p'_owner - p'_neighbour) for
+ *     the n_faces faces (neighbour read for f < internal only).
+ *   fv_correct_velocity: u, v, w -= volume inverse grad p'; p += min(alpha,
+ *     0.7 diagonal inverse) p'. */
+int b2_fv_pressure_assemble(int n_cells, const int32_t* d_offsets, const int32_t* d_faces,
+                            const float* d_sign, const int32_t* d_adjacent, const int32_t* d_entry,
+                            const int32_t* d_row_ptr, const int32_t* d_diag,
+                            const float* d_coefficient, const float* d_flux, float* d_values,
+                            float* d_rhs, int reference, void* stream);
+int b2_fv_correct_flux(int n_faces, const int32_t* d_owner, const int32_t* d_neighbour,
+                       const float* d_correction, const float* d_coefficient, float* d_flux,
+                       int internal, void* stream);
+int b2_fv_correct_velocity(int n_cells, const float* d_volume, const float* d_inverse,
+                           const float* d_diagonal, const float* d_gx, const float* d_gy,
+                           const float* d_gz, const float* d_correction, float* d_u, float* d_v,
+                           float* d_w, float* d_p, float alpha, void* stream);
+/* fv_pressure_assemble fused with the solver's refresh: one pass over the
+ * cells writes the matrix values (into d_values, the solver's pattern), the
+ * right-hand side and the fine level's L1 inverse diagonal; the coarse levels
+ * then refresh as b2_solver_refresh / b2_mixed_refresh does. d_values is the
+ * matrix to pass to the next solve. AMG solvers only. */
+int b2_solver_assemble_refresh(b2_solver* solver, const int32_t* d_offsets,
+                               const int32_t* d_faces, const float* d_sign,
+                               const int32_t* d_adjacent, const int32_t* d_entry,
+                               const float* d_coefficient, const float* d_flux, float* d_values,
+                               float* d_rhs, int reference, void* stream);
+int b2_mixed_assemble_refresh(b2_mixed* solver, const int32_t* d_offsets, const int32_t* d_faces,
+                              const float* d_sign, const int32_t* d_adjacent,
+                              const int32_t* d_entry, const float* d_coefficient,
+                              const float* d_flux, float* d_values, float* d_rhs, int reference,
+                              void* stream);
+
 /* Hierarchy introspection (the captured-hierarchy checks of the reference's
  * tests/linalg/test_solvers.cpp:487-555 read the same data back from launches).
  * Level 0 is the input matrix. Copies are synchronous device-to-host reads on

@@ -44,6 +44,7 @@ PRODUCT_CU = {
     "learned.cu": [],
     "learned_tc.cu": [],
     "setup_kernels.cu": EXACT,
+    "fv_kernels.cu": EXACT,
     "noalloc.cu": [],
 }
 PRODUCT_CPP = ["host/setup.cpp", "host/solver.cpp", "host/device_setup.cpp", "host/mixed.cpp",

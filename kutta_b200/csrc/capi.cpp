@@ -307,6 +307,94 @@ int b2_solver_level_copy(const b2_solver* s, int level, int32_t* row_ptr, int32_
   });
 }
 
+int b2_fv_pressure_assemble(int n, const int32_t* offsets, const int32_t* faces, const float* sign,
+                            const int32_t* adjacent, const int32_t* entry, const int32_t* rows,
+                            const int32_t* diag, const float* coefficient, const float* flux,
+                            float* values, float* rhs, int reference, void* stream) {
+  return guarded([&] {
+    KB2_REQUIRE(n >= 0, "assemble: negative cell count");
+    KB2_REQUIRE(n == 0 || (offsets && faces && sign && adjacent && entry && rows && diag &&
+                           coefficient && flux && values && rhs),
+                "assemble: null argument");
+    KB2_REQUIRE(reference >= -1 && reference < n, "assemble: reference cell out of range");
+    kb2::launch::fv_pressure_assemble(n, offsets, faces, sign, adjacent, entry, rows, diag,
+                                      coefficient, flux, values, rhs, reference,
+                                      as_stream(stream));
+    kb2::cuda_check(cudaGetLastError(), "fv_pressure_assemble");
+  });
+}
+
+int b2_fv_correct_flux(int n_faces, const int32_t* owner, const int32_t* neighbour,
+                       const float* correction, const float* coefficient, float* flux,
+                       int internal, void* stream) {
+  return guarded([&] {
+    KB2_REQUIRE(n_faces >= 0 && internal >= 0 && internal <= n_faces,
+                "correct_flux: invalid face counts");
+    KB2_REQUIRE(n_faces == 0 || (owner && (neighbour || internal == 0) && correction &&
+                                 coefficient && flux),
+                "correct_flux: null argument");
+    kb2::launch::fv_correct_flux(n_faces, owner, neighbour, correction, coefficient, flux,
+                                 internal, as_stream(stream));
+    kb2::cuda_check(cudaGetLastError(), "fv_correct_flux");
+  });
+}
+
+int b2_fv_correct_velocity(int n, const float* volume, const float* inverse, const float* diagonal,
+                           const float* gx, const float* gy, const float* gz,
+                           const float* correction, float* u, float* v, float* w, float* p,
+                           float alpha, void* stream) {
+  return guarded([&] {
+    KB2_REQUIRE(n >= 0, "correct_velocity: negative cell count");
+    KB2_REQUIRE(n == 0 || (volume && inverse && diagonal && gx && gy && gz && correction && u &&
+                           v && w && p),
+                "correct_velocity: null argument");
+    kb2::launch::fv_correct_velocity(n, volume, inverse, diagonal, gx, gy, gz, correction, u, v, w,
+                                     p, alpha, as_stream(stream));
+    kb2::cuda_check(cudaGetLastError(), "fv_correct_velocity");
+  });
+}
+
+namespace {
+kb2::FvPressure fv_pressure(const int32_t* offsets, const int32_t* faces, const float* sign,
+                            const int32_t* adjacent, const int32_t* entry,
+                            const float* coefficient, const float* flux, int reference) {
+  kb2::FvPressure fv;
+  fv.offsets = offsets;
+  fv.faces = faces;
+  fv.sign = sign;
+  fv.adjacent = adjacent;
+  fv.entry = entry;
+  fv.coefficient = coefficient;
+  fv.flux = flux;
+  fv.reference = reference;
+  return fv;
+}
+}  // namespace
+
+int b2_solver_assemble_refresh(b2_solver* s, const int32_t* offsets, const int32_t* faces,
+                               const float* sign, const int32_t* adjacent, const int32_t* entry,
+                               const float* coefficient, const float* flux, float* values,
+                               float* rhs, int reference, void* stream) {
+  return guarded([&] {
+    KB2_REQUIRE(s && s->s, "solver: null handle");
+    s->s->assemble_refresh(
+        fv_pressure(offsets, faces, sign, adjacent, entry, coefficient, flux, reference), values,
+        rhs, as_stream(stream));
+  });
+}
+
+int b2_mixed_assemble_refresh(b2_mixed* s, const int32_t* offsets, const int32_t* faces,
+                              const float* sign, const int32_t* adjacent, const int32_t* entry,
+                              const float* coefficient, const float* flux, float* values,
+                              float* rhs, int reference, void* stream) {
+  return guarded([&] {
+    KB2_REQUIRE(s && s->s, "solver: null handle");
+    s->s->assemble_refresh(
+        fv_pressure(offsets, faces, sign, adjacent, entry, coefficient, flux, reference), values,
+        rhs, as_stream(stream));
+  });
+}
+
 int b2_solver_level_transfer(const b2_solver* s, int level, int32_t* diag, int32_t* member_offsets,
                              int32_t* members, int32_t* entry_offsets, int32_t* entries,
                              void* stream) {

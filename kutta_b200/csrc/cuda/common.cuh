@@ -167,6 +167,28 @@ __device__ __forceinline__ double block_sum(double v, double* shared /* >= 32 */
   return total;
 }
 __device__ __forceinline__ double nan_max(double a, double b) { return (b > a || isnan(b)) ? b : a; }
+
+// krylov_diagonal's row (src/kutta/kernels/linalg.kern.h:52-70): the inverse
+// (L1) diagonal of row i into inverse[i]; returns its invalid flag (0 valid,
+// 1 zero diagonal, 2 nonfinite, 3 negative diagonal under L1).
+__device__ __forceinline__ float diagonal_row(int i, const int* __restrict__ rows,
+                                              const int* __restrict__ diag,
+                                              const float* __restrict__ vals,
+                                              float* __restrict__ inverse, int use_l1) {
+  const float d = vals[diag[i]];
+  float off = 0.0f, bad = 0.0f;
+  for (int j = rows[i]; j < rows[i + 1]; ++j) {
+    const float v = vals[j];
+    if (v - v != 0.0f) bad = 1.0f;
+    if (j != diag[i]) off += fabsf(v);
+  }
+  const float inv = d != 0.0f ? 1.0f / d : 0.0f;
+  const float l1 = fmaxf(fabsf(d), 0.5f * (fabsf(d) + off));
+  inverse[i] = use_l1 != 0 ? (l1 != 0.0f ? 1.0f / l1 : 0.0f) : inv;
+  return (bad != 0.0f || inv - inv != 0.0f || l1 - l1 != 0.0f)
+             ? 2.0f
+             : (use_l1 != 0 && d < 0.0f ? 3.0f : (d == 0.0f ? 1.0f : 0.0f));
+}
 __device__ __forceinline__ double warp_max(double v) {
 #pragma unroll
   for (int d = 16; d > 0; d >>= 1) v = nan_max(v, __shfl_down_sync(0xffffffffu, v, d));

@@ -235,22 +235,7 @@ __global__ void k_diagonal(int n, const int* __restrict__ rows, const int* __res
                            const float* __restrict__ vals, float* __restrict__ inverse,
                            int use_l1, DeviceReducer red, double* check, int slot) {
   double worst = 0;
-  ROWS(i, n) {
-    const float d = vals[diag[i]];
-    float off = 0.0f, bad = 0.0f;
-    for (int j = rows[i]; j < rows[i + 1]; ++j) {
-      const float v = vals[j];
-      if (v - v != 0.0f) bad = 1.0f;
-      if (j != diag[i]) off += fabsf(v);
-    }
-    const float inv = d != 0.0f ? 1.0f / d : 0.0f;
-    const float l1 = fmaxf(fabsf(d), 0.5f * (fabsf(d) + off));
-    inverse[i] = use_l1 != 0 ? (l1 != 0.0f ? 1.0f / l1 : 0.0f) : inv;
-    const float invalid = (bad != 0.0f || inv - inv != 0.0f || l1 - l1 != 0.0f)
-                              ? 2.0f
-                              : (use_l1 != 0 && d < 0.0f ? 3.0f : (d == 0.0f ? 1.0f : 0.0f));
-    worst = nan_max(worst, static_cast<double>(invalid));
-  }
+  ROWS(i, n) worst = nan_max(worst, diagonal_row(i, rows, diag, vals, inverse, use_l1));
   __shared__ double shared[32];
   worst = block_max(worst, shared);
   const Reducer r = as_reducer(red);

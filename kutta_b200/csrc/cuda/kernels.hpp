@@ -228,6 +228,25 @@ void gnn_layer_b(int n, const int* rows, const int* cols, const float* edge,
                  const float* wo, const float* node_scale, const double* sum2, float* z,
                  float beta, int* fault, cudaStream_t s);
 
+// ---- finite-volume steps around the pressure solve (fv_kernels.cu) ---------
+// fv_pressure_assemble (fv_flow.kern.h:164-183); the _l1 form also writes
+// the rows' inverse L1 diagonal and the max invalid flag into check[slot].
+void fv_pressure_assemble(int n, const int* offsets, const int* faces, const float* sign,
+                          const int* adjacent, const int* entry, const int* rows, const int* diag,
+                          const float* coefficient, const float* flux, float* values, float* rhs,
+                          int reference, cudaStream_t s);
+void fv_pressure_assemble_l1(int n, const int* offsets, const int* faces, const float* sign,
+                             const int* adjacent, const int* entry, const int* rows,
+                             const int* diag, const float* coefficient, const float* flux,
+                             float* values, float* rhs, int reference, float* inverse,
+                             DeviceReducer red, double* check, int slot, cudaStream_t s);
+void fv_correct_flux(int n, const int* owner, const int* neighbour, const float* correction,
+                     const float* coefficient, float* flux, int internal, cudaStream_t s);
+void fv_correct_velocity(int n, const float* volume, const float* inverse, const float* diagonal,
+                         const float* gx, const float* gy, const float* gz,
+                         const float* correction, float* u, float* v, float* w, float* p,
+                         float alpha, cudaStream_t s);
+
 // ---- AMG setup on the device (setup_kernels.cu) -----------------------------
 // out[0..n] = exclusive scan of in[0..n) (out[n] = total); block_sums holds
 // scan_scratch(n) ints.

@@ -25,6 +25,9 @@ class MixedSolver {
  public:
   MixedSolver(const CsrView& a, const MixedOptions& o);
   void refresh(const float* val, cudaStream_t s) { inner_.refresh(val, s); }
+  void assemble_refresh(const FvPressure& fv, float* values, float* rhs, cudaStream_t s) {
+    inner_.assemble_refresh(fv, values, rhs, s);
+  }
   // x: FP64 solution (initial guess in); b: FP32 right-hand side.
   MixedStats solve(const float* val, double* x, const float* b, const Control& c, cudaStream_t s);
   std::string describe() const;

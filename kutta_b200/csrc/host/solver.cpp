@@ -673,12 +673,36 @@ void Solver::refresh(const float* val, cudaStream_t s) {
     KB2_REQUIRE(host_values_[0] == 0, "Jacobi: invalid values or zero diagonal");
     return;
   }
+  refresh_levels(val, false, s);
+}
+
+// The pressure matrix assembled from face data into `values` (the level-0
+// values from now on) with its right-hand side, and the refresh, in one pass
+// over the cells for level 0: the assembly kernel also writes the L1 inverse
+// diagonal and its validity flag; the coarse levels follow as in refresh().
+void Solver::assemble_refresh(const FvPressure& fv, float* values, float* rhs, cudaStream_t s) {
+  KB2_REQUIRE(amg(), "assemble: needs an AMG solver");
+  KB2_REQUIRE(fv.offsets && fv.faces && fv.sign && fv.adjacent && fv.entry && fv.coefficient &&
+                  fv.flux && values && rhs,
+              "assemble: null argument");
+  KB2_REQUIRE(fv.reference >= -1 && fv.reference < n_, "assemble: reference cell out of range");
+  stream_ = s;
+  val_ = values;
+  auto& l = levels_[0];
+  launch::fv_pressure_assemble_l1(n_, fv.offsets, fv.faces, fv.sign, fv.adjacent, fv.entry,
+                                  l.row_ptr.get(), l.diag.get(), fv.coefficient, fv.flux, values,
+                                  rhs, fv.reference, l.l1.get(), reducer(), values_.get(), 0, s);
+  refresh_levels(values, true, s);
+}
+
+void Solver::refresh_levels(const float* val, bool fine_done, cudaStream_t s) {
   const float* matrix = val;
   std::vector<double> allowed;
   for (std::size_t i = 0; i < levels_.size(); ++i) {
     auto& l = levels_[i];
-    launch::diagonal(l.n, l.row_ptr.get(), l.diag.get(), matrix, l.l1.get(), 1, reducer(),
-                     values_.get(), static_cast<int>(i), s);
+    if (i > 0 || !fine_done)
+      launch::diagonal(l.n, l.row_ptr.get(), l.diag.get(), matrix, l.l1.get(), 1, reducer(),
+                       values_.get(), static_cast<int>(i), s);
     allowed.push_back(nullspace_ && l.n == 1 ? 1 : 0);
     if (i + 1 < levels_.size()) {
       auto& c = levels_[i + 1];

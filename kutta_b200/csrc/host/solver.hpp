@@ -18,6 +18,19 @@
 
 namespace kb2 {
 
+// Face data of the pressure assembly (fv_pressure_assemble's inputs,
+// src/kutta/kernels/fv_flow.kern.h:164-167), device pointers.
+struct FvPressure {
+  const int* offsets = nullptr;   // cell-face slot offsets [n + 1]
+  const int* faces = nullptr;     // face of each slot
+  const float* sign = nullptr;    // +1 on the owner side, -1 on the neighbour side
+  const int* adjacent = nullptr;  // cell across the face, -1 on the boundary
+  const int* entry = nullptr;     // CSR position of (cell, adjacent)
+  const float* coefficient = nullptr;  // per face
+  const float* flux = nullptr;         // per face
+  int reference = -1;                  // eliminated reference cell, or -1
+};
+
 struct Control {  // SolveControl, solver.hpp:18-23
   double rel_tol = 1e-2, abs_tol = 1e-12;
   int max_iter = 200, residual_check_interval = 8;
@@ -93,6 +106,8 @@ class Solver {
   // Bytes of kernels a wrapping driver launched (the FP64 refinement).
   void add_bytes(double bytes) { tally(bytes); }
   void refresh(const float* val, cudaStream_t s);
+  // Assembles the pressure matrix into `values` and rhs, then refreshes.
+  void assemble_refresh(const FvPressure& fv, float* values, float* rhs, cudaStream_t s);
   Stats solve(const float* val, float* x, const float* b, const Control& c, cudaStream_t s);
   std::string describe() const;
 
@@ -119,6 +134,9 @@ class Solver {
   bool device_pattern_symmetric(cudaStream_t s);
   void build_device_levels(const CsrView& a, cudaStream_t s);
   bool device_setup_ = false;
+  // Refresh from the level-0 values; fine_done: level 0's L1 diagonal and
+  // check slot are already written (by the fused assembly).
+  void refresh_levels(const float* val, bool fine_done, cudaStream_t s);
   void prepare_mixed(cudaStream_t s, int error_slot);
   void choose_coarsest(double smallest_pivot);
   bool dense_ok_ = false;  // the dense coarsest inverse is used (well conditioned)

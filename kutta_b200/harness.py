@@ -182,3 +182,77 @@ def graded_tet96(seed: int = 1, n: int = 96) -> HostSystem:
     D_f log-uniform over [1e-6, 1]."""
     return box_system(n, n, n, tet=True, seed=seed, band_layers=10, aspect=1000.0, ratio=1.2,
                       dmin=1e-6, dmax=1.0)
+
+# Finite-volume face data ------------------------------------------------------
+# Synthetic inputs of the reference's pressure assembly and correction kernels
+# (src/kutta/kernels/fv_flow.kern.h:164-201) for a CSR pattern, laid out as
+# src/kutta/fv/steady_solver.cpp passes them: cell-face slots (offsets, faces,
+# sign +1 on the owner side, adjacent cell or -1 on the boundary, CSR entry of
+# (cell, adjacent)), internal faces first, per-face coefficients and fluxes.
+# Each off-diagonal pair (i, j) becomes an internal face (owner i < j); a
+# seeded fraction of pairs gets a second face on the same CSR entry (cells
+# sharing several faces); a seeded fraction of cells gets boundary faces.
+# Coefficients are log-uniform positive, fluxes normal.
+
+@dataclasses.dataclass
+class FvCase:
+    n: int
+    rows: np.ndarray
+    cols: np.ndarray
+    diag: np.ndarray
+    owner: np.ndarray
+    neighbour: np.ndarray      # internal faces only
+    internal: int
+    offsets: np.ndarray
+    faces: np.ndarray
+    sign: np.ndarray
+    adjacent: np.ndarray
+    entry: np.ndarray
+    coefficient: np.ndarray
+    flux: np.ndarray
+    reference: int = -1
+
+    @property
+    def n_faces(self) -> int:
+        return len(self.owner)
+
+
+def fv_faces(row_ptr, col, diag, seed: int, duplicate: float = 0.1, boundary: float = 0.3,
+          reference: int = -1) -> FvCase:
+    rng = np.random.default_rng(seed)
+    n = len(row_ptr) - 1
+    rows = np.repeat(np.arange(n), np.diff(row_ptr))
+    upper = col > rows
+    own, nb = rows[upper].astype(np.int32), col[upper].astype(np.int32)
+    extra = rng.random(len(own)) < duplicate
+    own = np.concatenate([own, own[extra]])
+    nb = np.concatenate([nb, nb[extra]])
+    internal = len(own)
+    bcells = np.nonzero(rng.random(n) < boundary)[0]
+    bcells = np.concatenate([bcells, bcells[rng.random(len(bcells)) < 0.3]])  # some with two
+    owner = np.concatenate([own, np.sort(bcells)]).astype(np.int32)
+    nf = len(owner)
+    # Cell-face slots: every face on its owner's side, internal faces also on
+    # the neighbour's, grouped by cell in face order.
+    slot_cell = np.concatenate([owner, nb])
+    slot_face = np.concatenate([np.arange(nf), np.arange(internal)]).astype(np.int32)
+    slot_sign = np.concatenate([np.ones(nf), -np.ones(internal)]).astype(np.float32)
+    slot_adj = np.concatenate([np.concatenate([nb, -np.ones(nf - internal, np.int32)]), own])
+    order = np.lexsort((slot_face, slot_cell))
+    slot_cell, slot_face = slot_cell[order], slot_face[order]
+    slot_sign, slot_adj = slot_sign[order], slot_adj[order].astype(np.int32)
+    offsets = np.zeros(n + 1, np.int32)
+    np.add.at(offsets, slot_cell + 1, 1)
+    offsets = np.cumsum(offsets).astype(np.int32)
+    # CSR keys row * n + col are sorted, so one search finds every entry.
+    keys = rows.astype(np.int64) * n + np.asarray(col, np.int64)
+    entry = np.full(len(slot_cell), -1, np.int32)
+    inner = slot_adj >= 0
+    entry[inner] = np.searchsorted(keys, slot_cell[inner].astype(np.int64) * n + slot_adj[inner])
+    coefficient = np.exp(rng.uniform(np.log(1e-3), 0.0, nf)).astype(np.float32)
+    flux = rng.normal(size=nf).astype(np.float32)
+    return FvCase(n=n, rows=np.asarray(row_ptr, np.int32), cols=np.asarray(col, np.int32),
+                  diag=np.asarray(diag, np.int32), owner=owner, neighbour=nb.astype(np.int32),
+                  internal=internal, offsets=offsets, faces=slot_face, sign=slot_sign,
+                  adjacent=slot_adj, entry=entry, coefficient=coefficient, flux=flux,
+                  reference=reference)

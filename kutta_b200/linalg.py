@@ -175,6 +175,11 @@ _SIGNATURES = {
     "b2_solver_level_shape": (_I, [_P, _I, _P, _P]),
     "b2_solver_level_copy": (_I, [_P, _I, _P, _P, _P, _P, _P, _P]),
     "b2_solver_level_transfer": (_I, [_P, _I, _P, _P, _P, _P, _P, _P]),
+    "b2_fv_pressure_assemble": (_I, [_I] + [_P] * 11 + [_I, _P]),
+    "b2_fv_correct_flux": (_I, [_I, _P, _P, _P, _P, _P, _I, _P]),
+    "b2_fv_correct_velocity": (_I, [_I] + [_P] * 11 + [ctypes.c_float, _P]),
+    "b2_solver_assemble_refresh": (_I, [_P] + [_P] * 9 + [_I, _P]),
+    "b2_mixed_assemble_refresh": (_I, [_P] + [_P] * 9 + [_I, _P]),
     "b2_hierarchy_build": (_I, [_I, _I, _P, _P, _P, _P, _P, _I, _P]),
     "b2_hierarchy_levels": (_I, [_P]),
     "b2_hierarchy_level_shape": (_I, [_P, _I, _P, _P]),
@@ -349,6 +354,13 @@ class LinearSolver:
     def refresh(self, a: CsrMatrix) -> None:
         self._check_matrix(a)
         _check(_load().b2_solver_refresh(self._handle, _tptr(a.val), _stream()))
+
+    def assemble_refresh(self, a: CsrMatrix, fv: "FvPressure", rhs) -> None:
+        """b2_solver_assemble_refresh: assembles the pressure matrix into a.val
+        and rhs from the face data, refreshing the solver in the same pass."""
+        self._check_matrix(a)
+        _check(_load().b2_solver_assemble_refresh(self._handle, *fv.pointers(), _tptr(a.val),
+                                                  _tptr(rhs), fv.reference, _stream()))
 
     def solve(self, a: CsrMatrix, x, b, control: SolveControl | None = None) -> SolveStats:
         self._check_matrix(a)
@@ -540,6 +552,11 @@ class MixedSolver:
     def refresh(self, a: CsrMatrix) -> None:
         _check(_load().b2_mixed_refresh(self._handle, _tptr(a.val), _stream()))
 
+    def assemble_refresh(self, a: CsrMatrix, fv: "FvPressure", rhs) -> None:
+        """b2_mixed_assemble_refresh (see LinearSolver.assemble_refresh)."""
+        _check(_load().b2_mixed_assemble_refresh(self._handle, *fv.pointers(), _tptr(a.val),
+                                                 _tptr(rhs), fv.reference, _stream()))
+
     def solve(self, a: CsrMatrix, x64, b, control: SolveControl | None = None) -> MixedStats:
         """x64: float64 CUDA tensor (initial guess in, solution out); b: float32."""
         import torch
@@ -631,6 +648,50 @@ class LearnedStage:
         if getattr(self, "_handle", None) and _lib is not None:
             _lib.b2_gnn_destroy(self._handle)
             self._handle = None
+
+
+@dataclasses.dataclass
+class FvPressure:
+    """Face data of the pressure assembly (fv_pressure_assemble's inputs,
+    src/kutta/kernels/fv_flow.kern.h:164-167) as CUDA tensors: cell-face slot
+    offsets (int32, n_cells + 1), the face, side sign (+1 owner, -1
+    neighbour), adjacent cell (-1 boundary) and CSR entry of each slot, and
+    per-face coefficients and mass fluxes (float32); reference: an eliminated
+    cell or -1."""
+    offsets: object
+    faces: object
+    sign: object
+    adjacent: object
+    entry: object
+    coefficient: object
+    flux: object
+    reference: int = -1
+
+    def pointers(self):
+        return (_tptr(self.offsets), _tptr(self.faces), _tptr(self.sign), _tptr(self.adjacent),
+                _tptr(self.entry), _tptr(self.coefficient), _tptr(self.flux))
+
+
+def fv_pressure_assemble(a: CsrMatrix, fv: FvPressure, rhs) -> None:
+    """b2_fv_pressure_assemble: the pressure matrix into a.val and rhs."""
+    o, f, sg, adj, e, c, fl = fv.pointers()
+    _check(_load().b2_fv_pressure_assemble(a.n_rows, o, f, sg, adj, e, _tptr(a.row_ptr),
+                                           _tptr(a.diag), c, fl, _tptr(a.val), _tptr(rhs),
+                                           fv.reference, _stream()))
+
+
+def fv_correct_flux(owner, neighbour, correction, coefficient, flux, internal: int) -> None:
+    """b2_fv_correct_flux over owner.numel() faces."""
+    _check(_load().b2_fv_correct_flux(owner.numel(), _tptr(owner), _tptr(neighbour),
+                                      _tptr(correction), _tptr(coefficient), _tptr(flux),
+                                      internal, _stream()))
+
+
+def fv_correct_velocity(volume, inverse, diagonal, gx, gy, gz, correction, u, v, w, p,
+                        alpha: float) -> None:
+    """b2_fv_correct_velocity over volume.numel() cells."""
+    _check(_load().b2_fv_correct_velocity(volume.numel(), *(_tptr(t) for t in (
+        volume, inverse, diagonal, gx, gy, gz, correction, u, v, w, p)), alpha, _stream()))
 
 
 def dense_inverse(a: CsrMatrix, inverse, not_spd) -> None:

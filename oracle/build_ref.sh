@@ -19,7 +19,7 @@ fi
 mkdir -p "$OUT/gen"
 K="$REF/src/kutta/kernels"
 python3 "$REF/tools/kernelgen.py" --src-root "$REF/src" --out "$OUT/gen" \
-  "$K/amg.kern.h" "$K/blas.kern.h" "$K/linalg.kern.h" "$K/scalars.kern.h"
+  "$K/amg.kern.h" "$K/blas.kern.h" "$K/linalg.kern.h" "$K/scalars.kern.h" "$K/fv_flow.kern.h"
 SRC=(
   "$REF/src/kutta/linalg/amg.cpp"
   "$REF/src/kutta/linalg/csr.cpp"

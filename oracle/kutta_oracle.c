@@ -207,6 +207,62 @@ void ko_galerkin(int nnz_c, const int* offsets, const int* entries, const float*
     coarse[e] = sum + error;
   }
 }
+/* fv_pressure_assemble, fv_flow.kern.h:164-183: zero the row's face entries,
+ * subtract each internal face coefficient from its entry (faces may share
+ * one), accumulate the right-hand side from the signed fluxes; the diagonal
+ * is the upward-rounded sum of boundary and reference anchors and of the
+ * negated stored off-diagonals. The reference cell keeps a unit row. */
+void ko_fv_pressure_assemble(int n, const int* offsets, const int* faces, const float* sign,
+                             const int* adjacent, const int* entry, const int* rows,
+                             const int* diag, const float* coefficient, const float* flux,
+                             float* values, float* rhs, int reference) {
+  for (int i = 0; i < n; ++i) {
+    upper ap = {0.0f, 0.0f};
+    float b = 0.0f;
+    for (int j = offsets[i]; j < offsets[i + 1]; ++j)
+      if (adjacent[j] >= 0) values[entry[j]] = 0.0f;
+    for (int j = offsets[i]; j < offsets[i + 1]; ++j) {
+      const int f = faces[j], nb = adjacent[j];
+      const float d = coefficient[f];
+      const float term = sign[j] * flux[f];
+      b = b - term;
+      if (nb < 0 || nb == reference) ap = upper_add(ap, d);
+      if (nb >= 0 && nb != reference && i != reference) values[entry[j]] = values[entry[j]] - d;
+    }
+    for (int j = rows[i]; j < rows[i + 1]; ++j)
+      if (j != diag[i]) ap = upper_add(ap, -values[j]);
+    values[diag[i]] = i == reference ? 1.0f : upper_value(ap);
+    rhs[i] = i == reference ? 0.0f : b;
+  }
+}
+/* fv_correct_flux, fv_flow.kern.h:185-190. */
+void ko_fv_correct_flux(int n, const int* owner, const int* neighbour, const float* correction,
+                        const float* coefficient, float* flux, int internal) {
+  for (int i = 0; i < n; ++i) {
+    const float pc = correction[owner[i]];
+    const float pn = i < internal ? correction[neighbour[i]] : 0.0f;
+    const float step = coefficient[i] * (pc - pn);
+    flux[i] = flux[i] + step;
+  }
+}
+/* fv_correct_velocity, fv_flow.kern.h:192-201. */
+void ko_fv_correct_velocity(int n, const float* volume, const float* inverse,
+                            const float* diagonal, const float* gx, const float* gy,
+                            const float* gz, const float* correction, float* u, float* v,
+                            float* w, float* p, float alpha) {
+  for (int i = 0; i < n; ++i) {
+    const float d = volume[i] * inverse[i];
+    const float du = d * gx[i], dv = d * gy[i], dw = d * gz[i];
+    u[i] = u[i] - du;
+    v[i] = v[i] - dv;
+    w[i] = w[i] - dw;
+    const float bound = 0.7f * diagonal[i];
+    const float ratio = bound * inverse[i];
+    const float pa = fminf(alpha, ratio);
+    const float dp = pa * correction[i];
+    p[i] = p[i] + dp;
+  }
+}
 /* amg_m_matrix_diagonal, amg.kern.h:44-58. */
 static void m_matrix_diagonal(int nc, const int* offsets, const int* members, const int* fine_rows,
                               const int* fine_diag, const float* fine, const int* rows,

@@ -64,6 +64,20 @@ void ko_scalar(int op, float* scalars, int* status, int arg);
 void ko_solver_step(int n, float* x, float* r, const float* p, const float* q,
                     const float* scalars, const int* status);
 
+/* Finite-volume steps around the pressure solve, src/kutta/kernels/
+ * fv_flow.kern.h: fv_pressure_assemble (:164-183), fv_correct_flux (:185-190),
+ * fv_correct_velocity (:192-201). */
+void ko_fv_pressure_assemble(int n, const int* offsets, const int* faces, const float* sign,
+                             const int* adjacent, const int* entry, const int* rows,
+                             const int* diag, const float* coefficient, const float* flux,
+                             float* values, float* rhs, int reference);
+void ko_fv_correct_flux(int n, const int* owner, const int* neighbour, const float* correction,
+                        const float* coefficient, float* flux, int internal);
+void ko_fv_correct_velocity(int n, const float* volume, const float* inverse,
+                            const float* diagonal, const float* gx, const float* gy,
+                            const float* gz, const float* correction, float* u, float* v,
+                            float* w, float* p, float alpha);
+
 /* FP64 oracle: CG in double on the double-valued matrix, multi-threaded, from
  * x = 0 to ||b - A x|| <= rel_tol ||b||. Returns iterations, or -1. */
 int ko_cg64(int n, const int* row_ptr, const int* col, const double* val, const double* b,

@@ -4,13 +4,15 @@
 // tests, the golden-fixture generator and bench.py's reference/CPU-baseline arm
 // load it; the product never does.
 //
-// It exposes two things:
+// It exposes three things:
 //   kref_solve      set up, refresh and solve one system exactly as the reference
 //                   does (src/kutta/linalg/amg.cpp:345-406, solver.cpp:97-176);
 //   kref_hierarchy  capture the AMG hierarchy the reference actually solves with
 //                   (aggregates, coarse CSR patterns and values, L1 inverse
 //                   diagonals) from the kernels its V-cycle launches, the way
-//                   tests/linalg/test_solvers.cpp:509-521 reads them back.
+//                   tests/linalg/test_solvers.cpp:509-521 reads them back;
+//   kref_fv_*       the finite-volume kernels on either side of the pressure
+//                   solve (src/kutta/kernels/fv_flow.kern.h:164-201).
 #include <chrono>
 #include <cstring>
 #include <functional>
@@ -108,6 +110,12 @@ class WatchDevice final : public Device {
 };
 
 }  // namespace
+
+// Host array -> CPU-device buffer.
+template <class T>
+static Buffer<T> put(Device& dev, const T* p, std::size_t n) {
+  return dev.upload<T>(std::span<const T>(p, n));
+}
 
 extern "C" {
 
@@ -288,5 +296,67 @@ void kref_hierarchy_copy(void* h, int level, int* row_ptr, int* col, float* val,
     std::memcpy(aggregate, l.aggregate.data(), l.aggregate.size() * sizeof(int));
 }
 void kref_hierarchy_free(void* h) { delete static_cast<KrefHierarchy*>(h); }
+
+// The reference's own finite-volume kernels (fv_flow.kern.h:164-201) on the
+// serial CPU device, host arrays in and out. nc = cells, nf = faces, ns =
+// cell-face slots, nnz = matrix entries.
+int kref_fv_pressure_assemble(int nc, int nf, int ns, int nnz, const int* offsets, const int* faces,
+                              const float* sign, const int* adjacent, const int* entry,
+                              const int* rows, const int* diag, const float* coefficient,
+                              const float* flux, float* values, float* rhs, int reference) {
+  try {
+    auto dev = Device::create(Backend::Cpu);
+    auto d_values = put(*dev, values, nnz);
+    auto d_rhs = put(*dev, rhs, nc);
+    kern::fv_pressure_assemble(*dev, nc, put(*dev, offsets, nc + 1), put(*dev, faces, ns),
+                               put(*dev, sign, ns), put(*dev, adjacent, ns), put(*dev, entry, ns),
+                               put(*dev, rows, nc + 1), put(*dev, diag, nc),
+                               put(*dev, coefficient, nf), put(*dev, flux, nf), d_values, d_rhs,
+                               reference);
+    dev->download(d_values, std::span<float>(values, nnz));
+    dev->download(d_rhs, std::span<float>(rhs, nc));
+    return 0;
+  } catch (const std::exception& e) {
+    g_error = e.what();
+    return -1;
+  }
+}
+
+int kref_fv_correct_flux(int nf, int nc, const int* owner, const int* neighbour,
+                         const float* correction, const float* coefficient, float* flux,
+                         int internal) {
+  try {
+    auto dev = Device::create(Backend::Cpu);
+    auto d_flux = put(*dev, flux, nf);
+    kern::fv_correct_flux(*dev, nf, put(*dev, owner, nf), put(*dev, neighbour, internal),
+                          put(*dev, correction, nc), put(*dev, coefficient, nf), d_flux, internal);
+    dev->download(d_flux, std::span<float>(flux, nf));
+    return 0;
+  } catch (const std::exception& e) {
+    g_error = e.what();
+    return -1;
+  }
+}
+
+int kref_fv_correct_velocity(int nc, const float* volume, const float* inverse,
+                             const float* diagonal, const float* gx, const float* gy,
+                             const float* gz, const float* correction, float* u, float* v,
+                             float* w, float* p, float alpha) {
+  try {
+    auto dev = Device::create(Backend::Cpu);
+    auto du = put(*dev, u, nc), dv = put(*dev, v, nc), dw = put(*dev, w, nc), dp = put(*dev, p, nc);
+    kern::fv_correct_velocity(*dev, nc, put(*dev, volume, nc), put(*dev, inverse, nc),
+                              put(*dev, diagonal, nc), put(*dev, gx, nc), put(*dev, gy, nc),
+                              put(*dev, gz, nc), put(*dev, correction, nc), du, dv, dw, dp, alpha);
+    dev->download(du, std::span<float>(u, nc));
+    dev->download(dv, std::span<float>(v, nc));
+    dev->download(dw, std::span<float>(w, nc));
+    dev->download(dp, std::span<float>(p, nc));
+    return 0;
+  } catch (const std::exception& e) {
+    g_error = e.what();
+    return -1;
+  }
+}
 
 }  // extern "C"
