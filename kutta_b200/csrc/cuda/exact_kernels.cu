@@ -287,22 +287,30 @@ __global__ void k_galerkin(int nnz_c, const int* __restrict__ offsets,
   }
 }
 
-// amg_m_matrix_diagonal :44-58.
-__global__ void k_m_matrix_diagonal(int nc, const int* __restrict__ offsets,
-                                    const int* __restrict__ members,
-                                    const int* __restrict__ fine_rows,
-                                    const int* __restrict__ fine_diag,
-                                    const float* __restrict__ fine, const int* __restrict__ rows,
-                                    const int* __restrict__ diag, float* coarse) {
+// amg_m_matrix_diagonal :44-58 in two passes with the same roundings in the
+// same order: each fine row's surplus (its diagonal plus its off-diagonals,
+// upward rounded), independent per row and computed in parallel; then, per
+// coarse row, the upward-rounded sum of its members' surpluses in member
+// order minus its stored off-diagonals. Splitting the member loop out of the
+// per-coarse-row chain shortens the dependent sequence of each thread.
+__global__ void k_row_surplus(int n, const int* __restrict__ rows, const int* __restrict__ diag,
+                              const float* __restrict__ fine, float* __restrict__ surplus) {
+  ROWS(i, n) {
+    UpperSum sum{fine[diag[i]], 0.0f};
+    for (int j = rows[i]; j < rows[i + 1]; ++j)
+      if (j != diag[i]) sum = upper_add(sum, fine[j]);
+    surplus[i] = upper_value(sum);
+  }
+}
+
+__global__ void k_m_matrix_combine(int nc, const int* __restrict__ offsets,
+                                   const int* __restrict__ members,
+                                   const float* __restrict__ surplus, const int* __restrict__ rows,
+                                   const int* __restrict__ diag, float* coarse) {
   ROWS(g, nc) {
     UpperSum diagonal{0.0f, 0.0f};
-    for (int m = offsets[g]; m < offsets[g + 1]; ++m) {
-      const int row = members[m];
-      UpperSum surplus{fine[fine_diag[row]], 0.0f};
-      for (int j = fine_rows[row]; j < fine_rows[row + 1]; ++j)
-        if (j != fine_diag[row]) surplus = upper_add(surplus, fine[j]);
-      diagonal = upper_add(diagonal, upper_value(surplus));
-    }
+    for (int m = offsets[g]; m < offsets[g + 1]; ++m)
+      diagonal = upper_add(diagonal, surplus[members[m]]);
     for (int j = rows[g]; j < rows[g + 1]; ++j)
       if (j != diag[g]) diagonal = upper_add(diagonal, -coarse[j]);
     coarse[diag[g]] = upper_value(diagonal);
@@ -574,13 +582,15 @@ void galerkin(int nnz_c, const int* offsets, const int* entries, const float* fi
   ++counter;
   k_galerkin<<<blocks(nnz_c), kBlock, 0, s>>>(nnz_c, offsets, entries, fine, coarse);
 }
-void m_matrix_diagonal(int nc, const int* offsets, const int* members, const int* fine_rows,
+void m_matrix_diagonal(int nf, int nc, const int* offsets, const int* members, const int* fine_rows,
                        const int* fine_diag, const float* fine, const int* rows, const int* diag,
-                       float* coarse, cudaStream_t s) {
+                       float* coarse, float* surplus, cudaStream_t s) {
   if (nc <= 0) return;
   ++counter;
-  k_m_matrix_diagonal<<<blocks(nc), kBlock, 0, s>>>(nc, offsets, members, fine_rows, fine_diag,
-                                                    fine, rows, diag, coarse);
+  k_row_surplus<<<full_grid(nf), kBlock, 0, s>>>(nf, fine_rows, fine_diag, fine, surplus);
+  ++counter;
+  k_m_matrix_combine<<<full_grid(nc), kBlock, 0, s>>>(nc, offsets, members, surplus, rows, diag,
+                                                      coarse);
 }
 void pcg_step_dot(int n, float* x, float* r, const float* p, const float* q, DeviceReducer red,
                   float* scalars, int* status, cudaStream_t s) {

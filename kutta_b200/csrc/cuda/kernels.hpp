@@ -73,9 +73,10 @@ void prolong(int nf, const int* aggregate, const float* coarse, float* fine, con
              cudaStream_t s);
 void galerkin(int nnz_c, const int* offsets, const int* entries, const float* fine, float* coarse,
               cudaStream_t s);
-void m_matrix_diagonal(int nc, const int* offsets, const int* members, const int* fine_rows,
+// amg_m_matrix_diagonal: surplus holds nf floats of scratch.
+void m_matrix_diagonal(int nf, int nc, const int* offsets, const int* members, const int* fine_rows,
                        const int* fine_diag, const float* fine, const int* rows, const int* diag,
-                       float* coarse, cudaStream_t s);
+                       float* coarse, float* surplus, cudaStream_t s);
 
 // ---- Krylov vector updates (guarded by status) ----------------------------
 // x += a p; r -= a q; then r.r -> scalars[18] and solver_check(pcg = 1).

@@ -290,6 +290,102 @@ __global__ void __launch_bounds__(1024)
   }
 }
 
+// The same Cholesky factor and inverse for n <= kSharedDense, on chip and
+// with short dependent chains: L and X = L^-1 live in shared memory; each
+// elimination step updates the trailing lower triangle in parallel over its
+// (i, j) pairs (each element sees the same updates in the same k order as a
+// row-by-row update); X is built one elimination step at a time over all
+// right-hand sides of the identity at once; W = X^T X (symmetric) is written
+// to global memory. `L` (global) is not used.
+constexpr int kSharedDense = 112;  // 2 n^2 doubles <= 200 KB
+constexpr int kDenseThreads = 256;
+
+// Lower-triangle pair number p -> (i, j), j <= i, rows counted from 0.
+__device__ __forceinline__ void triangle_pair(int p, int& i, int& j) {
+  i = static_cast<int>((sqrt(8.0 * p + 1.0) - 1.0) * 0.5);
+  while ((i + 1) * (i + 2) / 2 <= p) ++i;
+  while (i * (i + 1) / 2 > p) --i;
+  j = p - i * (i + 1) / 2;
+}
+
+__global__ void __launch_bounds__(kDenseThreads)
+    k_dense_inverse_shared(int n, const int* __restrict__ rows, const int* __restrict__ cols,
+                           const float* __restrict__ vals, double* __restrict__ W, double* error,
+                           double* ratio) {
+  extern __shared__ double dense[];
+  double* Ls = dense;          // n x n, lower triangle
+  double* Xs = dense + n * n;  // n x n, X = L^-1 (lower triangle)
+  const int t = threadIdx.x, T = blockDim.x;
+  __shared__ int failed;
+  __shared__ double smallest, pivot;
+  __shared__ double diag0[kSharedDense];
+  if (t == 0) {
+    failed = 0;
+    smallest = 1.0;
+  }
+  for (int k = t; k < n * n; k += T) {
+    Ls[k] = 0.0;
+    Xs[k] = (k / n == k % n) ? 1.0 : 0.0;
+  }
+  __syncthreads();
+  for (int i = t; i < n; i += T)
+    for (int j = rows[i]; j < rows[i + 1]; ++j) {
+      if (cols[j] <= i) Ls[i * n + cols[j]] = vals[j];
+      if (cols[j] == i) diag0[i] = vals[j];
+    }
+  __syncthreads();
+  for (int k = 0; k < n; ++k) {
+    if (t == 0) {
+      double d = Ls[k * n + k];
+      if (!(d > 0.0)) {
+        failed = 1;
+        d = 1.0;
+      } else {
+        smallest = fmin(smallest, d / diag0[k]);
+      }
+      pivot = sqrt(d);
+      Ls[k * n + k] = pivot;
+    }
+    __syncthreads();
+    for (int i = k + 1 + t; i < n; i += T) Ls[i * n + k] /= pivot;
+    __syncthreads();
+    const int m = n - k - 1;  // trailing rows k+1 .. n-1
+    for (int p = t; p < m * (m + 1) / 2; p += T) {
+      int a, b;
+      triangle_pair(p, a, b);
+      const int i = k + 1 + a, j = k + 1 + b;
+      Ls[i * n + j] -= Ls[i * n + k] * Ls[j * n + k];
+    }
+    __syncthreads();
+  }
+  // X = L^-1: step k scales row k of X by 1 / L_kk, then removes L_ik X_k from
+  // the rows below (only columns j <= k of X are nonzero at that point).
+  for (int k = 0; k < n; ++k) {
+    const double inv = 1.0 / Ls[k * n + k];
+    for (int j = t; j <= k; j += T) Xs[k * n + j] *= inv;
+    __syncthreads();
+    const int below = n - k - 1;
+    for (int p = t; p < below * (k + 1); p += T) {
+      const int i = k + 1 + p / (k + 1), j = p % (k + 1);
+      Xs[i * n + j] -= Ls[i * n + k] * Xs[k * n + j];
+    }
+    __syncthreads();
+  }
+  // W = X^T X: W_ij = sum_{k >= max(i, j)} X_ki X_kj.
+  for (int p = t; p < n * (n + 1) / 2; p += T) {
+    int i, j;
+    triangle_pair(p, i, j);
+    double acc = 0.0;
+    for (int k = i; k < n; ++k) acc += Xs[k * n + i] * Xs[k * n + j];
+    W[static_cast<std::size_t>(i) * n + j] = acc;
+    W[static_cast<std::size_t>(j) * n + i] = acc;
+  }
+  if (t == 0) {
+    *error = failed ? 1.0 : 0.0;
+    if (ratio) *ratio = failed ? 0.0 : smallest;
+  }
+}
+
 // x = A^-1 b with the dense FP64 inverse: one warp per row, FP64 accumulation.
 __global__ void k_dense_solve(int n, const double* __restrict__ W, const float* __restrict__ b,
                               float* __restrict__ x, const int* __restrict__ status) {
@@ -388,6 +484,18 @@ void dense_inverse(int n, const int* rows, const int* cols, const float* vals, d
                    double* inverse, double* error, cudaStream_t s, double* ratio) {
   if (n <= 0) return;
   ++counter;
+  if (n <= kSharedDense) {
+    const int bytes = 2 * n * n * static_cast<int>(sizeof(double));
+    static bool raised = false;
+    if (!raised) {
+      cudaFuncSetAttribute(k_dense_inverse_shared, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           2 * kSharedDense * kSharedDense * static_cast<int>(sizeof(double)));
+      raised = true;
+    }
+    k_dense_inverse_shared<<<1, kDenseThreads, bytes, s>>>(n, rows, cols, vals, inverse, error,
+                                                            ratio);
+    return;
+  }
   const int threads = std::min(1024, ((n + 31) / 32) * 32);
   k_dense_inverse<<<1, threads, 0, s>>>(n, rows, cols, vals, lower, inverse, error, ratio);
 }

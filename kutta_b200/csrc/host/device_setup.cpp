@@ -176,9 +176,13 @@ class Builder {
                "upload");
     c.val.reset(nnz);
     launch::galerkin(c.nnz, c.entry_offsets.get(), c.entries.get(), fine.vals, c.val.get(), s_);
-    if (o_.m_matrix)
-      launch::m_matrix_diagonal(nc, c.member_offsets.get(), c.members.get(), fine.rows, fine.diag,
-                                fine.vals, c.row_ptr.get(), c.diag.get(), c.val.get(), s_);
+    if (o_.m_matrix) {
+      DArray<float> surplus(static_cast<std::size_t>(fine.n));
+      launch::m_matrix_diagonal(fine.n, nc, c.member_offsets.get(), c.members.get(), fine.rows,
+                                fine.diag, fine.vals, c.row_ptr.get(), c.diag.get(), c.val.get(),
+                                surplus.get(), s_);
+      wait(s_);  // the scratch is freed on return
+    }
     wait(s_);  // total_host_ is read by the copy above
   }
 

@@ -698,6 +698,8 @@ void Solver::assemble_refresh(const FvPressure& fv, float* values, float* rhs, c
 void Solver::refresh_levels(const float* val, bool fine_done, cudaStream_t s) {
   const float* matrix = val;
   std::vector<double> allowed;
+  if (options_.m_matrix && !surplus_.allocated() && levels_.size() > 1)
+    surplus_.reset(static_cast<std::size_t>(n_));
   for (std::size_t i = 0; i < levels_.size(); ++i) {
     auto& l = levels_[i];
     if (i > 0 || !fine_done)
@@ -708,9 +710,9 @@ void Solver::refresh_levels(const float* val, bool fine_done, cudaStream_t s) {
       auto& c = levels_[i + 1];
       launch::galerkin(c.nnz, l.entry_offsets.get(), l.entries.get(), matrix, c.val.get(), s);
       if (options_.m_matrix)
-        launch::m_matrix_diagonal(c.n, l.member_offsets.get(), l.members.get(), l.row_ptr.get(),
-                                  l.diag.get(), matrix, c.row_ptr.get(), c.diag.get(),
-                                  c.val.get(), s);
+        launch::m_matrix_diagonal(l.n, c.n, l.member_offsets.get(), l.members.get(),
+                                  l.row_ptr.get(), l.diag.get(), matrix, c.row_ptr.get(),
+                                  c.diag.get(), c.val.get(), surplus_.get(), s);
       matrix = c.val.get();
     }
   }

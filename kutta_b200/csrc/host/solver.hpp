@@ -253,6 +253,7 @@ class Solver {
   std::vector<DevLevel> levels_;
   double complexity_ = 0;
   DArray<float> jacobi_inverse_;  // Jacobi preconditioner
+  DArray<float> surplus_;         // M-matrix diagonal scratch (fine rows)
   float *r_ = nullptr, *z_ = nullptr, *p_ = nullptr, *q_ = nullptr, *shadow_ = nullptr,
         *s_ = nullptr, *t_ = nullptr, *zs_ = nullptr, *best_ = nullptr, *scratch_ = nullptr;
   DArray<float> scalars_, projection_;

@@ -112,12 +112,24 @@ def _coarsest(n_side=6, seed=4):
     return s
 
 
+DENSE_SYSTEMS = {
+    # Up to 112 rows the factor and inverse live in shared memory; above, in
+    # global memory.
+    "tet2_48": lambda: _coarsest(2),
+    "poisson_112": lambda: harness.poisson(7, 4, 4),
+    "poisson_113": lambda: harness.poisson(113, 1, 1),
+    "tet3_162": lambda: _coarsest(3),
+    "tet4_384": lambda: _coarsest(4),
+    "tet5_750": lambda: _coarsest(5),
+}
+
+
 @pytest.mark.gpu
-@pytest.mark.parametrize("n_side", [3, 4, 5])
-def test_dense_inverse_matches_fp64(cuda, n_side):
+@pytest.mark.parametrize("name", list(DENSE_SYSTEMS))
+def test_dense_inverse_matches_fp64(cuda, name):
     """The coarsest-level dense FP64 Cholesky inverse against numpy in FP64."""
     import torch
-    s = _coarsest(n_side)
+    s = DENSE_SYSTEMS[name]()
     n = s.n
     assert n <= 1024
     a = L.upload(s)
@@ -136,9 +148,10 @@ def test_dense_inverse_matches_fp64(cuda, n_side):
 
 
 @pytest.mark.gpu
-def test_dense_inverse_flags_non_spd(cuda):
+@pytest.mark.parametrize("n_side", [2, 3])
+def test_dense_inverse_flags_non_spd(cuda, n_side):
     import torch
-    s = _coarsest(3)
+    s = _coarsest(n_side)
     bad = s.val.copy()
     bad[s.diag[0]] = -1.0
     a = L.upload(harness.HostSystem(s.row_ptr, s.col, s.diag, bad, s.b))
