@@ -278,7 +278,8 @@ def run_ours(args, rank, world, local):
         achieved = p["fine_sweep_bytes"] / (sweep_ms * 1e-3) / 1e9 if sweep_ms > 0 else None
         peak, kind = _peaks()
         return {
-            "kernel": "k_smooth<false>: fine-level damped L1-Jacobi sweep (CSR, row per thread)",
+            "kernel": "fine-level damped L1-Jacobi post-sweep (CSR, row per thread; in the mixed "
+                      "solve k_smooth_dot2, with the flexible PCG's r.z and z.q fused)",
             "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
             "frac": achieved / peak if achieved else None, "peak_source": kind,
             "bytes_per_launch": p["fine_sweep_bytes"], "launch_ms": sweep_ms,

@@ -208,6 +208,32 @@ __global__ void k_smooth(int n, const int* __restrict__ rows, const int* __restr
   }
 }
 
+// The fine-level post-sweep of the flexible PCG (mixed solve) with the two
+// reductions that follow the preconditioner fused in: next as
+// k_smooth<false>, then b.next and next.q (b the Krylov residual r, next the
+// preconditioned z, q = A p) into scalars[offset..] with the epilogue, as
+// reduce_into(Dot2, r, z, z, q) computes them: the same grid, the same row
+// loop and the same products, so the same totals bit for bit.
+__global__ void k_smooth_dot2(int n, const int* __restrict__ rows, const int* __restrict__ cols,
+                              const float* __restrict__ vals, const float* __restrict__ x,
+                              const float* __restrict__ b, const float* __restrict__ inv,
+                              float* __restrict__ next, const float* __restrict__ q,
+                              DeviceReducer red, float* scalars, int offset, int* status,
+                              Epilogue epi) {
+  if (status[0] != 0) return;
+  double a = 0, c = 0;
+  ROWS(i, n) {
+    float sum = b[i], error = 0.0f;
+    const int end = rows[i + 1];
+    for (int j = rows[i]; j < end; ++j) residual_term(sum, error, vals[j], x[cols[j]]);
+    const float z = x[i] + (2.0f / 3.0f) * inv[i] * (sum + error);
+    next[i] = z;
+    a += static_cast<double>(b[i]) * static_cast<double>(z);
+    c += static_cast<double>(z) * static_cast<double>(q[i]);
+  }
+  finish(as_reducer(red), a, c, true, scalars, offset, status, epi);
+}
+
 // amg_coarse_solve, linalg.kern.h:126-147: whole <=24-row system in one thread.
 __global__ void k_coarse_solve(int count, const int* __restrict__ rows,
                                const int* __restrict__ cols, const float* __restrict__ vals,
@@ -552,6 +578,14 @@ void smooth(int n, const int* rows, const int* cols, const float* vals, const fl
     k_smooth<true><<<full_grid(n), kBlock, 0, s>>>(n, rows, cols, vals, x, b, inv, next, status);
   else
     k_smooth<false><<<full_grid(n), kBlock, 0, s>>>(n, rows, cols, vals, x, b, inv, next, status);
+}
+void smooth_dot2(int n, const int* rows, const int* cols, const float* vals, const float* x,
+                 const float* b, const float* inv, float* next, const float* q, DeviceReducer red,
+                 float* scalars, int offset, int* status, Epilogue epi, cudaStream_t s) {
+  if (n <= 0) return;
+  ++counter;
+  k_smooth_dot2<<<blocks(n), kBlock, 0, s>>>(n, rows, cols, vals, x, b, inv, next, q, red,
+                                             scalars, offset, status, epi);
 }
 void coarse_solve(int count, const int* rows, const int* cols, const float* vals, float* x,
                   const float* b, const float* inv, const int* status, int sweeps,

@@ -57,6 +57,11 @@ void residual(int n, const int* rows, const int* cols, const float* vals, const 
 void smooth(int n, const int* rows, const int* cols, const float* vals, const float* x,
             const float* b, const float* inv, float* next, const int* status, bool zero_start,
             cudaStream_t s);
+// The fine post-sweep with the flexible PCG's r.z and z.q (b = r, next = z)
+// reduced into scalars[offset..] and the epilogue run, as reduce_into(Dot2).
+void smooth_dot2(int n, const int* rows, const int* cols, const float* vals, const float* x,
+                 const float* b, const float* inv, float* next, const float* q, DeviceReducer red,
+                 float* scalars, int offset, int* status, Epilogue epi, cudaStream_t s);
 // <=24-row coarsest level, `sweeps` Jacobi sweeps in one thread (amg_coarse_solve).
 void coarse_solve(int count, const int* rows, const int* cols, const float* vals, float* x,
                   const float* b, const float* inv, const int* status, int sweeps,

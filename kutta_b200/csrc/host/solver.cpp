@@ -281,6 +281,8 @@ void Solver::set_profile(bool on) {
   prof_.fine_sweep_bytes = 8.0 * nnz_ + 4.0 * (n_ + 1) + 16.0 * n_;
   launch_mark_ = launch::counter.load();
   events_used_ = 0;
+  event_bytes_.clear();
+  timed_bytes_ = 0;
 }
 
 void Solver::collect_events() {
@@ -297,12 +299,17 @@ void Solver::collect_events() {
     std::vector<float> sorted = times;
     std::nth_element(sorted.begin(), sorted.begin() + sorted.size() / 2, sorted.end());
     const float median = sorted[sorted.size() / 2];
-    for (float ms : times)
-      if (ms >= 0.25f * median) {
-        prof_.fine_sweep_ms += ms;
+    for (std::size_t k = 0; k < times.size(); ++k)
+      if (times[k] >= 0.25f * median) {
+        prof_.fine_sweep_ms += times[k];
         ++prof_.fine_sweeps;
+        timed_bytes_ += k < event_bytes_.size() ? event_bytes_[k] : 0.0;
       }
+    // The average algorithmic bytes of the timed sweeps (a post-sweep with
+    // the flexible PCG's reductions fused also reads q).
+    if (prof_.fine_sweeps > 0) prof_.fine_sweep_bytes = timed_bytes_ / prof_.fine_sweeps;
   }
+  event_bytes_.clear();
   prof_.launches = launch::counter.load() - launch_mark_;
 }
 
@@ -362,13 +369,22 @@ void Solver::smooth(DevLevel& l, const int* rows, const int* cols, const float* 
       }
       cuda_check(cudaEventRecord(events_[events_used_++], stream_), "cudaEventRecord");
     }
+    // The last sweep of the fine level's post-smoothing (pre-smoothing always
+    // starts from zero) carries the fused reductions.
+    const bool with_dots = fine && fuse_dots_ && !zero_start && sweep + 1 == sweeps;
+    const double bytes =
+        zero ? 12.0 * l.n : 8.0 * l.nnz + 4.0 * (l.n + 1) + (with_dots ? 20.0 : 16.0) * l.n;
+    if (timed) event_bytes_.push_back(bytes);
     if (l.v16.allocated())
       launch::bf16_smooth(l.n, rows, cols, l.v16.get(), l.scale.get(), x, b, l.l1.get(), l.r,
                           status, zero, stream_);
+    else if (with_dots)
+      launch::smooth_dot2(l.n, rows, cols, vals, x, b, l.l1.get(), l.r, q_, reducer(),
+                          scalars_.get(), 4, status_.get(), Epilogue::PcgBetaFlexible, stream_);
     else
       launch::smooth(l.n, rows, cols, vals, x, b, l.l1.get(), l.r, status, zero, stream_);
     if (timed) cuda_check(cudaEventRecord(events_[events_used_++], stream_), "cudaEventRecord");
-    tally(zero ? 12.0 * l.n : 8.0 * l.nnz + 4.0 * (l.n + 1) + 16.0 * l.n);
+    tally(bytes);
     std::swap(x, l.r);  // ping-pong: the two buffers exchange roles (amg.cpp:280)
   }
 }
@@ -510,7 +526,7 @@ void Solver::inner(std::size_t index, const int* parent) {
 // (solver.cpp:65-68) preconditioner.
 void Solver::apply(const float* r, float*& z) {
   if (amg() && graphing()) {
-    graphed(r, z, 0, z, [&] { precondition(r, z); });
+    graphed(r, z, fuse_dots_ ? 1 : 0, z, [&] { precondition(r, z); });
   } else if (amg()) {
     precondition(r, z);
   } else {
@@ -812,12 +828,16 @@ void Solver::pcg(float* x, const float* b, const Control& c, double target, Stat
       launch::pcg_step_dot(n_, x, r_, p_, q_, reducer(), scalars_.get(), status_.get(), stream_);
       tally(8.0 * nnz_ + 4.0 * (n_ + 1) + 8.0 * n_ + 24.0 * n_);
       if (stats.iterations + j + 1 == c.max_iter) return;
+      const bool fused = can_fuse_dots();
+      fuse_dots_ = fused;
       apply(r_, z_);
-      tally((variable() ? 12.0 : 8.0) * n_ + 12.0 * n_);
-      if (variable())
-        launch::reduce_into(ReduceMode::Dot2, n_, r_, z_, z_, q_, reducer(), scalars_.get(), 4,
-                            status_.get(), true, Epilogue::PcgBetaFlexible, stream_);
-      else
+      fuse_dots_ = false;
+      tally((variable() ? (fused ? 4.0 : 12.0) : 8.0) * n_ + 12.0 * n_);
+      if (variable()) {
+        if (!fused)
+          launch::reduce_into(ReduceMode::Dot2, n_, r_, z_, z_, q_, reducer(), scalars_.get(), 4,
+                              status_.get(), true, Epilogue::PcgBetaFlexible, stream_);
+      } else
         launch::reduce_into(ReduceMode::Dot, n_, r_, z_, r_, z_, reducer(), scalars_.get(), 4,
                             status_.get(), true, Epilogue::PcgBeta, stream_);
       launch::direction(n_, z_, p_, scalars_.get(), status_.get(), stream_);

@@ -167,6 +167,15 @@ class Solver {
 
   // Preconditioner.
   void apply(const float* r, float*& z);
+  // Whether the flexible PCG's reductions after the preconditioner can ride
+  // on the fine post-sweep (nothing touches z after that sweep), and the
+  // request flag set around apply() when they do.
+  bool can_fuse_dots() const {
+    return amg() && variable() && !nullspace_ && levels_.size() > 1 && options_.post_sweeps >= 1 &&
+           !levels_[0].v16.allocated() &&
+           !(learned_ != nullptr && (learned_mode_ & kLearnedCycle));
+  }
+  bool fuse_dots_ = false;
   void precondition(const float* r, float*& z);
   // c = G(t), q = A c and the dots {c.t, c.Ac} for the safeguarded step.
   void learned_direction(const float* t);
@@ -279,6 +288,8 @@ class Solver {
   Profile prof_;
   long long launch_mark_ = 0;
   std::vector<cudaEvent_t> events_;
+  std::vector<double> event_bytes_;  // algorithmic bytes of each timed sweep
+  double timed_bytes_ = 0;
   std::size_t events_used_ = 0;
   long long sampled_ = 0;
 };

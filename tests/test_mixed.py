@@ -247,3 +247,30 @@ def test_cuda_graph_replay_is_bitwise_identical(cuda, k_levels):
     for (sg, xg), (sd, xd) in zip(out[True], out[False]):
         assert sg == sd
         assert np.array_equal(xg.view(np.uint64), xd.view(np.uint64))
+
+
+@pytest.mark.gpu
+def test_fused_post_sweep_reductions_are_exact(cuda):
+    """The flexible PCG's r.z and z.q ride on the fine post-sweep when nothing
+    changes z after it. A learned stage with all-zero weights turns that
+    fusion off (it acts after the cycle) but adds nothing to z (G = 0, step
+    0), so the fused and the unfused solves must agree bit for bit."""
+    import torch
+    s = harness.box_system(20, 20, 20, tet=True, seed=15)
+    a = L.upload(s)
+    b = torch.from_numpy(s.b).cuda()
+    out = []
+    for zero_stage in (False, True):
+        solver = L.make_mixed_solver(s)
+        solver.refresh(a)
+        if zero_stage:
+            g = L.LearnedStage(seed=1)
+            g.set_weights(np.zeros(L.LearnedStage.parameter_count(), np.float32))
+            solver.set_learned(g, L.LEARNED_CYCLE)
+        x = torch.zeros(s.n, dtype=torch.float64, device="cuda")
+        st = solver.solve(a, x, b, L.SolveControl(1e-8, 1e-30, 3000))
+        out.append((st.iterations, st.final_residual, x.cpu().numpy()))
+        if zero_stage:
+            solver.set_learned(None)
+    assert out[0][0] == out[1][0] and out[0][1] == out[1][1]
+    assert np.array_equal(out[0][2].view(np.uint64), out[1][2].view(np.uint64))
