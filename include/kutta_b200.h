@@ -198,6 +198,9 @@ typedef struct {
   int converged;
   double initial_residual;   /* ||b - A x0||, FP64 */
   double final_residual;     /* ||b - A x||, FP64, of the returned FP64 x */
+  int learned_fallback;      /* 1: a refinement stalled with the learned cycle stage
+                                attached, and the solve finished with the AMG cycle
+                                alone (the stage stays attached for later solves) */
 } b2_mixed_stats;
 
 typedef struct b2_mixed b2_mixed;

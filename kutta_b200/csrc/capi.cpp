@@ -541,6 +541,7 @@ int b2_mixed_solve(b2_mixed* s, const float* d_val, double* d_x, const float* d_
     const auto r = s->s->solve(d_val, d_x, d_b, c, as_stream(stream));
     if (stats) {
       stats->refinements = r.refinements;
+      stats->learned_fallback = r.learned_fallback ? 1 : 0;
       stats->iterations = r.iterations;
       stats->converged = r.converged ? 1 : 0;
       stats->initial_residual = r.initial_residual;

@@ -252,6 +252,8 @@ __global__ void k_gnn_step(int n, float* __restrict__ z, const float* __restrict
                            const double* __restrict__ dots) {
   const double den = dots[1];
   const float alpha = den > 0.0 && dots[0] > 0.0 ? static_cast<float>(dots[0] / den) : 0.0f;
+  // No step leaves z untouched, also where c is not finite (0 * NaN is NaN).
+  if (!(alpha > 0.0f) || !isfinite(alpha)) return;
   ROWS(i, n) z[i] = fmaf(alpha, c[i], z[i]);
 }
 
@@ -260,6 +262,7 @@ __global__ void k_gnn_step64(int n, double* __restrict__ x, const float* __restr
                              const double* __restrict__ dots) {
   const double den = dots[1];
   const double alpha = den > 0.0 && dots[0] > 0.0 ? dots[0] / den : 0.0;
+  if (!(alpha > 0.0) || !isfinite(alpha)) return;
   ROWS(i, n) x[i] += alpha * static_cast<double>(c[i]);
 }
 

@@ -54,6 +54,8 @@ MixedStats MixedSolver::solve(const float* val, double* x, const float* b, const
     r = residual(val, x, b, s);
   }
   int stalled = 0;
+  Gnn* const stage = inner_.learned();
+  const int mode = inner_.learned_mode();
   while (r > target && st.refinements < o_.max_refinements && st.iterations < c.max_iter) {
     cuda_check(cudaMemsetAsync(e_.get(), 0, sizeof(float) * static_cast<std::size_t>(n_), s),
                "memset");
@@ -72,8 +74,18 @@ MixedStats MixedSolver::solve(const float* val, double* x, const float* b, const
     ++st.refinements;
     stalled = next < 0.9 * r ? 0 : stalled + 1;
     r = next;
+    if (stalled > 0 && (mode & Solver::kLearnedCycle) && !st.learned_fallback) {
+      // The plain AMG cycle is the learned stage's fallback: a refinement
+      // that stalls with the stage attached is retried without it.
+      const int rest = mode & ~Solver::kLearnedCycle;
+      inner_.set_learned(rest != 0 ? stage : nullptr, rest);
+      st.learned_fallback = true;
+      stalled = 0;
+      continue;
+    }
     if (!std::isfinite(r) || stalled >= 2) break;
   }
+  if (st.learned_fallback) inner_.set_learned(stage, mode);
   inner_.check_learned(s);
   st.final_residual = r;
   st.converged = std::isfinite(r) && r <= target;

@@ -18,6 +18,9 @@ struct MixedOptions {
 struct MixedStats {
   int refinements = 0, iterations = 0;
   bool converged = false;
+  // The learned cycle stage was detached after a stalled refinement and the
+  // solve finished with the AMG cycle alone (the stage is re-attached after).
+  bool learned_fallback = false;
   double initial_residual = 0, final_residual = 0;
 };
 

@@ -191,6 +191,7 @@ class Solver {
   // network must outlive its attachment.
   void set_learned(Gnn* g, int mode);
   int learned_mode() const { return learned_ != nullptr ? learned_mode_ : 0; }
+  Gnn* learned() const { return learned_; }
   // x += alpha G(r) in FP64 for the residual r = b - A x, alpha =
   // max(0, c.t / c.Ac): the learned warm start (a no-op unless attached in
   // kLearnedWarmStart mode).

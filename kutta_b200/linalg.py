@@ -501,6 +501,7 @@ class MixedStats:
     converged: bool = False
     initial_residual: float = 0.0
     final_residual: float = 0.0
+    learned_fallback: bool = False
 
 
 class _MixedOptions(ctypes.Structure):
@@ -514,7 +515,7 @@ class _MixedOptions(ctypes.Structure):
 class _MixedStats(ctypes.Structure):
     _fields_ = [("refinements", ctypes.c_int), ("iterations", ctypes.c_int),
                 ("converged", ctypes.c_int), ("initial_residual", ctypes.c_double),
-                ("final_residual", ctypes.c_double)]
+                ("final_residual", ctypes.c_double), ("learned_fallback", ctypes.c_int)]
 
 
 def _mixed_struct(o: MixedOptions) -> _MixedOptions:
@@ -569,7 +570,7 @@ class MixedSolver:
         _check(_load().b2_mixed_solve(self._handle, _tptr(a.val), _tptr(x64), _tptr(b),
                                       ctypes.byref(c), ctypes.byref(st), _stream()))
         return MixedStats(st.refinements, st.iterations, bool(st.converged), st.initial_residual,
-                          st.final_residual)
+                          st.final_residual, bool(st.learned_fallback))
 
     def describe(self) -> str:
         buf = ctypes.create_string_buffer(512)

@@ -251,3 +251,56 @@ def test_learned_mode_is_validated(cuda):
     for bad in (0, 4, -1):
         with pytest.raises(L.KuttaError):
             solver.set_learned(g, bad)
+
+
+@pytest.mark.gpu
+def test_nonfinite_network_output_leaves_the_solve_unchanged(cuda):
+    """A stage whose output is not finite gets no step (alpha 0 and the
+    update skipped, since 0 * NaN is NaN): the solve equals the solve without
+    a stage, bit for bit, in both modes."""
+    import torch
+    s = harness.box_system(14, 14, 14, tet=True, seed=16)
+    a = L.upload(s)
+    b = torch.from_numpy(s.b).cuda()
+    out = []
+    for poisoned in (False, True):
+        solver = L.make_mixed_solver(s)
+        solver.refresh(a)
+        if poisoned:
+            g = L.LearnedStage(seed=2)
+            w = g.weights()
+            w[-L.LearnedStage.parameter_count() // 4:] = np.nan
+            g.set_weights(w)
+            solver.set_learned(g, L.LEARNED_CYCLE | L.LEARNED_WARM_START)
+        x = torch.zeros(s.n, dtype=torch.float64, device="cuda")
+        st = solver.solve(a, x, b, L.SolveControl(1e-8, 1e-30, 3000))
+        assert st.converged and not st.learned_fallback
+        out.append((st.iterations, st.final_residual, x.cpu().numpy()))
+        if poisoned:
+            solver.set_learned(None)
+    assert out[0][:2] == out[1][:2]
+    assert np.array_equal(out[0][2].view(np.uint64), out[1][2].view(np.uint64))
+
+
+@pytest.mark.gpu
+def test_stalled_refinement_falls_back_to_the_amg_cycle(cuda):
+    """The plain AMG cycle is the learned stage's fallback: asked for a
+    tolerance below the FP64 floor, the refinement must stall; the stage is
+    then detached for the rest of the solve, re-attached afterwards, and a
+    normal solve with it still meets its tolerance."""
+    import torch
+    s = harness.box_system(12, 12, 12, tet=True, seed=17)
+    a = L.upload(s)
+    b = torch.from_numpy(s.b).cuda()
+    solver = L.make_mixed_solver(s)
+    solver.refresh(a)
+    g = L.LearnedStage(seed=3)
+    solver.set_learned(g, L.LEARNED_CYCLE)
+    x = torch.zeros(s.n, dtype=torch.float64, device="cuda")
+    st = solver.solve(a, x, b, L.SolveControl(1e-20, 0.0, 3000))
+    assert st.learned_fallback and not st.converged
+    assert "learned stage" in solver.describe()
+    x.zero_()
+    st = solver.solve(a, x, b, L.SolveControl(1e-8, 1e-30, 3000))
+    assert st.converged and not st.learned_fallback
+    solver.set_learned(None)
