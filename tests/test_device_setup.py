@@ -55,7 +55,9 @@ CASES = [
 def _solver(s, structure, extra, setup, kind=L.SolverKind.AmgPcg):
     opts = L.AmgOptions(structure=structure, setup=setup, **extra)
     solver = L.make_amg_solver(kind, s, opts)
-    solver.refresh(L.upload(s))
+    a = L.upload(s)
+    solver.refresh(a)
+    solver._matrix = a  # level 0's values are the caller's matrix
     return solver
 
 
@@ -127,3 +129,40 @@ def test_nonsymmetric_pattern_falls_back_to_host_setup(cuda):
     for a, b in zip(host.levels(), device.levels()):
         assert np.array_equal(a[1], b[1]) and np.array_equal(a[5], b[5])
         assert np.array_equal(a[3].view(np.uint32), b[3].view(np.uint32))
+
+
+@pytest.mark.parametrize("mixed", [False, True], ids=["plain", "mixed"])
+def test_device_setup_equals_host_setup_at_full_size(cuda, mixed):
+    """The headline matrix (96^3 x 6 tets, 5,308,416 rows): every level's
+    aggregates, pattern, members and entry map, and (plain hierarchy) the
+    refreshed values, identical between the device and the host setup. For
+    the mixed hierarchy the solve from each is compared bit for bit."""
+    import torch
+    s = harness.pressure_tet96()
+    a = L.upload(s)
+    if mixed:
+        b = torch.from_numpy(s.b).cuda()
+        result = []
+        for setup in (L.Setup.Host, L.Setup.Device):
+            o = L.MixedOptions()
+            o.amg.setup = setup
+            solver = L.make_mixed_solver(s, o)
+            solver.refresh(a)
+            x = torch.zeros(s.n, dtype=torch.float64, device="cuda")
+            st = solver.solve(a, x, b, L.SolveControl(1e-6, 1e-30, 3000))
+            result.append((solver.describe(), st.iterations, x.cpu().numpy()))
+            del solver
+        assert result[0][:2] == result[1][:2]
+        assert np.array_equal(result[0][2].view(np.uint64), result[1][2].view(np.uint64))
+        return
+    host = _solver(s, M, {}, L.Setup.Host)
+    device = _solver(s, M, {}, L.Setup.Device)
+    assert device.describe() == host.describe()
+    hl, dl = host.levels(), device.levels()
+    assert [lv[0] for lv in hl] == [lv[0] for lv in dl]
+    for k, (h, d) in enumerate(zip(hl, dl)):
+        for a_h, a_d in zip(h[1:], d[1:]):
+            assert np.array_equal(a_h.view(np.uint32), a_d.view(np.uint32)), k
+        th, td = host.level_transfer(k), device.level_transfer(k)
+        for key in th:
+            assert np.array_equal(th[key], td[key]), (k, key)

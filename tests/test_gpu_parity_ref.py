@@ -29,6 +29,7 @@ def _solve_gpu(system, kind, amg_options=None, solver_options=None, rel_tol=1e-6
         torch.from_numpy(np.asarray(x0, np.float32)).cuda()
     st = solver.solve(a, x, b, L.SolveControl(rel_tol, abs_tol, max_iter, interval))
     torch.cuda.synchronize()
+    solver._matrix = a  # level 0's values are the caller's matrix: keep it alive
     return st, x.cpu().numpy(), solver
 
 
