@@ -81,6 +81,25 @@ def test_amg_matches_reference(cuda, name, make, kind, m_matrix):
 
 
 @needs_ref
+@pytest.mark.parametrize("make,kind,m_matrix", [
+    (lambda: harness.box_system(12, 12, 12, tet=True, seed=7), 3, True),
+    (lambda: _rhs(harness.poisson(20, 18, 1, 1, False, False, 3)), 4, False),
+], ids=["tet12_pcg", "poisson_wind3_bicg"])
+def test_one_sweep_cycles_match_reference(cuda, make, kind, m_matrix):
+    """V(1,1): the single zero-start pre-sweep and the residual run as one
+    fused pass; iterations and residuals must still be the reference's."""
+    s = make()
+    opts = L.AmgOptions(pre_sweeps=1, post_sweeps=1,
+                        structure=M if m_matrix else L.OperatorStructure.General)
+    st, x, solver = _solve_gpu(s, L.SolverKind(kind), amg_options=opts)
+    r = ref.solve(s, opts=ref.options(kind, structure=int(m_matrix), pre_sweeps=1,
+                                      post_sweeps=1),
+                  rel_tol=1e-6, abs_tol=1e-12, max_iter=2000)
+    assert solver.describe() == r.describe
+    _compare(st, x, r)
+
+
+@needs_ref
 @pytest.mark.parametrize("kind", [0, 1, 2])
 def test_jacobi_kinds_match_reference(cuda, kind):
     s = _rhs(harness.poisson(16, 12, 8, 1, False, False, 5 if kind == 2 else 0))
