@@ -189,3 +189,26 @@ def test_assemble_refresh_rejects_a_bad_reference_cell(cuda):
         solver.assemble_refresh(a, bad, rhs)
     with pytest.raises(L.KuttaError):
         L.fv_pressure_assemble(a, bad, rhs)
+
+
+def test_face_data_is_consistent():
+    """harness.fv_faces: every internal face sits in exactly two cell-face
+    slots (owner +1, neighbour -1) whose CSR entries are (cell, other cell);
+    every boundary face in one owner slot; shared entries occur."""
+    s = harness.box_system(6, 6, 6, tet=True, seed=1)
+    c = harness.fv_faces(s.row_ptr, s.col, s.diag, seed=2)
+    assert c.offsets[-1] == len(c.faces) == 2 * c.internal + (c.n_faces - c.internal)
+    cell = np.repeat(np.arange(c.n), np.diff(c.offsets))
+    seen = np.zeros(c.n_faces, np.int64)
+    np.add.at(seen, c.faces, 1)
+    assert np.all(seen[:c.internal] == 2) and np.all(seen[c.internal:] == 1)
+    inner = c.adjacent >= 0
+    assert np.all(inner == (c.faces < c.internal))
+    f = c.faces[inner]
+    own = c.sign[inner] > 0
+    assert np.all(np.where(own, c.owner[f], c.neighbour[f]) == cell[inner])
+    assert np.all(np.where(own, c.neighbour[f], c.owner[f]) == c.adjacent[inner])
+    assert np.all(c.cols[c.entry[inner]] == c.adjacent[inner])
+    rows = np.repeat(np.arange(c.n), np.diff(c.rows))
+    assert np.all(rows[c.entry[inner]] == cell[inner])
+    assert len(np.unique(c.entry[inner])) < inner.sum()  # some entries shared
