@@ -481,7 +481,7 @@ void b2_mixed_options_default(b2_mixed_options* o) {
   o->amg.cycle = B2_CYCLE_K;
   o->amg.pre_sweeps = o->amg.post_sweeps = 1;
   o->absorb_singletons = 1;
-  o->dense_rows = 512;
+  o->dense_rows = 112;  // the largest coarsest level inverted on chip
   o->coarse_bf16 = 1;
   o->inner_rel_tol = 1e-3;
   o->inner_max_iter = 300;

@@ -484,7 +484,7 @@ class MixedOptions:
         cycle=AmgCycle.K, pre_sweeps=1, post_sweeps=1,
         structure=OperatorStructure.SymmetricMMatrix))
     absorb_singletons: bool = True
-    dense_rows: int = 512
+    dense_rows: int = 112
     coarse_bf16: bool = True
     inner_rel_tol: float = 1e-3
     inner_max_iter: int = 300

@@ -13,7 +13,7 @@ from kutta_b200 import linalg as L
 from oracle import kutta_oracle as O
 
 
-def _oracle_levels(s, dense_rows=512):
+def _oracle_levels(s, dense_rows=112):
     o = O.Solver(s, O.options(O.AMG_PCG, pre_sweeps=2, post_sweeps=2, coarse_rows=dense_rows,
                               m_matrix=True, absorb=True))
     return o.levels()
@@ -25,7 +25,7 @@ def test_mixed_hierarchy_matches_oracle(seed, tet):
     mine = L.build_mixed_hierarchy(s)
     theirs = _oracle_levels(s)
     assert [m.n for m in mine] == [t["n"] for t in theirs]
-    assert mine[-1].n <= 512
+    assert mine[-1].n <= 112
     for i, (m, t) in enumerate(zip(mine, theirs)):
         assert np.array_equal(m.row_ptr, t["row_ptr"]) and np.array_equal(m.col, t["col"])
         if i > 0:
@@ -43,7 +43,7 @@ def test_absorption_removes_the_stall():
                                               coarse_rows=512))
     mixed = L.build_mixed_hierarchy(s)
     assert plain[-1].n > 2000
-    assert mixed[-1].n <= 512
+    assert mixed[-1].n <= 112
     assert sum(lv.row_ptr[-1] for lv in mixed) < sum(lv.row_ptr[-1] for lv in plain)
 
 
