@@ -386,6 +386,92 @@ __global__ void __launch_bounds__(kDenseThreads)
   }
 }
 
+// The same for kSharedDense < n <= kPackedDense: only the lower triangle, packed
+// (row i at i (i + 1) / 2), fits in shared memory, so L is inverted in place.
+// Column j of X = L^-1 (j from the right) needs the already inverted columns
+// k > j and column j of L: X_ij = -(sum_{k=j+1..i} X_ik L_kj) / L_jj, one warp
+// per row i with the sum split over the lanes; then W = X^T X.
+constexpr int kPackedDense = 236;  // (n (n + 1) / 2 + 2 n) doubles <= 227 KB
+constexpr int kPackedThreads = 1024;
+
+__device__ __forceinline__ int packed(int i, int j) { return i * (i + 1) / 2 + j; }
+
+__global__ void __launch_bounds__(kPackedThreads)
+    k_dense_inverse_packed(int n, const int* __restrict__ rows, const int* __restrict__ cols,
+                           const float* __restrict__ vals, double* __restrict__ W, double* error,
+                           double* ratio) {
+  extern __shared__ double dense[];
+  const int total = n * (n + 1) / 2;
+  double* P = dense;           // packed lower triangle: L, then X = L^-1
+  double* temp = P + total;    // one column's new entries
+  double* diag0 = temp + n;    // the input diagonal
+  const int t = threadIdx.x, T = blockDim.x, lane = t & 31, warp = t >> 5, warps = T >> 5;
+  __shared__ int failed;
+  __shared__ double smallest, pivot;
+  if (t == 0) {
+    failed = 0;
+    smallest = 1.0;
+  }
+  for (int k = t; k < total; k += T) P[k] = 0.0;
+  __syncthreads();
+  for (int i = t; i < n; i += T)
+    for (int j = rows[i]; j < rows[i + 1]; ++j) {
+      if (cols[j] <= i) P[packed(i, cols[j])] = vals[j];
+      if (cols[j] == i) diag0[i] = vals[j];
+    }
+  __syncthreads();
+  for (int k = 0; k < n; ++k) {
+    if (t == 0) {
+      double d = P[packed(k, k)];
+      if (!(d > 0.0)) {
+        failed = 1;
+        d = 1.0;
+      } else {
+        smallest = fmin(smallest, d / diag0[k]);
+      }
+      pivot = sqrt(d);
+      P[packed(k, k)] = pivot;
+    }
+    __syncthreads();
+    for (int i = k + 1 + t; i < n; i += T) P[packed(i, k)] /= pivot;
+    __syncthreads();
+    const int m = n - k - 1;
+    for (int p = t; p < m * (m + 1) / 2; p += T) {
+      int a, b;
+      triangle_pair(p, a, b);
+      const int i = k + 1 + a, j = k + 1 + b;
+      P[packed(i, j)] -= P[packed(i, k)] * P[packed(j, k)];
+    }
+    __syncthreads();
+  }
+  for (int j = n - 1; j >= 0; --j) {
+    const double ljj = P[packed(j, j)];  // read before this step's writes
+    for (int i = j + 1 + warp; i < n; i += warps) {
+      double acc = 0.0;
+      for (int k = j + 1 + lane; k <= i; k += 32) acc += P[packed(i, k)] * P[packed(k, j)];
+#pragma unroll
+      for (int d = 16; d > 0; d >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, d);
+      if (lane == 0) temp[i] = acc;
+    }
+    __syncthreads();
+    for (int i = j + 1 + t; i < n; i += T) P[packed(i, j)] = -temp[i] / ljj;
+    if (t == 0) P[packed(j, j)] = 1.0 / ljj;
+    __syncthreads();
+  }
+  for (int p = t; p < total; p += T) {
+    int i, j;
+    triangle_pair(p, i, j);
+    double acc = 0.0;
+    for (int k = i; k < n; ++k) acc += P[packed(k, i)] * P[packed(k, j)];
+    W[static_cast<std::size_t>(i) * n + j] = acc;
+    W[static_cast<std::size_t>(j) * n + i] = acc;
+  }
+  if (t == 0) {
+    *error = failed ? 1.0 : 0.0;
+    if (ratio) *ratio = failed ? 0.0 : smallest;
+  }
+}
+
 // x = A^-1 b with the dense FP64 inverse: one warp per row, FP64 accumulation.
 __global__ void k_dense_solve(int n, const double* __restrict__ W, const float* __restrict__ b,
                               float* __restrict__ x, const int* __restrict__ status) {
@@ -493,6 +579,19 @@ void dense_inverse(int n, const int* rows, const int* cols, const float* vals, d
       raised = true;
     }
     k_dense_inverse_shared<<<1, kDenseThreads, bytes, s>>>(n, rows, cols, vals, inverse, error,
+                                                            ratio);
+    return;
+  }
+  if (n <= kPackedDense) {
+    const int bytes = (n * (n + 1) / 2 + 2 * n) * static_cast<int>(sizeof(double));
+    static bool raised_packed = false;
+    if (!raised_packed) {
+      cudaFuncSetAttribute(
+          k_dense_inverse_packed, cudaFuncAttributeMaxDynamicSharedMemorySize,
+          (kPackedDense * (kPackedDense + 1) / 2 + 2 * kPackedDense) * static_cast<int>(sizeof(double)));
+      raised_packed = true;
+    }
+    k_dense_inverse_packed<<<1, kPackedThreads, bytes, s>>>(n, rows, cols, vals, inverse, error,
                                                             ratio);
     return;
   }

@@ -113,11 +113,14 @@ def _coarsest(n_side=6, seed=4):
 
 
 DENSE_SYSTEMS = {
-    # Up to 112 rows the factor and inverse live in shared memory; above, in
-    # global memory.
+    # Up to 112 rows the factor and inverse live in shared memory; up to 236
+    # rows the packed lower triangle does, inverted in place; above, global
+    # memory.
     "tet2_48": lambda: _coarsest(2),
     "poisson_112": lambda: harness.poisson(7, 4, 4),
     "poisson_113": lambda: harness.poisson(113, 1, 1),
+    "poisson_236": lambda: harness.poisson(59, 4, 1),
+    "poisson_237": lambda: harness.poisson(79, 3, 1),
     "tet3_162": lambda: _coarsest(3),
     "tet4_384": lambda: _coarsest(4),
     "tet5_750": lambda: _coarsest(5),
@@ -148,7 +151,7 @@ def test_dense_inverse_matches_fp64(cuda, name):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("n_side", [2, 3])
+@pytest.mark.parametrize("n_side", [2, 3, 4])
 def test_dense_inverse_flags_non_spd(cuda, n_side):
     import torch
     s = _coarsest(n_side)
