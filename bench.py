@@ -65,6 +65,18 @@ def _dist():
     return rank, world, local
 
 
+def _max_over_ranks(value: float, world: int, device) -> float:
+    """The largest of the ranks' values (every rank gets it): a multi-GPU time
+    is the slowest rank's. world == 1 returns the value unchanged."""
+    if world <= 1:
+        return value
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([value], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 def _workload(args):
     from kutta_b200 import harness
     n = args.size
@@ -175,11 +187,7 @@ def run_ours(args, rank, world, local):
         torch.cuda.synchronize()
 
     def max_over_ranks(ms):
-        if world > 1:
-            t = torch.tensor([ms], device=dev)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            return float(t.item())
-        return ms
+        return _max_over_ranks(ms, world, dev)
 
     a = L.upload(s, dev)
     b = torch.from_numpy(s.b).to(dev)
