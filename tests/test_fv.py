@@ -24,6 +24,8 @@ def _case(make, seed, reference=-1):
     s = make()
     if reference == "middle":
         reference = s.n // 2
+    elif reference == "last":
+        reference = s.n - 1
     return s, harness.fv_faces(s.row_ptr, s.col, s.diag, seed=seed, reference=reference)
 
 
@@ -40,7 +42,7 @@ def _velocity_inputs(n, seed):
 
 
 @needs_ref
-@pytest.mark.parametrize("reference", [-1, "middle"])
+@pytest.mark.parametrize("reference", [-1, 0, "middle", "last"])
 @pytest.mark.parametrize("name,make", SYSTEMS, ids=[c[0] for c in SYSTEMS])
 def test_oracle_assembly_matches_reference(name, make, reference):
     s, c = _case(make, seed=11, reference=reference)
