@@ -8,7 +8,9 @@
 #include <cmath>
 #include <limits>
 #include <numeric>
+#include <thread>
 #include <tuple>
+#include <vector>
 
 namespace kb2 {
 namespace {
@@ -259,6 +261,40 @@ std::vector<int> pairs(const CsrView& a, double threshold, bool exclude_isolated
   return map;
 }
 
+namespace {
+// The first failing index of a check over [0, n) and its message; n if none.
+struct Failure {
+  long long at;
+  const char* message;
+};
+
+// Scans [0, n) in contiguous chunks on the host's threads; check(begin, end)
+// returns its chunk's first failure. The earliest failure over all chunks is
+// raised, so a parallel scan reports what a serial one would.
+template <class Check>
+void first_failure(long long n, Check check) {
+  const long long grain = 1 << 16;
+  const long long chunks_wanted = (n + grain - 1) / grain;
+  const unsigned hardware = std::max(1u, std::thread::hardware_concurrency());
+  const long long threads = std::max(1LL, std::min<long long>(hardware, chunks_wanted));
+  std::vector<Failure> found(static_cast<std::size_t>(threads), Failure{n, nullptr});
+  if (threads == 1) {
+    found[0] = check(0, n);
+  } else {
+    std::vector<std::thread> pool;
+    const long long per = (n + threads - 1) / threads;
+    for (long long t = 0; t < threads; ++t)
+      pool.emplace_back([&, t] {
+        const long long begin = std::min(n, t * per), end = std::min(n, begin + per);
+        found[static_cast<std::size_t>(t)] = check(begin, end);
+      });
+    for (auto& th : pool) th.join();
+  }
+  for (const auto& f : found)  // chunks in order: the first one that failed
+    if (f.message != nullptr) throw Error(f.message);
+}
+}  // namespace
+
 void validate_host(const CsrView& a) {
   KB2_REQUIRE(a.n >= 0, "CSR: negative row count");
   KB2_REQUIRE(a.nnz >= 0, "CSR: exceeds 32-bit entry limit");
@@ -266,22 +302,36 @@ void validate_host(const CsrView& a) {
                   (a.nnz == 0 || (a.col != nullptr && a.val != nullptr)),
               "CSR: invalid array sizes");
   KB2_REQUIRE(a.row_ptr[0] == 0 && a.row_ptr[a.n] == a.nnz, "CSR: invalid row offsets");
-  for (int i = 0; i < a.n; ++i) {
-    KB2_REQUIRE(a.row_ptr[i] >= 0 && a.row_ptr[i] <= a.row_ptr[i + 1] && a.row_ptr[i + 1] <= a.nnz,
-                "CSR: invalid row range");
-    int previous = -1;
-    for (int j = a.row_ptr[i]; j < a.row_ptr[i + 1]; ++j) {
-      KB2_REQUIRE(a.col[j] > previous && a.col[j] < a.n,
-                  "CSR: columns must be in range, unique and sorted");
-      previous = a.col[j];
+  // Row ranges first (every row's range is then safe to read), then each
+  // row's columns and diagonal, then the values: the serial checks' order.
+  first_failure(a.n, [&](long long begin, long long end) {
+    for (long long r = begin; r < end; ++r) {
+      const int i = static_cast<int>(r);
+      if (!(a.row_ptr[i] >= 0 && a.row_ptr[i] <= a.row_ptr[i + 1] && a.row_ptr[i + 1] <= a.nnz))
+        return Failure{r, "CSR: invalid row range"};
     }
-    KB2_REQUIRE(a.diag[i] >= a.row_ptr[i] && a.diag[i] < a.row_ptr[i + 1] && a.col[a.diag[i]] == i,
-                "CSR: missing or incorrect diagonal");
-  }
-  for (int j = 0; j < a.nnz; ++j)
-    KB2_REQUIRE(std::isfinite(a.val[j]) &&
-                    std::fabs(a.val[j]) <= std::numeric_limits<float>::max(),
-                "CSR: nonfinite or out-of-range value");
+    return Failure{end, nullptr};
+  });
+  first_failure(a.n, [&](long long begin, long long end) {
+    for (long long r = begin; r < end; ++r) {
+      const int i = static_cast<int>(r);
+      int previous = -1;
+      for (int j = a.row_ptr[i]; j < a.row_ptr[i + 1]; ++j) {
+        if (!(a.col[j] > previous && a.col[j] < a.n))
+          return Failure{r, "CSR: columns must be in range, unique and sorted"};
+        previous = a.col[j];
+      }
+      if (!(a.diag[i] >= a.row_ptr[i] && a.diag[i] < a.row_ptr[i + 1] && a.col[a.diag[i]] == i))
+        return Failure{r, "CSR: missing or incorrect diagonal"};
+    }
+    return Failure{end, nullptr};
+  });
+  first_failure(a.nnz, [&](long long begin, long long end) {
+    for (long long j = begin; j < end; ++j)
+      if (!(std::isfinite(a.val[j]) && std::fabs(a.val[j]) <= std::numeric_limits<float>::max()))
+        return Failure{j, "CSR: nonfinite or out-of-range value"};
+    return Failure{end, nullptr};
+  });
 }
 
 std::vector<float> diagonal_values(const CsrView& a, bool l1, bool nullspace) {
@@ -314,22 +364,26 @@ void check_amg(Kind kind, const CsrView& a, const Options& o) {
               "AMG-PCG requires equal pre/post sweeps");
   validate_host(a);
   if (o.m_matrix) {
-    for (int i = 0; i < a.n; ++i) {
-      long double sum = 0;
-      for (int j = a.row_ptr[i]; j < a.row_ptr[i + 1]; ++j) {
-        const float value = static_cast<float>(a.val[j]);
-        sum += value;
-        const int column = a.col[j];
-        const int* first = a.col + a.row_ptr[column];
-        const int* last = a.col + a.row_ptr[column + 1];
-        const int* opposite = std::lower_bound(first, last, i);
-        KB2_REQUIRE(opposite != last && *opposite == i &&
-                        value == static_cast<float>(a.val[opposite - a.col]) &&
-                        (column == i || value <= 0),
-                    "AMG M-matrix: expected symmetric nonpositive edges");
+    first_failure(a.n, [&](long long begin, long long end) {
+      for (long long r = begin; r < end; ++r) {
+        const int i = static_cast<int>(r);
+        long double sum = 0;
+        for (int j = a.row_ptr[i]; j < a.row_ptr[i + 1]; ++j) {
+          const float value = static_cast<float>(a.val[j]);
+          sum += value;
+          const int column = a.col[j];
+          const int* first = a.col + a.row_ptr[column];
+          const int* last = a.col + a.row_ptr[column + 1];
+          const int* opposite = std::lower_bound(first, last, i);
+          if (!(opposite != last && *opposite == i &&
+                value == static_cast<float>(a.val[opposite - a.col]) &&
+                (column == i || value <= 0)))
+            return Failure{r, "AMG M-matrix: expected symmetric nonpositive edges"};
+        }
+        if (!(sum >= 0)) return Failure{r, "AMG M-matrix: expected diagonally dominant rows"};
       }
-      KB2_REQUIRE(sum >= 0, "AMG M-matrix: expected diagonally dominant rows");
-    }
+      return Failure{end, nullptr};
+    });
   }
 }
 

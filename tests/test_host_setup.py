@@ -129,6 +129,39 @@ def test_invalid_csr_and_options_are_rejected_like_the_reference():
         L.build_hierarchy(bad, L.AmgOptions(structure=M), spd=True)
 
 
+def test_first_failing_row_decides_the_error_on_large_inputs():
+    """The host checks scan large inputs in parallel chunks; as in the
+    reference's serial loops, the error reported is that of the first failing
+    row (or value), whichever chunk finds a later one first."""
+    s = harness.poisson(80, 80, 20)  # 128,000 rows: several chunks
+    late = s.n - 10
+    # Structure: a bad diagonal early, unsorted columns late.
+    off = next(j for j in range(s.row_ptr[10], s.row_ptr[11]) if s.col[j] != 10)
+    t = _bad(s, diag=(10, int(off)))
+    lo = int(s.row_ptr[late])
+    t.col[lo], t.col[lo + 1] = t.col[lo + 1], t.col[lo]
+    with pytest.raises(L.KuttaError, match="missing or incorrect diagonal"):
+        L.build_hierarchy(t)
+    # Values: a nonfinite value late only.
+    with pytest.raises(L.KuttaError, match="nonfinite or out-of-range"):
+        L.build_hierarchy(_bad(s, val=(int(s.row_ptr[late]), np.nan)))
+    # M-matrix: a positive edge early (its transpose too, to stay symmetric),
+    # a non-dominant row late.
+    m = harness.box_system(26, 26, 26, tet=False, seed=2)  # 17,576 rows
+    big = harness.box_system(42, 42, 42, tet=False, seed=2)  # 74,088 rows
+    for case in (m, big):
+        j = next(j for j in range(case.row_ptr[3], case.row_ptr[4]) if case.col[j] != 3)
+        c = int(case.col[j])
+        k = next(k for k in range(case.row_ptr[c], case.row_ptr[c + 1]) if case.col[k] == 3)
+        v = case.val.copy()
+        v[j], v[k] = -v[j], -v[k]
+        last = case.n - 3
+        v[case.diag[last]] *= 0.25
+        bad = harness.HostSystem(case.row_ptr, case.col, case.diag, v, case.b)
+        with pytest.raises(L.KuttaError, match="symmetric nonpositive edges"):
+            L.build_hierarchy(bad, L.AmgOptions(structure=M), spd=True)
+
+
 def test_empty_system_builds():
     """test_solvers.cpp:274-286: an empty CSR is a valid no-op."""
     e = harness.HostSystem(np.zeros(1, np.int32), np.zeros(0, np.int32), np.zeros(0, np.int32),
