@@ -1,6 +1,6 @@
 // Mixed-precision kernels (no reference counterpart): BF16 coarse operators,
 // the dense FP64 coarsest-level inverse, and the FP64 refinement residual.
-// Compiled with ordinary FMA contraction: these results are judged by the
+// Compiled with ordinary FMA contraction: these results are checked against the
 // FP64 true residual, not by bitwise agreement with the reference.
 #include <cuda_bf16.h>
 

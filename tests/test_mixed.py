@@ -2,7 +2,7 @@
 
 CPU: its hierarchy (pairing with singleton absorption) equals the oracle's
 restatement bit for bit and reaches the dense size where the reference's
-pairing stalls. GPU: it converges below the FP32 rounding floor, judged by the
+pairing stalls. GPU: it converges below the FP32 rounding floor, measured by the
 FP64 true residual of the returned FP64 solution and by the error against the
 FP64 CG oracle."""
 import numpy as np
