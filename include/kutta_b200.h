@@ -108,8 +108,11 @@ void b2_workspace_destroy(b2_workspace* workspace);
  * when options == NULL or `use_amg_options` == 0, make_amg_solver(kind, dev, a,
  * AmgOptions) (amg.hpp:26-27; amg.cpp:345-382) otherwise. The host CSR is the
  * reference's CsrMatrixHost (csr.hpp:16-28): row_ptr[n+1], col[nnz] sorted per
- * row, diag[n] the index of (i,i), val[nnz] as double. Setup runs on the host
- * (aggregation) and uploads the hierarchy to the current device. */
+ * row, diag[n] the index of (i,i), val[nnz] as double. The option, CSR,
+ * M-matrix, workspace-size and (Jacobi kinds) diagonal checks run on the host
+ * before any device work, in the reference's order and with its messages;
+ * the hierarchy is then built where options->setup says (B2_SETUP_DEVICE:
+ * on the current device, for structurally symmetric patterns). */
 int b2_solver_create(int kind, int n, int nnz, const int32_t* row_ptr, const int32_t* col,
                      const int32_t* diag, const double* val, const b2_options* options,
                      int use_amg_options, b2_solver** out);

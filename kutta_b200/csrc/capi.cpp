@@ -157,9 +157,13 @@ int b2_solver_create(int kind, int n, int nnz, const int32_t* row_ptr, const int
     *out = nullptr;
     KB2_REQUIRE(kind >= B2_JACOBI && kind <= B2_AMG_BICGSTAB, "unknown SolverKind");
     const auto k = static_cast<kb2::Kind>(kind);
+    const bool amg_factory = options && use_amg_options;
+    const bool amg_kind = k == kb2::Kind::AmgPcg || k == kb2::Kind::AmgBicgstab;
+    // make_amg_solver checks the kind first (amg.cpp:347-348).
+    KB2_REQUIRE(amg_kind || !amg_factory, "AMG: expected an AMG solver kind");
     const auto a = view(n, nnz, row_ptr, col, diag, val);
     kb2::Options o;
-    if (options && use_amg_options) {
+    if (amg_factory) {
       o = to_options(options);
     } else if (options) {
       // make_solver: AMG defaults with only nullspace and structure taken over
@@ -170,12 +174,17 @@ int b2_solver_create(int kind, int n, int nnz, const int32_t* row_ptr, const int
       o.device_setup = given.device_setup;
     }
     std::shared_ptr<kb2::Workspace> ws = options && options->workspace ? options->workspace->w : nullptr;
-    if (k == kb2::Kind::AmgPcg || k == kb2::Kind::AmgBicgstab) {
+    if (amg_kind) {
       kb2::check_amg(k, a, o);
     } else {
       kb2::validate_host(a);
       o.m_matrix = false;
     }
+    // The reference's last host checks before device work (krylov_solver,
+    // solver.cpp:396-406): the workspace size, then the Jacobi kinds' diagonal
+    // (Jacobi ctor, solver.cpp:56-60 -> diagonal_values :37-53).
+    KB2_REQUIRE(!ws || ws->rows() == n, "Krylov workspace size mismatch");
+    if (!amg_kind) (void)kb2::diagonal_values(a, false, false);
     auto solver = std::make_unique<kb2::Solver>(k, a, o, ws);
     *out = new b2_solver{std::move(solver)};
   });
