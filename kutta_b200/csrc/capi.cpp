@@ -233,7 +233,9 @@ int b2_csr_spmv(int n, int nnz, const int32_t* d_row_ptr, const int32_t* d_col,
                 const float* d_val, const float* d_x, float* d_y, void* stream) {
   return guarded([&] {
     KB2_REQUIRE(n >= 0 && nnz >= 0, "CSR: invalid array sizes");
-    KB2_REQUIRE(d_x != d_y || n == 0, "CSR: input/output aliasing is unsupported");
+    if (n == 0) return;  // nothing to compute, nothing queued
+    KB2_REQUIRE(d_row_ptr && d_x && d_y && (nnz == 0 || (d_col && d_val)), "CSR: null argument");
+    KB2_REQUIRE(d_x != d_y, "CSR: input/output aliasing is unsupported");
     kb2::launch::spmv(n, d_row_ptr, d_col, d_val, d_x, d_y, nullptr, as_stream(stream));
     kb2::cuda_check(cudaGetLastError(), "csr_spmv");
   });
@@ -244,7 +246,10 @@ int b2_csr_residual(int n, int nnz, const int32_t* d_row_ptr, const int32_t* d_c
                     void* stream) {
   return guarded([&] {
     KB2_REQUIRE(n >= 0 && nnz >= 0, "CSR: invalid array sizes");
-    KB2_REQUIRE((d_x != d_r && d_b != d_r) || n == 0, "CSR: residual RHS size or alias mismatch");
+    if (n == 0) return;
+    KB2_REQUIRE(d_row_ptr && d_x && d_b && d_r && (nnz == 0 || (d_col && d_val)),
+                "CSR: null argument");
+    KB2_REQUIRE(d_x != d_r && d_b != d_r, "CSR: residual RHS size or alias mismatch");
     kb2::launch::residual(n, d_row_ptr, d_col, d_val, d_x, d_b, d_r, nullptr, as_stream(stream));
     kb2::cuda_check(cudaGetLastError(), "csr_residual");
   });
@@ -277,7 +282,13 @@ int b2_amg_smooth(int n, const int32_t* d_row_ptr, const int32_t* d_col, const f
                   int zero_start, void* stream) {
   return guarded([&] {
     KB2_REQUIRE(n >= 0, "CSR: invalid array sizes");
-    KB2_REQUIRE((d_next != d_x && d_next != d_b) || n == 0, "smooth: output aliases an input");
+    if (n == 0) return;
+    // Every row holds its diagonal, so col and val are never empty; a zero
+    // start does not read x.
+    KB2_REQUIRE(d_row_ptr && d_col && d_val && d_b && d_inverse && d_next &&
+                    (zero_start || d_x),
+                "smooth: null argument");
+    KB2_REQUIRE(d_next != d_x && d_next != d_b, "smooth: output aliases an input");
     kb2::launch::smooth(n, d_row_ptr, d_col, d_val, d_x, d_b, d_inverse, d_next, nullptr,
                         zero_start != 0, as_stream(stream));
     kb2::cuda_check(cudaGetLastError(), "amg_smooth");
@@ -326,6 +337,7 @@ int b2_fv_pressure_assemble(int n, const int32_t* offsets, const int32_t* faces,
                            coefficient && flux && values && rhs),
                 "assemble: null argument");
     KB2_REQUIRE(reference >= -1 && reference < n, "assemble: reference cell out of range");
+    if (n == 0) return;
     kb2::launch::fv_pressure_assemble(n, offsets, faces, sign, adjacent, entry, rows, diag,
                                       coefficient, flux, values, rhs, reference,
                                       as_stream(stream));
@@ -342,6 +354,7 @@ int b2_fv_correct_flux(int n_faces, const int32_t* owner, const int32_t* neighbo
     KB2_REQUIRE(n_faces == 0 || (owner && (neighbour || internal == 0) && correction &&
                                  coefficient && flux),
                 "correct_flux: null argument");
+    if (n_faces == 0) return;
     kb2::launch::fv_correct_flux(n_faces, owner, neighbour, correction, coefficient, flux,
                                  internal, as_stream(stream));
     kb2::cuda_check(cudaGetLastError(), "fv_correct_flux");
@@ -357,6 +370,7 @@ int b2_fv_correct_velocity(int n, const float* volume, const float* inverse, con
     KB2_REQUIRE(n == 0 || (volume && inverse && diagonal && gx && gy && gz && correction && u &&
                            v && w && p),
                 "correct_velocity: null argument");
+    if (n == 0) return;
     kb2::launch::fv_correct_velocity(n, volume, inverse, diagonal, gx, gy, gz, correction, u, v, w,
                                      p, alpha, as_stream(stream));
     kb2::cuda_check(cudaGetLastError(), "fv_correct_velocity");

@@ -1,0 +1,104 @@
+"""The C ABI's argument contract, without a GPU: every entry point rejects a
+null handle, a null output or a null array of a non-empty input with
+B2_INVALID_ARGUMENT and a message, treats empty inputs (n = 0) as a no-op,
+and does either before any device work. On this CPU-only machine a device
+call fails with B2_DEVICE_ERROR, so that status showing up means a check
+came too late. The destroy functions accept NULL, as free() does."""
+import ctypes
+
+import pytest
+
+from kutta_b200 import linalg as L
+
+B2_OK, B2_INVALID_ARGUMENT, B2_DEVICE_ERROR = 0, 1, 3
+# The int-returning entry points that return a status (the others return counts).
+COUNTS = {"b2_gnn_parameter_count", "b2_solver_levels", "b2_hierarchy_levels"}
+STATUS_FUNCTIONS = [n for n, (res, _) in L._SIGNATURES.items() if res is ctypes.c_int
+                    and n not in COUNTS]
+# Entry points whose all-zero call is a valid empty operation.
+EMPTY_OK = {"b2_csr_spmv", "b2_csr_residual", "b2_amg_smooth", "b2_fv_correct_flux",
+            "b2_fv_correct_velocity"}
+
+
+def _args(name, size):
+    out = []
+    for a in L._SIGNATURES[name][1]:
+        if a is ctypes.c_float:
+            out.append(0.5)
+        elif a in (ctypes.c_int, ctypes.c_size_t, ctypes.c_uint64):
+            out.append(size)
+        else:
+            out.append(None)
+    return out
+
+
+def _call(name, args):
+    lib = L._load()
+    status = getattr(lib, name)(*args)
+    return status, L.last_error()
+
+
+@pytest.fixture(scope="module", autouse=True)
+def no_device():
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("checks that no device work happens need a machine without a GPU")
+
+
+@pytest.mark.parametrize("name", STATUS_FUNCTIONS)
+def test_zero_arguments_are_rejected_or_empty_before_device_work(name):
+    status, message = _call(name, _args(name, 0))
+    if name in EMPTY_OK:
+        assert status == B2_OK, message
+    else:
+        assert status == B2_INVALID_ARGUMENT, (status, message)
+        assert message
+
+
+@pytest.mark.parametrize("name", STATUS_FUNCTIONS)
+def test_null_arrays_of_non_empty_inputs_are_rejected(name):
+    """Sizes of 4 with every pointer NULL: a handle, an output or an array is
+    missing, whichever the entry point checks first."""
+    status, message = _call(name, _args(name, 4))
+    if name == "b2_workspace_create":  # no pointer inputs besides the output handle
+        assert status == B2_INVALID_ARGUMENT and "invalid arguments" in message
+        return
+    assert status == B2_INVALID_ARGUMENT, (status, message)
+    assert any(w in message for w in ("null", "out of range", "alias", "outside")), message
+
+
+def test_kernel_entry_points_name_the_missing_array():
+    lib = L._load()
+    x, y = ctypes.c_void_p(16), ctypes.c_void_p(32)  # never dereferenced: the checks fail first
+    assert lib.b2_csr_spmv(4, 8, None, None, None, x, y, None) == B2_INVALID_ARGUMENT
+    assert L.last_error() == "CSR: null argument"
+    assert lib.b2_csr_residual(4, 8, None, None, None, x, x, y, None) == B2_INVALID_ARGUMENT
+    assert L.last_error() == "CSR: null argument"
+    assert lib.b2_amg_smooth(4, None, None, None, None, x, x, y, 1, None) == B2_INVALID_ARGUMENT
+    assert L.last_error() == "smooth: null argument"
+
+
+def test_destroy_functions_accept_null():
+    lib = L._load()
+    for name in ("b2_workspace_destroy", "b2_solver_destroy", "b2_hierarchy_free",
+                 "b2_mixed_destroy", "b2_gnn_destroy"):
+        getattr(lib, name)(None)
+
+
+def test_describe_and_level_counts_of_null_handles_are_zero():
+    lib = L._load()
+    buf = ctypes.create_string_buffer(16)
+    assert lib.b2_solver_describe(None, buf, 16) == 0
+    assert lib.b2_mixed_describe(None, buf, 16) == 0
+    assert lib.b2_solver_levels(None) == 0
+    assert lib.b2_hierarchy_levels(None) == 0
+
+
+def test_last_error_reports_its_full_length_and_truncates():
+    lib = L._load()
+    assert lib.b2_solver_refresh(None, None, None) == B2_INVALID_ARGUMENT
+    full = lib.b2_last_error(None, 0)
+    assert full == len("solver: null handle")
+    small = ctypes.create_string_buffer(7)
+    assert lib.b2_last_error(small, 7) == full
+    assert small.value == b"solver"
