@@ -8,7 +8,9 @@ reference bit for bit: iterations, flags, both residuals and x. CPU only.
 - test_solvers.cpp:255-272: a small reference term is kept, not projected
   away (2x2, diagonal 1 + 2^-20; PCG-Jacobi and AMG-PCG);
 - test_solvers.cpp:603-629: BiCGStab freezes on a zero omega and on a zero
-  shadow product, at residual-check intervals 1, 8 and 31."""
+  shadow product, at residual-check intervals 1, 8 and 31;
+- test_solvers.cpp:393-407: an exact one-step exit (2 x = 1);
+- test_solvers.cpp:359-391: the residual-check interval changes no bits."""
 import numpy as np
 import pytest
 
@@ -16,7 +18,6 @@ from kutta_b200 import harness
 from oracle import kutta_oracle as O
 from oracle import ref
 
-needs_ref = pytest.mark.skipif(not ref.available(), reason="oracle/_ref not built")
 PCG_JACOBI, BICGSTAB_JACOBI = 1, 2
 
 
@@ -79,3 +80,30 @@ def test_bicgstab_freezes_on_breakdown(zero_omega, interval):
     assert o.final_residual == o.initial_residual
     assert o.x.tolist() == [0.0, 0.0]
     _same(o, r)
+
+
+@pytest.mark.parametrize("kind", [PCG_JACOBI, BICGSTAB_JACOBI], ids=["pcg_jacobi", "bicgstab"])
+def test_exact_one_step_exit(kind):
+    """test_solvers.cpp:393-407: 2 x = 1 converges in one step with a zero
+    final residual and x = 0.5."""
+    s = _system([0, 1], [0], [0], [2.0], [1.0])
+    o, r = _both(s, kind, 1e-6, 1e-12, 20)
+    assert o.converged and o.iterations == 1
+    assert o.final_residual == 0 and o.x.tolist() == [0.5]
+    _same(o, r)
+
+
+def test_residual_check_interval_changes_no_bits():
+    """test_solvers.cpp:359-391: a diagonally boosted upwind BiCGStab-Jacobi
+    solve gives the same iterations, final residual and x at residual-check
+    intervals 8 and 1 (the interval only batches host polls)."""
+    s = harness.poisson(8, 6, 4, 1, False, False, 5)
+    s.val[s.diag] += 100
+    s.b = harness.random_solution(s.n)
+    o8, r8 = _both(s, BICGSTAB_JACOBI, 1e-4, 1e-12, 100, 8)
+    o1, r1 = _both(s, BICGSTAB_JACOBI, 1e-4, 1e-12, 100, 1)
+    assert o8.converged
+    assert (o8.iterations, o8.final_residual) == (o1.iterations, o1.final_residual)
+    assert np.array_equal(o8.x.view(np.uint32), o1.x.view(np.uint32))
+    _same(o8, r8)
+    _same(o1, r1)
