@@ -219,6 +219,13 @@ int b2_mixed_refresh(b2_mixed* solver, const float* d_val, void* stream);
 /* d_x: n doubles, initial guess in, FP64 solution out. d_b: n floats. */
 int b2_mixed_solve(b2_mixed* solver, const float* d_val, double* d_x, const float* d_b,
                    const b2_control* control, b2_mixed_stats* stats, void* stream);
+/* The same solve with d_x as n floats, the form of LinearSolver::solve
+ * (solver.hpp:78-79): d_x is widened into an FP64 copy the solver keeps,
+ * solved, and rounded to nearest on return; final_residual is that of the
+ * FP64 solution. A rounded x is back at the FP32 floor (about 1e-7 relative
+ * on the pressure matrices here), so tighter targets need b2_mixed_solve. */
+int b2_mixed_solve_f32(b2_mixed* solver, const float* d_val, float* d_x, const float* d_b,
+                       const b2_control* control, b2_mixed_stats* stats, void* stream);
 size_t b2_mixed_describe(const b2_mixed* solver, char* buffer, size_t length);
 void b2_mixed_destroy(b2_mixed* solver);
 /* The mixed solve's coarsest-level step on its own: the dense FP64 Cholesky

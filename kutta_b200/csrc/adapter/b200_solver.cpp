@@ -19,6 +19,9 @@
 //   make_solver(kind, dev, a, options)        solver.cpp  -> make_b200_solver
 //   make_amg_solver(kind, dev, a, options)    amg.cpp:345 -> make_b200_amg_solver
 //
+// and a steady solver that opts into the mixed-precision pressure solve builds
+// it with make_b200_mixed_solver(a, options) in place of make_solver(AmgPcg, ...).
+//
 // The option checks (kinds, sweeps, M-matrix structure) run inside
 // b2_solver_create with the reference's messages; its status codes map back to
 // kutta::Error and kutta::NonfiniteError (core/types.hpp:24-33).
@@ -134,7 +137,59 @@ class B200Solver final : public LinearSolver {
   b2_solver* s_ = nullptr;
 };
 
+// The mixed-precision pressure solve (no reference counterpart) behind the
+// same interface. x stays FP32 as LinearSolver::solve has it: the library
+// widens it into an FP64 copy, refines, and rounds the solution back. The
+// reported final residual is the FP64 solution's; targets below the FP32
+// floor (about 1e-7 relative) need b2_mixed_solve and an FP64 x instead.
+class B200MixedSolver final : public LinearSolver {
+ public:
+  B200MixedSolver(const CsrMatrixHost& a, const b2_mixed_options& options) {
+    check_sizes(a);
+    check(b2_mixed_create(a.pattern.n_rows, a.pattern.nnz(), a.pattern.row_ptr.data(),
+                          a.pattern.col.data(), a.pattern.diag.data(), a.val.data(), &options,
+                          &s_));
+  }
+  ~B200MixedSolver() override { b2_mixed_destroy(s_); }
+  B200MixedSolver(const B200MixedSolver&) = delete;
+  B200MixedSolver& operator=(const B200MixedSolver&) = delete;
+
+  void refresh(Device& dev, const CsrMatrix& a) override {
+    check(b2_mixed_refresh(s_, ptr(a.val), cuda_stream(dev)));
+  }
+
+  SolveStats solve(Device& dev, const CsrMatrix& a, Buffer<float>& x, const Buffer<float>& b,
+                   const SolveControl& c) override {
+    const b2_control control{c.rel_tol, c.abs_tol, c.max_iter, c.residual_check_interval};
+    b2_mixed_stats st{};
+    check(b2_mixed_solve_f32(s_, ptr(a.val), ptr(x), ptr(b), &control, &st, cuda_stream(dev)));
+    return {st.iterations, st.initial_residual, st.final_residual, st.converged != 0};
+  }
+
+  std::string describe() const override {
+    char text[512];
+    b2_mixed_describe(s_, text, sizeof text);
+    return text;
+  }
+
+ private:
+  b2_mixed* s_ = nullptr;
+};
+
 }  // namespace
+
+// The pressure solver of steady_solver.cpp:578-580 in its mixed-precision
+// form: the library's tuned defaults, with the caller's structure and null
+// space. Only the SPD pressure equation takes it (flexible CG inside). It
+// keeps its own Krylov vectors, so a shared KrylovWorkspace is not used.
+std::unique_ptr<LinearSolver> make_b200_mixed_solver(const CsrMatrixHost& a,
+                                                     const SolverOptions& o) {
+  b2_mixed_options options;
+  b2_mixed_options_default(&options);
+  options.amg.nullspace = static_cast<int>(o.nullspace);
+  options.amg.structure = static_cast<int>(o.structure);
+  return std::make_unique<B200MixedSolver>(a, options);
+}
 
 std::unique_ptr<LinearSolver> make_b200_solver(SolverKind kind, const CsrMatrixHost& a,
                                                const SolverOptions& o) {

@@ -550,26 +550,42 @@ int b2_mixed_refresh(b2_mixed* s, const float* d_val, void* stream) {
   });
 }
 
+namespace {
+kb2::Control control_of(const b2_control* control) {
+  kb2::Control c;
+  if (control) {
+    c.rel_tol = control->rel_tol;
+    c.abs_tol = control->abs_tol;
+    c.max_iter = control->max_iter;
+    c.residual_check_interval = control->residual_check_interval;
+  }
+  return c;
+}
+
+void put_stats(const kb2::MixedStats& r, b2_mixed_stats* stats) {
+  if (!stats) return;
+  stats->refinements = r.refinements;
+  stats->learned_fallback = r.learned_fallback ? 1 : 0;
+  stats->iterations = r.iterations;
+  stats->converged = r.converged ? 1 : 0;
+  stats->initial_residual = r.initial_residual;
+  stats->final_residual = r.final_residual;
+}
+}  // namespace
+
 int b2_mixed_solve(b2_mixed* s, const float* d_val, double* d_x, const float* d_b,
                    const b2_control* control, b2_mixed_stats* stats, void* stream) {
   return guarded([&] {
     KB2_REQUIRE(s && s->s, "solver: null handle");
-    kb2::Control c;
-    if (control) {
-      c.rel_tol = control->rel_tol;
-      c.abs_tol = control->abs_tol;
-      c.max_iter = control->max_iter;
-      c.residual_check_interval = control->residual_check_interval;
-    }
-    const auto r = s->s->solve(d_val, d_x, d_b, c, as_stream(stream));
-    if (stats) {
-      stats->refinements = r.refinements;
-      stats->learned_fallback = r.learned_fallback ? 1 : 0;
-      stats->iterations = r.iterations;
-      stats->converged = r.converged ? 1 : 0;
-      stats->initial_residual = r.initial_residual;
-      stats->final_residual = r.final_residual;
-    }
+    put_stats(s->s->solve(d_val, d_x, d_b, control_of(control), as_stream(stream)), stats);
+  });
+}
+
+int b2_mixed_solve_f32(b2_mixed* s, const float* d_val, float* d_x, const float* d_b,
+                       const b2_control* control, b2_mixed_stats* stats, void* stream) {
+  return guarded([&] {
+    KB2_REQUIRE(s && s->s, "solver: null handle");
+    put_stats(s->s->solve32(d_val, d_x, d_b, control_of(control), as_stream(stream)), stats);
   });
 }
 

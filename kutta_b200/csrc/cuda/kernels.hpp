@@ -147,6 +147,10 @@ void residual64(int n, const int* rows, const int* cols, const float* vals, cons
                 cudaStream_t s);
 // x += e.
 void update64(int n, double* x, const float* e, cudaStream_t s);
+// y = double(x), and x = float(y) rounded to nearest: the FP32 form of the
+// mixed solve's x.
+void widen(int n, const float* x, double* y, cudaStream_t s);
+void narrow(int n, const double* y, float* x, cudaStream_t s);
 
 // ---- mixed V-cycle tail: the small coarse levels in one cluster launch ------
 // Rows of a tail level are split in power-of-two chunks of (1 << shift) rows,

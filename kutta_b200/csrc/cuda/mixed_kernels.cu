@@ -517,6 +517,14 @@ __global__ void k_update64(int n, double* __restrict__ x, const float* __restric
   ROWS(i, n) x[i] += static_cast<double>(e[i]);
 }
 
+__global__ void k_widen(int n, const float* __restrict__ x, double* __restrict__ y) {
+  ROWS(i, n) y[i] = static_cast<double>(x[i]);
+}
+
+__global__ void k_narrow(int n, const double* __restrict__ y, float* __restrict__ x) {
+  ROWS(i, n) x[i] = static_cast<float>(y[i]);
+}
+
 }  // namespace
 
 namespace launch {
@@ -615,6 +623,16 @@ void update64(int n, double* x, const float* e, cudaStream_t s) {
   if (n <= 0) return;
   ++counter;
   k_update64<<<rows_grid(n), kBlock, 0, s>>>(n, x, e);
+}
+void widen(int n, const float* x, double* y, cudaStream_t s) {
+  if (n <= 0) return;
+  ++counter;
+  k_widen<<<rows_grid(n), kBlock, 0, s>>>(n, x, y);
+}
+void narrow(int n, const double* y, float* x, cudaStream_t s) {
+  if (n <= 0) return;
+  ++counter;
+  k_narrow<<<rows_grid(n), kBlock, 0, s>>>(n, y, x);
 }
 
 }  // namespace launch

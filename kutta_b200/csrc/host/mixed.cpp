@@ -32,6 +32,17 @@ double MixedSolver::residual(const float* val, const double* x, const float* b, 
   return std::sqrt(host_[0]);
 }
 
+MixedStats MixedSolver::solve32(const float* val, float* x, const float* b, const Control& c,
+                                cudaStream_t s) {
+  KB2_REQUIRE(n_ == 0 || (x != nullptr && b != nullptr && x != b),
+              "solve: vector size or alias mismatch");
+  if (n_ > 0 && !x64_.allocated()) x64_.reset(static_cast<std::size_t>(n_));
+  launch::widen(n_, x, x64_.get(), s);
+  const MixedStats st = solve(val, x64_.get(), b, c, s);
+  launch::narrow(n_, x64_.get(), x, s);
+  return st;
+}
+
 MixedStats MixedSolver::solve(const float* val, double* x, const float* b, const Control& c,
                               cudaStream_t s) {
   KB2_REQUIRE(n_ == 0 || (x != nullptr && b != nullptr), "solve: vector size or alias mismatch");

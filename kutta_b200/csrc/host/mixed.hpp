@@ -33,6 +33,12 @@ class MixedSolver {
   }
   // x: FP64 solution (initial guess in); b: FP32 right-hand side.
   MixedStats solve(const float* val, double* x, const float* b, const Control& c, cudaStream_t s);
+  // The same solve for a caller that holds x in FP32 (the reference's
+  // LinearSolver::solve): x is widened into an FP64 copy the solver keeps,
+  // solved, and rounded back to nearest. A rounded x carries the FP32 floor
+  // again, so targets below it need the FP64 form.
+  MixedStats solve32(const float* val, float* x, const float* b, const Control& c,
+                     cudaStream_t s);
   std::string describe() const;
   Solver& inner() { return inner_; }
 
@@ -43,7 +49,7 @@ class MixedSolver {
   Solver inner_;
   int n_;
   DArray<float> rf_, e_;
-  DArray<double> partials_, norm_;
+  DArray<double> partials_, norm_, x64_;
   DArray<unsigned> ticket_;
   Pinned<double> host_{2};
 };

@@ -189,6 +189,7 @@ _SIGNATURES = {
     "b2_mixed_create": (_I, [_I, _I, _P, _P, _P, _P, _P, _P]),
     "b2_mixed_refresh": (_I, [_P, _P, _P]),
     "b2_mixed_solve": (_I, [_P, _P, _P, _P, _P, _P, _P]),
+    "b2_mixed_solve_f32": (_I, [_P, _P, _P, _P, _P, _P, _P]),
     "b2_mixed_describe": (ctypes.c_size_t, [_P, ctypes.c_char_p, ctypes.c_size_t]),
     "b2_mixed_destroy": (None, [_P]),
     "b2_mixed_hierarchy_build": (_I, [_I, _I, _P, _P, _P, _P, _P, _P]),
@@ -558,17 +559,21 @@ class MixedSolver:
         _check(_load().b2_mixed_assemble_refresh(self._handle, *fv.pointers(), _tptr(a.val),
                                                  _tptr(rhs), fv.reference, _stream()))
 
-    def solve(self, a: CsrMatrix, x64, b, control: SolveControl | None = None) -> MixedStats:
-        """x64: float64 CUDA tensor (initial guess in, solution out); b: float32."""
+    def solve(self, a: CsrMatrix, x, b, control: SolveControl | None = None) -> MixedStats:
+        """x: float64 CUDA tensor (initial guess in, FP64 solution out), or
+        float32 (b2_mixed_solve_f32: the solution rounded to FP32, as
+        LinearSolver.solve returns it); b: float32."""
         import torch
-        if x64.dtype != torch.float64 or x64.numel() != self.n_rows or b.numel() != self.n_rows:
+        if x.dtype not in (torch.float64, torch.float32) or x.numel() != self.n_rows \
+                or b.numel() != self.n_rows:
             raise KuttaError("solve: vector size or alias mismatch")
         control = control or SolveControl()
         c = _Control(control.rel_tol, control.abs_tol, control.max_iter,
                      control.residual_check_interval)
         st = _MixedStats()
-        _check(_load().b2_mixed_solve(self._handle, _tptr(a.val), _tptr(x64), _tptr(b),
-                                      ctypes.byref(c), ctypes.byref(st), _stream()))
+        entry = _load().b2_mixed_solve if x.dtype == torch.float64 else _load().b2_mixed_solve_f32
+        _check(entry(self._handle, _tptr(a.val), _tptr(x), _tptr(b), ctypes.byref(c),
+                     ctypes.byref(st), _stream()))
         return MixedStats(st.refinements, st.iterations, bool(st.converged), st.initial_residual,
                           st.final_residual, bool(st.learned_fallback))
 

@@ -24,6 +24,8 @@ std::unique_ptr<LinearSolver> make_b200_solver(SolverKind kind, const CsrMatrixH
                                                const SolverOptions& o);
 std::unique_ptr<LinearSolver> make_b200_amg_solver(SolverKind kind, const CsrMatrixHost& a,
                                                    const AmgOptions& o);
+std::unique_ptr<LinearSolver> make_b200_mixed_solver(const CsrMatrixHost& a,
+                                                     const SolverOptions& o);
 // The CUDA backend's accessors the adapter calls; no case reaches them.
 void* cuda_ptr(BufferHandle*) { return nullptr; }
 struct CUstream_st;
@@ -87,15 +89,20 @@ std::string flat(std::string s) {
   return s;
 }
 
+// With `mixed`, the adapter side is the mixed-precision factory and the
+// reference side the pressure solver it stands in for, make_solver(AmgPcg).
 void run(const char* name, const CsrMatrixHost& a, SolverKind kind, const AmgOptions* amg,
-         const SolverOptions* plain) {
+         const SolverOptions* plain, bool mixed = false) {
   auto dev = Device::create(Backend::Cpu);
   std::string rm, bm;
   const std::string rt = kind_of(
       [&] { (void)(amg ? make_amg_solver(kind, *dev, a, *amg) : make_solver(kind, *dev, a, *plain)); },
       rm);
   const std::string bt = kind_of(
-      [&] { (void)(amg ? make_b200_amg_solver(kind, a, *amg) : make_b200_solver(kind, a, *plain)); },
+      [&] {
+        (void)(mixed ? make_b200_mixed_solver(a, *plain)
+                     : amg ? make_b200_amg_solver(kind, a, *amg) : make_b200_solver(kind, a, *plain));
+      },
       bm);
   std::printf("%s|%s|%s|%s|%s\n", name, rt.c_str(), flat(rm).c_str(), bt.c_str(),
               flat(bm).c_str());
@@ -108,6 +115,10 @@ void amg_case(const char* name, const CsrMatrixHost& a, SolverKind kind, const A
 void plain_case(const char* name, const CsrMatrixHost& a, SolverKind kind,
                 const SolverOptions& o) {
   run(name, a, kind, nullptr, &o);
+}
+
+void mixed_case(const char* name, const CsrMatrixHost& a, const SolverOptions& o) {
+  run(name, a, SolverKind::AmgPcg, nullptr, &o, true);
 }
 
 }  // namespace
@@ -254,6 +265,28 @@ int main() {
     auto a = good;
     a.val[a.pattern.diag[60]] = 0.0;
     plain_case("zero_diagonal_jacobi", a, SolverKind::PcgJacobi, SolverOptions{});
+  }
+
+  // The mixed-precision factory against the pressure solver it replaces.
+  {
+    SolverOptions pressure;
+    pressure.structure = OperatorStructure::SymmetricMMatrix;
+    mixed_case("mixed_valid", good, pressure);
+    auto a = good;
+    a.val[a.pattern.diag[10]] *= 0.5;
+    mixed_case("mixed_m_not_dominant", a, pressure);
+    a = good;
+    a.val[3] = std::numeric_limits<double>::infinity();
+    mixed_case("mixed_infinite_value", a, pressure);
+    a = good;
+    a.pattern.col[a.pattern.row_ptr[n - 1]] = n;
+    mixed_case("mixed_column_out_of_range", a, pressure);
+    a = good;
+    a.val.pop_back();
+    mixed_case("mixed_value_count", a, pressure);
+    SolverOptions bad = pressure;
+    bad.nullspace = static_cast<NullSpace>(4);
+    mixed_case("mixed_nullspace_value", good, bad);
   }
   return 0;
 }

@@ -4,7 +4,8 @@ ABI. Compiled here against the reference's own headers, with warnings as
 errors, and linked with the reference's CPU library and libkutta_b200.so.
 tests/adapter_check.cpp then runs the reference's factories
 (make_amg_solver, make_solver on the CPU Device) and the adapter's on the same
-inputs. Every input the reference rejects before device work is rejected by
+inputs; the adapter's mixed-precision factory is compared with the pressure
+solver it stands in for, make_solver(AmgPcg). Every input the reference rejects before device work is rejected by
 the adapter with the same exception type and message, and the inputs it
 accepts pass every host check of the adapter (whose solver then needs a
 GPU). The AMG diagonal checks (solver.cpp:37-53) run on the device during
@@ -83,11 +84,12 @@ def test_adapter_rejects_what_the_reference_rejects(adapter_check):
     r = subprocess.run([str(adapter_check)], capture_output=True, text=True, timeout=120)
     assert r.returncode == 0, r.stdout + r.stderr
     rows = [line.split("|") for line in r.stdout.splitlines()]
-    assert len(rows) >= 25
+    assert len(rows) >= 32
     for name, ref_type, ref_message, b2_type, b2_message in rows:
         if ref_type == "none" or name in DEVICE_CHECKED:
             # Every host check passed; the adapter then stops at the missing GPU.
             assert b2_type == "Error" and b2_message.startswith("CUDA error"), (name, b2_message)
-            assert (ref_type == "none") == name.startswith(("valid", "nullspace_row")), name
+            assert (ref_type == "none") == name.startswith(("valid", "mixed_valid",
+                                                             "nullspace_row")), name
         else:
             assert (b2_type, b2_message) == (ref_type, _strip_location(ref_message)), name

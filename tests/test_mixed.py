@@ -277,3 +277,30 @@ def test_fused_post_sweep_reductions_are_exact(cuda):
             solver.set_learned(None)
     assert out[0][0] == out[1][0] and out[0][1] == out[1][1]
     assert np.array_equal(out[0][2].view(np.uint64), out[1][2].view(np.uint64))
+
+
+@pytest.mark.gpu
+def test_fp32_solution_is_the_rounded_fp64_solution(cuda):
+    """b2_mixed_solve_f32, the form LinearSolver.solve has (x in FP32): the same
+    solve as b2_mixed_solve from the widened guess, with the FP64 solution
+    rounded to nearest on return."""
+    import torch
+    s = harness.box_system(16, 16, 16, tet=True, seed=6)
+    solver = L.make_mixed_solver(s)
+    a = L.upload(s)
+    solver.refresh(a)
+    b = torch.from_numpy(s.b).cuda()
+    rng = np.random.default_rng(3)
+    for guess in (np.zeros(s.n, np.float32), rng.normal(size=s.n).astype(np.float32)):
+        x64 = torch.from_numpy(guess.astype(np.float64)).cuda()
+        st64 = solver.solve(a, x64, b, L.SolveControl(1e-6, 1e-30, 2000))
+        x32 = torch.from_numpy(guess.copy()).cuda()
+        st32 = solver.solve(a, x32, b, L.SolveControl(1e-6, 1e-30, 2000))
+        torch.cuda.synchronize()
+        assert st64.converged
+        assert (st32.refinements, st32.iterations, st32.converged) == \
+            (st64.refinements, st64.iterations, st64.converged)
+        assert (st32.initial_residual, st32.final_residual) == \
+            (st64.initial_residual, st64.final_residual)
+        rounded = x64.cpu().numpy().astype(np.float32)
+        assert np.array_equal(x32.cpu().numpy().view(np.uint32), rounded.view(np.uint32))
