@@ -130,6 +130,7 @@ int b2_solver_solve(b2_solver* solver, const float* d_val, float* d_x, const flo
 /* LinearSolver::describe(), solver.hpp:80. Returns the full length. */
 size_t b2_solver_describe(const b2_solver* solver, char* buffer, size_t length);
 
+/* ~LinearSolver(), solver.hpp:76. NULL is accepted. */
 void b2_solver_destroy(b2_solver* solver);
 
 /* spmv(dev, a, x, y) and residual(dev, a, x, b, r), csr.hpp:40-48 (kernels
@@ -154,6 +155,9 @@ typedef struct {
   double algorithmic_bytes;  /* all kernels of the profiled solves */
   long long solves;
 } b2_profile;
+/* Profiling (no reference counterpart): with enable = 1 the solver times its
+ * fine-level sweeps with CUDA events and counts its launches and algorithmic
+ * bytes until profiling is disabled; b2_solver_profile_read returns the totals. */
 int b2_solver_profile(b2_solver* solver, int enable);
 int b2_solver_profile_read(b2_solver* solver, b2_profile* out);
 /* Process-wide count of kernels launched by this library. */
@@ -211,6 +215,7 @@ typedef struct {
 
 typedef struct b2_mixed b2_mixed;
 
+/* The defaults listed beside each field above. */
 void b2_mixed_options_default(b2_mixed_options* options);
 int b2_mixed_create(int n, int nnz, const int32_t* row_ptr, const int32_t* col,
                     const int32_t* diag, const double* val, const b2_mixed_options* options,
@@ -270,6 +275,8 @@ int b2_mixed_hierarchy_build(int n, int nnz, const int32_t* row_ptr, const int32
  * energy loss 1 - (c.t)^2 / ((c.Ac)(t.e)) for c = G(t): the fraction of the
  * error's A-energy left after the best step along c. */
 typedef struct b2_gnn b2_gnn;
+/* A stage with weights drawn from `seed`; b2_gnn_set_weights loads trained
+ * ones (b2_gnn_parameter_count floats). */
 int b2_gnn_create(uint64_t seed, b2_gnn** out);
 void b2_gnn_destroy(b2_gnn* g);
 int b2_gnn_parameter_count(void);
