@@ -452,19 +452,14 @@ int b2_hierarchy_build(int n, int nnz, const int32_t* row_ptr, const int32_t* co
     const auto a = view(n, nnz, row_ptr, col, diag, val);
     const auto o = to_options(options);
     kb2::check_amg(spd ? kb2::Kind::AmgPcg : kb2::Kind::AmgBicgstab, a, o);
-    auto* h = new b2_hierarchy;
-    try {
-      h->h = kb2::build_hierarchy(a, o);
-    } catch (...) {
-      delete h;
-      throw;
-    }
+    auto h = std::make_unique<b2_hierarchy>();
+    h->h = kb2::build_hierarchy(a, o);
     h->fine.n = n;
     h->fine.row_ptr.assign(row_ptr, row_ptr + n + 1);
     h->fine.col.assign(col, col + nnz);
     h->fine.diag.assign(diag, diag + n);
     h->fine.val.assign(val, val + nnz);
-    *out = h;
+    *out = h.release();
   });
 }
 
@@ -716,19 +711,14 @@ int b2_mixed_hierarchy_build(int n, int nnz, const int32_t* row_ptr, const int32
     const auto a = view(n, nnz, row_ptr, col, diag, val);
     auto o = mixed_options(*options);
     kb2::check_amg(kb2::Kind::AmgPcg, a, o);
-    auto* h = new b2_hierarchy;
-    try {
-      h->h = kb2::build_hierarchy(a, o);
-    } catch (...) {
-      delete h;
-      throw;
-    }
+    auto h = std::make_unique<b2_hierarchy>();
+    h->h = kb2::build_hierarchy(a, o);
     h->fine.n = n;
     h->fine.row_ptr.assign(row_ptr, row_ptr + n + 1);
     h->fine.col.assign(col, col + nnz);
     h->fine.diag.assign(diag, diag + n);
     h->fine.val.assign(val, val + nnz);
-    *out = h;
+    *out = h.release();
   });
 }
 
