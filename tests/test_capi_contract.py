@@ -102,3 +102,23 @@ def test_last_error_reports_its_full_length_and_truncates():
     small = ctypes.create_string_buffer(7)
     assert lib.b2_last_error(small, 7) == full
     assert small.value == b"solver"
+
+
+def test_header_is_c99_and_a_c_caller_links_and_runs():
+    """tests/c_abi_check.c: the header compiles as C99 with -pedantic, a C
+    program links against the library, and its calls that fail before device
+    work return the declared statuses and the reference's messages."""
+    import pathlib
+    import subprocess
+    root = pathlib.Path(__file__).resolve().parent.parent
+    lib_dir = L.library_path().parent
+    out = lib_dir / "checks"
+    out.mkdir(exist_ok=True)
+    exe = out / "c_abi_check"
+    cmd = ["gcc", "-std=c99", "-Wall", "-Wextra", "-Werror", "-pedantic",
+           f"-I{root / 'include'}", str(root / "tests" / "c_abi_check.c"), "-o", str(exe),
+           f"-L{lib_dir}", "-lkutta_b200", f"-Wl,-rpath,{lib_dir}", "-Wl,--allow-shlib-undefined"]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    assert r.returncode == 0, r.stdout + r.stderr
+    r = subprocess.run([str(exe)], capture_output=True, text=True, timeout=60)
+    assert r.returncode == 0 and r.stdout.strip() == "ok", r.stdout + r.stderr
