@@ -196,3 +196,20 @@ def test_fp64_oracle_solves_to_tolerance():
     A = sp.csr_matrix((s.val, s.col, s.row_ptr), shape=(s.n, s.n))
     assert np.linalg.norm(s.b.astype(np.float64) - A @ x) <= 1e-11 * np.linalg.norm(s.b)
     assert A_res < 1e-4 * np.linalg.norm(s.b)
+
+
+@pytest.mark.skipif(not ref.available(), reason="oracle/_ref not built on this machine")
+@pytest.mark.parametrize("sweeps", [1, 2, 3])
+def test_oracle_equals_reference_library_at_other_sweep_counts(sweeps):
+    """V(s,s) pressure solves; the steady solver runs V(2,2) with the SST model
+    (steady_solver.cpp:578-580)."""
+    s = harness.box_system(10, 10, 10, tet=True, seed=3)
+    r = ref.solve(s, opts=ref.options(3, structure=1, pre_sweeps=sweeps, post_sweeps=sweeps),
+                  rel_tol=1e-6, abs_tol=1e-12, max_iter=500)
+    o = O.solve(s, opts=O.options(O.AMG_PCG, m_matrix=True, pre_sweeps=sweeps,
+                                  post_sweeps=sweeps),
+                rel_tol=1e-6, abs_tol=1e-12, max_iter=500)
+    assert (o.iterations, o.converged) == (r.iterations, r.converged)
+    assert (o.initial_residual, o.final_residual) == (r.initial_residual, r.final_residual)
+    assert np.array_equal(o.x.view(np.uint32), r.x.view(np.uint32))
+    assert o.describe == r.describe
