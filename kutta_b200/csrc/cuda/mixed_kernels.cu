@@ -525,6 +525,19 @@ __global__ void k_narrow(int n, const double* __restrict__ y, float* __restrict_
   ROWS(i, n) x[i] = static_cast<float>(y[i]);
 }
 
+// A kernel's dynamic shared-memory ceiling is an attribute of the function in
+// one device's context, so it is raised once per device this process uses
+// (bit d of `done` for device d < 64; higher devices raise it on every call).
+void raise_shared_limit(const void* kernel, int bytes, std::atomic<unsigned long long>& done) {
+  int device = 0;
+  if (cudaGetDevice(&device) != cudaSuccess) return;
+  const unsigned long long bit = device < 64 ? 1ull << device : 0;
+  if (bit && (done.load(std::memory_order_acquire) & bit)) return;
+  if (cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes) ==
+      cudaSuccess)
+    done.fetch_or(bit, std::memory_order_release);
+}
+
 }  // namespace
 
 namespace launch {
@@ -580,25 +593,20 @@ void dense_inverse(int n, const int* rows, const int* cols, const float* vals, d
   ++counter;
   if (n <= kSharedDense) {
     const int bytes = 2 * n * n * static_cast<int>(sizeof(double));
-    static bool raised = false;
-    if (!raised) {
-      cudaFuncSetAttribute(k_dense_inverse_shared, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                           2 * kSharedDense * kSharedDense * static_cast<int>(sizeof(double)));
-      raised = true;
-    }
+    static std::atomic<unsigned long long> raised{0};
+    raise_shared_limit(reinterpret_cast<const void*>(k_dense_inverse_shared),
+                       2 * kSharedDense * kSharedDense * static_cast<int>(sizeof(double)), raised);
     k_dense_inverse_shared<<<1, kDenseThreads, bytes, s>>>(n, rows, cols, vals, inverse, error,
                                                             ratio);
     return;
   }
   if (n <= kPackedDense) {
     const int bytes = (n * (n + 1) / 2 + 2 * n) * static_cast<int>(sizeof(double));
-    static bool raised_packed = false;
-    if (!raised_packed) {
-      cudaFuncSetAttribute(
-          k_dense_inverse_packed, cudaFuncAttributeMaxDynamicSharedMemorySize,
-          (kPackedDense * (kPackedDense + 1) / 2 + 2 * kPackedDense) * static_cast<int>(sizeof(double)));
-      raised_packed = true;
-    }
+    static std::atomic<unsigned long long> raised_packed{0};
+    raise_shared_limit(
+        reinterpret_cast<const void*>(k_dense_inverse_packed),
+        (kPackedDense * (kPackedDense + 1) / 2 + 2 * kPackedDense) * static_cast<int>(sizeof(double)),
+        raised_packed);
     k_dense_inverse_packed<<<1, kPackedThreads, bytes, s>>>(n, rows, cols, vals, inverse, error,
                                                             ratio);
     return;
