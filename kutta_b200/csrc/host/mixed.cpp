@@ -34,6 +34,7 @@ double MixedSolver::residual(const float* val, const double* x, const float* b, 
 
 MixedStats MixedSolver::solve32(const float* val, float* x, const float* b, const Control& c,
                                 cudaStream_t s) {
+  inner_.check_device();
   KB2_REQUIRE(n_ == 0 || (x != nullptr && b != nullptr && x != b),
               "solve: vector size or alias mismatch");
   if (n_ > 0 && !x64_.allocated()) x64_.reset(static_cast<std::size_t>(n_));
@@ -45,6 +46,7 @@ MixedStats MixedSolver::solve32(const float* val, float* x, const float* b, cons
 
 MixedStats MixedSolver::solve(const float* val, double* x, const float* b, const Control& c,
                               cudaStream_t s) {
+  inner_.check_device();
   KB2_REQUIRE(n_ == 0 || (x != nullptr && b != nullptr), "solve: vector size or alias mismatch");
   KB2_REQUIRE(c.max_iter >= 0 && std::isfinite(c.rel_tol) && c.rel_tol >= 0 &&
                   std::isfinite(c.abs_tol) && c.abs_tol >= 0 && c.residual_check_interval > 0,

@@ -275,6 +275,12 @@ Solver::~Solver() {
   if (capture_) cudaStreamDestroy(capture_);
 }
 
+void Solver::check_device() const {
+  int device = 0;
+  cuda_check(cudaGetDevice(&device), "cudaGetDevice");
+  KB2_REQUIRE(device == device_, "solver: device or matrix mismatch");
+}
+
 void Solver::set_profile(bool on) {
   profiling_ = on;
   prof_ = Profile{};
@@ -574,6 +580,7 @@ void Solver::learned_warm_start(const float* val, const float* r, double* x, cud
 
 void Solver::precondition_into(const float* val, const float* r, float* z, cudaStream_t s) {
   KB2_REQUIRE(amg(), "precondition: needs an AMG solver");
+  check_device();
   KB2_REQUIRE(n_ == 0 || (r != nullptr && z != nullptr && r != z),
               "precondition: null or aliased vector");
   if (n_ == 0) return;
@@ -676,6 +683,7 @@ void Solver::graphed(const void* k1, const void* k2, int k3, float* const& track
 // Krylov::refresh (solver.cpp:92-95) + Aggregation::refresh (amg.cpp:228-256) or
 // Jacobi::refresh (solver.cpp:61-64). One host wait for all validity checks.
 void Solver::refresh(const float* val, cudaStream_t s) {
+  check_device();
   stream_ = s;
   val_ = val;
   if (!amg()) {
@@ -698,6 +706,7 @@ void Solver::refresh(const float* val, cudaStream_t s) {
 // diagonal and its validity flag; the coarse levels follow as in refresh().
 void Solver::assemble_refresh(const FvPressure& fv, float* values, float* rhs, cudaStream_t s) {
   KB2_REQUIRE(amg(), "assemble: needs an AMG solver");
+  check_device();
   KB2_REQUIRE(fv.offsets && fv.faces && fv.sign && fv.adjacent && fv.entry && fv.coefficient &&
                   fv.flux && values && rhs,
               "assemble: null argument");
@@ -915,6 +924,7 @@ void Solver::bicgstab(float* x, const float* b, const Control& c, double target,
 
 // Krylov::solve, solver.cpp:97-176.
 Stats Solver::solve(const float* val, float* x, const float* b, const Control& c, cudaStream_t s) {
+  check_device();
   stream_ = s;
   val_ = val;
   KB2_REQUIRE((n_ == 0 || (x != nullptr && b != nullptr)) && (x != b || n_ == 0),

@@ -115,6 +115,9 @@ class Solver {
   const DevLevel& level(int i) const { return levels_[static_cast<std::size_t>(i)]; }
   int rows() const { return n_; }
   int entries() const { return nnz_; }
+  // Throws unless the current device is the one the solver was built on: its
+  // arrays live there (the reference's Device check, solver.cpp:194-195).
+  void check_device() const;
   const float* current_values() const { return val_; }
 
  private:
