@@ -44,6 +44,7 @@ Gnn::Slices Gnn::slices(float* base) const {
 // Uniform Glorot-style initialisation (fan-in 2 Cin for the two halves of a
 // layer), zero biases, small output weights.
 Gnn::Gnn(std::uint64_t seed) {
+  cuda_check(cudaGetDevice(&device_), "cudaGetDevice");
   const int count = parameter_count();
   std::vector<float> w(static_cast<std::size_t>(count), 0.0f);
   std::uint64_t state = seed * 0x2545F4914F6CDD1DULL + 1;
@@ -71,9 +72,16 @@ Gnn::Gnn(std::uint64_t seed) {
   cuda_check(cudaMemset(fault_.get(), 0, sizeof(int)), "memset");
 }
 
+void Gnn::check_device() const {
+  int device = 0;
+  cuda_check(cudaGetDevice(&device), "cudaGetDevice");
+  KB2_REQUIRE(device == device_, "learned stage: called on another device than its own");
+}
+
 void Gnn::bind(int n, const int* rows, const int* cols, const int* diag, const float* vals,
                cudaStream_t s) {
   KB2_REQUIRE(n > 0 && rows && cols && diag && vals, "learned stage: invalid matrix");
+  check_device();
   if (n != n_) {
     const auto rows_n = static_cast<std::size_t>(n);
     const auto wide = rows_n * kHidden;
@@ -107,6 +115,7 @@ void Gnn::bind(int n, const int* rows, const int* cols, const int* diag, const f
 
 void Gnn::forward(const float* r, float* z, float beta, cudaStream_t s) {
   KB2_REQUIRE(n_ > 0, "learned stage: no matrix bound");
+  check_device();
   const Slices p = slices(params_.get());
   float2* uv = reinterpret_cast<float2*>(uv_.get());
   launch::gnn_lift(n_, rows_, cols_, lift_.get(), r, scale_.get(), uv,
@@ -146,6 +155,7 @@ void Gnn::forward32(const float* r, float* z, cudaStream_t s) {
 float Gnn::train_step(const float* t, const float* e, float lr, cudaStream_t s) {
   KB2_REQUIRE(n_ > 0, "learned stage: no matrix bound");
   KB2_REQUIRE(t != nullptr && e != nullptr, "learned stage: null training vector");
+  check_device();
   const int count = parameter_count();
   const DeviceReducer red{partials_.get(), ticket_.get()};
   float* c = z_.get();

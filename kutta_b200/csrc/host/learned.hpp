@@ -41,8 +41,12 @@ class Gnn {
   std::vector<float> weights() const;
   void set_weights(const std::vector<float>& w);
   int rows() const { return n_; }
+  // The device the stage's arrays live on (current at construction).
+  int device() const { return device_; }
 
  private:
+  // Throws unless the current device is the stage's own.
+  void check_device() const;
   struct Slices {
     float *ws[kLayers], *wn[kLayers], *b[kLayers], *wo;
   };
@@ -51,6 +55,7 @@ class Gnn {
   // the backward pass of training.
   void forward32(const float* r, float* z, cudaStream_t s);
   int n_ = 0;
+  int device_ = 0;
   const int* rows_ = nullptr;
   const int* cols_ = nullptr;
   const float* vals_ = nullptr;

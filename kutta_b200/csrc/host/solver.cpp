@@ -598,6 +598,8 @@ void Solver::set_learned(Gnn* g, int mode) {
               "learned stage: needs an AMG solver with the flexible Krylov driver");
   KB2_REQUIRE(g == nullptr || (mode >= 1 && mode <= (kLearnedCycle | kLearnedWarmStart)),
               "learned stage: mode must be a nonempty set of cycle and warm start");
+  KB2_REQUIRE(g == nullptr || g->device() == device_,
+              "learned stage: built on another device than the solver");
   for (auto& graph : graphs_) cudaGraphExecDestroy(graph.exec);
   graphs_.clear();
   learned_ = g;
