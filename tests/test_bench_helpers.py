@@ -29,3 +29,47 @@ def test_blend_keeps_a_symmetric_m_matrix():
     t = harness.HostSystem(s.row_ptr, s.col, s.diag, vals, s.b)
     levels = L.build_hierarchy(t, L.AmgOptions(structure=L.OperatorStructure.SymmetricMMatrix))
     assert len(levels) > 1
+
+
+def test_clock_samples_are_summarised():
+    """bench.Clocks.stop: the median SM clock under sampling, the largest
+    reported maximum, and the throttle reasons seen Active in any sample."""
+    import bench
+    out = L.library_path().parent / "checks"
+    out.mkdir(exist_ok=True)
+    path = out / "clocks_sample.csv"
+    path.write_text(
+        "0, 1965, 1965, 640.1, 0x0000000000000000, Not Active, Not Active, Not Active, Not Active\n"
+        "0, 1800, 1965, 990.5, 0x0000000000000004, Not Active, Not Active, Not Active, Active\n"
+        "0, 1350, 1965, 998.0, 0x0000000000000004, Not Active, Not Active, Not Active, Active\n"
+        "garbled line\n")
+
+    class _Proc:
+        def terminate(self):
+            pass
+
+        def wait(self, timeout=None):
+            return 0
+
+    c = bench.Clocks(0)
+    c.proc, c.path = _Proc(), str(path)
+    summary = c.stop()
+    assert summary == {"sm_mhz": 1800.0, "sm_max_mhz": 1965.0, "reasons": ["sw_power_cap"],
+                       "samples": 3}
+    assert not path.exists()
+
+
+def test_peaks_and_traffic_come_from_the_committed_files():
+    import json
+
+    import bench
+    peak, source = bench._peaks()
+    if (bench.ROOT / "MEASURED_PEAKS.json").exists():
+        assert source == "measured"
+        assert peak == json.loads((bench.ROOT / "MEASURED_PEAKS.json").read_text())["hbm_gbs"]
+    else:
+        assert (peak, source) == (6650.0, "fallback")
+    entries = json.loads((bench.ROOT / "profiles" / "traffic.json").read_text())
+    for kernel, e in entries.items():
+        assert bench._traffic(kernel, e["workload"]) == e["dram_bytes_per_launch"]
+        assert bench._traffic(kernel, "another workload") is None
