@@ -8,6 +8,7 @@ import ctypes
 
 import pytest
 
+from kutta_b200 import harness
 from kutta_b200 import linalg as L
 
 B2_OK, B2_INVALID_ARGUMENT, B2_DEVICE_ERROR = 0, 1, 3
@@ -122,3 +123,33 @@ def test_header_is_c99_and_a_c_caller_links_and_runs():
     assert r.returncode == 0, r.stdout + r.stderr
     r = subprocess.run([str(exe)], capture_output=True, text=True, timeout=60)
     assert r.returncode == 0 and r.stdout.strip() == "ok", r.stdout + r.stderr
+
+
+def test_python_mirror_maps_statuses_and_checks_before_device_work():
+    """linalg.py raises the reference's exception types for the ABI's statuses,
+    and its factories reject what the reference rejects before device work;
+    an accepted input then meets the missing device as a DeviceError."""
+    s = harness.poisson(6, 5, 4)
+    m = L.AmgOptions(structure=L.OperatorStructure.SymmetricMMatrix)
+    with pytest.raises(L.KuttaError, match="AMG: expected an AMG solver kind"):
+        L.make_amg_solver(L.SolverKind.PcgJacobi, s, L.AmgOptions())
+    with pytest.raises(L.KuttaError, match="AMG-PCG requires equal pre/post sweeps"):
+        L.make_amg_solver(L.SolverKind.AmgPcg, s, L.AmgOptions(pre_sweeps=1, post_sweeps=2))
+    with pytest.raises(L.KuttaError, match="Krylov workspace size mismatch"):
+        L.make_solver(L.SolverKind.BicgstabJacobi, s,
+                      L.SolverOptions(workspace=L.KrylovWorkspace(s.n + 1)))
+    bad = harness.HostSystem(s.row_ptr, s.col, s.diag, s.val.copy(), s.b)
+    bad.val[bad.diag[7]] = 0.0
+    with pytest.raises(L.KuttaError, match="zero diagonal"):
+        L.make_solver(L.SolverKind.PcgJacobi, bad)
+    for make in (lambda: L.make_amg_solver(L.SolverKind.AmgPcg, s, m),
+                 lambda: L.make_solver(L.SolverKind.PcgJacobi, s),
+                 lambda: L.make_mixed_solver(s)):
+        with pytest.raises(L.DeviceError) as e:
+            make()
+        assert not isinstance(e.value, L.DeviceTimeout)
+    for code, kind in ((1, L.KuttaError), (2, L.NonfiniteError), (3, L.DeviceError),
+                       (4, L.DeviceTimeout), (5, L.DeviceError), (6, L.KuttaError)):
+        with pytest.raises(kind):
+            L._check(code)
+    L._check(0)
