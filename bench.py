@@ -29,6 +29,10 @@ L2, so no flush is needed between steps.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
 
+At N = 1 rank 0 adds two CPU-side entries after the timed work: `cpu_baseline`
+(the reference's CPU path on a bounded sample) and `fp64_oracle` (the returned
+x's error against an FP64 oracle solution).
+
 Under torchrun (N > 1) every rank runs an independent replica (the solve does
 not shard); rank 0 prints one JSON line.
 """
@@ -327,7 +331,7 @@ def run_ours(args, rank, world, local):
         "gpu_launches_per_step": int(launches) / args.steps,
         "clocks": clk,
     }
-    return line, s
+    return line, s, x64.cpu().numpy()
 
 
 def _cpu_model():
@@ -346,6 +350,38 @@ def _reference_sample(args, s):
     from oracle import ref
     opts = ref.options(3, structure=1, use_make_solver=True)
     return ref.solve(s, opts=opts, rel_tol=REL_TOL, abs_tol=1e-12, max_iter=args.cpu_sample_iters)
+
+
+def fp64_oracle(s, x, max_iter=20000):
+    """The returned solution's error against an FP64 oracle solution x64 on
+    the host cores. x64 = x + e, where e solves A e = b - A x (residual in
+    FP64) by the oracle's FP64 Jacobi-PCG until x64's relative residual is
+    about 1e-12 (stated in the result): the x64 of a CG from zero to 1e-12, in
+    fewer iterations when x is already close. The oracle is the checker here,
+    never the measured path; a failure is reported in the line instead of
+    failing the run."""
+    import numpy as np
+    import scipy.sparse as sp
+    t0 = time.perf_counter()
+    try:
+        from oracle import kutta_oracle as O
+        x = np.asarray(x, np.float64)
+        A = sp.csr_matrix((s.val, s.col, s.row_ptr), shape=(s.n, s.n))
+        b = s.b.astype(np.float64)
+        r = b - A @ x
+        r_norm = float(np.linalg.norm(r))
+        e, iterations = np.zeros(s.n), 0
+        if r_norm > 1e-12 * np.linalg.norm(b):
+            e, iterations = O.cg64(s, b=r, rel_tol=min(0.1, 1e-12 * np.linalg.norm(b) / r_norm),
+                                   max_iter=max_iter)
+        x64 = x + e
+        return {"relative_error": float(np.linalg.norm(e) / np.linalg.norm(x64)),
+                "oracle": "FP64 Jacobi-PCG on the residual equation (OpenMP, host cores)",
+                "oracle_relative_residual": float(np.linalg.norm(b - A @ x64) /
+                                                  np.linalg.norm(b)),
+                "oracle_iterations": int(iterations), "seconds": time.perf_counter() - t0}
+    except Exception as e:  # noqa: BLE001 - reported, not raised
+        return {"unavailable": f"{type(e).__name__}: {e}"}
 
 
 def cpu_baseline(args, s):
@@ -731,9 +767,10 @@ def main():
         import datetime
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
-    line, system = run_ours(args, rank, world, local)
+    line, system, x = run_ours(args, rank, world, local)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(args, system)
+        line["fp64_oracle"] = fp64_oracle(system, x)
     if rank == 0:
         print(json.dumps(line))
     if world > 1:

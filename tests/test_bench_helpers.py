@@ -73,3 +73,19 @@ def test_peaks_and_traffic_come_from_the_committed_files():
     for kernel, e in entries.items():
         assert bench._traffic(kernel, e["workload"]) == e["dram_bytes_per_launch"]
         assert bench._traffic(kernel, "another workload") is None
+
+
+def test_fp64_oracle_error_of_a_solution():
+    """bench.fp64_oracle: the relative error of a returned x against the FP64
+    CG oracle, and a reported (not raised) failure."""
+    import bench
+    from oracle import kutta_oracle as O
+    s = harness.box_system(8, 8, 8, tet=True, seed=2)
+    x64, _ = O.cg64(s, rel_tol=1e-13)
+    rng = np.random.default_rng(0)
+    x = x64 * (1 + 1e-4 * rng.standard_normal(s.n))
+    r = bench.fp64_oracle(s, x)
+    expected = np.linalg.norm(x - x64) / np.linalg.norm(x64)
+    assert abs(r["relative_error"] - expected) <= 1e-3 * expected
+    assert r["oracle_iterations"] > 0 and r["oracle_relative_residual"] < 1e-11
+    assert "unavailable" in bench.fp64_oracle(s, x[:-1])
