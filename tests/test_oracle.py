@@ -213,3 +213,21 @@ def test_oracle_equals_reference_library_at_other_sweep_counts(sweeps):
     assert (o.initial_residual, o.final_residual) == (r.initial_residual, r.final_residual)
     assert np.array_equal(o.x.view(np.uint32), r.x.view(np.uint32))
     assert o.describe == r.describe
+
+
+@pytest.mark.skipif(not ref.available(), reason="oracle/_ref not built on this machine")
+@pytest.mark.parametrize("kind", [1, O.AMG_PCG], ids=["pcg_jacobi", "amg_pcg"])
+def test_oracle_equals_reference_library_with_constant_nullspace(kind):
+    """A pure-Neumann pressure system (constant null space projected at every
+    level, test_solvers.cpp:102-115) with a compatible right-hand side."""
+    import scipy.sparse as sp
+    s = harness.poisson(12, 10, 6, 1, False, True)
+    A = sp.csr_matrix((s.val, s.col, s.row_ptr), shape=(s.n, s.n))
+    s.b = (A @ harness.random_solution(s.n).astype(np.float64)).astype(np.float32)
+    r = ref.solve(s, opts=ref.options(kind, nullspace=1), rel_tol=1e-6, abs_tol=1e-12,
+                  max_iter=500)
+    o = O.solve(s, kind, nullspace=True, rel_tol=1e-6, abs_tol=1e-12, max_iter=500)
+    assert r.converged
+    assert (o.iterations, o.converged) == (r.iterations, r.converged)
+    assert (o.initial_residual, o.final_residual) == (r.initial_residual, r.final_residual)
+    assert np.array_equal(o.x.view(np.uint32), r.x.view(np.uint32))
