@@ -231,3 +231,16 @@ def test_oracle_equals_reference_library_with_constant_nullspace(kind):
     assert (o.iterations, o.converged) == (r.iterations, r.converged)
     assert (o.initial_residual, o.final_residual) == (r.initial_residual, r.final_residual)
     assert np.array_equal(o.x.view(np.uint32), r.x.view(np.uint32))
+
+
+@pytest.mark.skipif(not ref.available(), reason="oracle/_ref not built on this machine")
+def test_oracle_equals_reference_library_on_a_graded_mesh():
+    """The graded near-wall band (aspect 1000:1, D_f over [1e-6, 1]) where the
+    FP32 solve stalls: the stall itself (iterations, final residual, best x)
+    must be the reference's."""
+    s = harness.box_system(12, 12, 12, tet=True, seed=4, band_layers=5, dmin=1e-6, dmax=1.0)
+    r = ref.solve(s, opts=ref.options(3, structure=1), rel_tol=1e-8, abs_tol=1e-30, max_iter=300)
+    o = O.solve(s, O.AMG_PCG, m_matrix=True, rel_tol=1e-8, abs_tol=1e-30, max_iter=300)
+    assert (o.iterations, o.converged) == (r.iterations, r.converged)
+    assert (o.initial_residual, o.final_residual) == (r.initial_residual, r.final_residual)
+    assert np.array_equal(o.x.view(np.uint32), r.x.view(np.uint32))
