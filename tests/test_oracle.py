@@ -64,6 +64,23 @@ def test_published_64cube_residual():
     assert f"{r.final_residual / r.initial_residual:.8e}" == "7.91394974e-07"
 
 
+@pytest.mark.parametrize("anisotropy,kind,iterations,converged,relative", [
+    (1, 1, 278, True, "6.85768115e-07"),
+    (1000, 1, 354, False, "1.53025686e-06"),
+    (1000, 3, 38, False, "1.51536251e-06"),
+], ids=["pcg_jacobi", "pcg_jacobi_aniso1000", "amg_pcg_aniso1000"])
+def test_published_64cube_lines(anisotropy, kind, iterations, converged, relative):
+    """The other 64^3 lines of the reference's published CPU log
+    (validation/results/colab_t4/logs/bench_linalg.log, x86, bitwise): random
+    forcing, SolveControl{1e-6, 1e-12, 2000}, isotropic PCG-Jacobi and the
+    1:1000 anisotropic case, where both solvers stop unconverged."""
+    s = harness.poisson(64, 64, 64, anisotropy)
+    s.b = harness.random_forcing(s.n)
+    r = O.solve(s, kind, rel_tol=1e-6, abs_tol=1e-12, max_iter=2000)
+    assert (r.iterations, r.converged) == (iterations, converged)
+    assert f"{r.final_residual / r.initial_residual:.8e}" == relative
+
+
 def test_published_32cube_iterations():
     """linalg/README.md:483-484 of the reference: 32^3 random forcing, 11 iterations."""
     s = harness.poisson(32, 32, 32)
