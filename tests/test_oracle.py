@@ -81,6 +81,18 @@ def test_published_64cube_lines(anisotropy, kind, iterations, converged, relativ
     assert f"{r.final_residual / r.initial_residual:.8e}" == relative
 
 
+@pytest.mark.slow
+def test_published_128cube_residual():
+    """bench_linalg.log of the reference, its largest line: 128^3 Poisson
+    (2.1M rows), random forcing, AMG-PCG, 21 iterations, relative residual
+    8.66568009e-07 (x86, bitwise). About half a minute on one core."""
+    s = harness.poisson(128, 128, 128)
+    s.b = harness.random_forcing(s.n)
+    r = O.solve(s, O.AMG_PCG, rel_tol=1e-6, abs_tol=1e-12, max_iter=2000)
+    assert (r.iterations, r.converged) == (21, True)
+    assert f"{r.final_residual / r.initial_residual:.8e}" == "8.66568009e-07"
+
+
 def test_published_32cube_iterations():
     """linalg/README.md:483-484 of the reference: 32^3 random forcing, 11 iterations."""
     s = harness.poisson(32, 32, 32)
