@@ -55,11 +55,6 @@ METRIC = "ms per pressure solve to rel-res 1e-6: learned+mixed vs plain AMG-PCG,
 UNIT = "ms/solve"
 REL_TOL = 1e-6
 
-# Iterations the reference's CPU path needs on the default workload (its full
-# run in this repository's oracle build: 160 iterations, then it stops at
-# relative residual 2.80e-6 without converging); the reference arm scales its
-# bounded per-iteration sample by this count.
-REFERENCE_ITERATIONS = {(96, 1): 160}
 
 
 def _dist():
@@ -345,12 +340,13 @@ def _cpu_model():
     return None
 
 
-def _reference_sample(args, s):
+def _reference_run(args, s, max_iter):
     """The reference's own CPU path (oracle/_ref; serial by design, 1 core):
-    setup + refresh + the first `cpu_sample_iters` PCG iterations."""
+    make_solver(AmgPcg, SymmetricMMatrix) setup, refresh, then PCG from x = 0
+    for at most `max_iter` iterations, each phase timed."""
     from oracle import ref
     opts = ref.options(3, structure=1, use_make_solver=True)
-    return ref.solve(s, opts=opts, rel_tol=REL_TOL, abs_tol=1e-12, max_iter=args.cpu_sample_iters)
+    return ref.solve(s, opts=opts, rel_tol=REL_TOL, abs_tol=1e-12, max_iter=max_iter)
 
 
 def fp64_oracle(s, x, max_iter=20000):
@@ -385,55 +381,82 @@ def fp64_oracle(s, x, max_iter=20000):
         return {"unavailable": f"{type(e).__name__}: {e}"}
 
 
-def cpu_baseline(args, s):
+def cpu_baseline(args, s, iterations):
+    """The reference's CPU path on a bounded sample of the workload (setup,
+    refresh and the first --cpu-sample-iters PCG iterations, about 20 s),
+    scaled to one solve by `iterations`: the iteration count of this run's
+    plain GPU solve, whose arithmetic and iterates are the reference's (the
+    GPU parity tests check the counts are equal). The full, unscaled solve is
+    what `--impl reference` times."""
     from oracle import ref
     if not ref.available():
         return None
-    iters = REFERENCE_ITERATIONS.get((args.size, args.seed))
-    r = _reference_sample(args, s)
+    r = _reference_run(args, s, args.cpu_sample_iters)
     per_iter = r.solve_s / max(r.iterations, 1)
-    if iters is None:
-        return {"value": None, "unit": UNIT, "cores": 1, "kind": "reference",
-                "sample": f"{r.iterations} iterations at {per_iter:.2f} s each; full iteration count "
-                          "unknown for this workload"}
-    return {"value": (r.refresh_s + per_iter * iters) * 1e3, "unit": UNIT, "cores": 1,
+    return {"value": (r.refresh_s + per_iter * iterations) * 1e3, "unit": UNIT, "cores": 1,
             "kind": "reference",
             "sample": f"reference CPU path (oracle/_ref, built from the reference sources): setup "
                       f"{r.setup_s:.1f} s (not counted), refresh {r.refresh_s * 1e3:.0f} ms, first "
                       f"{r.iterations} PCG iterations in {r.solve_s:.1f} s; per solve = refresh + "
-                      f"{per_iter:.2f} s/iteration x {iters} iterations (its full run stops there at "
-                      "rel 2.80e-6, not converged)", "cpu": _cpu_model()}
+                      f"{per_iter:.2f} s/iteration x {iterations} iterations (the plain GPU "
+                      "solve's count in this run, equal to the reference's); extrapolated, "
+                      "the reference arm times the full solve", "cpu": _cpu_model()}
+
+
+def _write_workload(args, path):
+    """--mode workload: the benchmark matrix and right-hand side, written as
+    .npz for the reference arm, which reads it without loading this
+    repository's generator library."""
+    import numpy as np
+    s = _workload(args)
+    np.savez(path, row_ptr=s.row_ptr, col=s.col, diag=s.diag, val=s.val, b=s.b)
+
+
+def _read_workload(args):
+    """The workload generated in a child process (`--mode workload`), so the
+    reference arm's process maps only the reference's own library."""
+    import types
+    import numpy as np
+    with tempfile.TemporaryDirectory() as tmp:
+        path = os.path.join(tmp, "workload.npz")
+        subprocess.run([sys.executable, str(ROOT / "bench.py"), "--mode", "workload",
+                        "--size", str(args.size), "--seed", str(args.seed), "--out", path],
+                       check=True)
+        d = np.load(path)
+        s = types.SimpleNamespace(**{k: d[k] for k in d.files})
+    s.n, s.nnz = len(s.diag), len(s.col)
+    return s
 
 
 def run_reference(args, rank, world):
     """--impl reference: the reference's own CPU implementation on the host
-    cores (serial by design: 1 thread); each step a bounded sample."""
+    cores (serial by design: 1 thread). One complete solve is timed: the
+    reference's make_solver setup (not counted, as the GPU arm's setup is not),
+    then refresh and PCG from x = 0 until it stops (converged or not), the
+    same step the GPU arm times. A solve takes about 9 minutes on the 5.3M-row
+    matrix, so one timed solve is the whole run (no warm-up: a serial CPU
+    solve has nothing to warm); `steps` and `warmup` say what ran."""
     if rank != 0:
         return None
     from oracle import ref
     if not ref.available():
         return {"impl": "reference", "unavailable": "oracle/_ref (the reference CPU build) is missing"}
-    s = _workload(args)
-    iters = REFERENCE_ITERATIONS.get((args.size, args.seed))
-    if iters is None:
-        return {"impl": "reference",
-                "unavailable": f"no recorded reference iteration count for size {args.size}"}
-    times = []
-    r = None
-    for k in range(args.warmup + args.steps):
-        r = _reference_sample(args, s)
-        if k >= args.warmup:
-            times.append((r.refresh_s + r.solve_s / max(r.iterations, 1) * iters) * 1e3)
-    value = statistics.median(times)
-    sample = (f"per step: reference setup + refresh + first {r.iterations} PCG iterations on the "
-              f"host; per solve = refresh + per-iteration time x {iters} iterations (the "
-              "reference's full count on this workload; it stops at rel 2.80e-6, not converged)")
+    s = _read_workload(args)
+    r = _reference_run(args, s, args.max_iter)
+    value = (r.refresh_s + r.solve_s) * 1e3
+    sample = (f"one complete reference solve on the host, timed: setup {r.setup_s:.1f} s (not "
+              f"counted), refresh {r.refresh_s * 1e3:.0f} ms, PCG {r.iterations} iterations in "
+              f"{r.solve_s:.1f} s, relative residual {r.final_residual / r.initial_residual:.3e}, "
+              f"converged {r.converged}")
     return {
-        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": value, "higher_is_better": False,
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": 1,
+        "warmup": 0, "requested": {"steps": args.steps, "warmup": args.warmup},
+        "ms_per_step": value, "higher_is_better": False,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32 (FP64 reductions)",
         "data": "synthetic (seeded FV pressure matrix; no dataset)",
         "config": _config(args, s, world), "impl": "reference",
+        "method": r.describe, "iterations": r.iterations, "converged": r.converged,
+        "relative_residual": r.final_residual / r.initial_residual,
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": 1, "kind": "reference",
                          "sample": sample, "cpu": _cpu_model()},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -736,7 +759,8 @@ def main():
     ap.add_argument("--cpu-sample-iters", type=int, default=2)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--mode", default="bench",
-                    choices=["bench", "profile", "sequence", "graded", "transport", "outer"],
+                    choices=["bench", "profile", "sequence", "graded", "transport", "outer",
+                             "workload"],
                     help="profile: one refresh + one solve (with --max-iter), for ncu captures; "
                          "sequence: successive warm-started solves on the graded mesh; "
                          "graded: the graded matrix to --rel-tol (default 1e-8); "
@@ -747,8 +771,12 @@ def main():
     ap.add_argument("--solves", type=int, default=300, help="sequence mode: number of solves")
     ap.add_argument("--rel-tol", type=float, default=None,
                     help="sequence / graded modes (defaults 1e-6 / 1e-8)")
+    ap.add_argument("--out", default=None, help="workload mode: the .npz to write")
     args = ap.parse_args()
     rank, world, local = _dist()
+    if args.mode == "workload":
+        _write_workload(args, args.out)
+        return
     if args.mode == "profile":
         profile_once(args)
         return
@@ -770,7 +798,7 @@ def main():
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
     line, system, x = run_ours(args, rank, world, local)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        line["cpu_baseline"] = cpu_baseline(args, system)
+        line["cpu_baseline"] = cpu_baseline(args, system, line["plain"]["iterations"])
         line["fp64_oracle"] = fp64_oracle(system, x)
     if rank == 0:
         print(json.dumps(line))

@@ -248,11 +248,14 @@ int b2_dense_inverse(int n, const int32_t* d_row_ptr, const int32_t* d_col, cons
  * risk running out of memory mid-step, and work queued while another
  * component records the stream. The same computation, with the n*n factor
  * scratch taken from a 2 MiB array built into the library (so n <= 512; larger
- * n is rejected with B2_INVALID_ARGUMENT). It calls no allocator. The array is
- * shared by all calls on a device: calls that overlap on the GPU race, so the
- * caller orders them. The first call on each device looks the array's address
- * up (and may load the library's device code); make it before any stream
- * capture. */
+ * n is rejected with B2_INVALID_ARGUMENT). It calls no allocator. Calls with
+ * n > 236 factor through the array, which all calls on a device share: such
+ * calls that overlap on the GPU race, so the caller orders them. Calls with
+ * n <= 236 factor in shared memory and never touch the array. The first call
+ * on each device looks the array's address up (and may load the library's
+ * device code); make it before any stream capture. A device reset
+ * (cudaDeviceReset) can move the array: do not call this entry point on a
+ * device after resetting it. */
 int b2_dense_inverse_noalloc(int n, const int32_t* d_row_ptr, const int32_t* d_col,
                              const float* d_val, double* d_inverse, double* d_not_spd,
                              void* stream);

@@ -11,16 +11,23 @@
 // Limits and sharing:
 // - n <= kNoAllocRows (512): the scratch is 512 x 512 doubles = 2 MiB, reserved
 //   on every GPU that loads this library, for as long as the process runs.
-// - Every call uses the same array. The kernel clears the part it uses before
-//   filling it, so leftovers from an earlier call never reach the result, but
-//   calls whose work overlaps on the GPU (different streams, or different
-//   threads on one device without ordering) race on the array and must be
-//   ordered by the caller.
+// - Operators of n > 236 rows are factored through the array. Every such call
+//   uses the same array: the kernel clears the part it uses before filling
+//   it, so leftovers from an earlier call never reach the result, but calls
+//   whose work overlaps on the GPU (different streams, or different threads on
+//   one device without ordering) race on the array and must be ordered by the
+//   caller. Operators of n <= 236 rows are factored in shared memory and never
+//   touch the array, so they need no ordering.
 // - The device address of the array is looked up once per device, on that
 //   device's first call (cudaGetSymbolAddress, which may load this library's
 //   device code). Make that first call before any stream capture begins.
+//   Later calls read the cached address without taking a lock. A device reset
+//   (cudaDeviceReset) unloads the library's device code, which can move the
+//   array; a process that resets a device must not call this entry point on
+//   that device afterwards.
 #include <cuda_runtime.h>
 
+#include <atomic>
 #include <cstdio>
 #include <mutex>
 
@@ -38,8 +45,8 @@ constexpr int kMaxDevices = 64;
 // cudaGetSymbolAddress below.
 static __device__ __align__(256) double g_dense_scratch[kNoAllocRows * kNoAllocRows];
 
-std::mutex g_lock;
-double* g_scratch_address[kMaxDevices] = {};
+std::mutex g_lock;  // taken only by a device's first lookup
+std::atomic<double*> g_scratch_address[kMaxDevices] = {};
 
 // Device address of the scratch on the current device (looked up once).
 int scratch_address(double** out) {
@@ -48,8 +55,12 @@ int scratch_address(double** out) {
   if (e != cudaSuccess) return report_error(B2_DEVICE_ERROR, cudaGetErrorString(e));
   if (device < 0 || device >= kMaxDevices)
     return report_error(B2_DEVICE_ERROR, "dense inverse (no allocation): device ordinal out of range");
+  if (double* cached = g_scratch_address[device].load(std::memory_order_acquire)) {
+    *out = cached;
+    return B2_OK;
+  }
   std::lock_guard<std::mutex> hold(g_lock);
-  if (!g_scratch_address[device]) {
+  if (!g_scratch_address[device].load(std::memory_order_relaxed)) {
     void* address = nullptr;
     e = cudaGetSymbolAddress(&address, g_dense_scratch);
     if (e != cudaSuccess || address == nullptr) {
@@ -59,9 +70,9 @@ int scratch_address(double** out) {
                     cudaGetErrorString(e));
       return report_error(B2_DEVICE_ERROR, message);
     }
-    g_scratch_address[device] = static_cast<double*>(address);
+    g_scratch_address[device].store(static_cast<double*>(address), std::memory_order_release);
   }
-  *out = g_scratch_address[device];
+  *out = g_scratch_address[device].load(std::memory_order_relaxed);
   return B2_OK;
 }
 }  // namespace

@@ -867,7 +867,9 @@ void Solver::pcg(float* x, const float* b, const Control& c, double target, Stat
       if (!replacement(x, b, target, stats, restarts, last_verified) ||
           stats.iterations == c.max_iter)
         break;
-      // Near a float residual floor, repeated candidates can stop after one update.
+      // Within 10x of the target the verified residual is close to what FP32
+      // can resolve, so a restarted batch may stop after a single update: poll
+      // after every update from here on.
       if (stats.final_residual <= 10 * target) check_interval = 1;
       restart();
     }

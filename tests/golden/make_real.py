@@ -22,6 +22,7 @@ from __future__ import annotations
 import gzip
 import hashlib
 import json
+import os
 import pathlib
 import sys
 
@@ -34,7 +35,9 @@ sys.path.insert(0, str(ROOT))
 from kutta_b200 import harness  # noqa: E402
 from oracle import ref  # noqa: E402
 
-SOURCE = pathlib.Path("/root/reference/validation/results/pressure_float")
+# The reference checkout (read-only), as for oracle/build.py.
+REFERENCE = pathlib.Path(os.environ.get("KUTTA_REFERENCE", "/root/reference"))
+SOURCE = REFERENCE / "validation" / "results" / "pressure_float"
 CASES = {
     "tmr_bump_pressure_it15": "bump_current_iteration15.coo.gz",
     "tmr_bump_pressure_it18": "bump_iteration18_reassembled.coo.gz",

@@ -11,9 +11,17 @@ GOLDEN = pathlib.Path(__file__).resolve().parent / "golden"
 
 
 def names():
-    """The seeded-system fixtures of tests/golden/make_golden.py (the real
-    matrices of make_real.py have their own format and tests)."""
-    return sorted(p.stem for p in GOLDEN.glob("*.npz") if not p.stem.startswith("tmr_"))
+    """The seeded-system solve fixtures of tests/golden/make_golden.py (the real
+    matrices of make_real.py have their own format and tests, and the
+    hierarchy-only fixtures their own loader)."""
+    return sorted(p.stem for p in GOLDEN.glob("*.npz")
+                  if not p.stem.startswith("tmr_") and not p.stem.endswith("_hierarchy"))
+
+
+def hierarchy_names():
+    """Fixtures holding only the reference's AMG hierarchy (level sizes and
+    array digests), for systems too large for a reference solve per fixture."""
+    return sorted(p.stem for p in GOLDEN.glob("*_hierarchy.npz"))
 
 
 def load(name):
@@ -27,12 +35,13 @@ def system(name):
     """The seeded input system of a fixture (checked against its stored digests)."""
     import sys
     sys.path.insert(0, str(GOLDEN))
-    from make_golden import CASES  # noqa: WPS433
+    from make_golden import CASES, HIERARCHIES  # noqa: WPS433
     sys.path.pop(0)
-    s = CASES[name][0]()
+    s = (CASES[name] if name in CASES else HIERARCHIES[name])[0]()
     meta, _ = load(name)
     assert digest(s.val) + digest(s.col) == meta["matrix_sha"], "generator drifted from fixture"
-    assert digest(s.b) == meta["rhs_sha"], "right-hand side drifted from fixture"
+    if "rhs_sha" in meta:
+        assert digest(s.b) == meta["rhs_sha"], "right-hand side drifted from fixture"
     return s
 
 

@@ -81,19 +81,23 @@ def test_amg_matches_reference(cuda, name, make, kind, m_matrix):
 
 
 @needs_ref
+@pytest.mark.parametrize("sweeps", [1, 2], ids=["V11", "V22"])
 @pytest.mark.parametrize("make,kind,m_matrix", [
     (lambda: harness.box_system(12, 12, 12, tet=True, seed=7), 3, True),
+    (lambda: harness.pressure_hex32(1), 3, True),
     (lambda: _rhs(harness.poisson(20, 18, 1, 1, False, False, 3)), 4, False),
-], ids=["tet12_pcg", "poisson_wind3_bicg"])
-def test_one_sweep_cycles_match_reference(cuda, make, kind, m_matrix):
-    """V(1,1): the single zero-start pre-sweep and the residual run as one
-    fused pass; iterations and residuals must still be the reference's."""
+], ids=["tet12_pcg", "hex32_pcg", "poisson_wind3_bicg"])
+def test_other_sweep_counts_match_reference(cuda, make, kind, m_matrix, sweeps):
+    """V(1,1), where the single zero-start pre-sweep and the residual run as one
+    fused pass, and V(2,2), the pressure solver of the SST configuration
+    (src/kutta/fv/steady_solver.cpp:575-578): iterations, residuals and x must
+    still be the reference's."""
     s = make()
-    opts = L.AmgOptions(pre_sweeps=1, post_sweeps=1,
+    opts = L.AmgOptions(pre_sweeps=sweeps, post_sweeps=sweeps,
                         structure=M if m_matrix else L.OperatorStructure.General)
     st, x, solver = _solve_gpu(s, L.SolverKind(kind), amg_options=opts)
-    r = ref.solve(s, opts=ref.options(kind, structure=int(m_matrix), pre_sweeps=1,
-                                      post_sweeps=1),
+    r = ref.solve(s, opts=ref.options(kind, structure=int(m_matrix), pre_sweeps=sweeps,
+                                      post_sweeps=sweeps),
                   rel_tol=1e-6, abs_tol=1e-12, max_iter=2000)
     assert solver.describe() == r.describe
     _compare(st, x, r)

@@ -41,11 +41,15 @@ def test_defaults_match_reference_structs():
     assert (c.rel_tol, c.abs_tol, c.max_iter, c.residual_check_interval) == (1e-2, 1e-12, 200, 8)
 
 
-@pytest.mark.parametrize("name", [n for n in G.names() if G.load(n)[0]["kind"] >= 3])
+@pytest.mark.parametrize("name", [n for n in G.names() if G.load(n)[0]["kind"] >= 3]
+                         + G.hierarchy_names())
 def test_host_hierarchy_matches_reference_fixture(name):
+    """Every AMG fixture, and the 5.3M-row tet pressure matrix's hierarchy
+    (about 20 s: generating the matrix and the host setup)."""
     meta, arrays = G.load(name)
     s = G.system(name)
-    opts = L.AmgOptions(structure=M if meta["m_matrix"] else L.OperatorStructure.General)
+    opts = L.AmgOptions(structure=M if meta["m_matrix"] else L.OperatorStructure.General,
+                        **meta.get("options", {}))
     levels = L.build_hierarchy(s, opts, spd=meta["kind"] == 3)
     assert [lv.n for lv in levels] == meta["levels"]
     for i, (lv, sha) in enumerate(zip(levels, meta["level_sha"])):

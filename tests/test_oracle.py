@@ -28,7 +28,7 @@ def i32(*v):
 def test_oracle_reproduces_reference_fixture(name):
     meta, arrays = G.load(name)
     s = G.system(name)
-    opts = O.options(meta["kind"], m_matrix=bool(meta["m_matrix"]))
+    opts = O.options(meta["kind"], m_matrix=bool(meta["m_matrix"]), **meta.get("options", {}))
     r = O.solve(s, opts=opts, rel_tol=meta["rel_tol"], abs_tol=meta["abs_tol"],
                 max_iter=meta["max_iter"])
     assert r.iterations == meta["iterations"]

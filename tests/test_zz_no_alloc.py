@@ -50,13 +50,20 @@ def _both(s):
             (want.cpu().numpy().reshape(n, n), want_flag.item()))
 
 
+# Operators of up to ON_CHIP_ROWS rows are factored in shared memory and never
+# touch the built-in scratch array; every case below is larger, so each call
+# factors through that array.
+ON_CHIP_ROWS = 236
+
+
 @pytest.mark.gpu
 def test_noalloc_matches_allocating_entry_point_twice(cuda):
     # First a larger operator, then a smaller one with other values: the second
-    # call reuses the scratch the first one filled.
-    first = harness.box_system(4, 4, 4, tet=True, seed=4)
-    second = harness.box_system(6, 6, 6, tet=False, seed=9)
-    assert second.n < first.n <= 512
+    # call reuses the part of the array the first one filled, and must not see
+    # its leftovers.
+    first = harness.box_system(4, 4, 4, tet=True, seed=4)    # 384 rows
+    second = harness.box_system(7, 7, 7, tet=False, seed=9)  # 343 rows
+    assert ON_CHIP_ROWS < second.n < first.n <= 512
     for s in (first, second):
         (got, got_flag), (want, want_flag) = _both(s)
         assert got_flag == want_flag == 0.0
@@ -65,12 +72,26 @@ def test_noalloc_matches_allocating_entry_point_twice(cuda):
 
 
 @pytest.mark.gpu
+def test_noalloc_at_its_size_limit(cuda):
+    s = harness.box_system(8, 8, 8, tet=False, seed=5)  # 512 rows: the whole array
+    assert s.n == 512
+    (got, got_flag), (want, want_flag) = _both(s)
+    assert got_flag == want_flag == 0.0
+    assert np.max(np.abs(got - want)) <= REL_TOL * np.max(np.abs(want))
+
+
+@pytest.mark.gpu
 def test_noalloc_flags_non_spd_like_allocating_entry_point(cuda):
-    s = harness.box_system(3, 3, 3, tet=True, seed=4)
+    s = harness.box_system(7, 7, 6, tet=False, seed=4)  # 294 rows
+    assert s.n > ON_CHIP_ROWS
     bad = s.val.copy()
     bad[s.diag[0]] = -1.0
     (_, got_flag), (_, want_flag) = _both(harness.HostSystem(s.row_ptr, s.col, s.diag, bad, s.b))
     assert got_flag == want_flag == 1.0
+    # The next call on the same array, with an SPD operator, is unaffected.
+    (got, got_flag), (want, want_flag) = _both(s)
+    assert got_flag == want_flag == 0.0
+    assert np.max(np.abs(got - want)) <= REL_TOL * np.max(np.abs(want))
 
 
 @pytest.mark.gpu
