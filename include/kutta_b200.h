@@ -291,6 +291,13 @@ int b2_gnn_bind(b2_gnn* g, int n, const int32_t* d_row_ptr, const int32_t* d_col
  * operands, FP32 accumulation); waits for the stream to report a device
  * fault of the stage. */
 int b2_gnn_apply(b2_gnn* g, const float* d_r, float* d_z, float beta, void* stream);
+/* Testing hook for the forward's bounded waits: each tensor-core tile polls
+ * its MMA's completion at most `polls` times (polls < 0 restores the built-in
+ * bound, 4,194,304) before its block gives up. A block that gives up records
+ * the fault, waits for its MMA once more with the full bound, frees its
+ * tensor memory and returns; b2_gnn_apply then returns B2_TIMEOUT and clears
+ * the fault. polls = 0 takes that path with a healthy MMA. */
+int b2_gnn_set_wait_limit(b2_gnn* g, long long polls);
 /* One training step on (d_t, d_e), A e = t for the bound matrix; *loss is the
  * energy loss before the step. */
 int b2_gnn_train_step(b2_gnn* g, const float* d_t, const float* d_e, float learning_rate,

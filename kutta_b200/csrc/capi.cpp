@@ -647,6 +647,13 @@ int b2_gnn_apply(b2_gnn* g, const float* d_r, float* d_z, float beta, void* stre
   });
 }
 
+int b2_gnn_set_wait_limit(b2_gnn* g, long long polls) {
+  return guarded([&] {
+    KB2_REQUIRE(g && g->g, "learned stage: null argument");
+    g->g->set_wait_polls(polls);
+  });
+}
+
 int b2_gnn_train_step(b2_gnn* g, const float* d_t, const float* d_e, float learning_rate,
                       float* loss, void* stream) {
   return guarded([&] {

@@ -232,11 +232,15 @@ void gnn_lift(int n, const int* rows, const int* cols, const float* lift, const 
               cudaStream_t s);
 void gnn_layer_a(int n, const int* rows, const int* cols, const float* edge, const float2* uv,
                  const float* first, const float* ws, const float* wn, const float* bias,
-                 const double* sum2, unsigned short* hout, int* fault, cudaStream_t s);
+                 const double* sum2, unsigned short* hout, int* fault, long long first_polls,
+                 cudaStream_t s);
+// first_polls: polls of each tile's first wait for its MMA before the CTA
+// gives up (< 0: the built-in bound); the drain wait after giving up always
+// takes the full bound, so the MMA completes before tensor memory is freed.
 void gnn_layer_b(int n, const int* rows, const int* cols, const float* edge,
                  const unsigned short* hin, const float* ws, const float* wn, const float* bias,
                  const float* wo, const float* node_scale, const double* sum2, float* z,
-                 float beta, int* fault, cudaStream_t s);
+                 float beta, int* fault, long long first_polls, cudaStream_t s);
 
 // ---- finite-volume steps around the pressure solve (fv_kernels.cu) ---------
 // fv_pressure_assemble (fv_flow.kern.h:164-183); the _l1 form also writes

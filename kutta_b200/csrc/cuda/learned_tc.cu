@@ -132,8 +132,8 @@ __device__ __forceinline__ bool mbar_try(uint32_t bar, uint32_t parity) {
       : "memory");
   return done != 0;
 }
-__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
-  for (long long k = 0; k < kSpinLimit; ++k)
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, long long polls) {
+  for (long long k = 0; k < polls; ++k)
     if (mbar_try(bar, parity)) return true;
   return false;
 }
@@ -227,7 +227,7 @@ __global__ void __launch_bounds__(kTcThreads, kLift ? 2 : 4)
                    const float* __restrict__ bias, const float* __restrict__ wo,
                    const float* __restrict__ node_scale, const double* __restrict__ sum2,
                    uint4* __restrict__ hout, float* __restrict__ z, float beta,
-                   int* __restrict__ fault) {
+                   int* __restrict__ fault, long long first_polls) {
   extern __shared__ uint8_t raw[];
   const uint32_t pad = (1024u - (smem_u32(raw) & 1023u)) & 1023u;
   uint8_t* tile_a = raw + pad;
@@ -363,7 +363,7 @@ __global__ void __launch_bounds__(kTcThreads, kLift ? 2 : 4)
         mma_bf16(tmem, adesc + 2 * k, bdesc + 2 * k, k > 0 ? 1u : 0u);
       mma_commit(bar_addr);
     }
-    const bool done = mbar_wait(bar_addr, phase);
+    const bool done = mbar_wait(bar_addr, phase, first_polls);
     if (__syncthreads_or(!done)) {
       failed = true;
       break;
@@ -394,7 +394,7 @@ __global__ void __launch_bounds__(kTcThreads, kLift ? 2 : 4)
   }
   if (failed) {
     if (tid == 0) atomicOr(fault, 1);
-    mbar_wait(bar_addr, phase);  // the late MMA, once more (bounded)
+    mbar_wait(bar_addr, phase, kSpinLimit);  // the late MMA, once more (full bound)
   }
   tc_fence_before();
   __syncthreads();
@@ -402,6 +402,12 @@ __global__ void __launch_bounds__(kTcThreads, kLift ? 2 : 4)
     tc_fence_after();
     tmem_dealloc(tmem, kTmemColumns);
   }
+}
+
+// The poll count of each tile's first wait for its MMA: kSpinLimit unless a
+// test asked for fewer (0..kSpinLimit).
+long long wait_polls(long long requested) {
+  return requested < 0 || requested > kSpinLimit ? kSpinLimit : requested;
 }
 
 int tc_grid(int n) {
@@ -423,23 +429,24 @@ void gnn_lift(int n, const int* rows, const int* cols, const float* lift, const 
 
 void gnn_layer_a(int n, const int* rows, const int* cols, const float* edge, const float2* uv,
                  const float* first, const float* ws, const float* wn, const float* bias,
-                 const double* sum2, unsigned short* hout, int* fault, cudaStream_t s) {
+                 const double* sum2, unsigned short* hout, int* fault, long long first_polls,
+                 cudaStream_t s) {
   if (n <= 0) return;
   ++counter;
   k_gnn_layer_tc<true><<<tc_grid(n), kTcThreads, kTcSmem, s>>>(
       n, rows, cols, edge, uv, nullptr, first, ws, wn, bias, nullptr, nullptr, sum2,
-      reinterpret_cast<uint4*>(hout), nullptr, 0.0f, fault);
+      reinterpret_cast<uint4*>(hout), nullptr, 0.0f, fault, wait_polls(first_polls));
 }
 
 void gnn_layer_b(int n, const int* rows, const int* cols, const float* edge,
                  const unsigned short* hin, const float* ws, const float* wn, const float* bias,
                  const float* wo, const float* node_scale, const double* sum2, float* z,
-                 float beta, int* fault, cudaStream_t s) {
+                 float beta, int* fault, long long first_polls, cudaStream_t s) {
   if (n <= 0) return;
   ++counter;
   k_gnn_layer_tc<false><<<tc_grid(n), kTcThreads, kTcSmem, s>>>(
       n, rows, cols, edge, nullptr, reinterpret_cast<const uint4*>(hin), nullptr, ws, wn, bias,
-      wo, node_scale, sum2, nullptr, z, beta, fault);
+      wo, node_scale, sum2, nullptr, z, beta, fault, wait_polls(first_polls));
 }
 
 }  // namespace launch

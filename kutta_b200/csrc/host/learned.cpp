@@ -121,9 +121,9 @@ void Gnn::forward(const float* r, float* z, float beta, cudaStream_t s) {
   launch::gnn_lift(n_, rows_, cols_, lift_.get(), r, scale_.get(), uv,
                    DeviceReducer{partials_.get(), ticket_.get()}, sums_.get(), s);
   launch::gnn_layer_a(n_, rows_, cols_, edge_.get(), uv, params_.get(), p.ws[1], p.wn[1], p.b[1],
-                      sums_.get(), h2_.get(), fault_.get(), s);
+                      sums_.get(), h2_.get(), fault_.get(), wait_polls_, s);
   launch::gnn_layer_b(n_, rows_, cols_, edge_.get(), h2_.get(), p.ws[2], p.wn[2], p.b[2], p.wo,
-                      scale_.get(), sums_.get(), z, beta, fault_.get(), s);
+                      scale_.get(), sums_.get(), z, beta, fault_.get(), wait_polls_, s);
 }
 
 void Gnn::check(cudaStream_t s) {

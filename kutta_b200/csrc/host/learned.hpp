@@ -43,6 +43,10 @@ class Gnn {
   int rows() const { return n_; }
   // The device the stage's arrays live on (current at construction).
   int device() const { return device_; }
+  // Polls of each tensor-core tile's first wait for its MMA before the CTA
+  // gives up and the forward reports a timeout (< 0: the built-in bound). A
+  // test sets 0 to take the timeout path with a healthy MMA.
+  void set_wait_polls(long long polls) { wait_polls_ = polls; }
 
  private:
   // Throws unless the current device is the stage's own.
@@ -71,6 +75,7 @@ class Gnn {
   DArray<float> h_[kLayers + 1], m_agg_[kLayers];
   DArray<float> dz_, z_, q_, dh_, dhs_, dm_, dagg_;
   int step_ = 0;
+  long long wait_polls_ = -1;
 };
 
 }  // namespace kb2

@@ -201,6 +201,7 @@ _SIGNATURES = {
     "b2_gnn_bind": (_I, [_P, _I, _P, _P, _P, _P, _P]),
     "b2_gnn_apply": (_I, [_P, _P, _P, ctypes.c_float, _P]),
     "b2_gnn_train_step": (_I, [_P, _P, _P, ctypes.c_float, _P, _P]),
+    "b2_gnn_set_wait_limit": (_I, [_P, ctypes.c_longlong]),
     "b2_gnn_get_weights": (_I, [_P, _P, ctypes.c_size_t]),
     "b2_gnn_set_weights": (_I, [_P, _P, ctypes.c_size_t]),
     "b2_mixed_set_learned": (_I, [_P, _P, _I]),
@@ -632,6 +633,12 @@ class LearnedStage:
 
     def apply(self, r, z, beta: float = 0.0) -> None:
         _check(_load().b2_gnn_apply(self._handle, _tptr(r), _tptr(z), beta, _stream()))
+
+    def set_wait_limit(self, polls: int) -> None:
+        """Testing hook: each tensor-core tile's first wait for its MMA polls at
+        most `polls` times (< 0: the built-in bound) before the forward gives
+        up and raises DeviceTimeout."""
+        _check(_load().b2_gnn_set_wait_limit(self._handle, int(polls)))
 
     def train_step(self, t, e, learning_rate: float = 1e-3) -> float:
         """One Adam step on the energy loss 1 - (c.t)^2 / ((c.Ac)(t.e)), c = G(t),

@@ -150,6 +150,29 @@ def test_forward_matches_torch(cuda, n_side):
 
 
 @pytest.mark.gpu
+def test_given_up_wait_reports_timeout_and_the_stage_recovers(cuda):
+    """The forward's bounded wait for each tile's MMA: with the first wait's
+    poll limit at 0 every tile gives up at once while its MMA is healthy.
+    Each block records the fault, waits for its MMA again with the full
+    bound, frees its tensor memory and returns, and the call raises
+    DeviceTimeout (B2_TIMEOUT). With the bound restored, the next call on the
+    same stage succeeds and gives the same result as before."""
+    import torch
+    s, a, g, r = _setup(n_side=9)
+    want = torch.zeros(s.n, device="cuda")
+    g.apply(r, want)
+    g.set_wait_limit(0)
+    z = torch.zeros(s.n, device="cuda")
+    with pytest.raises(L.DeviceTimeout):
+        g.apply(r, z)
+    g.set_wait_limit(-1)
+    again = torch.zeros(s.n, device="cuda")
+    g.apply(r, again)
+    torch.cuda.synchronize()
+    assert torch.equal(again, want)
+
+
+@pytest.mark.gpu
 def test_training_step_follows_torch_gradient(cuda):
     """One Adam step from zero moments moves every weight by about
     -lr sign(gradient): the signs of the CUDA step must be those of PyTorch's
