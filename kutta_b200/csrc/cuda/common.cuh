@@ -6,10 +6,47 @@
 // its explicit fma in the pair product is kept explicit here too).
 #pragma once
 
+#include <cstddef>
 #include <cstdint>
 #include <cuda_runtime.h>
+#include <utility>
 
 namespace kb2::dev {
+
+// ------------------------------------------------------------------------
+// Programmatic dependent launch. The solve is a chain of short dependent
+// kernels, each a few microseconds on these sizes, so the gap between one
+// kernel's end and the next one's start is a large share of the time. Every
+// solve-path kernel is launched with programmatic stream serialization: the
+// next kernel may be scheduled while the current one drains, and it waits
+// (griddepcontrol.wait, its very first instruction) until the previous grid
+// has completed and its memory is visible before touching any memory. So the
+// ordering of every read and write is exactly that of ordinary stream order;
+// only the launch latency overlaps. After its own wait a kernel lets its
+// dependents be scheduled.
+__device__ __forceinline__ void pdl_entry() {
+  asm volatile("griddepcontrol.wait;" ::: "memory");
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+// Whether launches carry the attribute (default yes; KUTTA_B200_PDL=0 turns it
+// off, for comparisons). Read once per process.
+bool pdl_enabled();
+// kernel<<<grid, block, smem, s>>>(args...) with the attribute.
+template <typename... Params, typename... Args>
+inline void pdl(void (*kernel)(Params...), dim3 grid, dim3 block, std::size_t smem,
+                cudaStream_t s, Args&&... args) {
+  cudaLaunchConfig_t config = {};
+  config.gridDim = grid;
+  config.blockDim = block;
+  config.dynamicSmemBytes = smem;
+  config.stream = s;
+  cudaLaunchAttribute attribute[1];
+  attribute[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attribute[0].val.programmaticStreamSerializationAllowed = 1;
+  config.attrs = attribute;
+  config.numAttrs = pdl_enabled() ? 1 : 0;
+  cudaLaunchKernelEx(&config, kernel, std::forward<Args>(args)...);
+}
 
 constexpr int kBlock = 256;          // threads per block for row kernels
 constexpr int kSms = 148;            // B200 streaming multiprocessors

@@ -11,8 +11,18 @@
 
 #include <algorithm>
 #include <atomic>
+#include <cstdlib>
 
 namespace kb2 {
+namespace dev {
+bool pdl_enabled() {
+  static const bool enabled = [] {
+    const char* v = std::getenv("KUTTA_B200_PDL");
+    return v == nullptr || v[0] != '0';
+  }();
+  return enabled;
+}
+}  // namespace dev
 namespace {
 using namespace dev;
 
@@ -136,6 +146,7 @@ __device__ __forceinline__ void finish(const Reducer& red, double a, double b, b
 __global__ void k_spmv(int n, const int* __restrict__ rows, const int* __restrict__ cols,
                        const float* __restrict__ vals, const float* __restrict__ x,
                        float* __restrict__ y, const int* __restrict__ status) {
+  pdl_entry();
   if (status && status[0] != 0) return;
   ROWS(i, n) {
     float sum = 0.0f, error = 0.0f;
@@ -151,6 +162,7 @@ __global__ void k_spmv_dot(int n, const int* __restrict__ rows, const int* __res
                            const float* __restrict__ vals, const float* __restrict__ p,
                            const float* __restrict__ w, float* __restrict__ q, DeviceReducer red,
                            float* scalars, int offset, int* status, Epilogue epi) {
+  pdl_entry();
   if (status[0] != 0) return;
   double acc = 0;
   ROWS(i, n) {
@@ -168,6 +180,7 @@ __global__ void k_residual(int n, const int* __restrict__ rows, const int* __res
                            const float* __restrict__ vals, const float* __restrict__ x,
                            const float* __restrict__ b, float* __restrict__ r,
                            const int* __restrict__ status) {
+  pdl_entry();
   if (status && status[0] != 0) return;
   ROWS(i, n) {
     float sum = b[i], error = 0.0f;
@@ -195,6 +208,7 @@ __global__ void k_smooth(int n, const int* __restrict__ rows, const int* __restr
                          const float* __restrict__ vals, const float* __restrict__ x,
                          const float* __restrict__ b, const float* __restrict__ inv,
                          float* __restrict__ next, const int* __restrict__ status) {
+  pdl_entry();
   if (status && status[0] != 0) return;
   ROWS(i, n) {
     if (kZero) {
@@ -220,6 +234,7 @@ __global__ void k_smooth_dot2(int n, const int* __restrict__ rows, const int* __
                               float* __restrict__ next, const float* __restrict__ q,
                               DeviceReducer red, float* scalars, int offset, int* status,
                               Epilogue epi) {
+  pdl_entry();
   if (status[0] != 0) return;
   double a = 0, c = 0;
   ROWS(i, n) {
@@ -240,6 +255,7 @@ __global__ void k_coarse_solve(int count, const int* __restrict__ rows,
                                float* __restrict__ x, const float* __restrict__ b,
                                const float* __restrict__ inv, const int* __restrict__ status,
                                int sweeps) {
+  pdl_entry();
   if (threadIdx.x != 0 || blockIdx.x != 0 || status[0] != 0) return;
   float current[24], r[24];
   for (int row = 0; row < count; ++row) current[row] = 0.0f;
@@ -260,6 +276,7 @@ __global__ void k_coarse_solve(int count, const int* __restrict__ rows,
 __global__ void k_diagonal(int n, const int* __restrict__ rows, const int* __restrict__ diag,
                            const float* __restrict__ vals, float* __restrict__ inverse,
                            int use_l1, DeviceReducer red, double* check, int slot) {
+  pdl_entry();
   double worst = 0;
   ROWS(i, n) worst = nan_max(worst, diagonal_row(i, rows, diag, vals, inverse, use_l1));
   __shared__ double shared[32];
@@ -278,6 +295,7 @@ __global__ void k_diagonal(int n, const int* __restrict__ rows, const int* __res
 __global__ void k_restrict(int nc, const int* __restrict__ offsets,
                            const int* __restrict__ members, const float* __restrict__ fine,
                            float* __restrict__ coarse, const int* __restrict__ status) {
+  pdl_entry();
   if (status[0] != 0) return;
   ROWS(g, nc) {
     float sum = 0.0f, error = 0.0f;
@@ -295,6 +313,7 @@ __global__ void k_restrict(int nc, const int* __restrict__ offsets,
 __global__ void k_prolong(int nf, const int* __restrict__ aggregate,
                           const float* __restrict__ coarse, float* __restrict__ fine,
                           const int* __restrict__ status) {
+  pdl_entry();
   if (status[0] != 0) return;
   ROWS(i, nf) {
     const int g = aggregate[i];
@@ -306,6 +325,7 @@ __global__ void k_prolong(int nf, const int* __restrict__ aggregate,
 __global__ void k_galerkin(int nnz_c, const int* __restrict__ offsets,
                            const int* __restrict__ entries, const float* __restrict__ fine,
                            float* __restrict__ coarse) {
+  pdl_entry();
   ROWS(e, nnz_c) {
     float sum = 0.0f, error = 0.0f;
     for (int j = offsets[e]; j < offsets[e + 1]; ++j) neumaier_term(sum, error, fine[entries[j]]);
@@ -321,6 +341,7 @@ __global__ void k_galerkin(int nnz_c, const int* __restrict__ offsets,
 // per-coarse-row chain shortens the dependent sequence of each thread.
 __global__ void k_row_surplus(int n, const int* __restrict__ rows, const int* __restrict__ diag,
                               const float* __restrict__ fine, float* __restrict__ surplus) {
+  pdl_entry();
   ROWS(i, n) {
     UpperSum sum{fine[diag[i]], 0.0f};
     for (int j = rows[i]; j < rows[i + 1]; ++j)
@@ -333,6 +354,7 @@ __global__ void k_m_matrix_combine(int nc, const int* __restrict__ offsets,
                                    const int* __restrict__ members,
                                    const float* __restrict__ surplus, const int* __restrict__ rows,
                                    const int* __restrict__ diag, float* coarse) {
+  pdl_entry();
   ROWS(g, nc) {
     UpperSum diagonal{0.0f, 0.0f};
     for (int m = offsets[g]; m < offsets[g + 1]; ++m)
@@ -348,6 +370,7 @@ __global__ void k_m_matrix_combine(int nc, const int* __restrict__ offsets,
 __global__ void k_pcg_step_dot(int n, float* __restrict__ x, float* __restrict__ r,
                                const float* __restrict__ p, const float* __restrict__ q,
                                DeviceReducer red, float* scalars, int* status) {
+  pdl_entry();
   if (status[0] != 0) return;
   const float alpha = kp_float(kp_load(scalars, 8));
   double acc = 0;
@@ -363,6 +386,7 @@ __global__ void k_pcg_step_dot(int n, float* __restrict__ x, float* __restrict__
 // solver_direction :128-131.
 __global__ void k_direction(int n, const float* __restrict__ z, float* __restrict__ p,
                             const float* __restrict__ scalars, const int* __restrict__ status) {
+  pdl_entry();
   if (status[0] != 0) return;
   const float beta = kp_float(kp_load(scalars, 10));
   ROWS(i, n) p[i] = z[i] + beta * p[i];
@@ -372,6 +396,7 @@ __global__ void k_direction(int n, const float* __restrict__ z, float* __restric
 __global__ void k_bicg_direction(int n, const float* __restrict__ r, const float* __restrict__ v,
                                  float* __restrict__ p, const float* __restrict__ scalars,
                                  const int* __restrict__ status) {
+  pdl_entry();
   if (status[0] != 0) return;
   const float beta = kp_float(kp_load(scalars, 10)), omega = kp_float(kp_load(scalars, 12));
   ROWS(i, n) p[i] = r[i] + beta * (p[i] - omega * v[i]);
@@ -381,6 +406,7 @@ __global__ void k_bicg_direction(int n, const float* __restrict__ r, const float
 __global__ void k_bicg_difference(int n, const float* __restrict__ r, const float* __restrict__ q,
                                   float* __restrict__ sv, const float* __restrict__ scalars,
                                   const int* __restrict__ status) {
+  pdl_entry();
   if (status[0] != 0) return;
   const float alpha = kp_float(kp_load(scalars, 8));
   ROWS(i, n) sv[i] = r[i] - alpha * q[i];
@@ -391,6 +417,7 @@ __global__ void k_bicg_step(int n, float* __restrict__ x, float* __restrict__ r,
                             const float* __restrict__ z, const float* __restrict__ zs,
                             const float* __restrict__ sv, const float* __restrict__ t,
                             const float* __restrict__ scalars, const int* __restrict__ status) {
+  pdl_entry();
   if (status[0] != 0) return;
   const float alpha = kp_float(kp_load(scalars, 8)), omega = kp_float(kp_load(scalars, 12));
   const bool s_only = status[2] != 0;
@@ -408,16 +435,19 @@ __global__ void k_bicg_step(int n, float* __restrict__ x, float* __restrict__ r,
 // krylov_multiply(_guarded), linalg.kern.h:72-75,119-122.
 __global__ void k_multiply(int n, const float* __restrict__ r, const float* __restrict__ inverse,
                            float* __restrict__ z, const int* __restrict__ status) {
+  pdl_entry();
   if (status && status[0] != 0) return;
   ROWS(i, n) z[i] = r[i] * inverse[i];
 }
 
 // axpy, blas.kern.h:5.
 __global__ void k_axpy(int n, float* __restrict__ y, const float* __restrict__ x, float a) {
+  pdl_entry();
   ROWS(i, n) y[i] = y[i] + a * x[i];
 }
 
-__global__ void k_fill(int n, float* __restrict__ x, float value) { ROWS(i, n) x[i] = value; }
+__global__ void k_fill(int n, float* __restrict__ x, float value) {
+  pdl_entry(); ROWS(i, n) x[i] = value; }
 
 // ---- reductions ---------------------------------------------------------------
 // Device::reduce_into (device.hpp:186-202) with FP64 accumulation.
@@ -425,6 +455,7 @@ __global__ void k_reduce_into(ReduceMode mode, int n, const float* __restrict__ 
                               const float* __restrict__ y, const float* __restrict__ u,
                               const float* __restrict__ v, DeviceReducer red, float* scalars,
                               int offset, int* status, bool guard, Epilogue epi) {
+  pdl_entry();
   if (guard && status[0] != 0) return;
   double a = 0, b = 0;
   const bool dual = mode == ReduceMode::Dot2;
@@ -440,6 +471,7 @@ __global__ void k_reduce_into(ReduceMode mode, int n, const float* __restrict__ 
 __global__ void k_reduce_value(ReduceMode mode, int n, const float* __restrict__ x,
                                const float* __restrict__ y, DeviceReducer red, double* out,
                                int slot) {
+  pdl_entry();
   __shared__ double shared[32];
   double a = 0;
   ROWS(i, n) {
@@ -459,6 +491,7 @@ __global__ void k_reduce_value(ReduceMode mode, int n, const float* __restrict__
 
 // solver_limits :51-55 (all 24 slots).
 __global__ void k_solver_limits(float* scalars, float th, float tl, float dh, float dl) {
+  pdl_entry();
   const int i = threadIdx.x;
   if (i < 24)
     scalars[i] = i == 20 ? th : (i == 21 ? tl : (i == 22 ? dh : (i == 23 ? dl : 0.0f)));
@@ -466,6 +499,7 @@ __global__ void k_solver_limits(float* scalars, float th, float tl, float dh, fl
 
 // solver_reset :56-62.
 __global__ void k_solver_reset(float* scalars, int* status, int iterations) {
+  pdl_entry();
   status[0] = 0;
   status[1] = iterations;
   status[2] = 0;
@@ -480,6 +514,7 @@ __global__ void k_solver_reset(float* scalars, int* status, int iterations) {
 // solver_project :150-152.
 __global__ void k_project(int n, float* __restrict__ x, const float* __restrict__ sum,
                           float count_hi, float count_lo) {
+  pdl_entry();
   const float mean = kp_float(kp_div(kp_load(sum, 0), kp(count_hi, count_lo)));
   ROWS(i, n) x[i] -= mean;
 }
@@ -489,6 +524,7 @@ __global__ void k_project(int n, float* __restrict__ x, const float* __restrict_
 // z.q, [6] b.b, [8] alpha, [10] beta. The level's status: 0 running, 1 keep the
 // accepted first correction, 2 fall back to the plain first cycle.
 __global__ void k_inner_alpha(float* scalars, int* status, const int* parent, int first) {
+  pdl_entry();
   if (first != 0) status[0] = parent[0] == 0 ? 0 : 2;
   if (status[0] != 0) return;
   const Pair denom = kp_load(scalars, 0);
@@ -504,6 +540,7 @@ __global__ void k_inner_first(int n, const float* __restrict__ b, const float* _
                               const float* __restrict__ q, float* __restrict__ x,
                               float* __restrict__ t, const float* __restrict__ scalars,
                               const int* __restrict__ status) {
+  pdl_entry();
   const bool running = status[0] == 0;
   const float alpha = kp_float(kp_load(scalars, 8));
   ROWS(i, n) {
@@ -514,11 +551,13 @@ __global__ void k_inner_first(int n, const float* __restrict__ b, const float* _
 
 // Adaptive exit: keep the first correction when |t|^2 <= |b|^2 / 16.
 __global__ void k_inner_check(const float* scalars, int* status) {
+  pdl_entry();
   if (status[0] != 0) return;
   if (kp_le(kp_load(scalars, 4), kp_mul(kp(0.0625f, 0.0f), kp_load(scalars, 6)))) status[0] = 1;
 }
 
 __global__ void k_inner_beta(float* scalars, int* status) {
+  pdl_entry();
   if (status[0] != 0) return;
   const Pair beta = kp_div(kp_neg(kp_load(scalars, 4)), kp_load(scalars, 0));
   if (!kp_coefficient(beta) || (kp_zero(beta) && !kp_zero(kp_load(scalars, 4))))
@@ -529,6 +568,7 @@ __global__ void k_inner_beta(float* scalars, int* status) {
 
 __global__ void k_inner_step(int n, float* __restrict__ x, const float* __restrict__ p,
                              const float* __restrict__ scalars, const int* __restrict__ status) {
+  pdl_entry();
   if (status[0] != 0) return;
   const float alpha = kp_float(kp_load(scalars, 8));
   ROWS(i, n) x[i] += alpha * p[i];
@@ -554,20 +594,20 @@ void spmv(int n, const int* rows, const int* cols, const float* vals, const floa
           const int* status, cudaStream_t s) {
   if (n <= 0) return;
   ++counter;
-  k_spmv<<<full_grid(n), kBlock, 0, s>>>(n, rows, cols, vals, x, y, status);
+  pdl(k_spmv, full_grid(n), kBlock, 0, s, n, rows, cols, vals, x, y, status);
 }
 void spmv_dot(int n, const int* rows, const int* cols, const float* vals, const float* p,
               const float* w, float* q, DeviceReducer red, float* scalars, int offset,
               int* status, Epilogue epi, cudaStream_t s) {
   ++counter;
-  k_spmv_dot<<<blocks(n), kBlock, 0, s>>>(n, rows, cols, vals, p, w, q, red, scalars, offset,
+  pdl(k_spmv_dot, blocks(n), kBlock, 0, s, n, rows, cols, vals, p, w, q, red, scalars, offset,
                                           status, epi);
 }
 void residual(int n, const int* rows, const int* cols, const float* vals, const float* x,
               const float* b, float* r, const int* status, cudaStream_t s) {
   if (n <= 0) return;
   ++counter;
-  k_residual<<<full_grid(n), kBlock, 0, s>>>(n, rows, cols, vals, x, b, r, status);
+  pdl(k_residual, full_grid(n), kBlock, 0, s, n, rows, cols, vals, x, b, r, status);
 }
 void smooth(int n, const int* rows, const int* cols, const float* vals, const float* x,
             const float* b, const float* inv, float* next, const int* status, bool zero_start,
@@ -575,150 +615,150 @@ void smooth(int n, const int* rows, const int* cols, const float* vals, const fl
   if (n <= 0) return;
   ++counter;
   if (zero_start)
-    k_smooth<true><<<full_grid(n), kBlock, 0, s>>>(n, rows, cols, vals, x, b, inv, next, status);
+    pdl(k_smooth<true>, full_grid(n), kBlock, 0, s, n, rows, cols, vals, x, b, inv, next, status);
   else
-    k_smooth<false><<<full_grid(n), kBlock, 0, s>>>(n, rows, cols, vals, x, b, inv, next, status);
+    pdl(k_smooth<false>, full_grid(n), kBlock, 0, s, n, rows, cols, vals, x, b, inv, next, status);
 }
 void smooth_dot2(int n, const int* rows, const int* cols, const float* vals, const float* x,
                  const float* b, const float* inv, float* next, const float* q, DeviceReducer red,
                  float* scalars, int offset, int* status, Epilogue epi, cudaStream_t s) {
   if (n <= 0) return;
   ++counter;
-  k_smooth_dot2<<<blocks(n), kBlock, 0, s>>>(n, rows, cols, vals, x, b, inv, next, q, red,
+  pdl(k_smooth_dot2, blocks(n), kBlock, 0, s, n, rows, cols, vals, x, b, inv, next, q, red,
                                              scalars, offset, status, epi);
 }
 void coarse_solve(int count, const int* rows, const int* cols, const float* vals, float* x,
                   const float* b, const float* inv, const int* status, int sweeps,
                   cudaStream_t s) {
   ++counter;
-  k_coarse_solve<<<1, 32, 0, s>>>(count, rows, cols, vals, x, b, inv, status, sweeps);
+  pdl(k_coarse_solve, 1, 32, 0, s, count, rows, cols, vals, x, b, inv, status, sweeps);
 }
 void diagonal(int n, const int* rows, const int* diag, const float* vals, float* inverse,
               int use_l1, DeviceReducer red, double* check, int slot, cudaStream_t s) {
   ++counter;
-  k_diagonal<<<blocks(n), kBlock, 0, s>>>(n, rows, diag, vals, inverse, use_l1, red, check, slot);
+  pdl(k_diagonal, blocks(n), kBlock, 0, s, n, rows, diag, vals, inverse, use_l1, red, check, slot);
 }
 void restrict_(int nc, const int* offsets, const int* members, const float* fine, float* coarse,
                const int* status, cudaStream_t s) {
   if (nc <= 0) return;
   ++counter;
-  k_restrict<<<blocks(nc), kBlock, 0, s>>>(nc, offsets, members, fine, coarse, status);
+  pdl(k_restrict, blocks(nc), kBlock, 0, s, nc, offsets, members, fine, coarse, status);
 }
 void prolong(int nf, const int* aggregate, const float* coarse, float* fine, const int* status,
              cudaStream_t s) {
   if (nf <= 0) return;
   ++counter;
-  k_prolong<<<blocks(nf), kBlock, 0, s>>>(nf, aggregate, coarse, fine, status);
+  pdl(k_prolong, blocks(nf), kBlock, 0, s, nf, aggregate, coarse, fine, status);
 }
 void galerkin(int nnz_c, const int* offsets, const int* entries, const float* fine, float* coarse,
               cudaStream_t s) {
   if (nnz_c <= 0) return;
   ++counter;
-  k_galerkin<<<blocks(nnz_c), kBlock, 0, s>>>(nnz_c, offsets, entries, fine, coarse);
+  pdl(k_galerkin, blocks(nnz_c), kBlock, 0, s, nnz_c, offsets, entries, fine, coarse);
 }
 void m_matrix_diagonal(int nf, int nc, const int* offsets, const int* members, const int* fine_rows,
                        const int* fine_diag, const float* fine, const int* rows, const int* diag,
                        float* coarse, float* surplus, cudaStream_t s) {
   if (nc <= 0) return;
   ++counter;
-  k_row_surplus<<<full_grid(nf), kBlock, 0, s>>>(nf, fine_rows, fine_diag, fine, surplus);
+  pdl(k_row_surplus, full_grid(nf), kBlock, 0, s, nf, fine_rows, fine_diag, fine, surplus);
   ++counter;
-  k_m_matrix_combine<<<full_grid(nc), kBlock, 0, s>>>(nc, offsets, members, surplus, rows, diag,
+  pdl(k_m_matrix_combine, full_grid(nc), kBlock, 0, s, nc, offsets, members, surplus, rows, diag,
                                                       coarse);
 }
 void pcg_step_dot(int n, float* x, float* r, const float* p, const float* q, DeviceReducer red,
                   float* scalars, int* status, cudaStream_t s) {
   ++counter;
-  k_pcg_step_dot<<<blocks(n), kBlock, 0, s>>>(n, x, r, p, q, red, scalars, status);
+  pdl(k_pcg_step_dot, blocks(n), kBlock, 0, s, n, x, r, p, q, red, scalars, status);
 }
 void direction(int n, const float* z, float* p, const float* scalars, const int* status,
                cudaStream_t s) {
   if (n <= 0) return;
   ++counter;
-  k_direction<<<blocks(n), kBlock, 0, s>>>(n, z, p, scalars, status);
+  pdl(k_direction, blocks(n), kBlock, 0, s, n, z, p, scalars, status);
 }
 void bicg_direction(int n, const float* r, const float* v, float* p, const float* scalars,
                     const int* status, cudaStream_t s) {
   if (n <= 0) return;
   ++counter;
-  k_bicg_direction<<<blocks(n), kBlock, 0, s>>>(n, r, v, p, scalars, status);
+  pdl(k_bicg_direction, blocks(n), kBlock, 0, s, n, r, v, p, scalars, status);
 }
 void bicg_difference(int n, const float* r, const float* q, float* sv, const float* scalars,
                      const int* status, cudaStream_t s) {
   if (n <= 0) return;
   ++counter;
-  k_bicg_difference<<<blocks(n), kBlock, 0, s>>>(n, r, q, sv, scalars, status);
+  pdl(k_bicg_difference, blocks(n), kBlock, 0, s, n, r, q, sv, scalars, status);
 }
 void bicg_step(int n, float* x, float* r, const float* z, const float* zs, const float* sv,
                const float* t, const float* scalars, const int* status, cudaStream_t s) {
   if (n <= 0) return;
   ++counter;
-  k_bicg_step<<<blocks(n), kBlock, 0, s>>>(n, x, r, z, zs, sv, t, scalars, status);
+  pdl(k_bicg_step, blocks(n), kBlock, 0, s, n, x, r, z, zs, sv, t, scalars, status);
 }
 void multiply(int n, const float* r, const float* inverse, float* z, const int* status,
               cudaStream_t s) {
   if (n <= 0) return;
   ++counter;
-  k_multiply<<<blocks(n), kBlock, 0, s>>>(n, r, inverse, z, status);
+  pdl(k_multiply, blocks(n), kBlock, 0, s, n, r, inverse, z, status);
 }
 void axpy(int n, float* y, const float* x, float a, cudaStream_t s) {
   if (n <= 0) return;
   ++counter;
-  k_axpy<<<blocks(n), kBlock, 0, s>>>(n, y, x, a);
+  pdl(k_axpy, blocks(n), kBlock, 0, s, n, y, x, a);
 }
 void fill(int n, float* x, float value, cudaStream_t s) {
   if (n <= 0) return;
   ++counter;
-  k_fill<<<blocks(n), kBlock, 0, s>>>(n, x, value);
+  pdl(k_fill, blocks(n), kBlock, 0, s, n, x, value);
 }
 void reduce_into(ReduceMode mode, int n, const float* x, const float* y, const float* u,
                  const float* v, DeviceReducer red, float* scalars, int offset, int* status,
                  bool guard, Epilogue epi, cudaStream_t s) {
   ++counter;
-  k_reduce_into<<<blocks(n), kBlock, 0, s>>>(mode, n, x, y, u, v, red, scalars, offset, status,
+  pdl(k_reduce_into, blocks(n), kBlock, 0, s, mode, n, x, y, u, v, red, scalars, offset, status,
                                              guard, epi);
 }
 void reduce_value(ReduceMode mode, int n, const float* x, const float* y, DeviceReducer red,
                   double* out, int slot, cudaStream_t s) {
   ++counter;
-  k_reduce_value<<<blocks(n), kBlock, 0, s>>>(mode, n, x, y, red, out, slot);
+  pdl(k_reduce_value, blocks(n), kBlock, 0, s, mode, n, x, y, red, out, slot);
 }
 void solver_limits(float* scalars, float th, float tl, float dh, float dl, cudaStream_t s) {
   ++counter;
-  k_solver_limits<<<1, 32, 0, s>>>(scalars, th, tl, dh, dl);
+  pdl(k_solver_limits, 1, 32, 0, s, scalars, th, tl, dh, dl);
 }
 void solver_reset(float* scalars, int* status, int iterations, cudaStream_t s) {
   ++counter;
-  k_solver_reset<<<1, 1, 0, s>>>(scalars, status, iterations);
+  pdl(k_solver_reset, 1, 1, 0, s, scalars, status, iterations);
 }
 void project(int n, float* x, const float* sum, float count_hi, float count_lo, cudaStream_t s) {
   if (n <= 0) return;
   ++counter;
-  k_project<<<blocks(n), kBlock, 0, s>>>(n, x, sum, count_hi, count_lo);
+  pdl(k_project, blocks(n), kBlock, 0, s, n, x, sum, count_hi, count_lo);
 }
 void inner_alpha(float* scalars, int* status, const int* parent, int first, cudaStream_t s) {
   ++counter;
-  k_inner_alpha<<<1, 1, 0, s>>>(scalars, status, parent, first);
+  pdl(k_inner_alpha, 1, 1, 0, s, scalars, status, parent, first);
 }
 void inner_first(int n, const float* b, const float* p, const float* q, float* x, float* t,
                  const float* scalars, const int* status, cudaStream_t s) {
   if (n <= 0) return;
   ++counter;
-  k_inner_first<<<blocks(n), kBlock, 0, s>>>(n, b, p, q, x, t, scalars, status);
+  pdl(k_inner_first, blocks(n), kBlock, 0, s, n, b, p, q, x, t, scalars, status);
 }
 void inner_check(const float* scalars, int* status, cudaStream_t s) {
   ++counter;
-  k_inner_check<<<1, 1, 0, s>>>(scalars, status);
+  pdl(k_inner_check, 1, 1, 0, s, scalars, status);
 }
 void inner_beta(float* scalars, int* status, cudaStream_t s) {
   ++counter;
-  k_inner_beta<<<1, 1, 0, s>>>(scalars, status);
+  pdl(k_inner_beta, 1, 1, 0, s, scalars, status);
 }
 void inner_step(int n, float* x, const float* p, const float* scalars, const int* status,
                 cudaStream_t s) {
   if (n <= 0) return;
   ++counter;
-  k_inner_step<<<blocks(n), kBlock, 0, s>>>(n, x, p, scalars, status);
+  pdl(k_inner_step, blocks(n), kBlock, 0, s, n, x, p, scalars, status);
 }
 
 }  // namespace launch

@@ -29,6 +29,7 @@ __device__ __forceinline__ float bf(unsigned short v) {
 // Row scale = max |a_ij| (FP32); stored value = bf16(a_ij / scale).
 __global__ void k_bf16_pack(int n, const int* __restrict__ rows, const float* __restrict__ vals,
                             unsigned short* __restrict__ v16, float* __restrict__ scale) {
+  pdl_entry();
   ROWS(i, n) {
     float m = 0.0f;
     for (int j = rows[i]; j < rows[i + 1]; ++j) m = fmaxf(m, fabsf(vals[j]));
@@ -106,6 +107,7 @@ __global__ void k_bf16_smooth(int n, const int* __restrict__ rows, const int* __
                               const float* __restrict__ scale, const float* __restrict__ x,
                               const float* __restrict__ b, const float* __restrict__ inv,
                               float* __restrict__ next, const int* __restrict__ status) {
+  pdl_entry();
   if (status[0] != 0) return;
   if (kZero) {
     ROWS(i, n) next[i] = (2.0f / 3.0f) * inv[i] * b[i];
@@ -122,6 +124,7 @@ __global__ void k_bf16_residual(int n, const int* __restrict__ rows, const int* 
                                 const float* __restrict__ scale, const float* __restrict__ x,
                                 const float* __restrict__ b, float* __restrict__ r,
                                 const int* __restrict__ status) {
+  pdl_entry();
   if (status[0] != 0) return;
   for_rows(n, [&](int i, int lane, bool valid) {
     const float acc = row_total(valid ? bf16_row_part(i, lane, rows, cols, v16, x) : 0.0f);
@@ -134,6 +137,7 @@ __global__ void k_bf16_residual(int n, const int* __restrict__ rows, const int* 
 __global__ void k_restrict_lanes(int nc, const int* __restrict__ offsets,
                                  const int* __restrict__ members, const float* __restrict__ fine,
                                  float* __restrict__ coarse, const int* __restrict__ status) {
+  pdl_entry();
   if (status[0] != 0) return;
   for_rows(nc, [&](int g, int lane, bool valid) {
     float acc = 0.0f;
@@ -183,6 +187,7 @@ __global__ void k_bf16_spmv_dot2(int n, const int* __restrict__ rows, const int*
                                  const float* __restrict__ w, float* __restrict__ q, bool gcr,
                                  DeviceReducer red, float* scalars,
                                  const int* __restrict__ status) {
+  pdl_entry();
   if (status[0] != 0) return;
   double a = 0.0, b = 0.0;
   for_rows(n, [&](int i, int lane, bool valid) {
@@ -206,6 +211,7 @@ __global__ void k_inner_first_dot(int n, const float* __restrict__ b, const floa
                                   const float* __restrict__ q, float* __restrict__ x,
                                   float* __restrict__ t, float* scalars,
                                   const int* __restrict__ status, DeviceReducer red) {
+  pdl_entry();
   const bool running = status[0] == 0;
   const float alpha = kp_float(kp_load(scalars, 8));
   double tt = 0.0, bb = 0.0;
@@ -231,6 +237,7 @@ __global__ void __launch_bounds__(1024)
     k_dense_inverse(int n, const int* __restrict__ rows, const int* __restrict__ cols,
                     const float* __restrict__ vals, double* __restrict__ L,
                     double* __restrict__ W, double* error, double* ratio) {
+  pdl_entry();
   const int t = threadIdx.x, T = blockDim.x;
   __shared__ int failed;
   __shared__ double smallest;
@@ -312,6 +319,7 @@ __global__ void __launch_bounds__(kDenseThreads)
     k_dense_inverse_shared(int n, const int* __restrict__ rows, const int* __restrict__ cols,
                            const float* __restrict__ vals, double* __restrict__ W, double* error,
                            double* ratio) {
+  pdl_entry();
   extern __shared__ double dense[];
   double* Ls = dense;          // n x n, lower triangle
   double* Xs = dense + n * n;  // n x n, X = L^-1 (lower triangle)
@@ -400,6 +408,7 @@ __global__ void __launch_bounds__(kPackedThreads)
     k_dense_inverse_packed(int n, const int* __restrict__ rows, const int* __restrict__ cols,
                            const float* __restrict__ vals, double* __restrict__ W, double* error,
                            double* ratio) {
+  pdl_entry();
   extern __shared__ double dense[];
   const int total = n * (n + 1) / 2;
   double* P = dense;           // packed lower triangle: L, then X = L^-1
@@ -475,6 +484,7 @@ __global__ void __launch_bounds__(kPackedThreads)
 // x = A^-1 b with the dense FP64 inverse: one warp per row, FP64 accumulation.
 __global__ void k_dense_solve(int n, const double* __restrict__ W, const float* __restrict__ b,
                               float* __restrict__ x, const int* __restrict__ status) {
+  pdl_entry();
   if (status[0] != 0) return;
   const int lane = threadIdx.x & 31;
   const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
@@ -494,6 +504,7 @@ __global__ void k_residual64(int n, const int* __restrict__ rows, const int* __r
                              const float* __restrict__ vals, const double* __restrict__ x,
                              const float* __restrict__ b, float* __restrict__ rf,
                              DeviceReducer red, double* out, int slot) {
+  pdl_entry();
   double acc = 0.0;
   ROWS(i, n) {
     double s = static_cast<double>(b[i]);
@@ -514,14 +525,17 @@ __global__ void k_residual64(int n, const int* __restrict__ rows, const int* __r
 }
 
 __global__ void k_update64(int n, double* __restrict__ x, const float* __restrict__ e) {
+  pdl_entry();
   ROWS(i, n) x[i] += static_cast<double>(e[i]);
 }
 
 __global__ void k_widen(int n, const float* __restrict__ x, double* __restrict__ y) {
+  pdl_entry();
   ROWS(i, n) y[i] = static_cast<double>(x[i]);
 }
 
 __global__ void k_narrow(int n, const double* __restrict__ y, float* __restrict__ x) {
+  pdl_entry();
   ROWS(i, n) x[i] = static_cast<float>(y[i]);
 }
 
@@ -546,7 +560,7 @@ void bf16_pack(int n, const int* rows, const float* vals, unsigned short* v16, f
                cudaStream_t s) {
   if (n <= 0) return;
   ++counter;
-  k_bf16_pack<<<rows_grid(n), kBlock, 0, s>>>(n, rows, vals, v16, scale);
+  pdl(k_bf16_pack, rows_grid(n), kBlock, 0, s, n, rows, vals, v16, scale);
 }
 void bf16_smooth(int n, const int* rows, const int* cols, const unsigned short* v16,
                  const float* scale, const float* x, const float* b, const float* inv, float* next,
@@ -554,15 +568,15 @@ void bf16_smooth(int n, const int* rows, const int* cols, const unsigned short* 
   if (n <= 0) return;
   ++counter;
   if (zero_start)
-    k_bf16_smooth<true><<<rows_grid(n), kBlock, 0, s>>>(n, rows, cols, v16, scale, x, b, inv, next, status);
+    pdl(k_bf16_smooth<true>, rows_grid(n), kBlock, 0, s, n, rows, cols, v16, scale, x, b, inv, next, status);
   else
-    k_bf16_smooth<false><<<lanes_grid(n, false), kBlock, 0, s>>>(n, rows, cols, v16, scale, x, b, inv, next, status);
+    pdl(k_bf16_smooth<false>, lanes_grid(n, false), kBlock, 0, s, n, rows, cols, v16, scale, x, b, inv, next, status);
 }
 void restrict_lanes(int nc, const int* offsets, const int* members, const float* fine,
                     float* coarse, const int* status, cudaStream_t s) {
   if (nc <= 0) return;
   ++counter;
-  k_restrict_lanes<<<lanes_grid(nc, false), kBlock, 0, s>>>(nc, offsets, members, fine, coarse,
+  pdl(k_restrict_lanes, lanes_grid(nc, false), kBlock, 0, s, nc, offsets, members, fine, coarse,
                                                             status);
 }
 void bf16_spmv_dot2(int n, const int* rows, const int* cols, const unsigned short* v16,
@@ -570,21 +584,21 @@ void bf16_spmv_dot2(int n, const int* rows, const int* cols, const unsigned shor
                     DeviceReducer red, float* scalars, const int* status, cudaStream_t s) {
   if (n <= 0) return;
   ++counter;
-  k_bf16_spmv_dot2<<<lanes_grid(n, true), kBlock, 0, s>>>(n, rows, cols, v16, scale, p, w, q,
+  pdl(k_bf16_spmv_dot2, lanes_grid(n, true), kBlock, 0, s, n, rows, cols, v16, scale, p, w, q,
                                                           gcr, red, scalars, status);
 }
 void inner_first_dot(int n, const float* b, const float* p, const float* q, float* x, float* t,
                      float* scalars, const int* status, DeviceReducer red, cudaStream_t s) {
   if (n <= 0) return;
   ++counter;
-  k_inner_first_dot<<<grid_for(n), kBlock, 0, s>>>(n, b, p, q, x, t, scalars, status, red);
+  pdl(k_inner_first_dot, grid_for(n), kBlock, 0, s, n, b, p, q, x, t, scalars, status, red);
 }
 void bf16_residual(int n, const int* rows, const int* cols, const unsigned short* v16,
                    const float* scale, const float* x, const float* b, float* r, const int* status,
                    cudaStream_t s) {
   if (n <= 0) return;
   ++counter;
-  k_bf16_residual<<<lanes_grid(n, false), kBlock, 0, s>>>(n, rows, cols, v16, scale, x, b, r,
+  pdl(k_bf16_residual, lanes_grid(n, false), kBlock, 0, s, n, rows, cols, v16, scale, x, b, r,
                                                           status);
 }
 void dense_inverse(int n, const int* rows, const int* cols, const float* vals, double* lower,
@@ -596,7 +610,7 @@ void dense_inverse(int n, const int* rows, const int* cols, const float* vals, d
     static std::atomic<unsigned long long> raised{0};
     raise_shared_limit(reinterpret_cast<const void*>(k_dense_inverse_shared),
                        2 * kSharedDense * kSharedDense * static_cast<int>(sizeof(double)), raised);
-    k_dense_inverse_shared<<<1, kDenseThreads, bytes, s>>>(n, rows, cols, vals, inverse, error,
+    pdl(k_dense_inverse_shared, 1, kDenseThreads, bytes, s, n, rows, cols, vals, inverse, error,
                                                             ratio);
     return;
   }
@@ -607,40 +621,40 @@ void dense_inverse(int n, const int* rows, const int* cols, const float* vals, d
         reinterpret_cast<const void*>(k_dense_inverse_packed),
         (kPackedDense * (kPackedDense + 1) / 2 + 2 * kPackedDense) * static_cast<int>(sizeof(double)),
         raised_packed);
-    k_dense_inverse_packed<<<1, kPackedThreads, bytes, s>>>(n, rows, cols, vals, inverse, error,
+    pdl(k_dense_inverse_packed, 1, kPackedThreads, bytes, s, n, rows, cols, vals, inverse, error,
                                                             ratio);
     return;
   }
   const int threads = std::min(1024, ((n + 31) / 32) * 32);
-  k_dense_inverse<<<1, threads, 0, s>>>(n, rows, cols, vals, lower, inverse, error, ratio);
+  pdl(k_dense_inverse, 1, threads, 0, s, n, rows, cols, vals, lower, inverse, error, ratio);
 }
 void dense_solve(int n, const double* inverse, const float* b, float* x, const int* status,
                  cudaStream_t s) {
   if (n <= 0) return;
   ++counter;
   const int blocks = std::min(1184, (n * 32 + kBlock - 1) / kBlock);
-  k_dense_solve<<<blocks, kBlock, 0, s>>>(n, inverse, b, x, status);
+  pdl(k_dense_solve, blocks, kBlock, 0, s, n, inverse, b, x, status);
 }
 void residual64(int n, const int* rows, const int* cols, const float* vals, const double* x,
                 const float* b, float* rf, DeviceReducer red, double* out, int slot,
                 cudaStream_t s) {
   ++counter;
-  k_residual64<<<grid_for(n), kBlock, 0, s>>>(n, rows, cols, vals, x, b, rf, red, out, slot);
+  pdl(k_residual64, grid_for(n), kBlock, 0, s, n, rows, cols, vals, x, b, rf, red, out, slot);
 }
 void update64(int n, double* x, const float* e, cudaStream_t s) {
   if (n <= 0) return;
   ++counter;
-  k_update64<<<rows_grid(n), kBlock, 0, s>>>(n, x, e);
+  pdl(k_update64, rows_grid(n), kBlock, 0, s, n, x, e);
 }
 void widen(int n, const float* x, double* y, cudaStream_t s) {
   if (n <= 0) return;
   ++counter;
-  k_widen<<<rows_grid(n), kBlock, 0, s>>>(n, x, y);
+  pdl(k_widen, rows_grid(n), kBlock, 0, s, n, x, y);
 }
 void narrow(int n, const double* y, float* x, cudaStream_t s) {
   if (n <= 0) return;
   ++counter;
-  k_narrow<<<rows_grid(n), kBlock, 0, s>>>(n, y, x);
+  pdl(k_narrow, rows_grid(n), kBlock, 0, s, n, y, x);
 }
 
 }  // namespace launch

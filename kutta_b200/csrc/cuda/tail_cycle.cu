@@ -152,6 +152,7 @@ __device__ void dense_solve(float* shared, const TailLevel& l, const double* W, 
 
 __global__ void __launch_bounds__(kTailThreads)
     k_tail_cycle(const __grid_constant__ TailPlan p, const int* __restrict__ status) {
+  dev::pdl_entry();
   // Uniform across the cluster: nothing else writes status while this runs.
   if (status[0] != 0) return;
   cg::cluster_group cluster = cg::this_cluster();
@@ -248,8 +249,11 @@ cudaLaunchConfig_t config_for(const TailPlan& p, cudaLaunchAttribute* attr, cuda
   attr[0].val.clusterDim.x = static_cast<unsigned>(p.cluster);
   attr[0].val.clusterDim.y = 1;
   attr[0].val.clusterDim.z = 1;
+  // Programmatic dependent launch, as for every solve-path kernel (common.cuh).
+  attr[1].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[1].val.programmaticStreamSerializationAllowed = 1;
   c.attrs = attr;
-  c.numAttrs = 1;
+  c.numAttrs = dev::pdl_enabled() ? 2 : 1;
   return c;
 }
 
@@ -265,7 +269,7 @@ bool tail_cluster_fits(int cluster, int smem_bytes) {
   TailPlan probe{};
   probe.cluster = cluster;
   probe.smem_bytes = smem_bytes;
-  cudaLaunchAttribute attr[1];
+  cudaLaunchAttribute attr[2];
   cudaLaunchConfig_t c = config_for(probe, attr, nullptr);
   int count = 0;
   if (cudaOccupancyMaxActiveClusters(&count, k_tail_cycle, &c) == cudaSuccess && count > 0)
@@ -276,7 +280,7 @@ bool tail_cluster_fits(int cluster, int smem_bytes) {
 
 void tail_cycle(const TailPlan& plan, const int* status, cudaStream_t s) {
   ++counter;
-  cudaLaunchAttribute attr[1];
+  cudaLaunchAttribute attr[2];
   cudaLaunchConfig_t c = config_for(plan, attr, s);
   cudaLaunchKernelEx(&c, k_tail_cycle, plan, status);
 }

@@ -26,7 +26,7 @@ def _args(name, size):
     for a in L._SIGNATURES[name][1]:
         if a is ctypes.c_float:
             out.append(0.5)
-        elif a in (ctypes.c_int, ctypes.c_size_t, ctypes.c_uint64):
+        elif a in (ctypes.c_int, ctypes.c_size_t, ctypes.c_uint64, ctypes.c_longlong):
             out.append(size)
         else:
             out.append(None)
