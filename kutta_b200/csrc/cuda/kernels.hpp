@@ -159,7 +159,7 @@ void narrow(int n, const double* y, float* x, cudaStream_t s);
 constexpr int kMaxTailLevels = 8;
 constexpr int kTailSharedBytes = 200 * 1024;  // dynamic shared memory per CTA, at most
 struct TailLevel {
-  int n, shift;
+  int n, shift;  // rows; each CTA owns the rows [rank << shift, (rank + 1) << shift)
   const int* rows;
   const int* cols;
   const unsigned short* v16;
@@ -169,13 +169,15 @@ struct TailLevel {
   const int* aggregate;
   const int* offsets;
   const int* members;
-  float* xg;
-  float* rg;
-  float* bg;
+  float* xg;  // first tail level: the result (global memory)
+  float* bg;  // first tail level: the right-hand side (global memory)
+  // Float offsets into each CTA's dynamic shared memory: full copies of the
+  // iterate and of the spare vector (residual, or the next sweep's iterate),
+  // n each, and the owned chunk of the right-hand side (1 << shift).
+  int xs, rs, bs;
 };
 struct TailPlan {
   int levels, pre, post, coarse_sweeps, cluster, smem_bytes;
-  int gathered, solution;  // shared offsets of the dense coarsest b and x (n each)
   const double* dense;     // coarsest dense FP64 inverse, or null for sweeps
   TailLevel level[kMaxTailLevels];
 };

@@ -7,18 +7,21 @@
 // 1024 threads where the device allows, else 8) runs the whole V-cycle of
 // those levels, with a cluster barrier between dependent steps.
 //
-// Each CTA owns a power-of-two chunk of rows per level. The level vectors stay
-// in global memory, where they are L2-resident: values written during the
-// launch are read with L2-only loads, which keeps them coherent across the
-// cluster's SMs (for these scattered gathers L2 measured faster than reading
-// other CTAs' shared memory), while the operators, constant during the launch,
-// are read through the read-only cache, where a CTA's rows stay between steps.
+// Each CTA owns a power-of-two chunk of rows per level and keeps, in its own
+// shared memory, a full copy of every level vector that rows gather from (the
+// iterate, and the residual the restriction sums). A step computes the owned
+// rows from the local copies and pushes each new value into every CTA's copy
+// with distributed-shared-memory stores; the cluster barrier that follows
+// makes them visible. So every gather is a local shared-memory read, and the
+// only traffic between SMs is one posted store per row and CTA per step. The
+// operators, constant during the launch, are read through the read-only
+// cache; each CTA reads only its own rows of them.
 //
-// Steps are merged where no neighbour value is needed: the zero-start sweep of
-// a level is done by whoever writes its right-hand side (the first step, or
-// the restriction), and every CTA solves the dense coarsest level itself, so
-// the prolongation from it reads the correction from the CTA's own shared
-// memory.
+// The first tail level's right-hand side comes from global memory and its
+// result goes back there; nothing else in between leaves the cluster. The
+// zero-start sweep of a level is done by whoever writes its right-hand side
+// (the first step, or the restriction), and every CTA solves the dense
+// coarsest level itself, so its solution needs no exchange.
 #include <cooperative_groups.h>
 #include <cuda_bf16.h>
 
@@ -50,10 +53,10 @@ __device__ __forceinline__ Rows owned(const TailLevel& l, int rank) {
   return Rows{base, max(0, min(1 << l.shift, l.n - base))};
 }
 
-// sum_j a_ij x_j of row i with the BF16 operator (without the row scale). The
-// entries are taken eight at a time, their neighbour values all requested
-// before any is used, so a thread keeps several loads in flight.
-__device__ __forceinline__ float row_product(const TailLevel& l, const float* x, int i) {
+// sum_j a_ij v_j of row i with the BF16 operator (without the row scale), v
+// a full copy in this CTA's shared memory. The entries are taken eight at a
+// time, their columns and values all requested before any is used.
+__device__ __forceinline__ float row_product(const TailLevel& l, const float* v, int i) {
   float acc = 0.0f;
   const int end = __ldg(l.rows + i + 1);
   for (int j0 = __ldg(l.rows + i); j0 < end; j0 += kBatch) {
@@ -64,90 +67,33 @@ __device__ __forceinline__ float row_product(const TailLevel& l, const float* x,
       c[u] = j0 + u < end ? __ldg(l.cols + j0 + u) : -1;
       a[u] = j0 + u < end ? bf(__ldg(l.v16 + j0 + u)) : 0.0f;
     }
-    float v[kBatch];
 #pragma unroll
-    for (int u = 0; u < kBatch; ++u) v[u] = c[u] >= 0 ? __ldcg(x + c[u]) : 0.0f;
-#pragma unroll
-    for (int u = 0; u < kBatch; ++u) acc = fmaf(a[u], v[u], acc);
+    for (int u = 0; u < kBatch; ++u) acc = fmaf(a[u], c[u] >= 0 ? v[c[u]] : 0.0f, acc);
   }
   return acc;
 }
 
-// next = x + omega inv (b - A x) on the owned rows.
-__device__ void sweep(const TailLevel& l, int rank, const float* x, float* next) {
+// Row i's value into every CTA's copy of the vector at shared offset `at`
+// (this CTA's own included). Visible to all after the next cluster barrier.
+__device__ __forceinline__ void push(cg::cluster_group& cluster, float* shared, int at, int i,
+                                     float v, int size) {
+  for (int d = 0; d < size; ++d) *cluster.map_shared_rank(shared + at + i, d) = v;
+}
+
+// One damped L1-Jacobi sweep of the owned rows, x read from the local copy at
+// `from`: the new values pushed to every copy at `to`, or, on the final sweep
+// of the first tail level, written to global memory.
+__device__ void sweep(cg::cluster_group& cluster, float* shared, const TailLevel& l, int rank,
+                      int size, int from, int to, bool final) {
   const Rows own = owned(l, rank);
+  const float* x = shared + from;
   for (int k = threadIdx.x; k < own.count; k += blockDim.x) {
     const int i = own.base + k;
-    const float r = __ldcg(l.bg + i) - __ldg(l.scale + i) * row_product(l, x, i);
-    __stcg(next + i, __ldcg(x + i) + kOmega * __ldg(l.inv + i) * r);
+    const float r = shared[l.bs + k] - __ldg(l.scale + i) * row_product(l, x, i);
+    const float next = x[i] + kOmega * __ldg(l.inv + i) * r;
+    if (final) __stcg(l.xg + i, next);
+    else push(cluster, shared, to, i, next, size);
   }
-}
-
-__device__ void residual(const TailLevel& l, int rank, const float* x, float* r) {
-  const Rows own = owned(l, rank);
-  for (int k = threadIdx.x; k < own.count; k += blockDim.x) {
-    const int i = own.base + k;
-    __stcg(r + i, __ldcg(l.bg + i) - __ldg(l.scale + i) * row_product(l, x, i));
-  }
-}
-
-// Coarse b = Kahan sum of the fine residual over each aggregate's members, in
-// member order; with `zero`, also the coarse zero-start sweep x = omega inv b.
-__device__ void restrict_to(const TailLevel& fine, const float* r, const TailLevel& coarse,
-                            float* coarse_x, bool zero, int rank) {
-  const Rows own = owned(coarse, rank);
-  for (int k = threadIdx.x; k < own.count; k += blockDim.x) {
-    const int g = own.base + k;
-    float sum = 0.0f, error = 0.0f;
-    const int end = __ldg(fine.offsets + g + 1);
-    for (int j0 = __ldg(fine.offsets + g); j0 < end; j0 += kBatch) {
-      int m[kBatch];
-#pragma unroll
-      for (int u = 0; u < kBatch; ++u) m[u] = j0 + u < end ? __ldg(fine.members + j0 + u) : -1;
-      float v[kBatch];
-#pragma unroll
-      for (int u = 0; u < kBatch; ++u) v[u] = m[u] >= 0 ? __ldcg(r + m[u]) : 0.0f;
-#pragma unroll
-      for (int u = 0; u < kBatch; ++u) {
-        if (m[u] < 0) break;
-        const float term = v[u] - error;
-        const float next = sum + term;
-        error = (next - sum) - term;
-        sum = next;
-      }
-    }
-    __stcg(coarse.bg + g, sum);
-    if (zero) __stcg(coarse_x + g, kOmega * __ldg(coarse.inv + g) * sum);
-  }
-}
-
-// x += e[aggregate] on the owned rows; e in global memory or, for the dense
-// coarsest, in this CTA's shared memory.
-__device__ void prolong(const TailLevel& fine, float* x, const float* e, bool e_shared, int rank) {
-  const Rows own = owned(fine, rank);
-  for (int k = threadIdx.x; k < own.count; k += blockDim.x) {
-    const int i = own.base + k;
-    const int g = __ldg(fine.aggregate + i);
-    if (g >= 0) __stcg(x + i, __ldcg(x + i) + (e_shared ? e[g] : __ldcg(e + g)));
-  }
-}
-
-// The whole coarsest solution x = W b with the dense FP64 inverse, into this
-// CTA's shared memory (every CTA computes it): b gathered first, then a warp
-// per row.
-__device__ void dense_solve(float* shared, const TailLevel& l, const double* W, int gathered,
-                            int solution) {
-  for (int k = threadIdx.x; k < l.n; k += blockDim.x) shared[gathered + k] = __ldcg(l.bg + k);
-  __syncthreads();
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, warps = blockDim.x >> 5;
-  for (int i = warp; i < l.n; i += warps) {
-    const double* row = W + static_cast<std::size_t>(i) * l.n;
-    double acc = 0.0;
-    for (int c = lane; c < l.n; c += 32) acc += row[c] * static_cast<double>(shared[gathered + c]);
-    for (int d = 16; d > 0; d >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, d);
-    if (lane == 0) shared[solution + i] = static_cast<float>(acc);
-  }
-  __syncthreads();
 }
 
 __global__ void __launch_bounds__(kTailThreads)
@@ -158,74 +104,131 @@ __global__ void __launch_bounds__(kTailThreads)
   cg::cluster_group cluster = cg::this_cluster();
   extern __shared__ float shared[];
   const int rank = static_cast<int>(cluster.block_rank());
+  const int size = static_cast<int>(cluster.num_blocks());
   const int last = p.levels - 1;
   const bool dense = p.dense != nullptr;
-  // Current iterate and spare buffer of each level (uniform across threads).
-  float* x[kMaxTailLevels];
-  float* spare[kMaxTailLevels];
+  // Shared offsets of each level's current iterate copy and of its spare copy
+  // (the residual, or the next sweep's iterate). Uniform across the cluster.
+  int x[kMaxTailLevels], spare[kMaxTailLevels];
   for (int l = 0; l < p.levels; ++l) {
-    x[l] = p.level[l].xg;
-    spare[l] = p.level[l].rg;
-  }
-  // The first tail level swaps roles (pre - 1) + post times; start so that its
-  // result ends in xg, the buffer the caller reads.
-  if (((p.pre - 1 + p.post) & 1) != 0) {
-    x[0] = p.level[0].rg;
-    spare[0] = p.level[0].xg;
+    x[l] = p.level[l].xs;
+    spare[l] = p.level[l].rs;
   }
   {
-    // Zero-start sweep of the first tail level from its right-hand side.
+    // The first tail level's right-hand side (owned rows) and its zero-start
+    // sweep.
     const TailLevel& L = p.level[0];
     const Rows own = owned(L, rank);
     for (int k = threadIdx.x; k < own.count; k += blockDim.x) {
       const int i = own.base + k;
-      __stcg(x[0] + i, kOmega * __ldg(L.inv + i) * __ldcg(L.bg + i));
+      const float b = __ldcg(L.bg + i);
+      shared[L.bs + k] = b;
+      push(cluster, shared, x[0], i, kOmega * __ldg(L.inv + i) * b, size);
     }
   }
   cluster.sync();
   for (int l = 0; l < last; ++l) {
     const TailLevel& L = p.level[l];
     for (int s = 1; s < p.pre; ++s) {
-      sweep(L, rank, x[l], spare[l]);
+      sweep(cluster, shared, L, rank, size, x[l], spare[l], false);
       cluster.sync();
-      float* t = x[l];
+      const int t = x[l];
       x[l] = spare[l];
       spare[l] = t;
     }
-    residual(L, rank, x[l], spare[l]);
+    {
+      // Residual of the owned rows into every copy of the spare vector.
+      const Rows own = owned(L, rank);
+      for (int k = threadIdx.x; k < own.count; k += blockDim.x) {
+        const int i = own.base + k;
+        push(cluster, shared, spare[l], i,
+             shared[L.bs + k] - __ldg(L.scale + i) * row_product(L, shared + x[l], i), size);
+      }
+    }
     cluster.sync();
-    const bool coarse_sweeps = l + 1 < last || !dense;
-    restrict_to(L, spare[l], p.level[l + 1], x[l + 1], coarse_sweeps, rank);
+    {
+      // Coarse b = Kahan sum of the residual over each owned aggregate's
+      // members, in member order; then the coarse zero-start sweep, or, for
+      // the dense coarsest, b itself into every CTA's copy.
+      const TailLevel& C = p.level[l + 1];
+      const bool to_dense = l + 1 == last && dense;
+      const Rows own = owned(C, rank);
+      const float* r = shared + spare[l];
+      for (int k = threadIdx.x; k < own.count; k += blockDim.x) {
+        const int g = own.base + k;
+        float sum = 0.0f, error = 0.0f;
+        const int end = __ldg(L.offsets + g + 1);
+        for (int j0 = __ldg(L.offsets + g); j0 < end; j0 += kBatch) {
+          int m[kBatch];
+#pragma unroll
+          for (int u = 0; u < kBatch; ++u) m[u] = j0 + u < end ? __ldg(L.members + j0 + u) : -1;
+#pragma unroll
+          for (int u = 0; u < kBatch; ++u) {
+            if (m[u] < 0) break;
+            const float term = r[m[u]] - error;
+            const float next = sum + term;
+            error = (next - sum) - term;
+            sum = next;
+          }
+        }
+        shared[C.bs + k] = sum;
+        if (to_dense) push(cluster, shared, C.rs, g, sum, size);
+        else push(cluster, shared, x[l + 1], g, kOmega * __ldg(C.inv + g) * sum, size);
+      }
+    }
     cluster.sync();
   }
-  const float* correction = nullptr;  // coarsest solution, when in shared memory
   if (dense) {
-    dense_solve(shared, p.level[last], p.dense, p.gathered, p.solution);
-    correction = shared + p.solution;
+    // Every CTA: the whole coarsest solution x = W b with the dense FP64
+    // inverse, a warp per row, into its own copy.
+    const TailLevel& C = p.level[last];
+    const float* b = shared + C.rs;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, warps = blockDim.x >> 5;
+    for (int i = warp; i < C.n; i += warps) {
+      const double* row = p.dense + static_cast<std::size_t>(i) * C.n;
+      double acc = 0.0;
+      for (int c = lane; c < C.n; c += 32) acc += __ldg(row + c) * static_cast<double>(b[c]);
+      for (int d = 16; d > 0; d >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, d);
+      if (lane == 0) shared[x[last] + i] = static_cast<float>(acc);
+    }
+    __syncthreads();
   } else {
-    // x[last] holds the zero-start sweep (written with the restriction).
+    // x[last] holds the zero-start sweep (pushed with the restriction).
     for (int s = 1; s < p.coarse_sweeps; ++s) {
-      sweep(p.level[last], rank, x[last], spare[last]);
+      sweep(cluster, shared, p.level[last], rank, size, x[last], spare[last], false);
       cluster.sync();
-      float* t = x[last];
+      const int t = x[last];
       x[last] = spare[last];
       spare[last] = t;
     }
   }
   for (int l = last - 1; l >= 0; --l) {
     const TailLevel& L = p.level[l];
-    const bool from_shared = l + 1 == last && correction != nullptr;
-    prolong(L, x[l], from_shared ? correction : x[l + 1], from_shared, rank);
+    {
+      // x += e[aggregate] on the owned rows, e the coarser level's result
+      // (every CTA holds all of it), into every copy.
+      const Rows own = owned(L, rank);
+      const float* e = shared + x[l + 1];
+      for (int k = threadIdx.x; k < own.count; k += blockDim.x) {
+        const int i = own.base + k;
+        const int g = __ldg(L.aggregate + i);
+        const float xi = shared[x[l] + i];
+        push(cluster, shared, x[l], i, g >= 0 ? xi + e[g] : xi, size);
+      }
+    }
     cluster.sync();
     for (int s = 0; s < p.post; ++s) {
-      sweep(L, rank, x[l], spare[l]);
-      // After the last sweep nothing in this launch reads another CTA's rows.
-      if (l > 0 || s + 1 < p.post) cluster.sync();
-      float* t = x[l];
+      const bool final = l == 0 && s + 1 == p.post;
+      sweep(cluster, shared, L, rank, size, x[l], spare[l], final);
+      if (final) break;
+      cluster.sync();
+      const int t = x[l];
       x[l] = spare[l];
       spare[l] = t;
     }
   }
+  // The last cluster barrier above followed the last store into another CTA's
+  // shared memory, so every CTA may exit now.
 }
 
 // The attribute is per function, shared by every solver on the device, so it

@@ -161,8 +161,11 @@ Solver::Solver(Kind kind, const CsrView& a, const Options& options,
 // The tail starts at the first coarse level with at most 16,384 rows (about a
 // row per thread of a 16-CTA cluster: larger levels run faster spread over
 // every SM) and needs at least two levels. CTA k owns rows
-// [k 2^shift, (k + 1) 2^shift) of each level, 2^shift >= ceil(n / cluster);
-// shared memory holds only the dense coarsest right-hand side and solution.
+// [k 2^shift, (k + 1) 2^shift) of each level, 2^shift >= ceil(n / cluster).
+// Each CTA's shared memory holds, per tail level, full copies of the iterate
+// and of the spare vector and its own chunk of the right-hand side
+// (2 n + 2^shift floats): under 160 KB for a 16,384-row first level. A plan
+// that does not fit the kernel's shared-memory ceiling runs without the tail.
 void Solver::plan_tail() {
   constexpr int kTailRows = 1 << 14;
   const std::size_t count = levels_.size();
@@ -184,6 +187,7 @@ void Solver::plan_tail() {
     p.cluster = cluster;
     p.dense = dense(coarsest) ? coarsest.dense_inverse.get() : nullptr;
     double bytes = 0;
+    int shared_floats = 0;
     for (int k = 0; k < p.levels; ++k) {
       const std::size_t i = start + static_cast<std::size_t>(k);
       const DevLevel& l = levels_[i];
@@ -204,8 +208,16 @@ void Solver::plan_tail() {
       t.offsets = last ? nullptr : l.member_offsets.get();
       t.members = last ? nullptr : l.members.get();
       t.xg = l.xa.get();
-      t.rg = l.ra.get();
       t.bg = l.b.get();
+      // Shared-memory copies, 16-byte aligned: x and spare (n each), the
+      // owned right-hand side chunk.
+      const auto aligned = [](int floats) { return (floats + 3) & ~3; };
+      t.xs = shared_floats;
+      shared_floats += aligned(l.n);
+      t.rs = shared_floats;
+      shared_floats += aligned(l.n);
+      t.bs = shared_floats;
+      shared_floats += aligned(1 << shift);
       const double sweep = 6.0 * l.nnz + 4.0 * (l.n + 1) + 16.0 * l.n;
       if (!last) {
         const double nc = levels_[start + static_cast<std::size_t>(k) + 1].n;
@@ -217,11 +229,7 @@ void Solver::plan_tail() {
         bytes += 12.0 * l.n + (p.coarse_sweeps - 1) * sweep;
       }
     }
-    if (p.dense) {
-      p.gathered = 0;
-      p.solution = coarsest.n;
-      p.smem_bytes = 2 * coarsest.n * static_cast<int>(sizeof(float));
-    }
+    p.smem_bytes = shared_floats * static_cast<int>(sizeof(float));
     if (!launch::tail_cluster_fits(cluster, p.smem_bytes)) continue;
     tail_ = p;
     tail_start_ = start;
