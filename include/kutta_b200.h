@@ -189,9 +189,11 @@ typedef struct {
   double inner_rel_tol;      /* residual reduction per refinement step (default 1e-3) */
   int inner_max_iter;        /* inner PCG iterations per refinement step (default 300) */
   int max_refinements;       /* default 30 */
-  int fused_coarse;          /* default 1: the coarse levels below 16,384 rows run as one
+  int fused_coarse;          /* default 0: 1 runs the coarse levels below 16,384 rows as one
                                 thread-block-cluster launch per V-cycle (BF16, no
-                                nullspace, below any K-cycle inner steps) */
+                                nullspace, below any K-cycle inner steps); with
+                                programmatic dependent launch their separate kernels
+                                measured faster on the pressure matrices here */
   int k_cycle_levels;        /* with amg.cycle = K: coarse levels 1..k take the inner
                                 Krylov step, the rest a V-cycle; 0 = every level
                                 (default 1) */
@@ -200,6 +202,13 @@ typedef struct {
                                 captured once as a CUDA graph and replayed (same kernels,
                                 same results); the solve stream may be the legacy default
                                 stream, capture uses an internal stream */
+  int packed_rows;           /* default 1: the fine level's residual, post-sweep and SpMV
+                                read a packed copy of the operator (per row the diagonal
+                                and up to 8 off-diagonal values with 16-bit column
+                                offsets), the same results bit for bit, rebuilt from the
+                                device values at every refresh; used when every row fits.
+                                The fine level then follows the values of the last
+                                refresh, as the coarse levels always do */
 } b2_mixed_options;
 
 typedef struct {

@@ -504,9 +504,10 @@ void b2_mixed_options_default(b2_mixed_options* o) {
   o->inner_rel_tol = 1e-3;
   o->inner_max_iter = 300;
   o->max_refinements = 30;
-  o->fused_coarse = 1;
+  o->fused_coarse = 0;
   o->k_cycle_levels = 1;
   o->cuda_graphs = 1;
+  o->packed_rows = 1;
 }
 
 int b2_mixed_create(int n, int nnz, const int32_t* row_ptr, const int32_t* col,
@@ -525,6 +526,7 @@ int b2_mixed_create(int n, int nnz, const int32_t* row_ptr, const int32_t* col,
     o.amg.dense_coarsest = true;
     o.amg.fused_tail = m.fused_coarse != 0;
     o.amg.graphs = m.cuda_graphs != 0;
+    o.amg.packed_fine = m.packed_rows != 0;
     KB2_REQUIRE(m.k_cycle_levels >= 0, "mixed: k_cycle_levels must be >= 0");
     o.amg.k_levels = m.k_cycle_levels;
     KB2_REQUIRE(std::isfinite(m.inner_rel_tol) && m.inner_rel_tol > 0 && m.inner_rel_tol < 1 &&

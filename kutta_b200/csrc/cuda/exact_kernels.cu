@@ -249,6 +249,172 @@ __global__ void k_smooth_dot2(int n, const int* __restrict__ rows, const int* __
   finish(as_reducer(red), a, c, true, scalars, offset, status, epi);
 }
 
+// ---- Packed rows (the mixed solve's fine operator) ---------------------------
+// The kernels are bounded to 32 registers a thread (8 blocks of 256 per SM):
+// their grids are the CSR kernels' (8 blocks per SM, one resident wave), and
+// at more registers part of the grid would wait for a second wave.
+// The row's values, absolute columns and diagonal, loaded with 128-bit (and
+// 64-bit) loads that stream past the caches: the operator is read once per
+// pass, the gathered vectors are what the caches should keep.
+template <int W>
+struct PackedRow {
+  float v[W];
+  int c[W];
+  float d;
+};
+template <int W>
+__device__ __forceinline__ PackedRow<W> packed_row(int i, const float* __restrict__ vals,
+                                                   const short* __restrict__ offsets,
+                                                   const float* __restrict__ diag) {
+  PackedRow<W> row;
+  const float4* v4 = reinterpret_cast<const float4*>(vals) + static_cast<std::size_t>(i) * (W / 4);
+#pragma unroll
+  for (int q = 0; q < W / 4; ++q) {
+    const float4 a = __ldcs(v4 + q);
+    row.v[4 * q] = a.x;
+    row.v[4 * q + 1] = a.y;
+    row.v[4 * q + 2] = a.z;
+    row.v[4 * q + 3] = a.w;
+  }
+  unsigned words[W / 2];
+  if constexpr (W == 4) {
+    const uint2 o = __ldcs(reinterpret_cast<const uint2*>(offsets) + i);
+    words[0] = o.x;
+    words[1] = o.y;
+  } else {
+    const uint4 o = __ldcs(reinterpret_cast<const uint4*>(offsets) + i);
+    words[0] = o.x;
+    words[1] = o.y;
+    words[2] = o.z;
+    words[3] = o.w;
+  }
+#pragma unroll
+  for (int k = 0; k < W; ++k) {
+    const int off = static_cast<short>((words[k / 2] >> (16 * (k & 1))) & 0xffffu);
+    row.c[k] = i + off;
+  }
+  row.d = __ldcs(diag + i);
+  return row;
+}
+
+// residual_term with the product's rounding error taken by one FMA instead of
+// Dekker's 4097 split: both give the exact error of v x when neither factor
+// exceeds 1e30 (the split's guard, kept) and no partial product underflows,
+// so the sums agree bit for bit there at a third of the instructions, which
+// keeps these streaming kernels memory-bound.
+__device__ __forceinline__ void residual_term_fma(float& sum, float& error, float v, float x) {
+  const float product = v * x;
+  const float term = -product;
+  const float next = sum + term;
+  error += fabsf(sum) >= fabsf(term) ? (sum - next) + term : (term - next) + sum;
+  if (fabsf(v) <= 1.0e30f && fabsf(x) <= 1.0e30f) error -= fmaf(v, x, -product);
+  sum = next;
+}
+
+// sum = b_i - sum_j a_ij x_j with residual_term_fma, in CSR column order;
+// unused slots (column i) are skipped.
+template <int W>
+__device__ __forceinline__ float packed_residual_row(int i, const PackedRow<W>& row, float bi,
+                                                     const float* __restrict__ x) {
+  float xv[W];
+#pragma unroll
+  for (int k = 0; k < W; ++k) xv[k] = x[row.c[k]];
+  const float xi = x[i];
+  float sum = bi, error = 0.0f;
+#pragma unroll
+  for (int k = 0; k < W; ++k)
+    if (row.c[k] < i) residual_term_fma(sum, error, row.v[k], xv[k]);
+  residual_term_fma(sum, error, row.d, xi);
+#pragma unroll
+  for (int k = 0; k < W; ++k)
+    if (row.c[k] > i) residual_term_fma(sum, error, row.v[k], xv[k]);
+  return sum + error;
+}
+
+template <int W>
+__global__ void __launch_bounds__(kBlock, 8) k_packed_residual(int n, const float* __restrict__ vals,
+                                  const short* __restrict__ offsets, const float* __restrict__ diag,
+                                  const float* __restrict__ x, const float* __restrict__ b,
+                                  float* __restrict__ r, const int* __restrict__ status) {
+  pdl_entry();
+  if (status && status[0] != 0) return;
+  ROWS(i, n) {
+    const PackedRow<W> row = packed_row<W>(i, vals, offsets, diag);
+    r[i] = packed_residual_row<W>(i, row, b[i], x);
+  }
+}
+
+// k_smooth_dot2 on packed rows.
+template <int W>
+__global__ void __launch_bounds__(kBlock, 8) k_packed_smooth_dot2(int n, const float* __restrict__ vals,
+                                     const short* __restrict__ offsets,
+                                     const float* __restrict__ diag, const float* __restrict__ x,
+                                     const float* __restrict__ b, const float* __restrict__ inv,
+                                     float* __restrict__ next, const float* __restrict__ q,
+                                     DeviceReducer red, float* scalars, int offset, int* status,
+                                     Epilogue epi) {
+  pdl_entry();
+  if (status[0] != 0) return;
+  double a = 0, c = 0;
+  ROWS(i, n) {
+    const PackedRow<W> row = packed_row<W>(i, vals, offsets, diag);
+    const float bi = b[i];
+    const float z = x[i] + (2.0f / 3.0f) * inv[i] * packed_residual_row<W>(i, row, bi, x);
+    next[i] = z;
+    a += static_cast<double>(bi) * static_cast<double>(z);
+    c += static_cast<double>(z) * static_cast<double>(q[i]);
+  }
+  finish(as_reducer(red), a, c, true, scalars, offset, status, epi);
+}
+
+// k_spmv_dot on packed rows (Kahan sum in CSR column order).
+template <int W>
+__global__ void __launch_bounds__(kBlock, 8) k_packed_spmv_dot(int n, const float* __restrict__ vals,
+                                  const short* __restrict__ offsets,
+                                  const float* __restrict__ diag, const float* __restrict__ p,
+                                  const float* __restrict__ w, float* __restrict__ q,
+                                  DeviceReducer red, float* scalars, int offset, int* status,
+                                  Epilogue epi) {
+  pdl_entry();
+  if (status[0] != 0) return;
+  double acc = 0;
+  ROWS(i, n) {
+    const PackedRow<W> row = packed_row<W>(i, vals, offsets, diag);
+    float pv[W];
+#pragma unroll
+    for (int k = 0; k < W; ++k) pv[k] = p[row.c[k]];
+    const float pi = p[i];
+    float sum = 0.0f, error = 0.0f;
+#pragma unroll
+    for (int k = 0; k < W; ++k)
+      if (row.c[k] < i) kahan_term(sum, error, row.v[k], pv[k]);
+    kahan_term(sum, error, row.d, pi);
+#pragma unroll
+    for (int k = 0; k < W; ++k)
+      if (row.c[k] > i) kahan_term(sum, error, row.v[k], pv[k]);
+    q[i] = sum;
+    acc += static_cast<double>(w[i]) * static_cast<double>(sum);
+  }
+  finish(as_reducer(red), acc, 0, false, scalars, offset, status, epi);
+}
+
+// Values of the packed rows: the row's off-diagonal values in column order,
+// then zeros; the diagonal apart.
+__global__ void k_pack_rows(int n, int width, const int* __restrict__ rows,
+                            const int* __restrict__ diag_index, const float* __restrict__ vals,
+                            float* __restrict__ packed, float* __restrict__ packed_diag) {
+  pdl_entry();
+  ROWS(i, n) {
+    float* out = packed + static_cast<std::size_t>(i) * width;
+    int k = 0;
+    const int d = diag_index[i];
+    for (int j = rows[i]; j < rows[i + 1]; ++j)
+      if (j != d) out[k++] = vals[j];
+    for (; k < width; ++k) out[k] = 0.0f;
+    packed_diag[i] = vals[d];
+  }
+}
+
 // amg_coarse_solve, linalg.kern.h:126-147: whole <=24-row system in one thread.
 __global__ void k_coarse_solve(int count, const int* __restrict__ rows,
                                const int* __restrict__ cols, const float* __restrict__ vals,
@@ -626,6 +792,47 @@ void smooth_dot2(int n, const int* rows, const int* cols, const float* vals, con
   ++counter;
   pdl(k_smooth_dot2, blocks(n), kBlock, 0, s, n, rows, cols, vals, x, b, inv, next, q, red,
                                              scalars, offset, status, epi);
+}
+void pack_rows(int n, int width, const int* rows, const int* cols, const int* diag,
+               const float* vals, float* packed, float* packed_diag, cudaStream_t s) {
+  (void)cols;
+  if (n <= 0) return;
+  ++counter;
+  pdl(k_pack_rows, full_grid(n), kBlock, 0, s, n, width, rows, diag, vals, packed, packed_diag);
+}
+void packed_residual(int n, PackedRows a, const float* x, const float* b, float* r,
+                     const int* status, cudaStream_t s) {
+  if (n <= 0) return;
+  ++counter;
+  if (a.width == 4)
+    pdl(k_packed_residual<4>, full_grid(n), kBlock, 0, s, n, a.vals, a.offsets, a.diag, x, b, r,
+        status);
+  else
+    pdl(k_packed_residual<8>, full_grid(n), kBlock, 0, s, n, a.vals, a.offsets, a.diag, x, b, r,
+        status);
+}
+void packed_spmv_dot(int n, PackedRows a, const float* p, const float* w, float* q,
+                     DeviceReducer red, float* scalars, int offset, int* status, Epilogue epi,
+                     cudaStream_t s) {
+  ++counter;
+  if (a.width == 4)
+    pdl(k_packed_spmv_dot<4>, blocks(n), kBlock, 0, s, n, a.vals, a.offsets, a.diag, p, w, q, red,
+        scalars, offset, status, epi);
+  else
+    pdl(k_packed_spmv_dot<8>, blocks(n), kBlock, 0, s, n, a.vals, a.offsets, a.diag, p, w, q, red,
+        scalars, offset, status, epi);
+}
+void packed_smooth_dot2(int n, PackedRows a, const float* x, const float* b, const float* inv,
+                        float* next, const float* q, DeviceReducer red, float* scalars,
+                        int offset, int* status, Epilogue epi, cudaStream_t s) {
+  if (n <= 0) return;
+  ++counter;
+  if (a.width == 4)
+    pdl(k_packed_smooth_dot2<4>, blocks(n), kBlock, 0, s, n, a.vals, a.offsets, a.diag, x, b, inv,
+        next, q, red, scalars, offset, status, epi);
+  else
+    pdl(k_packed_smooth_dot2<8>, blocks(n), kBlock, 0, s, n, a.vals, a.offsets, a.diag, x, b, inv,
+        next, q, red, scalars, offset, status, epi);
 }
 void coarse_solve(int count, const int* rows, const int* cols, const float* vals, float* x,
                   const float* b, const float* inv, const int* status, int sweeps,

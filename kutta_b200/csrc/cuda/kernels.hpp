@@ -49,6 +49,32 @@ void spmv(int n, const int* rows, const int* cols, const float* vals, const floa
 void spmv_dot(int n, const int* rows, const int* cols, const float* vals, const float* p,
               const float* w, float* q, DeviceReducer red, float* scalars, int offset,
               int* status, Epilogue epi, cudaStream_t s);
+// The mixed solve's packed copy of the fine operator ("packed rows"): per
+// row i the diagonal value diag[i] and `width` (4 or 8) off-diagonal slots,
+// values vals[width i + k] and int16 column offsets offsets[width i + k] =
+// col - i in column order, unused slots with offset 0 and value 0. A row is
+// 6 width + 4 bytes instead of CSR's 8 (entries) + 4 bytes: on a tet mesh 28
+// instead of 44. The kernels below visit a row's terms in CSR column order
+// (negative offsets, the diagonal, positive offsets) with the CSR kernels'
+// arithmetic, grids and reductions, so every result equals the CSR kernel's
+// bit for bit.
+struct PackedRows {
+  int width;
+  const float* vals;
+  const short* offsets;
+  const float* diag;
+};
+// Values of the packed rows from CSR values (pattern fixed at packing setup).
+void pack_rows(int n, int width, const int* rows, const int* cols, const int* diag,
+               const float* vals, float* packed, float* packed_diag, cudaStream_t s);
+void packed_residual(int n, PackedRows a, const float* x, const float* b, float* r,
+                     const int* status, cudaStream_t s);
+void packed_spmv_dot(int n, PackedRows a, const float* p, const float* w, float* q,
+                     DeviceReducer red, float* scalars, int offset, int* status, Epilogue epi,
+                     cudaStream_t s);
+void packed_smooth_dot2(int n, PackedRows a, const float* x, const float* b, const float* inv,
+                        float* next, const float* q, DeviceReducer red, float* scalars,
+                        int offset, int* status, Epilogue epi, cudaStream_t s);
 // r = b - A x, Neumaier + Dekker compensated (csr_residual). status may be null.
 void residual(int n, const int* rows, const int* cols, const float* vals, const float* x,
               const float* b, float* r, const int* status, cudaStream_t s);

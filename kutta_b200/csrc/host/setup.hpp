@@ -61,6 +61,12 @@ struct Options {  // AmgOptions, src/kutta/linalg/amg.hpp:8-20
   // Replay each AMG preconditioner application as a captured CUDA graph (the
   // same kernels with the same arguments, so the same results).
   bool graphs = false;
+  // Mixed solve: the fine level's residual, post-sweep and SpMV read a packed
+  // copy of the operator (packed rows: int16 column offsets, the diagonal
+  // apart; the same results bit for bit), refreshed from the values at every
+  // refresh. Used when every row has at most 8 off-diagonal entries within
+  // 32,767 columns of the diagonal.
+  bool packed_fine = false;
   // Build the hierarchy on the device (same aggregates, patterns and values as
   // the host setup) when the pattern is structurally symmetric.
   bool device_setup = true;

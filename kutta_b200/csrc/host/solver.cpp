@@ -154,8 +154,43 @@ Solver::Solver(Kind kind, const CsrView& a, const Options& options,
     KB2_REQUIRE(host_values_[0] == 0, "mixed: coarsest operator is not SPD");
     choose_coarsest(host_values_[1]);
     if (options_.fused_tail && options_.coarse_bf16 && !nullspace_) plan_tail();
+    if (options_.packed_fine) plan_packed(a, s);
   }
   wait(s);
+}
+
+// The packed rows' pattern: each row's off-diagonal column offsets in column
+// order, padded with 0 to the width (4 or 8). Left empty (the CSR kernels
+// serve) when a row has more than 8 off-diagonal entries or an offset does
+// not fit 16 bits.
+void Solver::plan_packed(const CsrView& a, cudaStream_t s) {
+  int longest = 0;
+  for (int i = 0; i < a.n; ++i) {
+    longest = std::max(longest, a.row_ptr[i + 1] - a.row_ptr[i] - 1);
+    for (int j = a.row_ptr[i]; j < a.row_ptr[i + 1]; ++j)
+      if (std::abs(a.col[j] - i) > 32767) return;
+  }
+  const int width = longest <= 4 ? 4 : (longest <= 8 ? 8 : 0);
+  if (width == 0 || a.n == 0) return;
+  // Values from the setup values, as the coarse levels are, until a refresh
+  // packs the device values.
+  const std::size_t slots = static_cast<std::size_t>(width) * static_cast<std::size_t>(a.n);
+  std::vector<short> offsets(slots, 0);
+  std::vector<float> values(slots, 0.0f), diagonal(static_cast<std::size_t>(a.n));
+  for (int i = 0; i < a.n; ++i) {
+    std::size_t k = static_cast<std::size_t>(width) * static_cast<std::size_t>(i);
+    for (int j = a.row_ptr[i]; j < a.row_ptr[i + 1]; ++j) {
+      if (j == a.diag[i]) continue;
+      offsets[k] = static_cast<short>(a.col[j] - i);
+      values[k++] = static_cast<float>(a.val[j]);
+    }
+    diagonal[static_cast<std::size_t>(i)] = static_cast<float>(a.val[a.diag[i]]);
+  }
+  packed_.offsets.upload(offsets, s);
+  packed_.vals.upload(values, s);
+  packed_.diag.upload(diagonal, s);
+  wait(s);  // the host arrays are released on return
+  packed_.width = width;
 }
 
 // The tail starts at the first coarse level with at most 16,384 rows (about a
@@ -273,8 +308,11 @@ void Solver::choose_coarsest(double smallest_pivot) {
 
 // ---------------------------------------------------------------- primitives --
 void Solver::residual(const float* x, const float* b, float* r) {
-  launch::residual(n_, rows0(), cols0(), val_, x, b, r, nullptr, stream_);
-  tally(8.0 * nnz_ + 4.0 * (n_ + 1) + 12.0 * n_);
+  if (packed_.width > 0)
+    launch::packed_residual(n_, packed(), x, b, r, nullptr, stream_);
+  else
+    launch::residual(n_, rows0(), cols0(), val_, x, b, r, nullptr, stream_);
+  tally(fine_operator_bytes() + 12.0 * n_);
 }
 
 Solver::~Solver() {
@@ -386,12 +424,19 @@ void Solver::smooth(DevLevel& l, const int* rows, const int* cols, const float* 
     // The last sweep of the fine level's post-smoothing (pre-smoothing always
     // starts from zero) carries the fused reductions.
     const bool with_dots = fine && fuse_dots_ && !zero_start && sweep + 1 == sweeps;
+    const bool packed_rows = with_dots && packed_.width > 0;
     const double bytes =
-        zero ? 12.0 * l.n : 8.0 * l.nnz + 4.0 * (l.n + 1) + (with_dots ? 20.0 : 16.0) * l.n;
+        zero ? 12.0 * l.n
+             : (packed_rows ? fine_operator_bytes() : 8.0 * l.nnz + 4.0 * (l.n + 1)) +
+                   (with_dots ? 20.0 : 16.0) * l.n;
     if (timed) event_bytes_.push_back(bytes);
     if (l.v16.allocated())
       launch::bf16_smooth(l.n, rows, cols, l.v16.get(), l.scale.get(), x, b, l.l1.get(), l.r,
                           status, zero, stream_);
+    else if (packed_rows)
+      launch::packed_smooth_dot2(l.n, packed(), x, b, l.l1.get(), l.r, q_, reducer(),
+                                 scalars_.get(), 4, status_.get(), Epilogue::PcgBetaFlexible,
+                                 stream_);
     else if (with_dots)
       launch::smooth_dot2(l.n, rows, cols, vals, x, b, l.l1.get(), l.r, q_, reducer(),
                           scalars_.get(), 4, status_.get(), Epilogue::PcgBetaFlexible, stream_);
@@ -440,6 +485,8 @@ void Solver::cycle(std::size_t index, const float* b, float*& x, const int* stat
     if (l.v16.allocated())
       launch::bf16_residual(l.n, rows, cols, l.v16.get(), l.scale.get(), x, b, l.r, status,
                             stream_);
+    else if (index == 0 && packed_.width > 0)
+      launch::packed_residual(l.n, packed(), x, b, l.r, status, stream_);
     else
       launch::residual(l.n, rows, cols, vals, x, b, l.r, status, stream_);
     auto& c = levels_[index + 1];
@@ -752,6 +799,9 @@ void Solver::refresh_levels(const float* val, bool fine_done, cudaStream_t s) {
     }
   }
   const int slots = static_cast<int>(levels_.size());
+  if (packed_.width > 0)
+    launch::pack_rows(n_, packed_.width, rows0(), cols0(), levels_[0].diag.get(), val,
+                      packed_.vals.get(), packed_.diag.get(), s);
   if (mixed()) prepare_mixed(s, slots);
   cuda_check(cudaMemcpyAsync(host_values_.get(), values_.get(),
                              sizeof(double) * (slots + (mixed() ? 2 : 0)), cudaMemcpyDeviceToHost, s),
@@ -842,10 +892,14 @@ void Solver::pcg(float* x, const float* b, const Control& c, double target, Stat
     verified_current_ = false;
     speculated_.reset();
     auto iterate = [&](int j) {
-      launch::spmv_dot(n_, rows0(), cols0(), val_, p_, p_, q_, reducer(), scalars_.get(), 2,
-                       status_.get(), Epilogue::PcgAlpha, stream_);
+      if (packed_.width > 0)
+        launch::packed_spmv_dot(n_, packed(), p_, p_, q_, reducer(), scalars_.get(), 2,
+                                status_.get(), Epilogue::PcgAlpha, stream_);
+      else
+        launch::spmv_dot(n_, rows0(), cols0(), val_, p_, p_, q_, reducer(), scalars_.get(), 2,
+                         status_.get(), Epilogue::PcgAlpha, stream_);
       launch::pcg_step_dot(n_, x, r_, p_, q_, reducer(), scalars_.get(), status_.get(), stream_);
-      tally(8.0 * nnz_ + 4.0 * (n_ + 1) + 8.0 * n_ + 24.0 * n_);
+      tally(fine_operator_bytes() + 8.0 * n_ + 24.0 * n_);
       if (stats.iterations + j + 1 == c.max_iter) return;
       const bool fused = can_fuse_dots();
       fuse_dots_ = fused;
@@ -1047,6 +1101,7 @@ std::string Solver::describe() const {
                   ? (dense_ok_ ? ", dense FP64 coarsest"
                                : ", nearly singular coarsest smoothed instead of its dense inverse")
                   : "");
+    if (packed_.width > 0) out << ", packed fine rows";
     if (tail_on_)
       out << ", levels " << tail_start_ << "-" << levels_.size() - 1 << " in one "
           << tail_.cluster << "-CTA cluster launch";

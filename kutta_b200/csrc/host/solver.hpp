@@ -150,6 +150,22 @@ class Solver {
   double tail_bytes_ = 0;
   launch::TailPlan tail_{};
   bool mixed() const { return options_.coarse_bf16 || options_.dense_coarsest; }
+  // The mixed solve's packed copy of the fine operator (width 0: CSR kernels).
+  struct Packed {
+    int width = 0;
+    DArray<float> vals, diag;
+    DArray<short> offsets;
+  } packed_;
+  void plan_packed(const CsrView& a, cudaStream_t s);
+  launch::PackedRows packed() const {
+    return launch::PackedRows{packed_.width, packed_.vals.get(), packed_.offsets.get(),
+                              packed_.diag.get()};
+  }
+  // Algorithmic bytes of one pass over the fine operator: CSR, or the packed
+  // rows' stored entries (padding slots are not counted).
+  double fine_operator_bytes() const {
+    return packed_.width > 0 ? 6.0 * (nnz_ - n_) + 4.0 * n_ : 8.0 * nnz_ + 4.0 * (n_ + 1);
+  }
   const int* rows0() const { return levels_[0].row_ptr.get(); }
   const int* cols0() const { return levels_[0].col.get(); }
 

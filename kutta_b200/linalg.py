@@ -491,9 +491,10 @@ class MixedOptions:
     inner_rel_tol: float = 1e-3
     inner_max_iter: int = 300
     max_refinements: int = 30
-    fused_coarse: bool = True
+    fused_coarse: bool = False
     k_cycle_levels: int = 1
     cuda_graphs: bool = True
+    packed_rows: bool = True
 
 
 @dataclasses.dataclass
@@ -511,7 +512,8 @@ class _MixedOptions(ctypes.Structure):
                 ("dense_rows", ctypes.c_int), ("coarse_bf16", ctypes.c_int),
                 ("inner_rel_tol", ctypes.c_double), ("inner_max_iter", ctypes.c_int),
                 ("max_refinements", ctypes.c_int), ("fused_coarse", ctypes.c_int),
-                ("k_cycle_levels", ctypes.c_int), ("cuda_graphs", ctypes.c_int)]
+                ("k_cycle_levels", ctypes.c_int), ("cuda_graphs", ctypes.c_int),
+                ("packed_rows", ctypes.c_int)]
 
 
 class _MixedStats(ctypes.Structure):
@@ -529,6 +531,7 @@ def _mixed_struct(o: MixedOptions) -> _MixedOptions:
     s.fused_coarse = int(o.fused_coarse)
     s.k_cycle_levels = int(o.k_cycle_levels)
     s.cuda_graphs = int(o.cuda_graphs)
+    s.packed_rows = int(o.packed_rows)
     return s
 
 

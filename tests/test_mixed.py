@@ -226,6 +226,47 @@ def test_fused_coarse_levels_match_separate_launches(cuda, name, make, amg):
         assert np.linalg.norm(xr - x64) / np.linalg.norm(x64) < 1e-5
 
 
+PACKED_CASES = [
+    # Tets: at most 4 off-diagonal entries per row (packed width 4).
+    ("tet40", lambda: harness.box_system(40, 40, 40, tet=True, seed=13)),
+    # Hexes: 6 off-diagonal entries (width 8, two slots unused).
+    ("hex32", lambda: harness.box_system(32, 32, 32, tet=False, seed=15)),
+    ("tet24_graded", lambda: harness.box_system(24, 24, 24, tet=True, seed=16, band_layers=6,
+                                                dmin=1e-6, dmax=1.0)),
+]
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name,make", PACKED_CASES, ids=[c[0] for c in PACKED_CASES])
+def test_packed_fine_rows_give_the_csr_results_bitwise(cuda, name, make):
+    """The fine level's packed rows (diagonal apart, 16-bit column offsets)
+    visit each row's terms in CSR column order with the same arithmetic,
+    grids and reductions: the mixed solve's statistics and FP64 solution equal
+    the CSR kernels' bit for bit, through refresh and two solves."""
+    import torch
+    s = make()
+    a = L.upload(s)
+    b = torch.from_numpy(s.b).cuda()
+    out = {}
+    for packed in (True, False):
+        solver = L.make_mixed_solver(s, L.MixedOptions(packed_rows=packed))
+        assert ("packed fine rows" in solver.describe()) == packed, solver.describe()
+        solver.refresh(a)
+        runs = []
+        for _ in range(2):
+            x = torch.zeros(s.n, dtype=torch.float64, device="cuda")
+            st = solver.solve(a, x, b, L.SolveControl(1e-8, 1e-30, 3000))
+            torch.cuda.synchronize()
+            runs.append((st, x.cpu().numpy()))
+        out[packed] = runs
+    for (sp, xp), (sc, xc) in zip(out[True], out[False]):
+        assert (sp.refinements, sp.iterations, sp.converged) == (sc.refinements, sc.iterations,
+                                                                 sc.converged)
+        assert (sp.initial_residual, sp.final_residual) == (sc.initial_residual, sc.final_residual)
+        assert np.array_equal(xp.view(np.uint64), xc.view(np.uint64))
+    assert out[True][0][0].converged
+
+
 @pytest.mark.gpu
 @pytest.mark.parametrize("k_levels", [1, 0], ids=["k_cycle_level1", "k_cycle_all"])
 def test_cuda_graph_replay_is_bitwise_identical(cuda, k_levels):
