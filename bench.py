@@ -1,6 +1,6 @@
 #!/usr/bin/env python3
 """Pressure-solve benchmark: ms per pressure solve to relative residual 1e-6,
-mixed-precision solve vs plain FP32 AMG-PCG on one B200.
+learned+mixed solve vs plain FP32 AMG-PCG on one B200.
 
 Workload (default): the 5.3M-cell pressure-correction matrix: a 96^3 jittered
 hex mesh of the unit cube (interior vertices +-0.15h, seed 1), each hex split
@@ -13,9 +13,12 @@ A step is one outer-iteration pressure solve as the reference's SIMPLEC step
 runs it: refresh(A), then solve from x = 0 to ||b - A x|| <= 1e-6 ||b||
 (SolveControl{1e-6, 1e-12, 2000}).
 
-* `value`: the mixed-precision solve (FP64 iterative refinement around an FP32
-  AMG-PCG with BF16 coarse levels and a dense FP64 coarsest solve; the FP64
-  true residual of the returned FP64 solution meets the tolerance).
+* `value`: the learned+mixed solve: the mixed-precision solve (FP64 iterative
+  refinement around an FP32 AMG-PCG with BF16 coarse levels and a dense FP64
+  coarsest solve; the FP64 true residual of the returned FP64 solution meets
+  the tolerance) with the trained learned stage as its warm start.
+  `mixed_alone` times the same solver without the stage, `learned_cycle` with
+  the stage after every AMG cycle instead.
 * `plain`: the reference's own method (make_solver(AmgPcg, SymmetricMMatrix):
   V(5,5) L1-Jacobi, bit-exact aggregation and arithmetic) on the same GPU. In
   FP32 it cannot reach 1e-6 on this matrix: the float-rounded exact solution
@@ -29,9 +32,11 @@ L2, so no flush is needed between steps.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
 
-At N = 1 rank 0 adds two CPU-side entries after the timed work: `cpu_baseline`
-(the reference's CPU path on a bounded sample) and `fp64_oracle` (the returned
-x's error against an FP64 oracle solution).
+At N = 1 rank 0 adds entries after the timed work: `cpu_baseline` (the
+reference's CPU path on a bounded sample), `fp64_oracle` (the returned x's
+error against an FP64 oracle solution) and `other_configs` (the graded
+near-wall matrix to 1e-8 and an unseen seed of the learned stage's 128^3
+evaluation configuration, each device-timed).
 
 Under torchrun (N > 1) every rank runs an independent replica (the solve does
 not shard); rank 0 prints one JSON line.
@@ -190,11 +195,17 @@ def run_ours(args, rank, world, local):
 
     a = L.upload(s, dev)
     b = torch.from_numpy(s.b).to(dev)
+    from kutta_b200 import learn
+    stage = learn.trained_stage()
 
-    # ---- mixed precision (the measured value) ----
+    # ---- learned+mixed: the metric's method, the measured value ----
+    # The mixed-precision solve with the trained learned stage as its warm
+    # start (one safeguarded step along G(b - A x0) before the refinement
+    # loop), the cheaper of the stage's two placements.
     t0 = time.perf_counter()
     mixed = L.make_mixed_solver(s)
     mixed_setup = time.perf_counter() - t0
+    mixed.set_learned(stage, L.LEARNED_WARM_START)
     x64 = torch.zeros(s.n, dtype=torch.float64, device=dev)
 
     def mixed_step():
@@ -211,6 +222,9 @@ def run_ours(args, rank, world, local):
     launches = L.kernel_launches() - launches0
     clk = clocks.stop()
     ms = max_over_ranks(ms)
+    last = stats[-1]
+    x_value = x64.cpu().numpy()  # the measured solve's FP64 solution
+    true_rel = float(np.linalg.norm(b64 - A @ x_value) / last.initial_residual)
     # The same steps again with profiling on, for the fine-sweep kernel time
     # and the algorithmic bytes. Profiling brackets individual sweeps with
     # events, so this pass launches kernels one by one instead of replaying
@@ -219,9 +233,6 @@ def run_ours(args, rank, world, local):
     prof_ms, _ = _timed(mixed_step, args.steps, stream, sync)
     prof = mixed.profile_read()
     mixed.profile(False)
-    last = stats[-1]
-    x_value = x64.cpu().numpy()  # the measured solve's FP64 solution
-    true_rel = float(np.linalg.norm(b64 - A @ x_value) / last.initial_residual)
 
     # ---- end to end through the public API with host buffers ----
     val_host = torch.from_numpy(s.val.astype(np.float32)).pin_memory()
@@ -242,24 +253,24 @@ def run_ours(args, rank, world, local):
     e2e_step()
     e2e_ms, _ = _timed(e2e_step, args.steps, stream, sync)
     e2e_ms = max_over_ranks(e2e_ms)
+    mixed.refresh(a)
 
-    # ---- the same solver with the trained learned stage after each cycle ----
-    from kutta_b200 import learn
-    stage = learn.trained_stage()
+    # ---- the same solver without the stage, and with it after each cycle ----
+    mixed.set_learned(None)
+    mixed_step()
+    alone_ms, astats = _timed(mixed_step, args.steps, stream, sync)
+    alone_ms = max_over_ranks(alone_ms)
     mixed.set_learned(stage, L.LEARNED_CYCLE)
     mixed_step()
-    learned_ms, lstats = _timed(mixed_step, max(1, min(args.steps, 5)), stream, sync)
-    learned_ms = max_over_ranks(learned_ms)
+    cycle_steps = max(1, min(args.steps, 5))
+    cycle_ms, cstats = _timed(mixed_step, cycle_steps, stream, sync)
+    cycle_ms = max_over_ranks(cycle_ms)
     mixed.set_learned(None)
-    llast = lstats[-1]
-    learned_line = {
-        "method": "as method, plus the learned stage (packaged trained weights, tensor-core "
-                  "forward) after each cycle: z += alpha G(r - A z), energy-optimal alpha",
-        "ms_per_solve": learned_ms, "iterations": llast.iterations,
-        "converged": llast.converged,
-        "relative_residual": llast.final_residual / llast.initial_residual,
-        "steps": max(1, min(args.steps, 5)),
-    }
+
+    def summary(step_ms, st, steps, method):
+        return {"method": method, "ms_per_solve": step_ms, "iterations": st.iterations,
+                "refinements": st.refinements, "converged": st.converged,
+                "relative_residual": st.final_residual / st.initial_residual, "steps": steps}
 
     # ---- plain FP32 AMG-PCG: the reference's method on the same GPU ----
     t0 = time.perf_counter()
@@ -281,13 +292,14 @@ def run_ours(args, rank, world, local):
     plain_ms = max_over_ranks(plain_ms)
     plast = pstats[-1]
 
-    def roofline(p, step_ms, steps, kernel_key="k_smooth_dot2"):
+    def roofline(p, step_ms, steps, kernel_key):
         sweep_ms = p["fine_sweep_ms"] / max(p["fine_sweeps"], 1)
         achieved = p["fine_sweep_bytes"] / (sweep_ms * 1e-3) / 1e9 if sweep_ms > 0 else None
         peak, kind = _peaks()
         return {
-            "kernel": "fine-level damped L1-Jacobi post-sweep (CSR, row per thread; in the mixed "
-                      "solve k_smooth_dot2, with the flexible PCG's r.z and z.q fused)",
+            "kernel": "fine-level damped L1-Jacobi post-sweep (one row per thread; in the mixed "
+                      "solve k_packed_smooth_dot2 on the packed fine rows, with the flexible "
+                      "PCG's r.z and z.q fused; in the plain solve k_smooth on CSR)",
             "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
             "frac": achieved / peak if achieved else None, "peak_source": kind,
             "bytes_per_launch": p["fine_sweep_bytes"], "launch_ms": sweep_ms,
@@ -300,15 +312,20 @@ def run_ours(args, rank, world, local):
         "metric": METRIC, "value": ms / world, "unit": UNIT, "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
         "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
-        "dtype": "f32 operator, bf16 coarse levels, f64 refinement/reductions/coarsest",
+        "dtype": "f32 operator, bf16 coarse levels, f64 refinement/reductions/coarsest; "
+                 "learned stage bf16 weights, f32 accumulation",
         "data": "synthetic (seeded FV pressure matrix; no dataset)",
         "config": _config(args, s, world),
-        "method": mixed.describe(),
-        "learned_mixed": learned_line,
+        "method": mixed.describe() + " + learned warm start (packaged trained weights, "
+                                     "tensor-core forward)",
         "refinements": last.refinements, "iterations": last.iterations,
         "converged": last.converged,
         "relative_residual": last.final_residual / last.initial_residual,
         "true_relative_residual_fp64": true_rel, "setup_s": mixed_setup,
+        "mixed_alone": summary(alone_ms, astats[-1], args.steps, mixed.describe()),
+        "learned_cycle": summary(cycle_ms, cstats[-1], cycle_steps,
+                                 "as method, with the learned stage after each cycle "
+                                 "(z += alpha G(r - A z)) instead of the warm start"),
         "plain": {
             "method": plain.describe() + " (reference arithmetic, bit-exact aggregation)",
             "ms_per_solve": plain_ms, "iterations": plast.iterations,
@@ -316,9 +333,9 @@ def run_ours(args, rank, world, local):
             "relative_residual": plast.final_residual / plast.initial_residual,
             "setup_s": plain_setup, "steps": max(1, args.plain_steps),
             "roofline": roofline(pprof, plain_ms, max(1, args.plain_steps), "k_smooth"),
-            "speedup_of_mixed": plain_ms / ms,
+            "speedup_of_value": plain_ms / ms,
         },
-        "roofline": dict(roofline(prof, prof_ms, args.steps),
+        "roofline": dict(roofline(prof, prof_ms, args.steps, "k_packed_smooth_dot2"),
                          timed_in="profiled pass of the same steps (kernels launched one by one)",
                          profiled_ms_per_step=prof_ms),
         "e2e": {"value": e2e_ms / world, "unit": UNIT,
@@ -328,6 +345,87 @@ def run_ours(args, rank, world, local):
         "clocks": clk,
     }
     return line, s, x_value
+
+
+def _device_ms(fn, steps):
+    import torch
+    best, out = None, None
+    for _ in range(steps):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record()
+        out = fn()
+        e1.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1)
+        best = ms if best is None else min(best, ms)
+    return best, out
+
+
+def other_configs(args):
+    """One device-timed refresh + solve (best of two) of the other
+    configurations, at N = 1 after the timed work: the graded near-wall
+    matrix to 1e-8 (mixed with and without the learned warm start, against
+    plain FP32 AMG-PCG, which stops at its FP32 floor), and an unseen seed of
+    the learned stage's evaluation configuration (128^3 jittered hex, smooth
+    log-normal D_f, Fourier right-hand side) to 1e-6."""
+    import numpy as np
+    import scipy.sparse as sp
+    import torch
+    from kutta_b200 import learn
+    from kutta_b200 import linalg as L
+    stage = learn.trained_stage()
+    out = {}
+
+    def arms(s, b, rel_tol, plain_steps):
+        A = sp.csr_matrix((s.val, s.col, s.row_ptr), shape=(s.n, s.n))
+        a = L.upload(s)
+        control = L.SolveControl(rel_tol, 1e-30, args.max_iter)
+        row = {"rows": s.n, "nnz": s.nnz, "rel_tol": rel_tol}
+        mixed = L.make_mixed_solver(s)
+        x64 = torch.zeros(s.n, dtype=torch.float64, device="cuda")
+        for name, mode in (("mixed", 0), ("learned+mixed", L.LEARNED_WARM_START),
+                           ("learned_cycle+mixed", L.LEARNED_CYCLE)):
+            mixed.set_learned(stage if mode else None, mode)
+
+            def step():
+                mixed.refresh(a)
+                x64.zero_()
+                return mixed.solve(a, x64, b, control)
+            ms, st = _device_ms(step, 2)
+            xr = x64.cpu().numpy()
+            row[name] = {"ms_per_solve": ms, "iterations": st.iterations,
+                         "refinements": st.refinements, "converged": st.converged,
+                         "true_relative_residual_fp64": float(
+                             np.linalg.norm(b.cpu().numpy().astype(np.float64) - A @ xr) /
+                             st.initial_residual)}
+        mixed.set_learned(None)
+        plain = L.make_solver(L.SolverKind.AmgPcg, s, L.SolverOptions(
+            structure=L.OperatorStructure.SymmetricMMatrix))
+        x = torch.zeros(s.n, dtype=torch.float32, device="cuda")
+
+        def pstep():
+            plain.refresh(a)
+            x.zero_()
+            return plain.solve(a, x, b, control)
+        ms, st = _device_ms(pstep, plain_steps)
+        row["plain"] = {"ms_per_solve": ms, "iterations": st.iterations,
+                        "converged": st.converged,
+                        "relative_residual": st.final_residual / st.initial_residual}
+        return row
+
+    s = _graded(args)
+    out["graded_1e-8"] = dict(
+        workload=f"graded_tet{args.size}: {args.size}^3 x 6 tets, 10-layer 1000:1 band at z = 0, "
+                 "D_f log-uniform [1e-6, 1]",
+        **arms(s, torch.from_numpy(s.b).cuda(), 1e-8, 1))
+    s = learn.system(128, 90001)
+    b = torch.from_numpy(learn.fourier_rhs(s, np.random.default_rng(90001))).cuda()
+    out["learned_eval_hex128"] = dict(
+        workload="hex128, unseen seed 90001: 128^3 jittered hex, smooth log-normal D_f "
+                 "(sigma 1.5, correlation 0.1), 16 Fourier modes + 10 % noise",
+        **arms(s, b, 1e-6, 1))
+    return out
 
 
 def _cpu_model():
@@ -758,6 +856,8 @@ def main():
     ap.add_argument("--plain-steps", type=int, default=3)
     ap.add_argument("--cpu-sample-iters", type=int, default=2)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-other-configs", action="store_true",
+                    help="skip the graded 1e-8 and learned-evaluation entries")
     ap.add_argument("--mode", default="bench",
                     choices=["bench", "profile", "sequence", "graded", "transport", "outer",
                              "workload"],
@@ -800,6 +900,8 @@ def main():
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(args, system, line["plain"]["iterations"])
         line["fp64_oracle"] = fp64_oracle(system, x)
+    if rank == 0 and world == 1 and not args.no_other_configs:
+        line["other_configs"] = other_configs(args)
     if rank == 0:
         print(json.dumps(line))
     if world > 1:
