@@ -308,9 +308,19 @@ int b2_gnn_apply(b2_gnn* g, const float* d_r, float* d_z, float beta, void* stre
  * the fault. polls = 0 takes that path with a healthy MMA. */
 int b2_gnn_set_wait_limit(b2_gnn* g, long long polls);
 /* One training step on (d_t, d_e), A e = t for the bound matrix; *loss is the
- * energy loss before the step. */
+ * energy loss before the step. The forward keeps FP32 activations; in the
+ * backward the two 32-wide layers' products ([dH | dM] = G [Ws | Wn] and the
+ * weight gradients [H | M | 1]^T G) run on the tensor cores (BF16 operands,
+ * FP32 accumulation), then one Adam step. */
 int b2_gnn_train_step(b2_gnn* g, const float* d_t, const float* d_e, float learning_rate,
                       float* loss, void* stream);
+/* The energy loss's gradient with respect to the b2_gnn_parameter_count()
+ * weights at their current values, for (d_t, d_e) as in b2_gnn_train_step,
+ * without a step: tensor_cores = 1 computes the 32-wide layers' backward as
+ * b2_gnn_train_step does, 0 in FP32 on CUDA cores. *loss (may be NULL)
+ * receives the loss. */
+int b2_gnn_gradient(b2_gnn* g, const float* d_t, const float* d_e, int tensor_cores,
+                    float* host_gradient, size_t count, float* loss, void* stream);
 int b2_gnn_get_weights(const b2_gnn* g, float* host, size_t count);
 int b2_gnn_set_weights(b2_gnn* g, const float* host, size_t count);
 /* Attaches g (NULL detaches) to a mixed solver; it is bound to the solver's

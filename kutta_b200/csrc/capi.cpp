@@ -667,6 +667,17 @@ int b2_gnn_train_step(b2_gnn* g, const float* d_t, const float* d_e, float learn
   });
 }
 
+int b2_gnn_gradient(b2_gnn* g, const float* d_t, const float* d_e, int tensor_cores,
+                    float* host_gradient, size_t count, float* loss, void* stream) {
+  return guarded([&] {
+    KB2_REQUIRE(g && g->g && d_t && d_e && host_gradient, "learned stage: null argument");
+    KB2_REQUIRE(count == static_cast<size_t>(kb2::Gnn::parameter_count()),
+                "learned stage: wrong number of weights");
+    const auto grad = g->g->gradient(d_t, d_e, tensor_cores != 0, loss, as_stream(stream));
+    std::memcpy(host_gradient, grad.data(), sizeof(float) * grad.size());
+  });
+}
+
 int b2_gnn_get_weights(const b2_gnn* g, float* host, size_t count) {
   return guarded([&] {
     KB2_REQUIRE(g && g->g && host, "learned stage: null argument");

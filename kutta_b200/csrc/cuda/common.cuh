@@ -6,12 +6,27 @@
 // its explicit fma in the pair product is kept explicit here too).
 #pragma once
 
+#include <atomic>
 #include <cstddef>
 #include <cstdint>
 #include <cuda_runtime.h>
 #include <utility>
 
 namespace kb2::dev {
+
+// A kernel's dynamic shared-memory ceiling is an attribute of the function in
+// one device's context, so it is raised once per device this process uses
+// (bit d of `done` for device d < 64; higher devices raise it on every call).
+inline void raise_shared_limit(const void* kernel, int bytes,
+                               std::atomic<unsigned long long>& done) {
+  int device = 0;
+  if (cudaGetDevice(&device) != cudaSuccess) return;
+  const unsigned long long bit = device < 64 ? 1ull << device : 0;
+  if (bit && (done.load(std::memory_order_acquire) & bit)) return;
+  if (cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes) ==
+      cudaSuccess)
+    done.fetch_or(bit, std::memory_order_release);
+}
 
 // ------------------------------------------------------------------------
 // Programmatic dependent launch. The solve is a chain of short dependent

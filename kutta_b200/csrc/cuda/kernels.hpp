@@ -243,6 +243,17 @@ void gnn_dense_back(int n, int Cin, const float* H, const float* M, const float*
                     const float* dOut, const float* Ws, const float* Wn, float* dH, float* dM,
                     float* dWs, float* dWn, float* db, cudaStream_t s);
 void gnn_add(std::size_t count, const float* a, const float* b, float* out, cudaStream_t s);
+// The same backward as gnn_dense_back for a 32-wide input (Cin = 32) on the
+// tensor cores (learned_tc.cu): [dH | dM] = G [Ws | Wn] per 128-row tile, and
+// [dWs^T; dWn^T; db] = [H | M | 1]^T G accumulated in tensor memory, BF16
+// operands and FP32 accumulation; dWs, dWn, db are added to (not
+// overwritten). partials: gnn_back_partials_floats() floats of scratch;
+// *fault is set if a tile's MMA did not complete.
+int gnn_back_partials_floats();
+void gnn_dense_back_tc(int n, const float* H, const float* M, const float* out,
+                       const float* dOut, const float* Ws, const float* Wn, float* dH, float* dM,
+                       float* dWs, float* dWn, float* db, float* partials, int* fault,
+                       cudaStream_t s);
 // z += max(0, dots[0] / dots[1]) c.
 void gnn_step(int n, float* z, const float* c, const double* dots, cudaStream_t s);
 void gnn_step64(int n, double* x, const float* c, const double* dots, cudaStream_t s);

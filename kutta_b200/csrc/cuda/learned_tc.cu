@@ -27,6 +27,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cstdint>
 
 #include "common.cuh"
@@ -148,13 +149,15 @@ __device__ __forceinline__ void tmem_dealloc(uint32_t taddr, uint32_t cols) {
   asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(taddr), "r"(cols)
                : "memory");
 }
-// D (tensor memory) = A B^T (+ D when accumulate != 0), one thread.
-__device__ __forceinline__ void mma_bf16(uint32_t d, uint64_t a, uint64_t b, uint32_t accumulate) {
+// D (tensor memory) = A B^T (+ D when accumulate != 0), one thread; `idesc`
+// the instruction descriptor (shape and types).
+__device__ __forceinline__ void mma_bf16(uint32_t d, uint64_t a, uint64_t b, uint32_t accumulate,
+                                         uint32_t idesc = kIdesc) {
   asm volatile(
       "{\n\t.reg .pred p;\n\t"
       "setp.ne.b32 p, %4, 0;\n\t"
       "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}"
-      ::"r"(d), "l"(a), "l"(b), "r"(kIdesc), "r"(accumulate), "r"(0u), "r"(0u), "r"(0u), "r"(0u)
+      ::"r"(d), "l"(a), "l"(b), "r"(idesc), "r"(accumulate), "r"(0u), "r"(0u), "r"(0u), "r"(0u)
       : "memory");
 }
 // Arrives once on the mbarrier when this thread's issued MMAs complete.
@@ -404,6 +407,227 @@ __global__ void __launch_bounds__(kTcThreads, kLift ? 2 : 4)
   }
 }
 
+// ---- backward of a 32-wide layer on the tensor cores ------------------------
+// Layer: out = relu(Ws H + Wn M + b), H and M n x 32 (M = W H), FP32 saved
+// activations. With G = dOut * (out > 0) (n x 32):
+//   dH = G Ws and dM = G Wn (rows i: dH_i[k] = sum_c Ws[c][k] G_i[c]),
+//   dWs = G^T H, dWn = G^T M, db = sum_i G_i.
+// A CTA of 256 threads owns one 128-row tile at a time and issues two GEMMs:
+//   1. D1 (128 x 64) = [G | 0] B1^T with B1[n][c] = Ws[c][n] (n < 32) or
+//      Wn[c][n - 32]: the tile's [dH | dM], read back by warps 0-3 and
+//      stored in FP32 (K = 32: two K = 16 steps of the 64-wide layout);
+//   2. D2 (128 x 32) += A2 B2^T with A2 = [H | M | 1]^T (M-rows: 32 channels
+//      of H, 32 of M, a row of ones; K = the tile's 128 rows in two 64-wide
+//      blocks) and B2 = G^T: accumulated in tensor memory over all the CTA's
+//      tiles, so D2 rows hold dWs^T, dWn^T and db. At the end warps 0-2 write
+//      the CTA's 65 x 32 partial sums; gnn_dense_back_reduce adds the CTAs'
+//      partials in block order.
+// Both GEMMs use the forward's operand layout: K-major, 128-byte rows,
+// 128-byte swizzle, BF16 operands, FP32 accumulators, M = 128. Waits are
+// bounded as in the forward.
+constexpr int kBackThreads = 256;
+constexpr int kBackA1 = 0;                     // [G | 0]: 128 rows x 128 B
+constexpr int kBackB1 = kBackA1 + 16384;       // [Ws | Wn]^T: 64 rows x 128 B
+constexpr int kBackA2 = kBackB1 + 8192;        // two K-blocks of 128 rows x 128 B
+constexpr int kBackB2 = kBackA2 + 2 * 16384;   // two K-blocks of 32 rows x 128 B
+constexpr int kBackTiles = kBackB2 + 2 * 4096;  // 64 KB of operand tiles
+constexpr int kBackSmem = 1024 + kBackTiles + 16;
+constexpr uint32_t kBackColumns = 128;         // D1: columns 0-63, D2: 64-95
+constexpr int kBackPartialRows = 65;           // dWs^T (32), dWn^T (32), db (1)
+// M = 128, N = 64 (D1).
+constexpr uint32_t kIdescN64 = (1u << 4) | (1u << 7) | (1u << 10) | ((64u >> 3) << 17) |
+                               ((static_cast<uint32_t>(kTile) >> 4) << 24);
+
+__device__ __forceinline__ void store_bf16(uint8_t* p, float v) {
+  *reinterpret_cast<__nv_bfloat16*>(p) = __float2bfloat16_rn(v);
+}
+
+__global__ void __launch_bounds__(kBackThreads, 2)
+    k_gnn_dense_back_tc(int n, const float* __restrict__ H, const float* __restrict__ M,
+                        const float* __restrict__ out, const float* __restrict__ dOut,
+                        const float* __restrict__ Ws, const float* __restrict__ Wn,
+                        float* __restrict__ dH, float* __restrict__ dM,
+                        float* __restrict__ partials, int* __restrict__ fault) {
+  extern __shared__ uint8_t raw[];
+  const uint32_t pad = (1024u - (smem_u32(raw) & 1023u)) & 1023u;
+  uint8_t* base = raw + pad;
+  uint64_t* bar = reinterpret_cast<uint64_t*>(base + kBackTiles);
+  uint32_t* slot = reinterpret_cast<uint32_t*>(bar + 1);
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+
+  {  // B1 row n (output channel of [dH | dM]), chunk q < 4 (8 input channels).
+    const int nrow = tid >> 2, q = tid & 3;
+    float v[8];
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+      const int c = 8 * q + k;
+      v[k] = nrow < kC ? Ws[c * kC + nrow] : Wn[c * kC + nrow - kC];
+    }
+    *reinterpret_cast<uint4*>(base + kBackB1 + sw128_offset(nrow, q)) = pack8(v);
+  }
+  // Rows 65-127 of both A2 blocks stay zero (they only feed D2 rows that are
+  // never read).
+  for (int k = tid; k < 2 * 63 * 8; k += kBackThreads) {
+    const int blk = k / (63 * 8), rest = k % (63 * 8);
+    *reinterpret_cast<uint4*>(base + kBackA2 + blk * 16384 + sw128_offset(65 + rest / 8, rest % 8)) =
+        make_uint4(0, 0, 0, 0);
+  }
+  if (tid == 0) mbar_init(smem_u32(bar), 1);
+  __syncwarp();
+  if (warp == 0) tmem_alloc(smem_u32(slot), kBackColumns);
+  proxy_fence();
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = *slot;
+  const uint32_t d1 = tmem, d2 = tmem + 64;
+  const uint64_t a1 = sw128_desc(smem_u32(base + kBackA1));
+  const uint64_t b1 = sw128_desc(smem_u32(base + kBackB1));
+  const uint32_t bar_addr = smem_u32(bar);
+  const int tiles = (n + kTile - 1) / kTile;
+  const int r = tid >> 1, half = tid & 1, c0 = 16 * half;
+  const int kb = r >> 6, kk = r & 63, kq = kk >> 3, ke = kk & 7;  // r as a K index of GEMM 2
+  uint8_t* a2 = base + kBackA2 + kb * 16384;
+  uint8_t* b2 = base + kBackB2 + kb * 4096;
+  uint32_t phase = 0;
+  bool failed = false, any = false;
+
+  for (int tile = blockIdx.x; tile < tiles; tile += gridDim.x) {
+    const int i = tile * kTile + r;
+    const bool valid = i < n;
+    float g[16], h[16], m[16];
+    if (valid) {
+      const std::size_t row = static_cast<std::size_t>(i) * kC + c0;
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        const float4 o = *reinterpret_cast<const float4*>(out + row + 4 * q);
+        const float4 d = *reinterpret_cast<const float4*>(dOut + row + 4 * q);
+        const float4 hv = *reinterpret_cast<const float4*>(H + row + 4 * q);
+        const float4 mv = *reinterpret_cast<const float4*>(M + row + 4 * q);
+        g[4 * q] = o.x > 0.0f ? d.x : 0.0f;
+        g[4 * q + 1] = o.y > 0.0f ? d.y : 0.0f;
+        g[4 * q + 2] = o.z > 0.0f ? d.z : 0.0f;
+        g[4 * q + 3] = o.w > 0.0f ? d.w : 0.0f;
+        h[4 * q] = hv.x;
+        h[4 * q + 1] = hv.y;
+        h[4 * q + 2] = hv.z;
+        h[4 * q + 3] = hv.w;
+        m[4 * q] = mv.x;
+        m[4 * q + 1] = mv.y;
+        m[4 * q + 2] = mv.z;
+        m[4 * q + 3] = mv.w;
+      }
+    } else {
+#pragma unroll
+      for (int k = 0; k < 16; ++k) g[k] = h[k] = m[k] = 0.0f;
+    }
+    // GEMM 1 operand: row r, K chunks 2 half and 2 half + 1 (channels c0..c0+15).
+    *reinterpret_cast<uint4*>(base + kBackA1 + sw128_offset(r, 2 * half)) = pack8(g);
+    *reinterpret_cast<uint4*>(base + kBackA1 + sw128_offset(r, 2 * half + 1)) = pack8(g + 8);
+    // GEMM 2 operands, transposed: element (channel, r) of A2 and B2.
+#pragma unroll
+    for (int k = 0; k < 16; ++k) {
+      const int c = c0 + k;
+      store_bf16(a2 + sw128_offset(c, kq) + 2 * ke, h[k]);
+      store_bf16(a2 + sw128_offset(kC + c, kq) + 2 * ke, m[k]);
+      store_bf16(b2 + sw128_offset(c, kq) + 2 * ke, g[k]);
+    }
+    if (half == 0) store_bf16(a2 + sw128_offset(2 * kC, kq) + 2 * ke, valid ? 1.0f : 0.0f);
+    proxy_fence();
+    tc_fence_before();
+    __syncthreads();
+    if (tid == 0) {
+      tc_fence_after();
+#pragma unroll
+      for (int k = 0; k < 2; ++k) mma_bf16(d1, a1 + 2 * k, b1 + 2 * k, k > 0 ? 1u : 0u, kIdescN64);
+#pragma unroll
+      for (int blk = 0; blk < 2; ++blk) {
+        const uint64_t a2d = sw128_desc(smem_u32(base + kBackA2 + blk * 16384));
+        const uint64_t b2d = sw128_desc(smem_u32(base + kBackB2 + blk * 4096));
+#pragma unroll
+        for (int k = 0; k < 4; ++k)
+          mma_bf16(d2, a2d + 2 * k, b2d + 2 * k, (any || blk > 0 || k > 0) ? 1u : 0u);
+      }
+      mma_commit(bar_addr);
+    }
+    any = true;
+    const bool done = mbar_wait(bar_addr, phase, kSpinLimit);
+    if (__syncthreads_or(!done)) {
+      failed = true;
+      break;
+    }
+    phase ^= 1u;
+    tc_fence_after();
+    if (warp < 4) {
+      float acc[32];
+      const uint32_t lanes = static_cast<uint32_t>(warp * 32) << 16;
+      const int row = tile * kTile + warp * 32 + lane;
+      tmem_load32(d1 + lanes, acc);
+      if (row < n) {
+        float4* dst = reinterpret_cast<float4*>(dH + static_cast<std::size_t>(row) * kC);
+#pragma unroll
+        for (int q = 0; q < 8; ++q)
+          dst[q] = make_float4(acc[4 * q], acc[4 * q + 1], acc[4 * q + 2], acc[4 * q + 3]);
+      }
+      tmem_load32(d1 + lanes + 32, acc);
+      if (row < n) {
+        float4* dst = reinterpret_cast<float4*>(dM + static_cast<std::size_t>(row) * kC);
+#pragma unroll
+        for (int q = 0; q < 8; ++q)
+          dst[q] = make_float4(acc[4 * q], acc[4 * q + 1], acc[4 * q + 2], acc[4 * q + 3]);
+      }
+    }
+    tc_fence_before();
+  }
+  if (failed) {
+    if (tid == 0) atomicOr(fault, 1);
+    mbar_wait(bar_addr, phase, kSpinLimit);  // the late MMAs, once more (full bound)
+  } else if (warp < 3) {
+    // This CTA's partial sums: D2 rows 0-64, 32 columns (zeros if it had no tile).
+    tc_fence_after();
+    float acc[32];
+    const int mrow = warp * 32 + lane;
+    if (any) {
+      tmem_load32(d2 + (static_cast<uint32_t>(warp * 32) << 16), acc);
+    } else {
+#pragma unroll
+      for (int k = 0; k < 32; ++k) acc[k] = 0.0f;
+    }
+    if (mrow < kBackPartialRows) {
+      float* dst = partials + (static_cast<std::size_t>(blockIdx.x) * kBackPartialRows + mrow) * kC;
+#pragma unroll
+      for (int k = 0; k < 32; ++k) dst[k] = acc[k];
+    }
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 0) {
+    tc_fence_after();
+    tmem_dealloc(tmem, kBackColumns);
+  }
+}
+
+// dWs[c][k] += sum_b P_b[k][c], dWn[c][k] += sum_b P_b[32 + k][c], db[c] +=
+// sum_b P_b[64][c], blocks in order.
+__global__ void k_gnn_dense_back_reduce(int blocks, const float* __restrict__ partials,
+                                        float* __restrict__ dWs, float* __restrict__ dWn,
+                                        float* __restrict__ db) {
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= kBackPartialRows * kC) return;
+  const int mrow = e / kC, c = e % kC;
+  float sum = 0.0f;
+  for (int b = 0; b < blocks; ++b)
+    sum += partials[(static_cast<std::size_t>(b) * kBackPartialRows + mrow) * kC + c];
+  if (mrow < kC) dWs[c * kC + mrow] += sum;
+  else if (mrow < 2 * kC) dWn[c * kC + mrow - kC] += sum;
+  else db[c] += sum;
+}
+
+int back_grid(int n) {
+  const int tiles = (n + kTile - 1) / kTile;
+  return std::max(1, std::min(tiles, kSms * 2));
+}
+
 // The poll count of each tile's first wait for its MMA: kSpinLimit unless a
 // test asked for fewer (0..kSpinLimit).
 long long wait_polls(long long requested) {
@@ -418,6 +642,23 @@ int tc_grid(int n) {
 }  // namespace
 
 namespace launch {
+
+int gnn_back_partials_floats() { return kSms * 2 * kBackPartialRows * kC; }
+
+void gnn_dense_back_tc(int n, const float* H, const float* M, const float* out,
+                       const float* dOut, const float* Ws, const float* Wn, float* dH, float* dM,
+                       float* dWs, float* dWn, float* db, float* partials, int* fault,
+                       cudaStream_t s) {
+  if (n <= 0) return;
+  static std::atomic<unsigned long long> raised{0};
+  raise_shared_limit(reinterpret_cast<const void*>(k_gnn_dense_back_tc), kBackSmem, raised);
+  counter += 2;
+  const int blocks = back_grid(n);
+  k_gnn_dense_back_tc<<<blocks, kBackThreads, kBackSmem, s>>>(n, H, M, out, dOut, Ws, Wn, dH, dM,
+                                                               partials, fault);
+  k_gnn_dense_back_reduce<<<(kBackPartialRows * kC + kBlock - 1) / kBlock, kBlock, 0, s>>>(
+      blocks, partials, dWs, dWn, db);
+}
 
 void gnn_lift(int n, const int* rows, const int* cols, const float* lift, const float* t,
               const float* node_scale, float2* uv, DeviceReducer red, double* sum2,

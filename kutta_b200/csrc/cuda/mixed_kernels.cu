@@ -539,19 +539,6 @@ __global__ void k_narrow(int n, const double* __restrict__ y, float* __restrict_
   ROWS(i, n) x[i] = static_cast<float>(y[i]);
 }
 
-// A kernel's dynamic shared-memory ceiling is an attribute of the function in
-// one device's context, so it is raised once per device this process uses
-// (bit d of `done` for device d < 64; higher devices raise it on every call).
-void raise_shared_limit(const void* kernel, int bytes, std::atomic<unsigned long long>& done) {
-  int device = 0;
-  if (cudaGetDevice(&device) != cudaSuccess) return;
-  const unsigned long long bit = device < 64 ? 1ull << device : 0;
-  if (bit && (done.load(std::memory_order_acquire) & bit)) return;
-  if (cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes) ==
-      cudaSuccess)
-    done.fetch_or(bit, std::memory_order_release);
-}
-
 }  // namespace
 
 namespace launch {

@@ -152,7 +152,12 @@ void Gnn::forward32(const float* r, float* z, cudaStream_t s) {
   launch::gnn_output(n_, h_[kLayers].get(), p.wo, scale_.get(), sums_.get(), z, 0.0f, s);
 }
 
-float Gnn::train_step(const float* t, const float* e, float lr, cudaStream_t s) {
+// The energy loss's gradient at the current weights into grads_ (and the loss
+// into loss_): the FP32 forward keeping every layer's activations, then the
+// backward, whose two 32-wide layers run on the tensor cores when asked
+// (gnn_dense_back_tc, BF16 operands, FP32 accumulation) and the 1-wide input
+// layer on CUDA cores.
+void Gnn::backward(const float* t, const float* e, bool tensor_cores, cudaStream_t s) {
   KB2_REQUIRE(n_ > 0, "learned stage: no matrix bound");
   KB2_REQUIRE(t != nullptr && e != nullptr, "learned stage: null training vector");
   check_device();
@@ -171,14 +176,28 @@ float Gnn::train_step(const float* t, const float* e, float lr, cudaStream_t s) 
   launch::gnn_output_back(n_, h_[kLayers].get(), p.wo, scale_.get(), sums_.get(), dz_.get(),
                           dh_.get(), g.wo, s);
   for (int l = kLayers - 1; l >= 0; --l) {
-    launch::gnn_dense_back(n_, cin(l), h_[l].get(), m_agg_[l].get(), h_[l + 1].get(), dh_.get(),
-                           p.ws[l], p.wn[l], dhs_.get(), dm_.get(), g.ws[l], g.wn[l], g.b[l], s);
+    if (tensor_cores && cin(l) == kHidden) {
+      if (!back_partials_.allocated())
+        back_partials_.reset(static_cast<std::size_t>(launch::gnn_back_partials_floats()));
+      launch::gnn_dense_back_tc(n_, h_[l].get(), m_agg_[l].get(), h_[l + 1].get(), dh_.get(),
+                                p.ws[l], p.wn[l], dhs_.get(), dm_.get(), g.ws[l], g.wn[l],
+                                g.b[l], back_partials_.get(), fault_.get(), s);
+    } else {
+      launch::gnn_dense_back(n_, cin(l), h_[l].get(), m_agg_[l].get(), h_[l + 1].get(),
+                             dh_.get(), p.ws[l], p.wn[l], dhs_.get(), dm_.get(), g.ws[l],
+                             g.wn[l], g.b[l], s);
+    }
     if (l > 0) {
       // dL/dh[l] = Ws^T G + W^T (Wn^T G); W is symmetric.
       launch::gnn_aggregate(n_, cin(l), rows_, cols_, edge_.get(), dm_.get(), dagg_.get(), s);
       launch::gnn_add(static_cast<std::size_t>(n_) * cin(l), dhs_.get(), dagg_.get(), dh_.get(), s);
     }
   }
+}
+
+float Gnn::train_step(const float* t, const float* e, float lr, cudaStream_t s) {
+  backward(t, e, true, s);
+  const int count = parameter_count();
   ++step_;
   const float beta1 = 0.9f, beta2 = 0.999f;
   launch::gnn_adam(count, params_.get(), grads_.get(), m_.get(), v_.get(), lr, beta1, beta2, 1e-8f,
@@ -187,8 +206,23 @@ float Gnn::train_step(const float* t, const float* e, float lr, cudaStream_t s) 
   float loss = 0;
   cuda_check(cudaMemcpyAsync(&loss, loss_.get(), sizeof(float), cudaMemcpyDeviceToHost, s),
              "loss readback");
-  wait(s);
+  check(s);  // waits; a tensor-core tile that did not complete raises a timeout
   return loss;
+}
+
+std::vector<float> Gnn::gradient(const float* t, const float* e, bool tensor_cores, float* loss,
+                                 cudaStream_t s) {
+  backward(t, e, tensor_cores, s);
+  std::vector<float> out(static_cast<std::size_t>(parameter_count()));
+  cuda_check(cudaMemcpyAsync(out.data(), grads_.get(), sizeof(float) * out.size(),
+                             cudaMemcpyDeviceToHost, s),
+             "gradient readback");
+  float value = 0;
+  cuda_check(cudaMemcpyAsync(&value, loss_.get(), sizeof(float), cudaMemcpyDeviceToHost, s),
+             "loss readback");
+  check(s);
+  if (loss) *loss = value;
+  return out;
 }
 
 std::vector<float> Gnn::weights() const {

@@ -36,8 +36,14 @@ class Gnn {
   // complete (host wait on s).
   void check(cudaStream_t s);
   // One Adam step on the energy loss of G(t) for A e = t (the bound matrix);
-  // returns that loss before the step (host wait).
+  // returns that loss before the step (host wait). The backward's two 32-wide
+  // layers run on the tensor cores.
   float train_step(const float* t, const float* e, float lr, cudaStream_t s);
+  // The energy loss's gradient at the current weights (no step), with the
+  // 32-wide layers' backward on the tensor cores or on CUDA cores in FP32;
+  // *loss (if not null) receives the loss. Host wait.
+  std::vector<float> gradient(const float* t, const float* e, bool tensor_cores, float* loss,
+                              cudaStream_t s);
   std::vector<float> weights() const;
   void set_weights(const std::vector<float>& w);
   int rows() const { return n_; }
@@ -58,6 +64,9 @@ class Gnn {
   // The FP32 forward of learned.cu, keeping every layer's activations for
   // the backward pass of training.
   void forward32(const float* r, float* z, cudaStream_t s);
+  // Gradient of the energy loss into grads_, the loss into loss_.
+  void backward(const float* t, const float* e, bool tensor_cores, cudaStream_t s);
+  DArray<float> back_partials_;  // per-CTA partial weight gradients (tensor-core backward)
   int n_ = 0;
   int device_ = 0;
   const int* rows_ = nullptr;

@@ -202,6 +202,7 @@ _SIGNATURES = {
     "b2_gnn_apply": (_I, [_P, _P, _P, ctypes.c_float, _P]),
     "b2_gnn_train_step": (_I, [_P, _P, _P, ctypes.c_float, _P, _P]),
     "b2_gnn_set_wait_limit": (_I, [_P, ctypes.c_longlong]),
+    "b2_gnn_gradient": (_I, [_P, _P, _P, _I, _P, ctypes.c_size_t, _P, _P]),
     "b2_gnn_get_weights": (_I, [_P, _P, ctypes.c_size_t]),
     "b2_gnn_set_weights": (_I, [_P, _P, ctypes.c_size_t]),
     "b2_mixed_set_learned": (_I, [_P, _P, _I]),
@@ -650,6 +651,16 @@ class LearnedStage:
         _check(_load().b2_gnn_train_step(self._handle, _tptr(t), _tptr(e), learning_rate,
                                          ctypes.byref(loss), _stream()))
         return float(loss.value)
+
+    def gradient(self, t, e, tensor_cores: bool = True) -> tuple[np.ndarray, float]:
+        """(gradient of the energy loss at the current weights, loss), no step;
+        tensor_cores: the 32-wide layers' backward on the tensor cores (as
+        train_step) or in FP32 on CUDA cores."""
+        g = np.empty(self.parameter_count(), np.float32)
+        loss = ctypes.c_float()
+        _check(_load().b2_gnn_gradient(self._handle, _tptr(t), _tptr(e), int(tensor_cores),
+                                       _ptr(g), g.size, ctypes.byref(loss), _stream()))
+        return g, float(loss.value)
 
     def weights(self) -> np.ndarray:
         w = np.empty(self.parameter_count(), np.float32)
