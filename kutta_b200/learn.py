@@ -3,15 +3,17 @@
 Training data: seeded 64^3 jittered hex meshes of the unit cube with smooth
 log-normal D_f (sigma 1.5, correlation length 0.1), right-hand sides of 16
 seeded Fourier modes over the cell centroids plus 10 % white noise (scaled by
-cell volume), and their solutions x computed by the mixed solve itself to
-relative 1e-8 in FP64. Each (matrix, b, x) triple yields the pairs the stage
-sees inside the solve: for a residual r of an iterate x_k (x_k = 0, and x_k
-from a solve to relative 1e-3), z = M(r) is one application of the AMG
-preconditioner, t = r - A z what it leaves and e = (x - x_k) - z the error with
-A e = t. Training runs the CUDA forward, backward and Adam kernels
-(b2_gnn_train_step) over the pairs in a seeded random order, on the energy loss
-1 - (c.t)^2 / ((c.Ac)(t.e)) for c = G(t): the fraction of the error's A-energy
-that the best step along c leaves.
+cell volume), and their solutions x computed by the plain FP32 AMG-PCG (the
+reference's method) to relative 1e-6 or its FP32 floor. Each (matrix, b, x)
+triple yields the pairs the stage sees inside the mixed solve: for an iterate
+x_k (x_k = 0, and the plain solver's solution to relative 1e-3), z = M(r) is
+one application of the mixed solve's AMG preconditioner to r = b - A x_k,
+e = (x - x_k) - z the error it leaves and t = A e (FP64), so A e = t holds
+exactly. Training runs the CUDA forward, the backward (its 32-wide layers on
+the tensor cores) and the Adam step (b2_gnn_train_step) over the pairs in a
+seeded random order, on the energy loss 1 - (c.t)^2 / ((c.Ac)(t.e)) for
+c = G(t): the fraction of the error's A-energy that the best step along c
+leaves.
 
 Evaluation: unseen 128^3 seeds of the same family, the mixed solve to
 relative 1e-6 with and without the stage attached, and the plain FP32
@@ -62,43 +64,50 @@ def _csr64(s: harness.HostSystem):
                                    (s.n, s.n)).cuda()
 
 
-def pairs(s: harness.HostSystem, a: L.CsrMatrix, solver: L.MixedSolver, b, x):
-    """(t, e) pairs with A e = t from the solution x of A x = b: the residual
-    of x_k = 0 and of a solve to relative 1e-3, each after one application of
-    the preconditioner."""
+def pairs(s: harness.HostSystem, a: L.CsrMatrix, solver, preconditioner: L.MixedSolver, b, x):
+    """(t, e) pairs with A e = t exactly, from the plain solver's solution x of
+    A x = b: for the iterates x_k = 0 and x_k = the plain solver's 1e-3
+    solution, z is one application of the mixed preconditioner (where the
+    stage is used) to r = b - A x_k, e = (x - x_k) - z the error that remains,
+    and t = A e in FP64 (the residual the stage sees, up to the plain
+    solution's own small error)."""
     import torch
     A = _csr64(s)
     out = []
-    xk = torch.zeros(s.n, dtype=torch.float64, device="cuda")
+    xk = torch.zeros(s.n, dtype=torch.float32, device="cuda")
     for tol in (None, 1e-3):
         if tol is not None:
             solver.solve(a, xk, b, L.SolveControl(tol, 1e-30, 3000))
-        r = (b.double() - A @ xk).float()
+        r = (b.double() - A @ xk.double()).float()
         z = torch.zeros(s.n, dtype=torch.float32, device="cuda")
-        solver.precondition(a, r, z)
-        t = r.double() - A @ z.double()
-        e = (x - xk) - z.double()
+        preconditioner.precondition(a, r, z)
+        e = (x - xk.double()) - z.double()
+        t = A @ e
         out.append((t.float(), e.float()))
     return out
 
 
 def training_set(count: int, n_side: int, rhs_per_system: int, seed0: int):
-    """[(device matrix, t, e)] from `count` systems x `rhs_per_system` solves."""
+    """[(device matrix, t, e)] from `count` systems x `rhs_per_system` solves of
+    the plain FP32 AMG-PCG (the reference's method; to relative 1e-6 or its
+    FP32 floor, whichever it reaches)."""
     import torch
     rng = np.random.default_rng(seed0)
     data = []
     for k in range(count):
         s = system(n_side, seed0 + k)
         a = L.upload(s)
-        solver = L.make_mixed_solver(s)
-        solver.refresh(a)
+        plain = L.make_solver(L.SolverKind.AmgPcg, s, L.SolverOptions(
+            structure=L.OperatorStructure.SymmetricMMatrix))
+        plain.refresh(a)
+        mixed = L.make_mixed_solver(s)
+        mixed.refresh(a)
         for _ in range(rhs_per_system):
             b = torch.from_numpy(fourier_rhs(s, rng)).cuda()
-            x = torch.zeros(s.n, dtype=torch.float64, device="cuda")
-            st = solver.solve(a, x, b, L.SolveControl(1e-8, 1e-30, 3000))
-            if st.converged:
-                data.extend((a, t, e) for t, e in pairs(s, a, solver, b, x))
-        del solver
+            x = torch.zeros(s.n, dtype=torch.float32, device="cuda")
+            plain.solve(a, x, b, L.SolveControl(1e-6, 1e-30, 3000))
+            data.extend((a, t, e) for t, e in pairs(s, a, plain, mixed, b, x.double()))
+        del plain, mixed
     return data
 
 
@@ -174,11 +183,14 @@ def evaluate(stage: L.LearnedStage | None, n_side: int, seeds, rel_tol: float = 
             row[name] = {"ms": best, "iterations": st.iterations, "converged": bool(st.converged),
                          "relative_residual": st.final_residual / st.initial_residual}
             if g is not None:
-                x_true = torch.zeros(s.n, dtype=torch.float64, device="cuda")
                 solver.set_learned(None)
-                solver.solve(a, x_true, b, L.SolveControl(1e-8, 1e-30, 3000))
-                row["held_out_energy_loss"] = held_out_loss(g, [(a, t, e) for t, e in
-                                                                pairs(s, a, solver, b, x_true)])
+                plain = L.make_solver(L.SolverKind.AmgPcg, s, L.SolverOptions(
+                    structure=L.OperatorStructure.SymmetricMMatrix))
+                plain.refresh(a)
+                x_plain = torch.zeros(s.n, dtype=torch.float32, device="cuda")
+                plain.solve(a, x_plain, b, L.SolveControl(1e-6, 1e-30, 3000))
+                row["held_out_energy_loss"] = held_out_loss(
+                    g, [(a, t, e) for t, e in pairs(s, a, plain, solver, b, x_plain.double())])
             del solver
         results.append(row)
     return {"rel_tol": rel_tol, "mesh": f"{n_side}^3 jittered hex, smooth log-normal D_f "
