@@ -6,7 +6,7 @@ seeded Fourier modes over the cell centroids plus 10 % white noise (scaled by
 cell volume), and their solutions x computed by the plain FP32 AMG-PCG (the
 reference's method) to relative 1e-6 or its FP32 floor. Each (matrix, b, x)
 triple yields the pairs the stage sees inside the mixed solve: for an iterate
-x_k (x_k = 0, and the plain solver's solution to relative 1e-3), z = M(r) is
+x_k (x_k = 0, and the mixed solve's iterate at relative 1e-3), z = M(r) is
 one application of the mixed solve's AMG preconditioner to r = b - A x_k,
 e = (x - x_k) - z the error it leaves and t = A e (FP64), so A e = t holds
 exactly. Training runs the CUDA forward, the backward (its 32-wide layers on
@@ -64,24 +64,24 @@ def _csr64(s: harness.HostSystem):
                                    (s.n, s.n)).cuda()
 
 
-def pairs(s: harness.HostSystem, a: L.CsrMatrix, solver, preconditioner: L.MixedSolver, b, x):
+def pairs(s: harness.HostSystem, a: L.CsrMatrix, mixed: L.MixedSolver, b, x):
     """(t, e) pairs with A e = t exactly, from the plain solver's solution x of
-    A x = b: for the iterates x_k = 0 and x_k = the plain solver's 1e-3
-    solution, z is one application of the mixed preconditioner (where the
-    stage is used) to r = b - A x_k, e = (x - x_k) - z the error that remains,
-    and t = A e in FP64 (the residual the stage sees, up to the plain
-    solution's own small error)."""
+    A x = b, for the iterates the stage meets inside the mixed solve: x_k = 0,
+    and the mixed solve's own iterate at relative 1e-3. z is one application
+    of the mixed solve's preconditioner to r = b - A x_k, e = (x - x_k) - z the
+    error that remains, and t = A e in FP64 (the residual the stage sees, up
+    to the plain solution's own small error)."""
     import torch
     A = _csr64(s)
     out = []
-    xk = torch.zeros(s.n, dtype=torch.float32, device="cuda")
+    xk = torch.zeros(s.n, dtype=torch.float64, device="cuda")
     for tol in (None, 1e-3):
         if tol is not None:
-            solver.solve(a, xk, b, L.SolveControl(tol, 1e-30, 3000))
-        r = (b.double() - A @ xk.double()).float()
+            mixed.solve(a, xk, b, L.SolveControl(tol, 1e-30, 3000))
+        r = (b.double() - A @ xk).float()
         z = torch.zeros(s.n, dtype=torch.float32, device="cuda")
-        preconditioner.precondition(a, r, z)
-        e = (x - xk.double()) - z.double()
+        mixed.precondition(a, r, z)
+        e = (x - xk) - z.double()
         t = A @ e
         out.append((t.float(), e.float()))
     return out
@@ -106,7 +106,7 @@ def training_set(count: int, n_side: int, rhs_per_system: int, seed0: int):
             b = torch.from_numpy(fourier_rhs(s, rng)).cuda()
             x = torch.zeros(s.n, dtype=torch.float32, device="cuda")
             plain.solve(a, x, b, L.SolveControl(1e-6, 1e-30, 3000))
-            data.extend((a, t, e) for t, e in pairs(s, a, plain, mixed, b, x.double()))
+            data.extend((a, t, e) for t, e in pairs(s, a, mixed, b, x.double()))
         del plain, mixed
     return data
 
@@ -190,7 +190,7 @@ def evaluate(stage: L.LearnedStage | None, n_side: int, seeds, rel_tol: float = 
                 x_plain = torch.zeros(s.n, dtype=torch.float32, device="cuda")
                 plain.solve(a, x_plain, b, L.SolveControl(1e-6, 1e-30, 3000))
                 row["held_out_energy_loss"] = held_out_loss(
-                    g, [(a, t, e) for t, e in pairs(s, a, plain, solver, b, x_plain.double())])
+                    g, [(a, t, e) for t, e in pairs(s, a, solver, b, x_plain.double())])
             del solver
         results.append(row)
     return {"rel_tol": rel_tol, "mesh": f"{n_side}^3 jittered hex, smooth log-normal D_f "
