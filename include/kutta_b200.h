@@ -331,7 +331,9 @@ int b2_gnn_set_weights(b2_gnn* g, const float* host, size_t count);
  *     max(0, c.t / c.Ac), so the stage never makes the error larger in the
  *     A-norm (the flexible inner PCG absorbs the variable preconditioner);
  *   B2_LEARNED_WARM_START: before the refinement loop, the initial guess x0
- *     takes the same safeguarded step along G(b - A x0). */
+ *     takes a safeguarded step along c = G(r), r = b - A x0, of the length
+ *     max(0, r.Ac / Ac.Ac) that minimises the new residual (the solve stops
+ *     on the residual), so the warm start never raises it. */
 #define B2_LEARNED_CYCLE 1
 #define B2_LEARNED_WARM_START 2
 int b2_mixed_set_learned(b2_mixed* solver, b2_gnn* g, int mode);

@@ -623,14 +623,22 @@ void Solver::learned_direction(const float* t) {
   tally(8.0 * nnz_ + 4.0 * (n_ + 1) + 8.0 * n_ + 16.0 * n_);
 }
 
+// The warm start takes the step along c = G(r) that minimises the residual,
+// alpha = max(0, r.Ac / Ac.Ac): the solve stops on the residual, and the
+// energy-optimal step of the cycle stage can raise it (1.25x on the white-noise
+// right-hand side of the pressure matrices here), which costs the refinement
+// loop iterations. This step never raises the residual.
 void Solver::learned_warm_start(const float* val, const float* r, double* x, cudaStream_t s) {
   if (learned_ == nullptr || !(learned_mode_ & kLearnedWarmStart)) return;
   stream_ = s;
   val_ = val;
   reset(0);
   learned_direction(r);
-  launch::gnn_step64(n_, x, learned_correction_.get(), learned_dots_.get(), stream_);
-  tally(20.0 * n_);
+  const float* q = learned_product_.get();
+  launch::reduce_value(ReduceMode::Dot, n_, q, r, reducer(), learned_dots_.get(), 2, stream_);
+  launch::reduce_value(ReduceMode::Dot, n_, q, q, reducer(), learned_dots_.get(), 3, stream_);
+  launch::gnn_step64(n_, x, learned_correction_.get(), learned_dots_.get() + 2, stream_);
+  tally(16.0 * n_ + 20.0 * n_);
 }
 
 void Solver::precondition_into(const float* val, const float* r, float* z, cudaStream_t s) {
@@ -664,7 +672,7 @@ void Solver::set_learned(Gnn* g, int mode) {
       learned_residual_.reset(static_cast<std::size_t>(n_));
       learned_correction_.reset(static_cast<std::size_t>(n_));
       learned_product_.reset(static_cast<std::size_t>(n_));
-      learned_dots_.reset(2);
+      learned_dots_.reset(4);
     }
     if (val_ != nullptr) g->bind(n_, rows0(), cols0(), levels_[0].diag.get(), val_, stream_);
   }

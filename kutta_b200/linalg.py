@@ -597,8 +597,9 @@ class MixedSolver:
 
     def set_learned(self, stage: "LearnedStage | None", mode: int = LEARNED_CYCLE) -> None:
         """Attaches a learned stage (None detaches): after each AMG cycle
-        (LEARNED_CYCLE) and/or as a warm-start step (LEARNED_WARM_START); the
-        stage must stay alive while attached."""
+        (LEARNED_CYCLE, the energy-optimal step) and/or as a warm-start step
+        (LEARNED_WARM_START, the residual-optimal step); the stage must stay
+        alive while attached."""
         self._learned = stage
         _check(_load().b2_mixed_set_learned(self._handle, stage._handle if stage else None,
                                             int(mode) if stage else 0))

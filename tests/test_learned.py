@@ -309,6 +309,35 @@ def test_learned_stage_in_mixed_solve(cuda, mode):
 
 
 @pytest.mark.gpu
+def test_warm_start_never_raises_the_residual(cuda):
+    """The learned warm start's step along c = G(b - A x0) has the length that
+    minimises the new residual, clipped at zero: with max_iter = 0 the solve
+    returns right after the warm start, and its FP64 residual is no larger
+    than the initial one (here on a white-noise right-hand side, where the
+    energy-optimal length would raise it)."""
+    import scipy.sparse as sp
+    import torch
+    from kutta_b200 import learn
+    s = harness.box_system(16, 16, 16, tet=True, seed=9)
+    a = L.upload(s)
+    solver = L.make_mixed_solver(s)
+    solver.refresh(a)
+    stage = learn.trained_stage()
+    solver.set_learned(stage, L.LEARNED_WARM_START)
+    b = torch.from_numpy(s.b).cuda()
+    x = torch.zeros(s.n, dtype=torch.float64, device="cuda")
+    st = solver.solve(a, x, b, L.SolveControl(1e-6, 1e-30, 0))
+    torch.cuda.synchronize()
+    solver.set_learned(None)
+    assert st.iterations == 0
+    A = sp.csr_matrix((s.val, s.col, s.row_ptr), shape=(s.n, s.n))
+    true = float(np.linalg.norm(s.b.astype(np.float64) - A @ x.cpu().numpy()))
+    assert true == pytest.approx(st.final_residual, rel=1e-6)
+    assert st.final_residual <= st.initial_residual
+    assert np.any(x.cpu().numpy() != 0.0)  # a step was taken
+
+
+@pytest.mark.gpu
 def test_learned_mode_is_validated(cuda):
     s = harness.box_system(6, 6, 6, tet=True, seed=2)
     a = L.upload(s)
