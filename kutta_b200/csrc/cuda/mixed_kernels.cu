@@ -226,75 +226,226 @@ __global__ void k_inner_first_dot(int n, const float* __restrict__ b, const floa
   finish_dot2(red, tt, bb, scalars, 4);
 }
 
-// Dense FP64 Cholesky of the coarsest operator and its explicit inverse, in one
-// block (n <= 1024). L is n x n row-major scratch and W the n x n inverse, both
-// in global memory (the level is small, so both stay in cache). *error is
-// written at the end: 1 if a pivot was not positive (the operator is not SPD;
-// such a pivot is replaced by 1 so the kernel ends), else 0. If `ratio` is not
-// null, *ratio is the smallest pivot relative to its row's diagonal (0 if one
-// failed): close to 0 when the operator is nearly singular.
-__global__ void __launch_bounds__(1024)
-    k_dense_inverse(int n, const int* __restrict__ rows, const int* __restrict__ cols,
-                    const float* __restrict__ vals, double* __restrict__ L,
-                    double* __restrict__ W, double* error, double* ratio) {
+// Dense FP64 Cholesky of the coarsest operator and its explicit inverse for
+// kPackedDense < n <= 1024, blocked in 32 x 32 blocks and spread over many
+// CTAs (a sequence of launches at refresh time). L is n x n row-major scratch
+// in global memory (2 MB at n = 512, L2-resident) and W the n x n inverse.
+//   1. L = the lower triangle of A (the strict upper triangle is free; the
+//      original diagonal is kept there for the pivot ratio: a_kk at L[k][n-1],
+//      a_{n-1,n-1} at L[0][n-2]);
+//   2. per 32-column panel: the diagonal block factored in one CTA (shared
+//      memory), the rows below solved against it (a thread per row), the
+//      trailing lower triangle updated tile by tile (a CTA per 32 x 32 tile);
+//   3. X = L^-1 into W's lower triangle: the diagonal blocks inverted in
+//      parallel, then block diagonal d = 1, 2, ...: X_ij = -X_ii sum_{k=j}^{i-1}
+//      L_ik X_kj for i - j = d, a CTA per block;
+//   4. W = X^T X tile by tile into L's buffer, then copied to W.
+// Every element is summed in a fixed order, so the result is deterministic.
+// *error = 1 if a pivot was not positive (it is replaced by 1 so the kernels
+// finish), else 0; with `ratio`, *ratio is the smallest pivot relative to its
+// row's original diagonal (0 if one failed).
+constexpr int kNb = 32;                         // block size
+constexpr int kNbThreads = kNb * kNb;           // one thread per block element
+
+__device__ __forceinline__ std::size_t at(int n, int i, int j) {
+  return static_cast<std::size_t>(i) * n + j;
+}
+// Where row k's original diagonal is kept (strict upper triangle of L).
+__device__ __forceinline__ std::size_t diag_slot(int n, int k) {
+  return k < n - 1 ? at(n, k, n - 1) : at(n, 0, n - 2);
+}
+
+__global__ void k_dense_zero(std::size_t count, double* __restrict__ L) {
   pdl_entry();
-  const int t = threadIdx.x, T = blockDim.x;
-  __shared__ int failed;
-  __shared__ double smallest;
-  __shared__ double diag0[1024];
-  if (t == 0) {
-    failed = 0;
-    smallest = 1.0;
-  }
-  for (int k = t; k < n * n; k += T) L[k] = 0.0;
-  __syncthreads();
-  for (int i = t; i < n; i += T)
+  for (std::size_t k = blockIdx.x * static_cast<std::size_t>(blockDim.x) + threadIdx.x; k < count;
+       k += static_cast<std::size_t>(gridDim.x) * blockDim.x)
+    L[k] = 0.0;
+}
+
+__global__ void k_dense_scatter(int n, const int* __restrict__ rows, const int* __restrict__ cols,
+                                const float* __restrict__ vals, double* __restrict__ L,
+                                double* error, double* ratio) {
+  pdl_entry();
+  ROWS(i, n) {
     for (int j = rows[i]; j < rows[i + 1]; ++j) {
-      if (cols[j] <= i) L[static_cast<std::size_t>(i) * n + cols[j]] = vals[j];
-      if (cols[j] == i) diag0[i] = vals[j];
+      const int c = cols[j];
+      if (c <= i) L[at(n, i, c)] = vals[j];
+      if (c == i) L[diag_slot(n, i)] = vals[j];
     }
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    *error = 0.0;
+    if (ratio) *ratio = 1.0;
+  }
+}
+
+// Factor the diagonal block of panel k0 (b = min(32, n - k0) columns) in place.
+__global__ void __launch_bounds__(kNbThreads)
+    k_dense_panel_factor(int n, int k0, double* __restrict__ L, double* error, double* ratio) {
+  pdl_entry();
+  __shared__ double D[kNb][kNb + 1];
+  const int b = min(kNb, n - k0);
+  const int r = threadIdx.x / kNb, c = threadIdx.x % kNb;
+  if (r < b && c <= r) D[r][c] = L[at(n, k0 + r, k0 + c)];
   __syncthreads();
-  __shared__ double pivot;
-  for (int k = 0; k < n; ++k) {
-    if (t == 0) {
-      double d = L[static_cast<std::size_t>(k) * n + k];
+  for (int k = 0; k < b; ++k) {
+    if (threadIdx.x == 0) {
+      double d = D[k][k];
       if (!(d > 0.0)) {
-        failed = 1;
+        *error = 1.0;
+        if (ratio) *ratio = 0.0;
         d = 1.0;
-      } else {
-        smallest = fmin(smallest, d / diag0[k]);
+      } else if (ratio && *error == 0.0) {
+        *ratio = fmin(*ratio, d / L[diag_slot(n, k0 + k)]);
       }
-      pivot = sqrt(d);
-      L[static_cast<std::size_t>(k) * n + k] = pivot;
+      D[k][k] = sqrt(d);
     }
     __syncthreads();
-    for (int i = k + 1 + t; i < n; i += T) L[static_cast<std::size_t>(i) * n + k] /= pivot;
+    if (c == k && r > k && r < b) D[r][k] /= D[k][k];
     __syncthreads();
-    for (int i = k + 1 + t; i < n; i += T) {
-      const double lik = L[static_cast<std::size_t>(i) * n + k];
-      double* row = L + static_cast<std::size_t>(i) * n;
-      for (int j = k + 1; j <= i; ++j) row[j] -= lik * L[static_cast<std::size_t>(j) * n + k];
-    }
+    if (r < b && c > k && c <= r) D[r][c] -= D[r][k] * D[c][k];
     __syncthreads();
   }
-  // Column j of the inverse: L y = e_j, then L^T z = y (thread per column).
-  for (int j = t; j < n; j += T) {
-    for (int i = 0; i < n; ++i) {
-      double s = i == j ? 1.0 : 0.0;
-      if (i > j)
-        for (int k = j; k < i; ++k) s -= L[static_cast<std::size_t>(i) * n + k] * W[static_cast<std::size_t>(k) * n + j];
-      W[static_cast<std::size_t>(i) * n + j] = i < j ? 0.0 : s / L[static_cast<std::size_t>(i) * n + i];
-    }
-    for (int i = n - 1; i >= 0; --i) {
-      double s = W[static_cast<std::size_t>(i) * n + j];
-      for (int k = i + 1; k < n; ++k) s -= L[static_cast<std::size_t>(k) * n + i] * W[static_cast<std::size_t>(k) * n + j];
-      W[static_cast<std::size_t>(i) * n + j] = s / L[static_cast<std::size_t>(i) * n + i];
+  if (r < b && c <= r) L[at(n, k0 + r, k0 + c)] = D[r][c];
+}
+
+// The rows below panel k0: x L_kk^T = a for each row's panel slice x.
+__global__ void k_dense_panel_solve(int n, int k0, double* __restrict__ L) {
+  pdl_entry();
+  __shared__ double D[kNb][kNb + 1];
+  const int b = min(kNb, n - k0);
+  for (int e = threadIdx.x; e < kNb * kNb; e += blockDim.x) {
+    const int r = e / kNb, c = e % kNb;
+    D[r][c] = r < b && c <= r ? L[at(n, k0 + r, k0 + c)] : 0.0;
+  }
+  __syncthreads();
+  const int i = k0 + b + blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  double x[kNb];
+#pragma unroll
+  for (int c = 0; c < kNb; ++c) x[c] = c < b ? L[at(n, i, k0 + c)] : 0.0;
+#pragma unroll
+  for (int c = 0; c < kNb; ++c) {
+    if (c >= b) break;
+    double v = x[c];
+    for (int m = 0; m < c; ++m) v -= x[m] * D[c][m];
+    x[c] = v / D[c][c];
+  }
+#pragma unroll
+  for (int c = 0; c < kNb; ++c)
+    if (c < b) L[at(n, i, k0 + c)] = x[c];
+}
+
+// Trailing update below panel k0: L_ij -= sum_c L_ic L_jc over the panel's
+// columns, for j <= i in the rows after the panel. Block (bx, by) of the
+// grid is tile (ti, tj) = (by, bx) of the trailing part; tiles above the
+// diagonal do nothing.
+__global__ void __launch_bounds__(kNbThreads)
+    k_dense_panel_update(int n, int k0, double* __restrict__ L) {
+  pdl_entry();
+  const int ti = blockIdx.y, tj = blockIdx.x;
+  if (tj > ti) return;
+  __shared__ double Pi[kNb][kNb + 1], Pj[kNb][kNb + 1];
+  const int b = min(kNb, n - k0);
+  const int base = k0 + b;
+  const int r = threadIdx.x / kNb, c = threadIdx.x % kNb;
+  const int i0 = base + ti * kNb, j0 = base + tj * kNb;
+  Pi[r][c] = i0 + r < n && c < b ? L[at(n, i0 + r, k0 + c)] : 0.0;
+  Pj[r][c] = j0 + r < n && c < b ? L[at(n, j0 + r, k0 + c)] : 0.0;
+  __syncthreads();
+  const int i = i0 + r, j = j0 + c;
+  if (i >= n || j >= n || j > i) return;
+  double sum = 0.0;
+  for (int m = 0; m < b; ++m) sum += Pi[r][m] * Pj[c][m];
+  L[at(n, i, j)] -= sum;
+}
+
+// X_pp = L_pp^-1 for every diagonal block p (a CTA each), into W.
+__global__ void __launch_bounds__(kNbThreads)
+    k_dense_block_inverse(int n, const double* __restrict__ L, double* __restrict__ W) {
+  pdl_entry();
+  __shared__ double D[kNb][kNb + 1], X[kNb][kNb + 1];
+  const int k0 = blockIdx.x * kNb;
+  const int b = min(kNb, n - k0);
+  const int r = threadIdx.x / kNb, c = threadIdx.x % kNb;
+  D[r][c] = r < b && c <= r ? L[at(n, k0 + r, k0 + c)] : 0.0;
+  X[r][c] = 0.0;
+  __syncthreads();
+  // Column c of X: L_pp X[:, c] = e_c, forward substitution by thread (0, c).
+  if (r == 0 && c < b) {
+    for (int i = c; i < b; ++i) {
+      double v = i == c ? 1.0 : 0.0;
+      for (int m = c; m < i; ++m) v -= D[i][m] * X[m][c];
+      X[i][c] = v / D[i][i];
     }
   }
-  if (t == 0) {
-    *error = failed ? 1.0 : 0.0;
-    if (ratio) *ratio = failed ? 0.0 : smallest;
+  __syncthreads();
+  if (r < b && c <= r) W[at(n, k0 + r, k0 + c)] = X[r][c];
+}
+
+// Block diagonal d of X: X_ij = -X_ii sum_{k=j}^{i-1} L_ik X_kj, i = j + d
+// (block indices), a CTA per j.
+__global__ void __launch_bounds__(kNbThreads)
+    k_dense_block_offdiag(int n, int d, const double* __restrict__ L, double* __restrict__ W) {
+  pdl_entry();
+  __shared__ double A[kNb][kNb + 1], B[kNb][kNb + 1];
+  const int jb = blockIdx.x, ib = jb + d;
+  const int i0 = ib * kNb, j0 = jb * kNb;
+  const int r = threadIdx.x / kNb, c = threadIdx.x % kNb;
+  double sum = 0.0;  // S[r][c]
+  for (int kb = jb; kb < ib; ++kb) {
+    const int k0 = kb * kNb;
+    // A = L_ik (rows i0.., columns k0..), B = X_kj (rows k0.., columns j0..);
+    // X_kj is lower triangular when k == j.
+    A[r][c] = i0 + r < n ? L[at(n, i0 + r, k0 + c)] : 0.0;
+    B[r][c] = k0 + r < n && (kb > jb || c <= r) ? W[at(n, k0 + r, j0 + c)] : 0.0;
+    __syncthreads();
+    for (int m = 0; m < kNb; ++m) sum += A[r][m] * B[m][c];
+    __syncthreads();
   }
+  // X_ij = -X_ii S, X_ii lower triangular.
+  A[r][c] = i0 + r < n && c <= r ? W[at(n, i0 + r, i0 + c)] : 0.0;
+  B[r][c] = sum;
+  __syncthreads();
+  double x = 0.0;
+  for (int m = 0; m <= r; ++m) x -= A[r][m] * B[m][c];
+  if (i0 + r < n && j0 + c < n) W[at(n, i0 + r, j0 + c)] = x;
+}
+
+// Tile (ti, tj), tj <= ti, of W = X^T X: sum over block rows k >= ti of
+// X_k,ti^T X_k,tj (X lower triangular in W), into out (both (i, j) and (j, i)).
+__global__ void __launch_bounds__(kNbThreads)
+    k_dense_gram(int n, const double* __restrict__ X, double* __restrict__ out) {
+  pdl_entry();
+  const int ti = blockIdx.y, tj = blockIdx.x;
+  if (tj > ti) return;
+  __shared__ double A[kNb][kNb + 1], B[kNb][kNb + 1];
+  const int nb = (n + kNb - 1) / kNb;
+  const int r = threadIdx.x / kNb, c = threadIdx.x % kNb;
+  const int i = ti * kNb + r, j = tj * kNb + c;
+  double sum = 0.0;
+  for (int kb = ti; kb < nb; ++kb) {
+    const int k0 = kb * kNb;
+    // A[m][r] = X[k0 + m][ti*32 + r], B[m][c] = X[k0 + m][tj*32 + c] (zero above the diagonal).
+    const int kr = k0 + r;
+    A[r][c] = kr < n && ti * kNb + c < n && ti * kNb + c <= kr ? X[at(n, kr, ti * kNb + c)] : 0.0;
+    B[r][c] = kr < n && tj * kNb + c < n && tj * kNb + c <= kr ? X[at(n, kr, tj * kNb + c)] : 0.0;
+    __syncthreads();
+    for (int m = 0; m < kNb; ++m) sum += A[m][r] * B[m][c];
+    __syncthreads();
+  }
+  if (i < n && j < n) {
+    out[at(n, i, j)] = sum;
+    out[at(n, j, i)] = sum;
+  }
+}
+
+__global__ void k_dense_copy(std::size_t count, const double* __restrict__ from,
+                             double* __restrict__ to) {
+  pdl_entry();
+  for (std::size_t k = blockIdx.x * static_cast<std::size_t>(blockDim.x) + threadIdx.x; k < count;
+       k += static_cast<std::size_t>(gridDim.x) * blockDim.x)
+    to[k] = from[k];
 }
 
 // The same Cholesky factor and inverse for n <= kSharedDense, on chip and
@@ -612,8 +763,30 @@ void dense_inverse(int n, const int* rows, const int* cols, const float* vals, d
                                                             ratio);
     return;
   }
-  const int threads = std::min(1024, ((n + 31) / 32) * 32);
-  pdl(k_dense_inverse, 1, threads, 0, s, n, rows, cols, vals, lower, inverse, error, ratio);
+  // Blocked, over many CTAs (see k_dense_panel_factor and the kernels after it).
+  const std::size_t count = static_cast<std::size_t>(n) * n;
+  const int nb = (n + kNb - 1) / kNb;
+  const int fill = static_cast<int>(std::min<std::size_t>((count + kBlock - 1) / kBlock, 1184));
+  counter += 4 * nb + 2;
+  pdl(k_dense_zero, fill, kBlock, 0, s, count, lower);
+  pdl(k_dense_scatter, (n + kBlock - 1) / kBlock, kBlock, 0, s, n, rows, cols, vals, lower, error,
+      ratio);
+  for (int p = 0; p < nb; ++p) {
+    const int k0 = p * kNb;
+    pdl(k_dense_panel_factor, 1, kNbThreads, 0, s, n, k0, lower, error, ratio);
+    const int below = n - k0 - kNb;
+    if (below > 0) {
+      pdl(k_dense_panel_solve, (below + 127) / 128, 128, 0, s, n, k0, lower);
+      const int tiles = (below + kNb - 1) / kNb;
+      pdl(k_dense_panel_update, dim3(tiles, tiles), kNbThreads, 0, s, n, k0, lower);
+    }
+  }
+  pdl(k_dense_block_inverse, nb, kNbThreads, 0, s, n, static_cast<const double*>(lower), inverse);
+  for (int d = 1; d < nb; ++d)
+    pdl(k_dense_block_offdiag, nb - d, kNbThreads, 0, s, n, d, static_cast<const double*>(lower),
+        inverse);
+  pdl(k_dense_gram, dim3(nb, nb), kNbThreads, 0, s, n, static_cast<const double*>(inverse), lower);
+  pdl(k_dense_copy, fill, kBlock, 0, s, count, static_cast<const double*>(lower), inverse);
 }
 void dense_solve(int n, const double* inverse, const float* b, float* x, const int* status,
                  cudaStream_t s) {

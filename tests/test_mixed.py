@@ -114,8 +114,9 @@ def _coarsest(n_side=6, seed=4):
 
 DENSE_SYSTEMS = {
     # Up to 112 rows the factor and inverse live in shared memory; up to 236
-    # rows the packed lower triangle does, inverted in place; above, global
-    # memory.
+    # rows the packed lower triangle does, inverted in place; above, a blocked
+    # Cholesky, block inverse and Gram product over many CTAs (32-row blocks:
+    # 237, 384 and 750 rows leave ragged last blocks).
     "tet2_48": lambda: _coarsest(2),
     "poisson_112": lambda: harness.poisson(7, 4, 4),
     "poisson_113": lambda: harness.poisson(113, 1, 1),

@@ -103,11 +103,10 @@ def test_mixed_solve_below_fp32_floor_on_real_matrix(cuda, name, rhs):
     reaches 1e-7 in FP64 (true residual of the returned FP64 solution) on all
     four cases. These matrices are extremely ill conditioned: when
     cond(A) * 6e-8 exceeds 1, an FP32 inner solve cannot resolve the large
-    near-null part of a correction, so refinement contracts slowly; the
-    one-sweep default tuned on the synthetic pressure matrices does not reach
-    1e-6 on the it15 smooth case. The coarsest level is also kept larger than
-    the default (up to 512 rows, solved exactly by its dense inverse): with a
-    112-row coarsest the it18 smooth case stops at 1.7e-7."""
+    near-null part of a correction, so refinement contracts slowly. The
+    coarsest level is kept larger than the default (up to 512 rows, solved
+    exactly by its dense inverse): with a 112-row coarsest the it18 smooth
+    case stops at 1.7e-7."""
     import scipy.sparse as sp
     import torch
     _, arrays = _load(name)
@@ -127,3 +126,29 @@ def test_mixed_solve_below_fp32_floor_on_real_matrix(cuda, name, rhs):
           f"rel={true / st.initial_residual:.2e}")
     assert st.converged, st
     assert true <= 1e-7 * st.initial_residual * 1.0001
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", NAMES)
+@pytest.mark.parametrize("rhs", ["random", "smooth"])
+def test_mixed_solve_default_sweeps_on_real_matrix(cuda, name, rhs):
+    """The mixed solve's default cycle (one pre- and one post-sweep) with a
+    coarsest level of up to 512 rows, formed by the blocked dense inverse,
+    reaches relative 1e-6 in FP64 on all four cases (the it15 smooth case in
+    about 2,100 inner iterations over 7 refinements)."""
+    import scipy.sparse as sp
+    import torch
+    _, arrays = _load(name)
+    s = _system(arrays, rhs)
+    solver = L.make_mixed_solver(s, L.MixedOptions(dense_rows=512))
+    a = L.upload(s)
+    solver.refresh(a)
+    assert "dense FP64 coarsest" in solver.describe()
+    b = torch.from_numpy(s.b).cuda()
+    x = torch.zeros(s.n, dtype=torch.float64, device="cuda")
+    st = solver.solve(a, x, b, L.SolveControl(1e-6, 1e-30, 5000))
+    torch.cuda.synchronize()
+    A = sp.csr_matrix((s.val, s.col, s.row_ptr), shape=(s.n, s.n))
+    true = np.linalg.norm(s.b.astype(np.float64) - A @ x.cpu().numpy())
+    assert st.converged, st
+    assert true <= 1e-6 * st.initial_residual * 1.0001
