@@ -415,6 +415,148 @@ int b2_hierarchy_level_copy(const b2_hierarchy* h, int level, int32_t* row_ptr, 
                             float* val, float* inverse_l1, int32_t* aggregate);
 void b2_hierarchy_free(b2_hierarchy* h);
 
+/* ---- Coupled (4x4-block) pressure-velocity solve ---------------------------
+ * kutta::fv::CoupledSolver (src/kutta/fv/coupled_solver.hpp:61-101): momentum
+ * and continuity in one block system per outer iteration, solved in delta
+ * form by block BiCGStab with a block aggregation-AMG V-cycle (damped block
+ * Jacobi smoothing). Unknowns per cell: (du, dv, dw, dp~), dp~ = dp / wc,
+ * wc = density x velocity_scale.
+ *
+ * The reference's constructor takes its DeviceMesh, Stencil, PolyMesh,
+ * MeshGeometry, boundary kinds and pressure least-squares fit
+ * (coupled_solver.hpp:69-74); b2_coupled_mesh carries the arrays of those it
+ * reads, as HOST arrays (setup runs on the host, as the reference's does). */
+typedef struct {
+  int n_cells, n_faces, n_internal;  /* internal faces first, owner < neighbour */
+  const int32_t* owner;              /* n_faces */
+  const int32_t* neighbour;          /* n_internal */
+  const int32_t* cell_face_offsets;  /* n_cells + 1: DeviceMesh::cell_face_offsets */
+  const int32_t* cell_faces;         /* per entry */
+  const float* cell_face_sign;       /* per entry: +1 owner, -1 neighbour */
+  const int32_t* adjacent;           /* per entry: Stencil::adjacent (other cell or
+                                        -(boundary face + 1)) */
+  const float *area_x, *area_y, *area_z;  /* n_faces: DeviceMesh::area */
+  const double* face_area;           /* 3 n_faces, (x, y, z) per face: MeshGeometry */
+  const double* cell_centroid;       /* 3 n_cells: MeshGeometry */
+  const float *owner_to_face_x, *owner_to_face_y, *owner_to_face_z;  /* n_faces */
+  const float *neighbour_to_face_x, *neighbour_to_face_y,
+      *neighbour_to_face_z;          /* n_internal */
+  const float *lsq_x, *lsq_y, *lsq_z;  /* per entry: BoundaryLeastSquares::rows() */
+  const float *boundary_delta_x, *boundary_delta_y,
+      *boundary_delta_z;             /* per boundary face: ::boundary_delta */
+  const float* lsq_inverse;          /* 6 n_cells planes (xx xy xz yy yz zz):
+                                        ::inverse_values() */
+  const float* diffusion;            /* n_faces: Stencil::diffusion */
+  const float* volume;               /* n_cells: DeviceMesh::volume */
+  const int32_t* boundary_kind;      /* per boundary face: fv_flow.kern.h:3-4 */
+  const int32_t* pattern_row_ptr;    /* Stencil::pattern (the momentum rows' CSR */
+  const int32_t* pattern_col;        /* pattern, diagonal included) */
+  const int32_t* pattern_diag;
+  const int32_t* low_order;          /* n_cells flags (low-order pressure faces) or NULL */
+} b2_coupled_mesh;
+
+/* CoupledOptions, coupled_solver.hpp:26-38. recompute selects the reference's
+ * memory-limited operator (CoupledEdgeStorage::Recompute); its results equal
+ * the cached operator's, and this library always caches. */
+typedef struct {
+  int pre_sweeps, post_sweeps, coarsest_sweeps; /* defaults 1, 2, 8 */
+  float smoother_damping;                       /* default 0.7 */
+  double courant;                               /* default 200 */
+  int coarsest_rows;                            /* default 48 */
+  int aggregation_passes;                       /* default 3 */
+  int recompute;                                /* default 0 */
+} b2_coupled_options;
+
+/* CoupledResiduals, coupled_solver.hpp:41-55: device arrays. d_net_outflow
+ * may be NULL (the net outflow is then summed from d_mass). */
+typedef struct {
+  const float *d_ru, *d_rv, *d_rw;  /* momentum residuals b - A u, n_cells each */
+  const float* d_mass;              /* n_faces, kg/s out of owner */
+  const float* d_viscosity;         /* n_faces */
+  const float* d_physical_diagonal; /* n_cells */
+  const float* d_face_weights;      /* n_cells */
+  const float* d_net_outflow;       /* n_cells or NULL */
+  double density, velocity_scale;
+} b2_coupled_residuals;
+
+typedef struct b2_coupled b2_coupled;
+typedef struct b2_coupled_setup b2_coupled_setup;
+
+void b2_coupled_options_default(b2_coupled_options* options);
+/* CoupledSolver::CoupledSolver (coupled_solver.cpp:464-470). reference >= 0
+ * anchors a closed domain's pressure in that cell. Host arrays are read
+ * during the call only. */
+int b2_coupled_create(const b2_coupled_mesh* mesh, int reference,
+                      const b2_coupled_options* options, void* stream, b2_coupled** out);
+/* CoupledSolver::capture_diagonal (coupled_solver.cpp:472-477): one momentum
+ * component's assembled CSR (device, over the stencil pattern) and its
+ * physical diagonal (device, n_cells). */
+int b2_coupled_capture_diagonal(b2_coupled* solver, int component, const int32_t* d_row_ptr,
+                                const int32_t* d_diag, const float* d_val,
+                                const float* d_physical, void* stream);
+/* CoupledSolver::solve (coupled_solver.cpp:479-512): assembles the Jacobian and
+ * right-hand side, then solves for the update; stats as SolveStats. */
+int b2_coupled_solve(b2_coupled* solver, const b2_coupled_residuals* residuals,
+                     const b2_control* control, b2_stats* stats, void* stream);
+/* CoupledSolver::update (coupled_solver.cpp:514-522): u += alpha_u du,
+ * p += alpha_p wc dp~, then the closed-domain gauge. Device arrays. */
+int b2_coupled_update(b2_coupled* solver, float* d_u, float* d_v, float* d_w, float* d_p,
+                      double alpha_u, double alpha_p, void* stream);
+/* The float-pair form (coupled_solver.cpp:524-535, CoupledPairs). */
+int b2_coupled_paired_update(b2_coupled* solver, float* d_u, float* d_v, float* d_w, float* d_p,
+                             float* d_u_lo, float* d_v_lo, float* d_w_lo, float* d_p_lo,
+                             double alpha_u, double alpha_p, float velocity_slack,
+                             float pressure_slack, void* stream);
+/* CoupledSolver::bytes / describe (coupled_solver.cpp:537-546). */
+size_t b2_coupled_bytes(const b2_coupled* solver);
+size_t b2_coupled_describe(const b2_coupled* solver, char* buffer, size_t length);
+void b2_coupled_destroy(b2_coupled* solver);
+
+/* Introspection of the last solve, synchronous reads on `stream` into host
+ * arrays (any pointer may be NULL). what: 0 the solution, 1 the right-hand
+ * side (each 4 n_cells floats as planes [u | v | w | p~]), 2 the cell data
+ * (27 n_cells floats, the reference's packed planes: du dv dw cd | G | H |
+ * Q | cs | iu iv iw hx iu hy iv hz iw schur), 3 the face coefficients
+ * (n_faces). Returns the float count. */
+long long b2_coupled_copy(const b2_coupled* solver, int what, float* out, void* stream);
+/* Levels (the fine level is 0) and a coarse level's operator: rows[n + 1],
+ * cols[nnz], diag[n], a[nnz], c[nnz], g[3 nnz], h[3 nnz], d[11 n], and the
+ * aggregate of each row of level - 1 (level - 1 rows). */
+int b2_coupled_levels(const b2_coupled* solver);
+int b2_coupled_level_shape(const b2_coupled* solver, int level, int* n, int* nnz);
+int b2_coupled_level_copy(const b2_coupled* solver, int level, int32_t* rows, int32_t* cols,
+                          int32_t* diag, float* a, float* c, float* g, float* h, float* d,
+                          int32_t* aggregate, void* stream);
+/* The fine block operator on device vectors of float4 per cell (u, v, w, p~):
+ * op 0 y = J x, 1 y = b - J x, 2 one damped block-Jacobi sweep from x, 3 the
+ * same from x = 0 (x not read). Uses the Jacobian of the last solve. */
+int b2_coupled_apply(b2_coupled* solver, int op, const float* d_x, const float* d_b, float* d_y,
+                     void* stream);
+
+/* The same on coarse level `level` >= 1 (float4 per coarse row): op 1 y =
+ * b - J x, 2 / 3 one sweep from x / from x = 0; op 4 y = the restriction of
+ * level - 1's x (member sums), op 5 y += the prolongation of x to level - 1
+ * (y has level - 1 rows). */
+int b2_coupled_level_apply(b2_coupled* solver, int level, int op, const float* d_x,
+                           const float* d_b, float* d_y, void* stream);
+
+/* Host-only Coupled setup (no GPU needed): the pressure-force sensitivities
+ * and the aggregation hierarchy b2_coupled_create builds
+ * (coupled_solver.cpp:27-46 pair_rows, :49-85 members_of and contract, :132-289). */
+int b2_coupled_setup_build(const b2_coupled_mesh* mesh, const b2_coupled_options* options,
+                           b2_coupled_setup** out);
+int b2_coupled_setup_levels(const b2_coupled_setup* setup);
+int b2_coupled_setup_level_shape(const b2_coupled_setup* setup, int level, int* n, int* nnz);
+/* Level >= 1: rows, cols, diag; every level but the coarsest: its aggregate
+ * (level rows), member offsets (next level rows + 1) and members. */
+int b2_coupled_setup_level_copy(const b2_coupled_setup* setup, int level, int32_t* rows,
+                                int32_t* cols, int32_t* diag, int32_t* aggregate,
+                                int32_t* member_offsets, int32_t* members);
+/* 27 n_cells floats: G in planes 4-6, Q in planes 10-18, zero elsewhere. */
+int b2_coupled_setup_cell(const b2_coupled_setup* setup, float* out);
+int b2_coupled_setup_width(const b2_coupled_setup* setup);
+void b2_coupled_setup_free(b2_coupled_setup* setup);
+
 #ifdef __cplusplus
 }
 #endif

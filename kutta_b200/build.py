@@ -46,9 +46,10 @@ PRODUCT_CU = {
     "setup_kernels.cu": EXACT,
     "fv_kernels.cu": EXACT,
     "noalloc.cu": [],
+    "coupled_kernels.cu": EXACT,
 }
 PRODUCT_CPP = ["host/setup.cpp", "host/solver.cpp", "host/device_setup.cpp", "host/mixed.cpp",
-               "host/learned.cpp", "capi.cpp"]
+               "host/learned.cpp", "host/coupled_setup.cpp", "host/coupled.cpp", "capi.cpp"]
 
 
 def _hash(paths, extra=""):

@@ -10,6 +10,8 @@
 #include <string>
 
 #include "cuda/kernels.hpp"
+#include "host/coupled.hpp"
+#include "host/coupled_setup.hpp"
 #include "host/mixed.hpp"
 #include "host/setup.hpp"
 
@@ -30,6 +32,12 @@ struct b2_hierarchy {
 };
 struct b2_mixed {
   std::unique_ptr<kb2::MixedSolver> s;
+};
+struct b2_coupled {
+  std::unique_ptr<kb2::CoupledSolver> s;
+};
+struct b2_coupled_setup {
+  kb2::CoupledSetup s;
 };
 struct b2_gnn {
   std::unique_ptr<kb2::Gnn> g;
@@ -109,6 +117,77 @@ namespace kb2 {
 // translation units.
 int report_error(int code, const char* message) { return fail(code, message); }
 }  // namespace kb2
+
+// Coupled-solve argument conversion (used by the b2_coupled_* entry points).
+namespace {
+kb2::CoupledMeshHost coupled_mesh(const b2_coupled_mesh* m) {
+  KB2_REQUIRE(m != nullptr, "coupled: null mesh");
+  kb2::CoupledMeshHost h;
+  h.n_cells = m->n_cells;
+  h.n_faces = m->n_faces;
+  h.n_internal = m->n_internal;
+  h.owner = m->owner;
+  h.neighbour = m->neighbour;
+  h.cell_face_offsets = m->cell_face_offsets;
+  h.cell_faces = m->cell_faces;
+  h.cell_face_sign = m->cell_face_sign;
+  h.adjacent = m->adjacent;
+  h.area_x = m->area_x;
+  h.area_y = m->area_y;
+  h.area_z = m->area_z;
+  h.face_area = m->face_area;
+  h.cell_centroid = m->cell_centroid;
+  h.owner_to_face_x = m->owner_to_face_x;
+  h.owner_to_face_y = m->owner_to_face_y;
+  h.owner_to_face_z = m->owner_to_face_z;
+  h.neighbour_to_face_x = m->neighbour_to_face_x;
+  h.neighbour_to_face_y = m->neighbour_to_face_y;
+  h.neighbour_to_face_z = m->neighbour_to_face_z;
+  h.lsq_x = m->lsq_x;
+  h.lsq_y = m->lsq_y;
+  h.lsq_z = m->lsq_z;
+  h.boundary_delta_x = m->boundary_delta_x;
+  h.boundary_delta_y = m->boundary_delta_y;
+  h.boundary_delta_z = m->boundary_delta_z;
+  h.lsq_inverse = m->lsq_inverse;
+  h.diffusion = m->diffusion;
+  h.volume = m->volume;
+  h.boundary_kind = m->boundary_kind;
+  h.pattern_row_ptr = m->pattern_row_ptr;
+  h.pattern_col = m->pattern_col;
+  h.pattern_diag = m->pattern_diag;
+  h.low_order = m->low_order;
+  return h;
+}
+kb2::CoupledOptions coupled_options(const b2_coupled_options* o) {
+  b2_coupled_options defaults;
+  b2_coupled_options_default(&defaults);
+  const b2_coupled_options& c = o ? *o : defaults;
+  kb2::CoupledOptions r;
+  r.pre_sweeps = c.pre_sweeps;
+  r.post_sweeps = c.post_sweeps;
+  r.coarsest_sweeps = c.coarsest_sweeps;
+  r.smoother_damping = c.smoother_damping;
+  r.courant = c.courant;
+  r.coarsest_rows = c.coarsest_rows;
+  r.aggregation_passes = c.aggregation_passes;
+  r.recompute = c.recompute;
+  return r;
+}
+kb2::CoupledSolver& coupled(b2_coupled* s) {
+  KB2_REQUIRE(s && s->s, "coupled: null solver");
+  return *s->s;
+}
+const kb2::CoupledSolver& coupled_view(const b2_coupled* s) {
+  KB2_REQUIRE(s && s->s, "coupled: null solver");
+  return *s->s;
+}
+template <class T>
+void read_back(T* out, const T* d, std::size_t n, cudaStream_t s) {
+  if (!out || n == 0) return;
+  kb2::cuda_check(cudaMemcpyAsync(out, d, n * sizeof(T), cudaMemcpyDeviceToHost, s), "read back");
+}
+}  // namespace
 
 extern "C" {
 
@@ -741,5 +820,267 @@ int b2_mixed_hierarchy_build(int n, int nnz, const int32_t* row_ptr, const int32
     *out = h.release();
   });
 }
+
+// ---- Coupled (4x4-block) solve ----------------------------------------------
+
+
+void b2_coupled_options_default(b2_coupled_options* o) {
+  if (!o) return;
+  const kb2::CoupledOptions d;
+  o->pre_sweeps = d.pre_sweeps;
+  o->post_sweeps = d.post_sweeps;
+  o->coarsest_sweeps = d.coarsest_sweeps;
+  o->smoother_damping = d.smoother_damping;
+  o->courant = d.courant;
+  o->coarsest_rows = d.coarsest_rows;
+  o->aggregation_passes = d.aggregation_passes;
+  o->recompute = d.recompute;
+}
+
+int b2_coupled_create(const b2_coupled_mesh* mesh, int reference,
+                      const b2_coupled_options* options, void* stream, b2_coupled** out) {
+  return guarded([&] {
+    KB2_REQUIRE(out != nullptr, "coupled: null output handle");
+    *out = nullptr;
+    auto h = std::make_unique<b2_coupled>();
+    h->s = std::make_unique<kb2::CoupledSolver>(coupled_mesh(mesh), reference,
+                                                coupled_options(options), as_stream(stream));
+    kb2::wait(as_stream(stream));
+    *out = h.release();
+  });
+}
+
+int b2_coupled_capture_diagonal(b2_coupled* s, int component, const int32_t* d_row_ptr,
+                                const int32_t* d_diag, const float* d_val,
+                                const float* d_physical, void* stream) {
+  return guarded([&] {
+    KB2_REQUIRE(d_row_ptr && d_diag && d_val && d_physical, "coupled: null diagonal input");
+    coupled(s).capture_diagonal(component, d_row_ptr, d_diag, d_val, d_physical,
+                                as_stream(stream));
+  });
+}
+
+int b2_coupled_solve(b2_coupled* s, const b2_coupled_residuals* in, const b2_control* control,
+                     b2_stats* stats, void* stream) {
+  return guarded([&] {
+    KB2_REQUIRE(in != nullptr, "coupled: null residuals");
+    kb2::CoupledSolveInputs i;
+    i.ru = in->d_ru;
+    i.rv = in->d_rv;
+    i.rw = in->d_rw;
+    i.mass = in->d_mass;
+    i.viscosity = in->d_viscosity;
+    i.physical_diagonal = in->d_physical_diagonal;
+    i.face_weights = in->d_face_weights;
+    i.net_outflow = in->d_net_outflow;
+    b2_control defaults;
+    b2_control_default(&defaults);
+    const b2_control& c = control ? *control : defaults;
+    kb2::Control k;
+    k.rel_tol = c.rel_tol;
+    k.abs_tol = c.abs_tol;
+    k.max_iter = c.max_iter;
+    k.residual_check_interval = c.residual_check_interval;
+    const auto r = coupled(s).solve(i, in->density, in->velocity_scale, k, as_stream(stream));
+    if (stats) {
+      stats->iterations = r.iterations;
+      stats->converged = r.converged ? 1 : 0;
+      stats->initial_residual = r.initial_residual;
+      stats->final_residual = r.final_residual;
+    }
+  });
+}
+
+int b2_coupled_update(b2_coupled* s, float* d_u, float* d_v, float* d_w, float* d_p,
+                      double alpha_u, double alpha_p, void* stream) {
+  return guarded([&] {
+    KB2_REQUIRE(d_u && d_v && d_w && d_p, "coupled: null field");
+    coupled(s).update(d_u, d_v, d_w, d_p, alpha_u, alpha_p, as_stream(stream));
+  });
+}
+
+int b2_coupled_paired_update(b2_coupled* s, float* d_u, float* d_v, float* d_w, float* d_p,
+                             float* d_u_lo, float* d_v_lo, float* d_w_lo, float* d_p_lo,
+                             double alpha_u, double alpha_p, float velocity_slack,
+                             float pressure_slack, void* stream) {
+  return guarded([&] {
+    KB2_REQUIRE(d_u && d_v && d_w && d_p && d_u_lo && d_v_lo && d_w_lo && d_p_lo,
+                "coupled: null field");
+    coupled(s).paired_update(d_u, d_v, d_w, d_p, d_u_lo, d_v_lo, d_w_lo, d_p_lo, alpha_u,
+                             alpha_p, velocity_slack, pressure_slack, as_stream(stream));
+  });
+}
+
+size_t b2_coupled_bytes(const b2_coupled* s) { return s && s->s ? s->s->bytes() : 0; }
+
+size_t b2_coupled_describe(const b2_coupled* s, char* buffer, size_t length) {
+  if (!s || !s->s) return 0;
+  const auto d = s->s->describe();
+  if (buffer && length) std::snprintf(buffer, length, "%s", d.c_str());
+  return d.size();
+}
+
+void b2_coupled_destroy(b2_coupled* s) { delete s; }
+
+long long b2_coupled_copy(const b2_coupled* s, int what, float* out, void* stream) {
+  long long count = -1;
+  const int rc = guarded([&] {
+    const auto& c = coupled_view(s);
+    const cudaStream_t st = as_stream(stream);
+    const std::size_t n = c.cells();
+    if (what == 0 || what == 1) {
+      count = static_cast<long long>(4 * n);
+      if (!out) return;
+      std::vector<float> aos(4 * n);
+      read_back(aos.data(), what == 0 ? c.solution() : c.rhs(), 4 * n, st);
+      kb2::wait(st);
+      for (std::size_t i = 0; i < n; ++i)
+        for (int k = 0; k < 4; ++k) out[k * n + i] = aos[4 * i + k];
+    } else if (what == 2) {
+      count = static_cast<long long>(27 * n);
+      if (!out) return;
+      read_back(out, c.cell_data(), 20 * n, st);
+      std::vector<float> inv(4 * n), inv_h(4 * n);
+      c.copy_inverse(inv.data(), inv_h.data(), st);
+      kb2::wait(st);
+      for (std::size_t i = 0; i < n; ++i) {
+        out[20 * n + i] = inv[4 * i];
+        out[21 * n + i] = inv[4 * i + 1];
+        out[22 * n + i] = inv[4 * i + 2];
+        out[23 * n + i] = inv_h[4 * i];
+        out[24 * n + i] = inv_h[4 * i + 1];
+        out[25 * n + i] = inv_h[4 * i + 2];
+        out[26 * n + i] = inv[4 * i + 3];
+      }
+    } else if (what == 3) {
+      count = c.faces();
+      if (!out) return;
+      read_back(out, c.face_coefficients(), static_cast<std::size_t>(c.faces()), st);
+      kb2::wait(st);
+    } else {
+      KB2_REQUIRE(false, "coupled: unknown array");
+    }
+  });
+  return rc == B2_OK ? count : -1;
+}
+
+int b2_coupled_levels(const b2_coupled* s) { return s && s->s ? s->s->levels() : 0; }
+
+int b2_coupled_level_shape(const b2_coupled* s, int level, int* n, int* nnz) {
+  return guarded([&] {
+    const auto& c = coupled_view(s);
+    KB2_REQUIRE(level >= 0 && level < c.levels(), "coupled: level out of range");
+    if (n) *n = c.level_rows(level);
+    if (nnz) *nnz = level == 0 ? 0 : c.level(level).nnz;
+  });
+}
+
+int b2_coupled_level_copy(const b2_coupled* s, int level, int32_t* rows, int32_t* cols,
+                          int32_t* diag, float* a, float* c_out, float* g, float* h, float* d,
+                          int32_t* aggregate, void* stream) {
+  return guarded([&] {
+    const auto& c = coupled_view(s);
+    KB2_REQUIRE(level >= 1 && level < c.levels(), "coupled: level out of range");
+    const cudaStream_t st = as_stream(stream);
+    const auto& l = c.level(level);
+    const std::size_t n = l.n, nnz = l.nnz;
+    read_back(rows, l.rows, n + 1, st);
+    read_back(cols, l.cols, nnz, st);
+    read_back(diag, l.diag, n, st);
+    read_back(a, static_cast<const float*>(l.a), nnz, st);
+    read_back(c_out, static_cast<const float*>(l.c), nnz, st);
+    read_back(g, static_cast<const float*>(l.g), 3 * nnz, st);
+    read_back(h, static_cast<const float*>(l.h), 3 * nnz, st);
+    read_back(d, static_cast<const float*>(l.d), 11 * n, st);
+    read_back(aggregate, c.transfer(level - 1).aggregate,
+              static_cast<std::size_t>(c.level_rows(level - 1)), st);
+    kb2::wait(st);
+  });
+}
+
+int b2_coupled_apply(b2_coupled* s, int op, const float* d_x, const float* d_b, float* d_y,
+                     void* stream) {
+  return guarded([&] {
+    auto& c = coupled(s);
+    KB2_REQUIRE(d_y && (op == 3 || d_x) && (op == 0 || d_b), "coupled: null vector");
+    const cudaStream_t st = as_stream(stream);
+    if (op == 0)
+      c.apply(d_x, d_y, st);
+    else if (op == 1)
+      c.residual(d_x, d_b, d_y, st);
+    else if (op == 2 || op == 3)
+      c.smooth(d_x, d_b, d_y, op == 3, st);
+    else
+      KB2_REQUIRE(false, "coupled: unknown operator");
+    kb2::cuda_check(cudaGetLastError(), "coupled apply");
+  });
+}
+
+int b2_coupled_level_apply(b2_coupled* s, int level, int op, const float* d_x,
+                           const float* d_b, float* d_y, void* stream) {
+  return guarded([&] {
+    const bool needs_b = op == 1 || op == 2 || op == 3;
+    KB2_REQUIRE(d_y && (op == 3 || d_x) && (!needs_b || d_b), "coupled: null vector");
+    coupled(s).level_apply(level, op, d_x, d_b, d_y, as_stream(stream));
+    kb2::cuda_check(cudaGetLastError(), "coupled level apply");
+  });
+}
+
+int b2_coupled_setup_build(const b2_coupled_mesh* mesh, const b2_coupled_options* options,
+                           b2_coupled_setup** out) {
+  return guarded([&] {
+    KB2_REQUIRE(out != nullptr, "coupled: null output handle");
+    *out = nullptr;
+    auto h = std::make_unique<b2_coupled_setup>();
+    h->s = kb2::coupled_setup(coupled_mesh(mesh), coupled_options(options));
+    *out = h.release();
+  });
+}
+
+int b2_coupled_setup_levels(const b2_coupled_setup* s) {
+  return s ? static_cast<int>(s->s.levels.size()) + 1 : 0;
+}
+
+int b2_coupled_setup_level_shape(const b2_coupled_setup* s, int level, int* n, int* nnz) {
+  return guarded([&] {
+    KB2_REQUIRE(s && level >= 0 && level < b2_coupled_setup_levels(s), "level out of range");
+    if (n) *n = level == 0 ? s->s.n : s->s.levels[level - 1].n;
+    if (nnz) *nnz = level == 0 ? 0 : s->s.levels[level - 1].nnz;
+  });
+}
+
+int b2_coupled_setup_level_copy(const b2_coupled_setup* s, int level, int32_t* rows,
+                                int32_t* cols, int32_t* diag, int32_t* aggregate,
+                                int32_t* member_offsets, int32_t* members) {
+  return guarded([&] {
+    KB2_REQUIRE(s && level >= 0 && level < b2_coupled_setup_levels(s), "level out of range");
+    const auto copy = [](int32_t* out, const std::vector<int>& v) {
+      if (out && !v.empty()) std::memcpy(out, v.data(), v.size() * sizeof(int));
+    };
+    if (level > 0) {
+      const auto& l = s->s.levels[level - 1];
+      copy(rows, l.rows);
+      copy(cols, l.cols);
+      copy(diag, l.diag);
+    }
+    if (level < static_cast<int>(s->s.transfers.size())) {
+      const auto& t = s->s.transfers[level];
+      copy(aggregate, t.aggregate);
+      copy(member_offsets, t.offsets);
+      copy(members, t.members);
+    }
+  });
+}
+
+int b2_coupled_setup_cell(const b2_coupled_setup* s, float* out) {
+  return guarded([&] {
+    KB2_REQUIRE(s && out, "coupled: null argument");
+    std::memcpy(out, s->s.cell.data(), s->s.cell.size() * sizeof(float));
+  });
+}
+
+int b2_coupled_setup_width(const b2_coupled_setup* s) { return s ? s->s.width : 0; }
+
+void b2_coupled_setup_free(b2_coupled_setup* s) { delete s; }
 
 }  // extern "C"

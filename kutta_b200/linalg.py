@@ -209,6 +209,29 @@ _SIGNATURES = {
     "b2_mixed_precondition": (_I, [_P, _P, _P, _P, _P]),
     "b2_mixed_profile": (_I, [_P, _I]),
     "b2_mixed_profile_read": (_I, [_P, _P]),
+    "b2_coupled_options_default": (None, [_P]),
+    "b2_coupled_create": (_I, [_P, _I, _P, _P, _P]),
+    "b2_coupled_capture_diagonal": (_I, [_P, _I, _P, _P, _P, _P, _P]),
+    "b2_coupled_solve": (_I, [_P, _P, _P, _P, _P]),
+    "b2_coupled_update": (_I, [_P, _P, _P, _P, _P, ctypes.c_double, ctypes.c_double, _P]),
+    "b2_coupled_paired_update": (_I, [_P] + [_P] * 8 + [ctypes.c_double, ctypes.c_double,
+                                                         ctypes.c_float, ctypes.c_float, _P]),
+    "b2_coupled_bytes": (ctypes.c_size_t, [_P]),
+    "b2_coupled_describe": (ctypes.c_size_t, [_P, ctypes.c_char_p, ctypes.c_size_t]),
+    "b2_coupled_destroy": (None, [_P]),
+    "b2_coupled_copy": (ctypes.c_longlong, [_P, _I, _P, _P]),
+    "b2_coupled_levels": (_I, [_P]),
+    "b2_coupled_level_shape": (_I, [_P, _I, _P, _P]),
+    "b2_coupled_level_copy": (_I, [_P, _I] + [_P] * 10),
+    "b2_coupled_apply": (_I, [_P, _I, _P, _P, _P, _P]),
+    "b2_coupled_level_apply": (_I, [_P, _I, _I, _P, _P, _P, _P]),
+    "b2_coupled_setup_build": (_I, [_P, _P, _P]),
+    "b2_coupled_setup_levels": (_I, [_P]),
+    "b2_coupled_setup_level_shape": (_I, [_P, _I, _P, _P]),
+    "b2_coupled_setup_level_copy": (_I, [_P, _I] + [_P] * 6),
+    "b2_coupled_setup_cell": (_I, [_P, _P]),
+    "b2_coupled_setup_width": (_I, [_P]),
+    "b2_coupled_setup_free": (None, [_P]),
 }
 
 _lib = None
@@ -811,3 +834,229 @@ def build_hierarchy(a, options: AmgOptions | None = None, spd: bool = True) -> l
     finally:
         lib.b2_hierarchy_free(handle)
     return out
+
+
+# ---- Coupled (4x4-block) pressure-velocity solve -----------------------------------
+# kutta::fv::CoupledSolver (src/kutta/fv/coupled_solver.hpp:61-101).
+
+@dataclasses.dataclass
+class CoupledOptions:  # coupled_solver.hpp:26-38
+    pre_sweeps: int = 1
+    post_sweeps: int = 2
+    coarsest_sweeps: int = 8
+    smoother_damping: float = 0.7
+    courant: float = 200.0
+    coarsest_rows: int = 48
+    aggregation_passes: int = 3
+    recompute: bool = False
+
+
+class _CoupledOptions(ctypes.Structure):
+    _fields_ = [("pre_sweeps", ctypes.c_int), ("post_sweeps", ctypes.c_int),
+                ("coarsest_sweeps", ctypes.c_int), ("smoother_damping", ctypes.c_float),
+                ("courant", ctypes.c_double), ("coarsest_rows", ctypes.c_int),
+                ("aggregation_passes", ctypes.c_int), ("recompute", ctypes.c_int)]
+
+
+def _coupled_options(o: CoupledOptions | None) -> _CoupledOptions:
+    o = o or CoupledOptions()
+    return _CoupledOptions(o.pre_sweeps, o.post_sweeps, o.coarsest_sweeps, o.smoother_damping,
+                           o.courant, o.coarsest_rows, o.aggregation_passes, int(o.recompute))
+
+
+# b2_coupled_mesh field order: (name, dtype) of each host array.
+_COUPLED_MESH = [
+    ("owner", np.int32), ("neighbour", np.int32), ("cell_face_offsets", np.int32),
+    ("cell_faces", np.int32), ("cell_face_sign", np.float32), ("adjacent", np.int32),
+    ("area_x", np.float32), ("area_y", np.float32), ("area_z", np.float32),
+    ("face_area", np.float64), ("cell_centroid", np.float64),
+    ("owner_to_face_x", np.float32), ("owner_to_face_y", np.float32),
+    ("owner_to_face_z", np.float32), ("neighbour_to_face_x", np.float32),
+    ("neighbour_to_face_y", np.float32), ("neighbour_to_face_z", np.float32),
+    ("lsq_x", np.float32), ("lsq_y", np.float32), ("lsq_z", np.float32),
+    ("boundary_delta_x", np.float32), ("boundary_delta_y", np.float32),
+    ("boundary_delta_z", np.float32), ("lsq_inverse", np.float32), ("diffusion", np.float32),
+    ("volume", np.float32), ("boundary_kind", np.int32), ("pattern_row_ptr", np.int32),
+    ("pattern_col", np.int32), ("pattern_diag", np.int32), ("low_order", np.int32),
+]
+
+
+class _CoupledMesh(ctypes.Structure):
+    _fields_ = [("n_cells", ctypes.c_int), ("n_faces", ctypes.c_int),
+                ("n_internal", ctypes.c_int)] + [(name, _P) for name, _ in _COUPLED_MESH]
+
+
+class _CoupledResiduals(ctypes.Structure):
+    _fields_ = [(name, _P) for name in ("ru", "rv", "rw", "mass", "viscosity",
+                                        "physical_diagonal", "face_weights", "net_outflow")] + \
+               [("density", ctypes.c_double), ("velocity_scale", ctypes.c_double)]
+
+
+class CoupledMesh:
+    """The host arrays of b2_coupled_mesh, by name (the keys a reference box
+    case or coupled_harness.box_hex gives; `lsq_x` are the pressure fit's rows,
+    `low_order` is optional). The arrays are kept alive with the struct."""
+
+    def __init__(self, arrays: dict):
+        sizes = np.asarray(arrays["sizes"])
+        self.n_cells, self.n_faces, self.n_internal = (int(v) for v in sizes[:3])
+        self._keep = {}
+        fields = {}
+        for name, dtype in _COUPLED_MESH:
+            src = name if name not in ("lsq_x", "lsq_y", "lsq_z") else name
+            a = arrays.get(src)
+            if a is None:
+                fields[name] = None
+                continue
+            a = np.ascontiguousarray(a, dtype=dtype)
+            self._keep[name] = a
+            fields[name] = _ptr(a)
+        self.struct = _CoupledMesh(self.n_cells, self.n_faces, self.n_internal,
+                                   *(fields[name] for name, _ in _COUPLED_MESH))
+
+
+class CoupledSolver:
+    """b2_coupled: the Coupled block solve. Vectors are CUDA tensors on torch's
+    current stream: per-cell and per-face float32 fields, momentum CSR
+    arrays over the stencil pattern."""
+
+    def __init__(self, mesh, reference: int = -1, options: CoupledOptions | None = None):
+        lib = _load()
+        self.mesh = mesh if isinstance(mesh, CoupledMesh) else CoupledMesh(mesh)
+        opts = _coupled_options(options)
+        handle = ctypes.c_void_p()
+        _check(lib.b2_coupled_create(ctypes.byref(self.mesh.struct), int(reference),
+                                     ctypes.byref(opts), _stream(), ctypes.byref(handle)))
+        self._handle = handle
+        self.n_cells = self.mesh.n_cells
+        self.n_faces = self.mesh.n_faces
+
+    def capture_diagonal(self, component: int, row_ptr, diag, values, physical) -> None:
+        _check(_load().b2_coupled_capture_diagonal(self._handle, int(component), _tptr(row_ptr),
+                                                   _tptr(diag), _tptr(values), _tptr(physical),
+                                                   _stream()))
+
+    def solve(self, fields: dict, control: SolveControl | None = None) -> SolveStats:
+        """fields: ru, rv, rw, mass, viscosity, physical_diagonal, face_weights
+        (CUDA float32 tensors), net_outflow (tensor or None), density and
+        velocity_scale (floats)."""
+        r = _CoupledResiduals(*(_tptr(fields.get(k)) for k in (
+            "ru", "rv", "rw", "mass", "viscosity", "physical_diagonal", "face_weights",
+            "net_outflow")), float(fields["density"]), float(fields["velocity_scale"]))
+        control = control or SolveControl(0.1, 1e-12, 20)
+        c = _Control(control.rel_tol, control.abs_tol, control.max_iter,
+                     control.residual_check_interval)
+        st = _Stats()
+        _check(_load().b2_coupled_solve(self._handle, ctypes.byref(r), ctypes.byref(c),
+                                        ctypes.byref(st), _stream()))
+        return SolveStats(st.iterations, st.initial_residual, st.final_residual,
+                          bool(st.converged))
+
+    def update(self, u, v, w, p, alpha_u: float, alpha_p: float) -> None:
+        _check(_load().b2_coupled_update(self._handle, _tptr(u), _tptr(v), _tptr(w), _tptr(p),
+                                         float(alpha_u), float(alpha_p), _stream()))
+
+    def paired_update(self, u, v, w, p, u_lo, v_lo, w_lo, p_lo, alpha_u: float,
+                      alpha_p: float, velocity_slack: float, pressure_slack: float) -> None:
+        _check(_load().b2_coupled_paired_update(
+            self._handle, *(_tptr(t) for t in (u, v, w, p, u_lo, v_lo, w_lo, p_lo)),
+            float(alpha_u), float(alpha_p), float(velocity_slack), float(pressure_slack),
+            _stream()))
+
+    def bytes(self) -> int:
+        return int(_load().b2_coupled_bytes(self._handle))
+
+    def describe(self) -> str:
+        buf = ctypes.create_string_buffer(512)
+        _load().b2_coupled_describe(self._handle, buf, 512)
+        return buf.value.decode()
+
+    def copy(self, what: str) -> np.ndarray:
+        """'x' / 'rhs' (4n, planes [u|v|w|p~]), 'cell' (27n), 'coefficient' (n_faces)."""
+        code = {"x": 0, "rhs": 1, "cell": 2, "coefficient": 3}[what]
+        lib = _load()
+        count = lib.b2_coupled_copy(self._handle, code, None, _stream())
+        if count < 0:
+            _check(1)
+        out = np.zeros(count, np.float32)
+        if lib.b2_coupled_copy(self._handle, code, _ptr(out), _stream()) < 0:
+            _check(1)
+        return out
+
+    def levels(self) -> int:
+        return int(_load().b2_coupled_levels(self._handle))
+
+    def level(self, k: int) -> dict:
+        """Coarse level k >= 1: rows, cols, diag, a, c, g, h, d and the aggregate
+        of level k - 1."""
+        lib = _load()
+        n, nnz = ctypes.c_int(), ctypes.c_int()
+        _check(lib.b2_coupled_level_shape(self._handle, k, ctypes.byref(n), ctypes.byref(nnz)))
+        prev = ctypes.c_int()
+        _check(lib.b2_coupled_level_shape(self._handle, k - 1, ctypes.byref(prev), None))
+        n, nnz = n.value, nnz.value
+        out = {"rows": np.zeros(n + 1, np.int32), "cols": np.zeros(nnz, np.int32),
+               "diag": np.zeros(n, np.int32), "a": np.zeros(nnz, np.float32),
+               "c": np.zeros(nnz, np.float32), "g": np.zeros(3 * nnz, np.float32),
+               "h": np.zeros(3 * nnz, np.float32), "d": np.zeros(11 * n, np.float32),
+               "aggregate": np.zeros(prev.value, np.int32)}
+        _check(lib.b2_coupled_level_copy(self._handle, k, *(_ptr(out[key]) for key in (
+            "rows", "cols", "diag", "a", "c", "g", "h", "d", "aggregate")), _stream()))
+        return out
+
+    def apply(self, op: str, x, b, y) -> None:
+        """op 'spmv' (y = J x), 'residual' (y = b - J x), 'smooth' (one sweep
+        from x), 'smooth_zero' (from x = 0); float4-per-cell CUDA tensors."""
+        code = {"spmv": 0, "residual": 1, "smooth": 2, "smooth_zero": 3}[op]
+        _check(_load().b2_coupled_apply(self._handle, code, _tptr(x), _tptr(b), _tptr(y),
+                                        _stream()))
+
+    def level_apply(self, level: int, op: str, x, b, y) -> None:
+        """On coarse level `level` >= 1: 'residual', 'smooth', 'smooth_zero';
+        'restrict' (x on level - 1, y on level), 'prolong' (y on level - 1 +=
+        x on level)."""
+        code = {"residual": 1, "smooth": 2, "smooth_zero": 3, "restrict": 4, "prolong": 5}[op]
+        _check(_load().b2_coupled_level_apply(self._handle, int(level), code, _tptr(x), _tptr(b),
+                                              _tptr(y), _stream()))
+
+    def __del__(self):
+        if getattr(self, "_handle", None) and _lib is not None:
+            _lib.b2_coupled_destroy(self._handle)
+            self._handle = None
+
+
+def build_coupled_setup(mesh, options: CoupledOptions | None = None) -> dict:
+    """Host-only Coupled setup (b2_coupled_setup_build): 'cell' (27n with the
+    sensitivities), 'width', and per level its n, rows/cols/diag (coarse
+    levels) and aggregate/member_offsets/members (all but the coarsest)."""
+    lib = _load()
+    mesh = mesh if isinstance(mesh, CoupledMesh) else CoupledMesh(mesh)
+    opts = _coupled_options(options)
+    h = ctypes.c_void_p()
+    _check(lib.b2_coupled_setup_build(ctypes.byref(mesh.struct), ctypes.byref(opts),
+                                      ctypes.byref(h)))
+    try:
+        cell = np.zeros(27 * mesh.n_cells, np.float32)
+        _check(lib.b2_coupled_setup_cell(h, _ptr(cell)))
+        count = lib.b2_coupled_setup_levels(h)
+        sizes = []
+        for k in range(count):
+            n, nnz = ctypes.c_int(), ctypes.c_int()
+            _check(lib.b2_coupled_setup_level_shape(h, k, ctypes.byref(n), ctypes.byref(nnz)))
+            sizes.append((n.value, nnz.value))
+        levels = []
+        for k, (n, nnz) in enumerate(sizes):
+            lv = {"n": n}
+            if k > 0:
+                lv.update(rows=np.zeros(n + 1, np.int32), cols=np.zeros(nnz, np.int32),
+                          diag=np.zeros(n, np.int32))
+            if k + 1 < count:
+                lv.update(aggregate=np.zeros(n, np.int32),
+                          member_offsets=np.zeros(sizes[k + 1][0] + 1, np.int32),
+                          members=np.zeros(n, np.int32))
+            _check(lib.b2_coupled_setup_level_copy(h, k, *(_ptr(lv.get(key)) for key in (
+                "rows", "cols", "diag", "aggregate", "member_offsets", "members"))))
+            levels.append(lv)
+        return {"cell": cell, "width": int(lib.b2_coupled_setup_width(h)), "levels": levels}
+    finally:
+        lib.b2_coupled_setup_free(h)

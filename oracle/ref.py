@@ -162,3 +162,125 @@ def hierarchy(system, opts: Options | None = None) -> list[RefLevel]:
     finally:
         lib.kref_hierarchy_free(h)
     return out
+
+
+# ---- the reference's Coupled block solve (oracle/ref_coupled.cpp) ---------------
+
+class CoupledOptions(ctypes.Structure):
+    _fields_ = [("pre_sweeps", ctypes.c_int), ("post_sweeps", ctypes.c_int),
+                ("coarsest_sweeps", ctypes.c_int), ("coarsest_rows", ctypes.c_int),
+                ("aggregation_passes", ctypes.c_int), ("recompute", ctypes.c_int),
+                ("smoother_damping", ctypes.c_double), ("courant", ctypes.c_double)]
+
+
+def coupled_options(*, pre_sweeps=1, post_sweeps=2, coarsest_sweeps=8, coarsest_rows=48,
+                    aggregation_passes=3, recompute=False, smoother_damping=0.7,
+                    courant=200.0) -> CoupledOptions:
+    """CoupledOptions defaults of src/kutta/fv/coupled_solver.hpp:26-38."""
+    return CoupledOptions(pre_sweeps, post_sweeps, coarsest_sweeps, coarsest_rows,
+                          aggregation_passes, int(recompute), smoother_damping, courant)
+
+
+_DTYPES = {b"i": np.int32, b"f": np.float32, b"d": np.float64}
+
+
+def _coupled_lib():
+    lib = _load()
+    if not getattr(lib, "_coupled_typed", False):
+        P = ctypes.c_void_p
+        F = ctypes.POINTER(ctypes.c_float)
+        D = ctypes.POINTER(ctypes.c_double)
+        I = ctypes.POINTER(ctypes.c_int)
+        lib.kref_coupled_last_error.restype = ctypes.c_char_p
+        lib.kref_coupled_mesh.restype = P
+        lib.kref_coupled_mesh.argtypes = [ctypes.c_int] * 4 + [D, D, I]
+        lib.kref_coupled_solve.restype = ctypes.c_int
+        lib.kref_coupled_solve.argtypes = (
+            [P, ctypes.POINTER(CoupledOptions)] + [F] * 14 +
+            [ctypes.c_double, ctypes.c_double, ctypes.c_int, ctypes.c_double, ctypes.c_double,
+             ctypes.c_int, ctypes.c_int, I, I, D, ctypes.c_char_p, ctypes.c_int])
+        lib.kref_coupled_array.restype = ctypes.c_longlong
+        lib.kref_coupled_array.argtypes = [P, ctypes.c_char_p, P, ctypes.c_char_p]
+        lib.kref_coupled_names.restype = ctypes.c_int
+        lib.kref_coupled_names.argtypes = [P, ctypes.c_char_p, ctypes.c_int]
+        lib.kref_coupled_free.argtypes = [P]
+        lib._coupled_typed = True
+    return lib
+
+
+class CoupledCase:
+    """A box mesh built by the reference (make_box_hex / make_box_tet) with its
+    geometry, device mesh, stencil and pressure least-squares fit; `arrays`
+    holds every array a Coupled solver reads, by name."""
+
+    def __init__(self, tet: bool, nx: int, ny: int, nz: int, lo=(0, 0, 0), hi=(1, 1, 1),
+                 patch_kinds=(1, 2, 0, 0, 3, 3)):
+        self._lib = _coupled_lib()
+        lo = np.array(lo, np.float64)
+        hi = np.array(hi, np.float64)
+        kinds = np.array(patch_kinds, np.int32)
+        self._h = self._lib.kref_coupled_mesh(int(tet), nx, ny, nz, _ptr(lo, ctypes.c_double),
+                                              _ptr(hi, ctypes.c_double), _ptr(kinds, ctypes.c_int))
+        if not self._h:
+            raise RuntimeError(self._lib.kref_coupled_last_error().decode())
+        self.arrays = self._read_all()
+
+    def _read_all(self) -> dict:
+        size = self._lib.kref_coupled_names(self._h, None, 0)
+        buf = ctypes.create_string_buffer(size)
+        self._lib.kref_coupled_names(self._h, buf, size)
+        out = {}
+        for name in buf.value.decode().split():
+            t = ctypes.create_string_buffer(1)
+            nbytes = self._lib.kref_coupled_array(self._h, name.encode(), None, t)
+            a = np.zeros(nbytes // np.dtype(_DTYPES[t.raw]).itemsize, _DTYPES[t.raw])
+            self._lib.kref_coupled_array(self._h, name.encode(), a.ctypes.data, t)
+            out[name] = a
+        return out
+
+    def solve(self, fields: dict, opts: CoupledOptions | None = None, *, rel_tol=0.1,
+              abs_tol=1e-12, max_iter=20, capture=True) -> dict:
+        """One CoupledSolver construction + solve + update on this mesh. `fields`
+        holds momentum_u/v/w (over the stencil pattern), physical_u/v/w,
+        ru/rv/rw, mass, viscosity, physical_diagonal, face_weights,
+        net_outflow (or None), density, velocity_scale and reference. Returns
+        the captured arrays plus iterations, converged, residuals, seconds and
+        describe."""
+        lib = self._lib
+        opts = opts or coupled_options()
+        f32 = {k: np.ascontiguousarray(fields[k], np.float32) for k in (
+            "momentum_u", "momentum_v", "momentum_w", "physical_u", "physical_v", "physical_w",
+            "ru", "rv", "rw", "mass", "viscosity", "physical_diagonal", "face_weights")}
+        net = fields.get("net_outflow")
+        net = None if net is None else np.ascontiguousarray(net, np.float32)
+        it, conv = ctypes.c_int(), ctypes.c_int()
+        res = np.zeros(4, np.float64)
+        desc = ctypes.create_string_buffer(512)
+        F = ctypes.c_float
+        rc = lib.kref_coupled_solve(
+            self._h, ctypes.byref(opts), *(_ptr(f32[k], F) for k in (
+                "momentum_u", "momentum_v", "momentum_w", "physical_u", "physical_v",
+                "physical_w", "ru", "rv", "rw", "mass", "viscosity", "physical_diagonal",
+                "face_weights")),
+            _ptr(net, F) if net is not None else None, float(fields["density"]),
+            float(fields["velocity_scale"]), int(fields["reference"]), rel_tol, abs_tol,
+            max_iter, int(capture), ctypes.byref(it), ctypes.byref(conv),
+            _ptr(res, ctypes.c_double), desc, 512)
+        if rc != 0:
+            raise RuntimeError(lib.kref_coupled_last_error().decode())
+        out = self._read_all() if capture else {}
+        out.update(iterations=it.value, converged=bool(conv.value), initial_residual=res[0],
+                   final_residual=res[1], setup_s=res[2], solve_s=res[3],
+                   describe=desc.value.decode())
+        return out
+
+    def close(self):
+        if self._h:
+            self._lib.kref_coupled_free(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
