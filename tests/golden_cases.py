@@ -12,10 +12,12 @@ GOLDEN = pathlib.Path(__file__).resolve().parent / "golden"
 
 def names():
     """The seeded-system solve fixtures of tests/golden/make_golden.py (the real
-    matrices of make_real.py have their own format and tests, and the
-    hierarchy-only fixtures their own loader)."""
+    matrices of make_real.py and the Coupled cases of make_coupled.py have
+    their own formats and tests, and the hierarchy-only fixtures their own
+    loader)."""
     return sorted(p.stem for p in GOLDEN.glob("*.npz")
-                  if not p.stem.startswith("tmr_") and not p.stem.endswith("_hierarchy"))
+                  if not p.stem.startswith(("tmr_", "coupled_"))
+                  and not p.stem.endswith("_hierarchy"))
 
 
 def hierarchy_names():

@@ -13,7 +13,8 @@ from kutta_b200 import linalg as L
 
 B2_OK, B2_INVALID_ARGUMENT, B2_DEVICE_ERROR = 0, 1, 3
 # The int-returning entry points that return a status (the others return counts).
-COUNTS = {"b2_gnn_parameter_count", "b2_solver_levels", "b2_hierarchy_levels"}
+COUNTS = {"b2_gnn_parameter_count", "b2_solver_levels", "b2_hierarchy_levels",
+          "b2_coupled_levels", "b2_coupled_setup_levels", "b2_coupled_setup_width"}
 STATUS_FUNCTIONS = [n for n, (res, _) in L._SIGNATURES.items() if res is ctypes.c_int
                     and n not in COUNTS]
 # Entry points whose all-zero call is a valid empty operation.
@@ -24,7 +25,7 @@ EMPTY_OK = {"b2_csr_spmv", "b2_csr_residual", "b2_amg_smooth", "b2_fv_correct_fl
 def _args(name, size):
     out = []
     for a in L._SIGNATURES[name][1]:
-        if a is ctypes.c_float:
+        if a in (ctypes.c_float, ctypes.c_double):
             out.append(0.5)
         elif a in (ctypes.c_int, ctypes.c_size_t, ctypes.c_uint64, ctypes.c_longlong):
             out.append(size)
