@@ -844,6 +844,101 @@ def run_outer(args):
             "peak_source": kind, "steps": args.steps}
 
 
+def run_coupled(args):
+    """The Coupled (4x4-block) pressure-velocity solve of the pseudo-transient
+    Coupled scheme (src/kutta/fv/coupled_solver.cpp) on a structured hex box
+    of --cells-per-side^3 cells (inlet, pressure outlet, walls, symmetry
+    planes) with seeded flow fields (kutta_b200/coupled_harness.py): one step
+    is the three momentum-diagonal captures plus CoupledSolver::solve
+    (Jacobian assembly, Galerkin hierarchy refresh, block BiCGStab to the
+    steady solver's control: relative 0.1, at most 20 iterations), device-
+    timed over --steps after --warmup. The fine damped block-Jacobi sweep is
+    timed on its own for its HBM fraction. The reference's own CPU solve
+    (oracle/_ref) runs on a smaller box of the same kind as the CPU baseline."""
+    import numpy as np
+    import torch
+    from kutta_b200 import coupled_harness as H
+    from kutta_b200 import linalg as L
+    torch.cuda.set_device(0)
+    side = args.cells_per_side
+    t0 = time.perf_counter()
+    mesh = H.box_hex(side, side, side)
+    fields = H.flow_fields(mesh, args.seed)
+    make_s = time.perf_counter() - t0
+    n, nf, ni, entries, nnz = (int(v) for v in mesh["sizes"])
+    t = lambda a: torch.from_numpy(np.ascontiguousarray(a)).cuda()  # noqa: E731
+    dev = {k: (t(v) if isinstance(v, np.ndarray) else v) for k, v in fields.items()}
+    rows, diag = t(mesh["pattern_row_ptr"]), t(mesh["pattern_diag"])
+    t0 = time.perf_counter()
+    solver = L.CoupledSolver(mesh, -1, L.CoupledOptions())
+    setup_s = time.perf_counter() - t0
+    control = L.SolveControl(args.coupled_rel_tol, 1e-12, args.coupled_max_iter)
+
+    def step():
+        for k, c in enumerate("uvw"):
+            solver.capture_diagonal(k, rows, diag, dev["momentum_" + c], dev["physical_" + c])
+        return solver.solve(dev, control)
+
+    for _ in range(args.warmup):
+        step()
+    launches0 = L.kernel_launches()
+    ms, results = _timed(step, args.steps, torch.cuda.current_stream(), torch.cuda.synchronize)
+    launches = (L.kernel_launches() - launches0) // args.steps
+    st = results[-1]
+    # The fine sweep alone: per cell x, b, next (float4 each) and the five
+    # per-cell records (88 bytes); per internal cell-face slot the edge
+    # (a, gx, gy, gz), h and (neighbour, face) (28 bytes); per face its
+    # (sx, sy, sz, rc) record (16 bytes).
+    width_slots = int(np.sum(mesh["adjacent"] >= 0))
+    sweep_bytes = n * (48 + 88) + width_slots * 28 + nf * 16
+    x4 = torch.randn(4 * n, device="cuda")
+    b4 = torch.randn(4 * n, device="cuda")
+    y4 = torch.empty(4 * n, device="cuda")
+    for _ in range(3):
+        solver.apply("smooth", x4, b4, y4)
+    reps = 50
+    sweep_ms, _ = _timed(lambda: solver.apply("smooth", x4, b4, y4), reps,
+                         torch.cuda.current_stream(), torch.cuda.synchronize)
+    spmv_ms, _ = _timed(lambda: solver.apply("spmv", x4, b4, y4), reps,
+                        torch.cuda.current_stream(), torch.cuda.synchronize)
+    peak, kind = _peaks()
+    achieved = sweep_bytes / (sweep_ms * 1e-3) / 1e9
+    out = {"mode": "coupled",
+           "workload": f"coupled_hex{side}: {side}^3 hex box, {n} cells, {nf} faces, "
+                       f"{width_slots} internal cell-face slots, 4 unknowns per cell",
+           "method": solver.describe(), "control": [control.rel_tol, control.abs_tol,
+                                                     control.max_iter],
+           "ms_per_solve": ms, "iterations": st.iterations, "converged": st.converged,
+           "initial_residual": st.initial_residual, "final_residual": st.final_residual,
+           "gpu_launches_per_solve": launches, "setup_s": setup_s, "mesh_and_fields_s": make_s,
+           "device_bytes": solver.bytes(), "steps": args.steps, "warmup": args.warmup,
+           "fine_sweep": {"kernel": "k_cpl_fine_smooth", "ms": sweep_ms,
+                          "bytes_per_launch": sweep_bytes, "achieved_gbs": achieved,
+                          "peak_gbs": peak, "peak_source": kind, "frac": achieved / peak},
+           "fine_spmv_ms": spmv_ms}
+    if not args.no_cpu_baseline:
+        try:
+            from oracle import ref
+            if ref.available():
+                cside = args.coupled_cpu_side
+                case = ref.CoupledCase(False, cside, cside, cside)
+                f = H.flow_fields(case.arrays, args.seed)
+                r = case.solve(f, ref.coupled_options(), rel_tol=control.rel_tol,
+                               abs_tol=control.abs_tol, max_iter=control.max_iter, capture=False)
+                cells = int(case.arrays["sizes"][0])
+                out["cpu_baseline"] = {
+                    "kind": "reference", "cores": 1,
+                    "sample": f"the reference's CoupledSolver (oracle/_ref, serial CPU device) "
+                              f"on a {cside}^3 hex box of the same kind ({cells} cells)",
+                    "ms_per_solve": r["solve_s"] * 1e3, "iterations": r["iterations"],
+                    "construct_s": r["setup_s"], "describe": r["describe"],
+                    "ns_per_cell_iteration": r["solve_s"] * 1e9 / cells / max(1, r["iterations"])}
+                out["ns_per_cell_iteration"] = ms * 1e6 / n / max(1, st.iterations)
+        except Exception as e:  # the baseline is informative only
+            out["cpu_baseline"] = {"unavailable": str(e)}
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -860,18 +955,24 @@ def main():
                     help="skip the graded 1e-8 and learned-evaluation entries")
     ap.add_argument("--mode", default="bench",
                     choices=["bench", "profile", "sequence", "graded", "transport", "outer",
-                             "workload"],
+                             "workload", "coupled"],
                     help="profile: one refresh + one solve (with --max-iter), for ncu captures; "
                          "sequence: successive warm-started solves on the graded mesh; "
                          "graded: the graded matrix to --rel-tol (default 1e-8); "
                          "transport: the non-symmetric twin with AMG-BiCGStab and "
                          "BiCGStab-Jacobi (default 1e-6); outer: the pressure assembly fused "
-                         "with the refresh, and the flux/velocity corrections")
+                         "with the refresh, and the flux/velocity corrections; coupled: the "
+                         "Coupled 4x4-block solve on a hex box")
     ap.add_argument("--method", default="mixed", choices=["mixed", "plain"])
     ap.add_argument("--solves", type=int, default=300, help="sequence mode: number of solves")
     ap.add_argument("--rel-tol", type=float, default=None,
                     help="sequence / graded modes (defaults 1e-6 / 1e-8)")
     ap.add_argument("--out", default=None, help="workload mode: the .npz to write")
+    ap.add_argument("--cells-per-side", type=int, default=128, help="coupled mode: box side")
+    ap.add_argument("--coupled-rel-tol", type=float, default=0.1)
+    ap.add_argument("--coupled-max-iter", type=int, default=20)
+    ap.add_argument("--coupled-cpu-side", type=int, default=128,
+                    help="coupled mode: box side of the reference CPU baseline")
     args = ap.parse_args()
     rank, world, local = _dist()
     if args.mode == "workload":
@@ -880,11 +981,11 @@ def main():
     if args.mode == "profile":
         profile_once(args)
         return
-    if args.mode in ("sequence", "graded", "transport", "outer"):
+    if args.mode in ("sequence", "graded", "transport", "outer", "coupled"):
         if args.rel_tol is None:
             args.rel_tol = 1e-8 if args.mode == "graded" else 1e-6
         run = {"sequence": run_sequence, "graded": run_graded, "transport": run_transport,
-               "outer": run_outer}
+               "outer": run_outer, "coupled": run_coupled}
         print(json.dumps(run[args.mode](args)))
         return
     if args.impl == "reference":
