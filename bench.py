@@ -882,7 +882,10 @@ def run_coupled(args):
     for _ in range(args.warmup):
         step()
     launches0 = L.kernel_launches()
+    clocks = Clocks(0)
+    clocks.start()
     ms, results = _timed(step, args.steps, torch.cuda.current_stream(), torch.cuda.synchronize)
+    clk = clocks.stop()
     launches = (L.kernel_launches() - launches0) // args.steps
     st = results[-1]
     # The fine sweep alone: per cell x, b, next (float4 each) and the five
@@ -915,7 +918,7 @@ def run_coupled(args):
            "fine_sweep": {"kernel": "k_cpl_fine_smooth", "ms": sweep_ms,
                           "bytes_per_launch": sweep_bytes, "achieved_gbs": achieved,
                           "peak_gbs": peak, "peak_source": kind, "frac": achieved / peak},
-           "fine_spmv_ms": spmv_ms}
+           "fine_spmv_ms": spmv_ms, "clocks": clk}
     if not args.no_cpu_baseline:
         try:
             from oracle import ref
