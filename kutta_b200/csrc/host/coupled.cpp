@@ -5,6 +5,7 @@
 #include "coupled.hpp"
 
 #include <cmath>
+#include <cstdlib>
 #include <sstream>
 #include <utility>
 
@@ -20,6 +21,10 @@ std::vector<T> copy_of(const T* p, std::size_t n) {
 CoupledSolver::CoupledSolver(const CoupledMeshHost& m, int reference,
                              const CoupledOptions& options, cudaStream_t s)
     : stream_(s), options_(options), n_(m.n_cells), reference_(reference) {
+  // KUTTA_B200_COUPLED_GRAPHS=0 launches every kernel of an iteration
+  // directly instead of replaying a graph (the same results), for comparisons.
+  const char* graphs = std::getenv("KUTTA_B200_COUPLED_GRAPHS");
+  graphs_enabled_ = !(graphs && std::string(graphs) == "0");
   KB2_REQUIRE(reference < m.n_cells, "coupled: reference cell out of range");
   CoupledSetup setup = coupled_setup(m, options);
   width_ = setup.width;
@@ -86,9 +91,11 @@ CoupledSolver::CoupledSolver(const CoupledMeshHost& m, int reference,
     own(l.g, 3 * nnz);
     own(l.h, 3 * nnz);
     own(l.d, 11 * cn);
-    own(l.x, cn);
     own(l.b, cn);
-    own(l.tmp, cn);
+    own(l.store[0], cn);
+    own(l.store[1], cn);
+    l.x = l.store[0].get();
+    l.tmp = l.store[1].get();
     l.op = CoupledLevel{src.n, src.nnz, l.rows.get(), l.cols.get(), l.diag.get(),
                         l.a.get(),  l.c.get(),   l.g.get(),    l.h.get(),    l.d.get()};
     levels_.push_back(std::move(l));
@@ -118,6 +125,88 @@ CoupledSolver::CoupledSolver(const CoupledMeshHost& m, int reference,
   cuda_check(cudaMemsetAsync(x_, 0, n * sizeof(float4), s), "memset");
   cuda_check(cudaMemsetAsync(link_.get(), 0xff, slots * sizeof(int2), s), "memset");
   cuda_check(cudaGetLastError(), "coupled setup");
+}
+
+CoupledSolver::~CoupledSolver() {
+  for (auto& g : graphs_)
+    if (g.exec) cudaGraphExecDestroy(g.exec);
+  if (capture_) cudaStreamDestroy(capture_);
+}
+
+std::vector<float4*> CoupledSolver::roles() const {
+  std::vector<float4*> r{x_, z_, zs_, tmp_};
+  for (const auto& l : levels_) {
+    r.push_back(l.x);
+    r.push_back(l.tmp);
+  }
+  return r;
+}
+
+void CoupledSolver::set_roles(const std::vector<float4*>& r) {
+  x_ = r[0];
+  z_ = r[1];
+  zs_ = r[2];
+  tmp_ = r[3];
+  for (std::size_t k = 0; k < levels_.size(); ++k) {
+    levels_[k].x = r[4 + 2 * k];
+    levels_[k].tmp = r[5 + 2 * k];
+  }
+}
+
+// The iteration's ~100 launches cost more host time than several of its
+// kernels take on the device, and the solve waits on the host after every
+// iteration (the status read), so the GPU idles while they are enqueued.
+// Captured once per buffer-role state (the smoother's ping-pong cycles
+// through three), each iteration is then one graph launch. A capture runs on
+// an internal stream and executes nothing; the graph is launched on the
+// solve stream.
+template <class Body>
+void CoupledSolver::iteration(Body body) {
+  if (!graphs_enabled_) {
+    body();
+    return;
+  }
+  const auto before = roles();
+  for (const auto& g : graphs_)
+    if (g.before == before) {
+      cuda_check(cudaGraphLaunch(g.exec, stream_), "cudaGraphLaunch");
+      launch::counter += g.launches;
+      set_roles(g.after);
+      return;
+    }
+  if (capture_ == nullptr)
+    cuda_check(cudaStreamCreateWithFlags(&capture_, cudaStreamNonBlocking), "cudaStreamCreate");
+  const cudaStream_t solve = stream_;
+  stream_ = capture_;
+  const long long launches0 = launch::counter.load();
+  cudaGraph_t graph = nullptr;
+  cuda_check(cudaStreamBeginCapture(capture_, cudaStreamCaptureModeThreadLocal), "capture");
+  try {
+    body();
+  } catch (...) {
+    cudaStreamEndCapture(capture_, &graph);
+    if (graph) cudaGraphDestroy(graph);
+    stream_ = solve;
+    set_roles(before);
+    throw;
+  }
+  const cudaError_t ended = cudaStreamEndCapture(capture_, &graph);
+  stream_ = solve;
+  cuda_check(ended, "capture");
+  IterationGraph g;
+  g.before = before;
+  g.after = roles();
+  g.launches = launch::counter.load() - launches0;
+  launch::counter -= g.launches;  // counted when launched
+  const cudaError_t made = cudaGraphInstantiate(&g.exec, graph, 0);
+  cudaGraphDestroy(graph);
+  cuda_check(made, "cudaGraphInstantiate");
+  cuda_check(cudaGraphLaunch(g.exec, stream_), "cudaGraphLaunch");
+  launch::counter += g.launches;
+  if (graphs_.size() < 8)
+    graphs_.push_back(std::move(g));
+  else
+    cudaGraphExecDestroy(g.exec);  // deferred by CUDA until the launch ends
 }
 
 CoupledFine CoupledSolver::fine() const {
@@ -150,7 +239,7 @@ void CoupledSolver::fine_smooth(float4*& out, const float4* rhs, int sweeps, boo
 
 void CoupledSolver::coarse_smooth(Level& l, int sweeps, bool first) {
   for (int k = 0; k < sweeps; ++k) {
-    launch::cpl_coarse_smooth(l.op, l.x.get(), l.b.get(), l.tmp.get(), options_.smoother_damping,
+    launch::cpl_coarse_smooth(l.op, l.x, l.b.get(), l.tmp, options_.smoother_damping,
                               first && k == 0, stream_);
     std::swap(l.x, l.tmp);
   }
@@ -166,11 +255,11 @@ void CoupledSolver::cycle(std::size_t k) {
   }
   auto& c = levels_[k + 1];
   coarse_smooth(l, options_.pre_sweeps, true);
-  launch::cpl_coarse_residual(l.op, l.x.get(), l.b.get(), l.tmp.get(), stream_);
+  launch::cpl_coarse_residual(l.op, l.x, l.b.get(), l.tmp, stream_);
   const auto& t = transfers_[k + 1].view;
-  launch::cpl_restrict(c.op.n, t.offsets, t.members, l.tmp.get(), c.b.get(), stream_);
+  launch::cpl_restrict(c.op.n, t.offsets, t.members, l.tmp, c.b.get(), stream_);
   cycle(k + 1);
-  launch::cpl_prolong(l.op.n, t.aggregate, c.x.get(), l.x.get(), stream_);
+  launch::cpl_prolong(l.op.n, t.aggregate, c.x, l.x, stream_);
   coarse_smooth(l, options_.post_sweeps, false);
 }
 
@@ -183,7 +272,7 @@ void CoupledSolver::precondition(const float4* rhs, float4*& out) {
     launch::cpl_fine_residual(n_, fine(), width_, out, rhs, tmp_, stream_);
     launch::cpl_restrict(c.op.n, t.offsets, t.members, tmp_, c.b.get(), stream_);
     cycle(0);
-    launch::cpl_prolong(n_, t.aggregate, c.x.get(), out, stream_);
+    launch::cpl_prolong(n_, t.aggregate, c.x, out, stream_);
   }
   fine_smooth(out, rhs, options_.post_sweeps, false);
 }
@@ -197,19 +286,19 @@ void CoupledSolver::galerkin(const CoupledSolveInputs& in) {
   for (std::size_t k = 1; k < levels_.size(); ++k)
     launch::cpl_galerkin_coarse(levels_[k].op, transfers_[k].view, levels_[k - 1].op, stream_);
   for (auto& l : levels_)
-    launch::cpl_coarse_prepare(l.op, reinterpret_cast<float*>(l.tmp.get()), stream_);
+    launch::cpl_coarse_prepare(l.op, reinterpret_cast<float*>(l.tmp), stream_);
 }
 
 double CoupledSolver::norm(const float4* v) {
   const float* f = reinterpret_cast<const float*>(v);
   launch::reduce_value(ReduceMode::Dot, 4 * n_, f, f, DeviceReducer{partials_.get(), ticket_.get()},
                        values_.get(), 0, stream_);
-  double out = 0;
-  cuda_check(cudaMemcpyAsync(&out, values_.get(), sizeof(double), cudaMemcpyDeviceToHost, stream_),
+  cuda_check(cudaMemcpyAsync(host_value_.get(), values_.get(), sizeof(double),
+                             cudaMemcpyDeviceToHost, stream_),
              "norm readback");
   wait(stream_);
   cuda_check(cudaGetLastError(), "coupled norm");
-  return std::sqrt(out);
+  return std::sqrt(host_value_[0]);
 }
 
 // ---- the block BiCGStab (coupled_solver.cpp:389-451) -----------------------------
@@ -251,26 +340,28 @@ Stats CoupledSolver::bicgstab(const Control& c) {
   };
   restart();
   int restarts = 0;
-  Pinned<int> state(3);
+  Pinned<int>& state = host_status_;
   while (stats.iterations < c.max_iter) {
-    launch::reduce_into(ReduceMode::Dot, n4, F(shadow_), F(r_), F(shadow_), F(r_), red, sc, 0, st,
-                        true, Epilogue::BicgBeta, stream_);
-    launch::bicg_direction(n4, F(r_), F(q_), F(p_), sc, st, stream_);
-    precondition(p_.get(), z_);
-    launch::cpl_fine_spmv(n_, fine(), width_, z_, q_.get(), stream_);
-    launch::reduce_into(ReduceMode::Dot, n4, F(shadow_), F(q_), F(shadow_), F(q_), red, sc, 2, st,
-                        true, Epilogue::BicgAlpha, stream_);
-    launch::bicg_difference(n4, F(r_), F(q_), F(sv_), sc, st, stream_);
-    launch::reduce_into(ReduceMode::Dot, n4, F(sv_), F(sv_), F(sv_), F(sv_), red, sc, 16, st, true,
-                        Epilogue::BicgS, stream_);
-    precondition(sv_.get(), zs_);
-    launch::cpl_fine_spmv(n_, fine(), width_, zs_, t_.get(), stream_);
-    launch::reduce_into(ReduceMode::Dot2, n4, F(t_), F(t_), F(t_), F(sv_), red, sc, 2, st, true,
-                        Epilogue::BicgOmega, stream_);
-    launch::bicg_step(n4, reinterpret_cast<float*>(x_), F(r_), reinterpret_cast<float*>(z_),
-                      reinterpret_cast<float*>(zs_), F(sv_), F(t_), sc, st, stream_);
-    launch::reduce_into(ReduceMode::Dot, n4, F(r_), F(r_), F(r_), F(r_), red, sc, 18, st, true,
-                        Epilogue::CheckBicg, stream_);
+    iteration([&] {
+      launch::reduce_into(ReduceMode::Dot, n4, F(shadow_), F(r_), F(shadow_), F(r_), red, sc, 0, st,
+                          true, Epilogue::BicgBeta, stream_);
+      launch::bicg_direction(n4, F(r_), F(q_), F(p_), sc, st, stream_);
+      precondition(p_.get(), z_);
+      launch::cpl_fine_spmv(n_, fine(), width_, z_, q_.get(), stream_);
+      launch::reduce_into(ReduceMode::Dot, n4, F(shadow_), F(q_), F(shadow_), F(q_), red, sc, 2, st,
+                          true, Epilogue::BicgAlpha, stream_);
+      launch::bicg_difference(n4, F(r_), F(q_), F(sv_), sc, st, stream_);
+      launch::reduce_into(ReduceMode::Dot, n4, F(sv_), F(sv_), F(sv_), F(sv_), red, sc, 16, st, true,
+                          Epilogue::BicgS, stream_);
+      precondition(sv_.get(), zs_);
+      launch::cpl_fine_spmv(n_, fine(), width_, zs_, t_.get(), stream_);
+      launch::reduce_into(ReduceMode::Dot2, n4, F(t_), F(t_), F(t_), F(sv_), red, sc, 2, st, true,
+                          Epilogue::BicgOmega, stream_);
+      launch::bicg_step(n4, reinterpret_cast<float*>(x_), F(r_), reinterpret_cast<float*>(z_),
+                        reinterpret_cast<float*>(zs_), F(sv_), F(t_), sc, st, stream_);
+      launch::reduce_into(ReduceMode::Dot, n4, F(r_), F(r_), F(r_), F(r_), red, sc, 18, st, true,
+                          Epilogue::CheckBicg, stream_);
+    });
     cuda_check(cudaMemcpyAsync(state.get(), st, 3 * sizeof(int), cudaMemcpyDeviceToHost, stream_),
                "status readback");
     wait(stream_);

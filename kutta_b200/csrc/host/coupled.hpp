@@ -24,6 +24,7 @@ class CoupledSolver {
                 cudaStream_t s);
   CoupledSolver(const CoupledSolver&) = delete;
   CoupledSolver& operator=(const CoupledSolver&) = delete;
+  ~CoupledSolver();
 
   // One momentum component's assembled diagonal (device CSR over the stencil
   // pattern and its physical diagonal), floored and relaxed by the Courant
@@ -75,7 +76,15 @@ class CoupledSolver {
     CoupledLevel op;
     DArray<int> rows, cols, diag;
     DArray<float> a, c, g, h, d;
-    DArray<float4> x, b, tmp;
+    DArray<float4> b, store[2];
+    float4 *x = nullptr, *tmp = nullptr;  // the smoother's ping-pong roles over store
+  };
+  // One BiCGStab iteration as a CUDA graph, for the buffer roles it starts
+  // from; `after` are the roles it leaves.
+  struct IterationGraph {
+    std::vector<float4*> before, after;
+    cudaGraphExec_t exec = nullptr;
+    long long launches = 0;
   };
   struct Transfer {
     CoupledTransfer view;
@@ -98,6 +107,11 @@ class CoupledSolver {
   void precondition(const float4* rhs, float4*& out);
   void galerkin(const CoupledSolveInputs& in);
   double norm(const float4* v);
+  std::vector<float4*> roles() const;
+  void set_roles(const std::vector<float4*>& r);
+  // Runs `body` (kernel launches only) directly, or as a cached graph.
+  template <class Body>
+  void iteration(Body body);
   Stats bicgstab(const Control& c);
   Stats bounded(Stats stats, double target);
 
@@ -127,6 +141,13 @@ class CoupledSolver {
   DArray<double> partials_, values_;
   DArray<unsigned> ticket_;
   CoupledSolveInputs inputs_;
+  // Pinned host words for the per-iteration status and the norms (a pinned
+  // allocation per solve costs milliseconds and its release synchronises).
+  Pinned<int> host_status_{3};
+  Pinned<double> host_value_{1};
+  bool graphs_enabled_ = true;
+  cudaStream_t capture_ = nullptr;
+  std::vector<IterationGraph> graphs_;
 };
 
 }  // namespace kb2

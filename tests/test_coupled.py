@@ -378,3 +378,23 @@ def test_coupled_coarse_kernels_match_oracle(cuda, name):
         agg = lv["aggregate"][:nf]
         want_p = np.concatenate([base[c * nf:(c + 1) * nf] + x[c * n + agg] for c in range(4)])
         assert np.array_equal(bits(_planes(yf.cpu().numpy(), nf)), bits(want_p)), k
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", ["coupled_tet6x5x4_tight", "coupled_hex12x10x8_closed"])
+def test_graph_replay_changes_no_bits(cuda, name, monkeypatch):
+    """Each BiCGStab iteration replayed as a CUDA graph (the default) gives
+    the directly launched iterations' solution and statistics bit for bit,
+    over two solves (the second replays graphs captured in the first)."""
+    meta, mesh, fields, _ = load(name)
+    runs = []
+    for graphs in ("1", "0"):
+        monkeypatch.setenv("KUTTA_B200_COUPLED_GRAPHS", graphs)
+        s, st, d = _solver(meta, mesh, fields)
+        rel, abs_, max_iter = meta["control"]
+        st2 = s.solve(d, L.SolveControl(rel, abs_, max_iter))
+        runs.append((st, st2, s.copy("x")))
+    (a1, a2, ax), (b1, b2, bx) = runs
+    assert (a1.iterations, a1.final_residual) == (b1.iterations, b1.final_residual)
+    assert (a2.iterations, a2.final_residual) == (b2.iterations, b2.final_residual)
+    assert np.array_equal(bits(ax), bits(bx))
