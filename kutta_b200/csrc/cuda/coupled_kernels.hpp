@@ -67,6 +67,23 @@ struct CoupledTransfer {
   const int* members = nullptr;
 };
 
+// The V-cycle of the small coarse levels (each at most kMaxRows rows) as one
+// single-block launch: levels 0 .. levels-1 of the tail, the first receiving
+// its right-hand side from the level above; x/tmp are each level's current
+// ping-pong roles.
+struct CoupledTail {
+  static constexpr int kMaxLevels = 12;
+  static constexpr int kMaxRows = 1024;
+  int levels = 0;
+  int pre = 1, post = 2, coarsest = 8;
+  float omega = 0.7f;
+  CoupledLevel op[kMaxLevels];
+  CoupledTransfer down[kMaxLevels];  // down[k]: tail level k -> k + 1
+  float4* x[kMaxLevels];
+  float4* tmp[kMaxLevels];
+  float4* b[kMaxLevels];
+};
+
 namespace launch {
 
 // Plane = the cell data's slot k (momentum diagonal of component k).
@@ -100,6 +117,8 @@ void cpl_restrict(int nc, const int* offsets, const int* members, const float4* 
                   float4* coarse, cudaStream_t s);
 void cpl_prolong(int nf, const int* aggregate, const float4* coarse, float4* fine,
                  cudaStream_t s);
+
+void cpl_tail(const CoupledTail& t, cudaStream_t s);
 
 void cpl_update(int n, const float4* delta, float* u, float* v, float* w, float* p, float alpha_u,
                 float alpha_p, cudaStream_t s);

@@ -107,6 +107,14 @@ CoupledSolver::CoupledSolver(const CoupledMeshHost& m, int reference,
     t.view = CoupledTransfer{t.aggregate.get(), t.offsets.get(), t.members.get()};
     transfers_.push_back(std::move(t));
   }
+  // Levels from `tail_` down are small enough for the one-block V-cycle
+  // (KUTTA_B200_COUPLED_TAIL=0: separate launches, the same results).
+  const char* tail = std::getenv("KUTTA_B200_COUPLED_TAIL");
+  tail_ = levels_.size();
+  if (!(tail && std::string(tail) == "0"))
+    while (tail_ > 0 && levels_[tail_ - 1].op.n <= CoupledTail::kMaxRows &&
+           levels_.size() - (tail_ - 1) <= static_cast<std::size_t>(CoupledTail::kMaxLevels))
+      --tail_;
   for (auto* v : {&b_, &r_, &shadow_, &p_, &q_, &sv_, &t_}) own(*v, n);
   for (auto& v : store_) own(v, n);
   x_ = store_[0].get();
@@ -248,6 +256,30 @@ void CoupledSolver::coarse_smooth(Level& l, int sweeps, bool first) {
 // Coarse level k receives its right-hand side in levels_[k].b
 // (coupled_solver.cpp:331-347).
 void CoupledSolver::cycle(std::size_t k) {
+  if (k == tail_) {
+    CoupledTail t;
+    t.levels = static_cast<int>(levels_.size() - k);
+    t.pre = options_.pre_sweeps;
+    t.post = options_.post_sweeps;
+    t.coarsest = options_.coarsest_sweeps;
+    t.omega = options_.smoother_damping;
+    for (int j = 0; j < t.levels; ++j) {
+      auto& l = levels_[k + j];
+      t.op[j] = l.op;
+      t.x[j] = l.x;
+      t.tmp[j] = l.tmp;
+      t.b[j] = l.b.get();
+      if (j + 1 < t.levels) t.down[j] = transfers_[k + j + 1].view;
+    }
+    launch::cpl_tail(t, stream_);
+    // The roles the separate launches would leave: each level swaps once per
+    // sweep.
+    for (int j = 0; j < t.levels; ++j) {
+      const int sweeps = j + 1 < t.levels ? t.pre + t.post : t.coarsest;
+      if (sweeps % 2) std::swap(levels_[k + j].x, levels_[k + j].tmp);
+    }
+    return;
+  }
   auto& l = levels_[k];
   if (k + 1 == levels_.size()) {
     coarse_smooth(l, options_.coarsest_sweeps, true);

@@ -146,6 +146,9 @@ class CoupledSolver {
   Pinned<int> host_status_{3};
   Pinned<double> host_value_{1};
   bool graphs_enabled_ = true;
+  // The first coarse level (index into levels_) from which the V-cycle runs
+  // as one launch (levels_.size(): none).
+  std::size_t tail_ = 0;
   cudaStream_t capture_ = nullptr;
   std::vector<IterationGraph> graphs_;
 };

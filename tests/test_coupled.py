@@ -398,3 +398,23 @@ def test_graph_replay_changes_no_bits(cuda, name, monkeypatch):
     assert (a1.iterations, a1.final_residual) == (b1.iterations, b1.final_residual)
     assert (a2.iterations, a2.final_residual) == (b2.iterations, b2.final_residual)
     assert np.array_equal(bits(ax), bits(bx))
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", ["coupled_tet6x5x4_tight", "coupled_hex12x10x8_closed",
+                                  "coupled_hex10x8x6_v22_net"])
+def test_one_block_tail_changes_no_bits(cuda, name, monkeypatch):
+    """The small coarse levels' V-cycle in one launch (the default on these
+    sizes) gives the separate launches' solution and statistics bit for bit."""
+    meta, mesh, fields, _ = load(name)
+    runs = []
+    for tail in ("1", "0"):
+        monkeypatch.setenv("KUTTA_B200_COUPLED_TAIL", tail)
+        s, st, d = _solver(meta, mesh, fields)
+        rel, abs_, max_iter = meta["control"]
+        st2 = s.solve(d, L.SolveControl(rel, abs_, max_iter))
+        runs.append((st, st2, s.copy("x")))
+    (a1, a2, ax), (b1, b2, bx) = runs
+    assert (a1.iterations, a1.final_residual) == (b1.iterations, b1.final_residual)
+    assert (a2.iterations, a2.final_residual) == (b2.iterations, b2.final_residual)
+    assert np.array_equal(bits(ax), bits(bx))
