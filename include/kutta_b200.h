@@ -289,7 +289,8 @@ int b2_mixed_hierarchy_build(int n, int nnz, const int32_t* row_ptr, const int32
  * error's A-energy left after the best step along c. */
 typedef struct b2_gnn b2_gnn;
 /* A stage with weights drawn from `seed`; b2_gnn_set_weights loads trained
- * ones (b2_gnn_parameter_count floats). */
+ * ones (b2_gnn_parameter_count floats; the count without the geometry gate's
+ * two parameters is accepted too, leaving the gate off). */
 int b2_gnn_create(uint64_t seed, b2_gnn** out);
 void b2_gnn_destroy(b2_gnn* g);
 int b2_gnn_parameter_count(void);
@@ -297,6 +298,15 @@ int b2_gnn_parameter_count(void);
  * bound and bind again after its values change. */
 int b2_gnn_bind(b2_gnn* g, int n, const int32_t* d_row_ptr, const int32_t* d_col,
                 const int32_t* d_diag, const float* d_val, void* stream);
+/* The geometry of the matrices bound from now on (takes effect at the next
+ * bind, including a mixed solver's refresh): d_geometry holds, per entry of
+ * the bound CSR pattern, the face's geometric coefficient |A_f| / |c_N - c_P|
+ * (0 on the diagonal), or is NULL for none. Each edge weight w_ij is then
+ * gated, E_ij = w_ij exp(theta_0 tanh(theta_1 rho_ij)) with rho_ij =
+ * log((g_ij / sqrt(G_i G_j)) / w_ij), G_i = sum_j g_ij: an edge feature from
+ * the face coefficient and the geometry, theta the last two weights. Keep the
+ * array alive while bound. */
+int b2_gnn_set_geometry(b2_gnn* g, const float* d_geometry);
 /* d_z = beta d_z + G(d_r), beta 0 or 1: the tensor-core forward (BF16
  * operands, FP32 accumulation); waits for the stream to report a device
  * fault of the stage. */

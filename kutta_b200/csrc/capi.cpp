@@ -757,6 +757,13 @@ int b2_gnn_gradient(b2_gnn* g, const float* d_t, const float* d_e, int tensor_co
   });
 }
 
+int b2_gnn_set_geometry(b2_gnn* g, const float* d_geometry) {
+  return guarded([&] {
+    KB2_REQUIRE(g && g->g, "learned stage: null argument");
+    g->g->set_geometry(d_geometry);
+  });
+}
+
 int b2_gnn_get_weights(const b2_gnn* g, float* host, size_t count) {
   return guarded([&] {
     KB2_REQUIRE(g && g->g && host, "learned stage: null argument");

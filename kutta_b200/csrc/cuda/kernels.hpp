@@ -220,6 +220,20 @@ void tail_cycle(const TailPlan& plan, const int* status, cudaStream_t s);
 // w_ij / sqrt(a_jj) and node scales 1 / sqrt(a_ii) from the matrix values.
 void gnn_graph(int n, const int* rows, const int* cols, const int* diag, const float* vals,
                float* edge, float* lift, float* node_scale, cudaStream_t s);
+// Geometry gate: G_i = sum_j g_ij, rho_ij = log((g_ij / sqrt(G_i G_j)) /
+// w_ij) clamped to [-20, 20] (0 where not positive); then E = w gamma and
+// lift = lift_w gamma with gamma = exp(theta[0] tanh(theta[1] rho)).
+void gnn_geometry(int n, const int* rows, const int* cols, const float* geometry,
+                  const float* edge_w, float* G, float* rho, cudaStream_t s);
+void gnn_gate(int nnz, const float* edge_w, const float* lift_w, const float* rho,
+              const float* theta, float* edge, float* lift, cudaStream_t s);
+// dedge_ij (+)= sum_c dM[i][c] H[j][c] (C <= 32 channels).
+void gnn_edge_grad(int n, int C, const int* rows, const int* cols, const float* dM,
+                   const float* H, float* dedge, bool accumulate, cudaStream_t s);
+// fa = dE/dtheta[0], fb = dE/dtheta[1] per edge; grad[0..1] = dots[0..1].
+void gnn_gate_factors(int nnz, const float* edge, const float* rho, const float* theta,
+                      float* fa, float* fb, cudaStream_t s);
+void gnn_store_gate_grad(const double* dots, float* grad, cudaStream_t s);
 // H0 = node_scale * r; then H0 /= rho, rho = sqrt(sum2[0] / n) (the RMS of
 // H0, reduced on the device in between).
 void gnn_input(int n, const float* r, const float* node_scale, float* H0, cudaStream_t s);

@@ -2,8 +2,10 @@
 // message-passing network over the matrix graph (the cell-face graph of the
 // pressure operator), its backward pass and an Adam step, all in FP32.
 //
-// Graph features come from the matrix alone (the solver sees no geometry):
-// edge weight w_ij = -a_ij / sqrt(a_ii a_jj), node scale s_i = 1 / sqrt(a_ii).
+// Graph features come from the matrix: edge weight w_ij = -a_ij / sqrt(a_ii
+// a_jj), node scale s_i = 1 / sqrt(a_ii); with the faces' geometric
+// coefficients bound as well, each edge weight is gated by a learned function
+// of a geometry feature (k_gnn_gate below).
 // Layer l maps H (n x Cin) to H' (n x 32):
 //   M = W H  (M_i = sum_j w_ij H_j),   H'_i = relu(Ws H_i + Wn M_i + b);
 // the output is z_i = s_i (wo . H3_i). Since w is symmetric, the backward of
@@ -49,6 +51,79 @@ __global__ void k_gnn_graph(int n, const int* __restrict__ rows, const int* __re
       lift[j] = dc > 0.0f ? w * rsqrtf(dc) : 0.0f;
     }
   }
+}
+
+// Geometry edge feature. With g_ij the face's geometric coefficient
+// |A_f| / |c_N - c_P| and G_i = sum_j g_ij, the geometric analogue of w is
+// gh_ij = g_ij / sqrt(G_i G_j); rho_ij = log(gh_ij / w_ij) (clamped to
+// [-20, 20], 0 where either is not positive) compares the face's share of
+// the operator with its share of the geometry: for a diffusion operator, the
+// face's diffusivity relative to its cells'. It is symmetric in (i, j).
+__global__ void k_gnn_geometry_sums(int n, const int* __restrict__ rows,
+                                    const float* __restrict__ geometry, float* __restrict__ G) {
+  ROWS(i, n) {
+    float s = 0.0f;
+    for (int j = rows[i]; j < rows[i + 1]; ++j) s += geometry[j];
+    G[i] = s;
+  }
+}
+__global__ void k_gnn_geometry_rho(int n, const int* __restrict__ rows,
+                                   const int* __restrict__ cols, const float* __restrict__ geometry,
+                                   const float* __restrict__ G, const float* __restrict__ edge_w,
+                                   float* __restrict__ rho) {
+  ROWS(i, n) {
+    for (int j = rows[i]; j < rows[i + 1]; ++j) {
+      const int c = cols[j];
+      const float g = geometry[j], w = edge_w[j];
+      const float gg = G[i] * G[c];
+      float r = 0.0f;
+      if (g > 0.0f && w > 0.0f && gg > 0.0f) r = fminf(fmaxf(logf(g * rsqrtf(gg) / w), -20.0f), 20.0f);
+      rho[j] = r;
+    }
+  }
+}
+// E = w gamma, gamma = exp(theta_a tanh(theta_b rho)), for the edge and the
+// input-lift weights; theta read from the parameters on the device.
+__global__ void k_gnn_gate(int nnz, const float* __restrict__ edge_w,
+                           const float* __restrict__ lift_w, const float* __restrict__ rho,
+                           const float* __restrict__ theta, float* __restrict__ edge,
+                           float* __restrict__ lift) {
+  const float ta = theta[0], tb = theta[1];
+  ROWS(j, nnz) {
+    const float gamma = expf(ta * tanhf(tb * rho[j]));
+    edge[j] = edge_w[j] * gamma;
+    lift[j] = lift_w[j] * gamma;
+  }
+}
+// dL/dE_ij (+)= sum_c dM[i][c] H[j][c], the aggregation M = E H's gradient
+// with respect to each edge weight (one warp per row, lane = channel).
+__global__ void k_gnn_edge_grad(int n, int C, const int* __restrict__ rows,
+                                const int* __restrict__ cols, const float* __restrict__ dM,
+                                const float* __restrict__ H, float* __restrict__ dedge,
+                                int accumulate) {
+  const int lane = threadIdx.x & 31;
+  WARP_ROWS(i, n) {
+    const float d = lane < C ? dM[static_cast<std::size_t>(i) * C + lane] : 0.0f;
+    for (int j = rows[i]; j < rows[i + 1]; ++j) {
+      float v = lane < C ? d * H[static_cast<std::size_t>(cols[j]) * C + lane] : 0.0f;
+      for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+      if (lane == 0) dedge[j] = accumulate ? dedge[j] + v : v;
+    }
+  }
+}
+// dE/dtheta_a = E tanh(theta_b rho), dE/dtheta_b = E theta_a (1 - tanh^2) rho.
+__global__ void k_gnn_gate_factors(int nnz, const float* __restrict__ edge,
+                                   const float* __restrict__ rho, const float* __restrict__ theta,
+                                   float* __restrict__ fa, float* __restrict__ fb) {
+  const float ta = theta[0], tb = theta[1];
+  ROWS(j, nnz) {
+    const float th = tanhf(tb * rho[j]);
+    fa[j] = edge[j] * th;
+    fb[j] = edge[j] * ta * (1.0f - th * th) * rho[j];
+  }
+}
+__global__ void k_gnn_store_gate_grad(const double* __restrict__ dots, float* __restrict__ grad) {
+  if (blockIdx.x == 0 && threadIdx.x < 2) grad[threadIdx.x] = static_cast<float>(dots[threadIdx.x]);
 }
 
 // M = W H (C channels).
@@ -292,6 +367,36 @@ void gnn_graph(int n, const int* rows, const int* cols, const int* diag, const f
   if (n <= 0) return;
   ++counter;
   k_gnn_graph<<<grid_for(n), kBlock, 0, s>>>(n, rows, cols, diag, vals, edge, lift, node_scale);
+}
+void gnn_geometry(int n, const int* rows, const int* cols, const float* geometry,
+                  const float* edge_w, float* G, float* rho, cudaStream_t s) {
+  if (n <= 0) return;
+  counter += 2;
+  k_gnn_geometry_sums<<<grid_for(n), kBlock, 0, s>>>(n, rows, geometry, G);
+  k_gnn_geometry_rho<<<grid_for(n), kBlock, 0, s>>>(n, rows, cols, geometry, G, edge_w, rho);
+}
+void gnn_gate(int nnz, const float* edge_w, const float* lift_w, const float* rho,
+              const float* theta, float* edge, float* lift, cudaStream_t s) {
+  if (nnz <= 0) return;
+  ++counter;
+  k_gnn_gate<<<grid_for(nnz), kBlock, 0, s>>>(nnz, edge_w, lift_w, rho, theta, edge, lift);
+}
+void gnn_edge_grad(int n, int C, const int* rows, const int* cols, const float* dM,
+                   const float* H, float* dedge, bool accumulate, cudaStream_t s) {
+  if (n <= 0) return;
+  ++counter;
+  k_gnn_edge_grad<<<warp_grid(n), kBlock, 0, s>>>(n, C, rows, cols, dM, H, dedge,
+                                                  accumulate ? 1 : 0);
+}
+void gnn_gate_factors(int nnz, const float* edge, const float* rho, const float* theta,
+                      float* fa, float* fb, cudaStream_t s) {
+  if (nnz <= 0) return;
+  ++counter;
+  k_gnn_gate_factors<<<grid_for(nnz), kBlock, 0, s>>>(nnz, edge, rho, theta, fa, fb);
+}
+void gnn_store_gate_grad(const double* dots, float* grad, cudaStream_t s) {
+  ++counter;
+  k_gnn_store_gate_grad<<<1, 32, 0, s>>>(dots, grad);
 }
 void gnn_input(int n, const float* r, const float* node_scale, float* H0, cudaStream_t s) {
   if (n <= 0) return;

@@ -33,6 +33,8 @@ typedef struct {
   int faces;        // interior faces
   double* centroid; // 3n, cell centroids (x, y, z) in the stored order; NULL for poisson
   double* boundary; // n, the Dirichlet boundary term in each diagonal; NULL for poisson
+  double* geometry; // nnz, the face's geometric coefficient |A_f| / |c_N - c_P| per
+                    // off-diagonal entry (0 on the diagonal); NULL for poisson
 } kh_system;
 
 // ---------------------------------------------------------------- random ----
@@ -60,6 +62,7 @@ void kh_free(kh_system* s) {
   if (!s) return;
   free(s->row_ptr); free(s->col); free(s->diag); free(s->val);
   free(s->b); free(s->volume); free(s->new_to_old); free(s->centroid); free(s->boundary);
+  free(s->geometry);
   free(s);
 }
 
@@ -472,10 +475,12 @@ static kh_system* assemble(const kh_mesh* m, int renumber, double dmin, double d
   float* coef_no = (float*)malloc(sizeof(float) * (size_t)(m->faces_int ? m->faces_int : 1));   // off-diag in neighbour row
   float* add_o = (float*)malloc(sizeof(float) * (size_t)(m->faces_int ? m->faces_int : 1));     // diagonal share, owner
   float* add_n = (float*)malloc(sizeof(float) * (size_t)(m->faces_int ? m->faces_int : 1));     // diagonal share, neighbour
+  double* geo = (double*)malloc(sizeof(double) * (size_t)(m->faces_int ? m->faces_int : 1));   // |A_f| / dist
   for (int f = 0; f < m->faces_int; ++f) {
     const int P = m->owner[f], N = m->neighbour[f];
     const double dist = norm3(sub(m->centroid[N], m->centroid[P]));
     const double A = norm3(m->area[f]);
+    geo[f] = A / dist;
     if (convection <= 0) {
       const float a = (float)(0.5 * (D[P] + D[N]) * A / dist);
       coef_on[f] = -a; coef_no[f] = -a; add_o[f] = a; add_n[f] = a;
@@ -523,6 +528,7 @@ static kh_system* assemble(const kh_mesh* m, int renumber, double dmin, double d
   s->volume = (double*)malloc(sizeof(double) * (size_t)n);
   s->centroid = (double*)malloc(sizeof(double) * 3 * (size_t)n);
   s->boundary = (double*)malloc(sizeof(double) * (size_t)n);
+  s->geometry = (double*)malloc(sizeof(double) * (size_t)s->nnz);
   s->new_to_old = new_to_old;
   // faces per old cell
   int* foff = deg;  // reuse adjacency offsets: same counts per cell
@@ -536,7 +542,7 @@ static kh_system* assemble(const kh_mesh* m, int renumber, double dmin, double d
   free(cur);
   int nnz = 0;
   s->row_ptr[0] = 0;
-  typedef struct { int col; float v; } ent;
+  typedef struct { int col; float v; double g; } ent;
   ent* row = (ent*)malloc(sizeof(ent) * 64);
   for (int r = 0; r < n; ++r) {
     const int c = new_to_old[r];
@@ -548,6 +554,7 @@ static kh_system* assemble(const kh_mesh* m, int renumber, double dmin, double d
       const int other = own ? m->neighbour[f] : m->owner[f];
       row[cnt].col = old_to_new[other];
       row[cnt].v = own ? coef_on[f] : coef_no[f];
+      row[cnt].g = geo[f];
       dsum += own ? add_o[f] : add_n[f];
       ++cnt;
     }
@@ -561,13 +568,14 @@ static kh_system* assemble(const kh_mesh* m, int renumber, double dmin, double d
     } else {
       dval = (float)(dsum / 0.7L);
     }
-    row[cnt].col = r; row[cnt].v = dval; ++cnt;
+    row[cnt].col = r; row[cnt].v = dval; row[cnt].g = 0.0; ++cnt;
     for (int a = 1; a < cnt; ++a)
       for (int b2 = a; b2 > 0 && row[b2 - 1].col > row[b2].col; --b2) { ent t = row[b2]; row[b2] = row[b2 - 1]; row[b2 - 1] = t; }
     for (int a = 0; a < cnt; ++a) {
       if (row[a].col == r) s->diag[r] = nnz;
       s->col[nnz] = row[a].col;
       s->val[nnz] = (double)row[a].v;
+      s->geometry[nnz] = row[a].g;
       ++nnz;
     }
     s->row_ptr[r + 1] = nnz;
@@ -579,6 +587,7 @@ static kh_system* assemble(const kh_mesh* m, int renumber, double dmin, double d
     s->b[r] = (float)(normal01(rng) * m->volume[c]);
   }
   free(row); free(fface); free(bnd); free(coef_on); free(coef_no); free(add_o); free(add_n);
+  free(geo);
   free(adj); free(deg); free(old_to_new); free(D);
   return s;
 }

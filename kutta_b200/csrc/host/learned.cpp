@@ -21,7 +21,7 @@ int cin(int layer) { return layer == 0 ? 1 : Gnn::kHidden; }
 }  // namespace
 
 int Gnn::parameter_count() {
-  int count = kHidden;  // wo
+  int count = kHidden + kGate;  // wo, theta
   for (int l = 0; l < kLayers; ++l) count += 2 * kHidden * cin(l) + kHidden;
   return count;
 }
@@ -67,7 +67,7 @@ Gnn::Gnn(std::uint64_t seed) {
   partials_.reset(kReducePartials);
   ticket_.reset(1);
   cuda_check(cudaMemset(ticket_.get(), 0, sizeof(unsigned)), "memset");
-  sums_.reset(4);
+  sums_.reset(6);
   fault_.reset(1);
   cuda_check(cudaMemset(fault_.get(), 0, sizeof(int)), "memset");
 }
@@ -107,10 +107,28 @@ void Gnn::bind(int n, const int* rows, const int* cols, const int* diag, const f
     lift_.reset(static_cast<std::size_t>(nnz));
   }
   n_ = n;
+  nnz_ = nnz;
   rows_ = rows;
   cols_ = cols;
   vals_ = vals;
-  launch::gnn_graph(n, rows, cols, diag, vals, edge_.get(), lift_.get(), scale_.get(), s);
+  gated_ = geometry_ != nullptr;
+  if (!gated_) {
+    launch::gnn_graph(n, rows, cols, diag, vals, edge_.get(), lift_.get(), scale_.get(), s);
+    return;
+  }
+  const auto count = static_cast<std::size_t>(nnz);
+  for (auto* a : {&edge_w_, &lift_w_, &rho_, &dedge_, &gate_fa_, &gate_fb_})
+    if (a->size() != count) a->reset(count);
+  if (node_g_.size() != static_cast<std::size_t>(n)) node_g_.reset(static_cast<std::size_t>(n));
+  launch::gnn_graph(n, rows, cols, diag, vals, edge_w_.get(), lift_w_.get(), scale_.get(), s);
+  launch::gnn_geometry(n, rows, cols, geometry_, edge_w_.get(), node_g_.get(), rho_.get(), s);
+  regate(s);
+}
+
+void Gnn::regate(cudaStream_t s) {
+  if (!gated_) return;
+  launch::gnn_gate(nnz_, edge_w_.get(), lift_w_.get(), rho_.get(),
+                   params_.get() + base_parameter_count(), edge_.get(), lift_.get(), s);
 }
 
 void Gnn::forward(const float* r, float* z, float beta, cudaStream_t s) {
@@ -187,11 +205,25 @@ void Gnn::backward(const float* t, const float* e, bool tensor_cores, cudaStream
                              dh_.get(), p.ws[l], p.wn[l], dhs_.get(), dm_.get(), g.ws[l],
                              g.wn[l], g.b[l], s);
     }
+    if (gated_)  // dL/dE from this layer's aggregation M = E h[l]
+      launch::gnn_edge_grad(n_, cin(l), rows_, cols_, dm_.get(), h_[l].get(), dedge_.get(),
+                            l != kLayers - 1, s);
     if (l > 0) {
       // dL/dh[l] = Ws^T G + W^T (Wn^T G); W is symmetric.
       launch::gnn_aggregate(n_, cin(l), rows_, cols_, edge_.get(), dm_.get(), dagg_.get(), s);
       launch::gnn_add(static_cast<std::size_t>(n_) * cin(l), dhs_.get(), dagg_.get(), dh_.get(), s);
     }
+  }
+  if (gated_) {
+    // dL/dtheta = sum over edges of dL/dE dE/dtheta (FP64 dots).
+    const float* theta = params_.get() + base_parameter_count();
+    launch::gnn_gate_factors(nnz_, edge_.get(), rho_.get(), theta, gate_fa_.get(),
+                             gate_fb_.get(), s);
+    launch::reduce_value(ReduceMode::Dot, nnz_, dedge_.get(), gate_fa_.get(), red, sums_.get(), 4,
+                         s);
+    launch::reduce_value(ReduceMode::Dot, nnz_, dedge_.get(), gate_fb_.get(), red, sums_.get(), 5,
+                         s);
+    launch::gnn_store_gate_grad(sums_.get() + 4, grads_.get() + base_parameter_count(), s);
   }
 }
 
@@ -203,6 +235,7 @@ float Gnn::train_step(const float* t, const float* e, float lr, cudaStream_t s) 
   launch::gnn_adam(count, params_.get(), grads_.get(), m_.get(), v_.get(), lr, beta1, beta2, 1e-8f,
                    1.0f - std::pow(beta1, static_cast<float>(step_)),
                    1.0f - std::pow(beta2, static_cast<float>(step_)), s);
+  regate(s);  // the gate's theta moved
   float loss = 0;
   cuda_check(cudaMemcpyAsync(&loss, loss_.get(), sizeof(float), cudaMemcpyDeviceToHost, s),
              "loss readback");
@@ -233,13 +266,20 @@ std::vector<float> Gnn::weights() const {
 }
 
 void Gnn::set_weights(const std::vector<float>& w) {
-  KB2_REQUIRE(w.size() == static_cast<std::size_t>(parameter_count()),
+  const auto count = static_cast<std::size_t>(parameter_count());
+  KB2_REQUIRE(w.size() == count || w.size() == static_cast<std::size_t>(base_parameter_count()),
               "learned stage: wrong number of weights");
-  cuda_check(cudaMemcpy(params_.get(), w.data(), sizeof(float) * w.size(), cudaMemcpyHostToDevice),
+  std::vector<float> all(w);
+  all.resize(count, 0.0f);  // weights without the gate: theta = 0
+  cuda_check(cudaMemcpy(params_.get(), all.data(), sizeof(float) * count, cudaMemcpyHostToDevice),
              "weights");
   step_ = 0;
-  cuda_check(cudaMemset(m_.get(), 0, sizeof(float) * w.size()), "memset");
-  cuda_check(cudaMemset(v_.get(), 0, sizeof(float) * w.size()), "memset");
+  cuda_check(cudaMemset(m_.get(), 0, sizeof(float) * count), "memset");
+  cuda_check(cudaMemset(v_.get(), 0, sizeof(float) * count), "memset");
+  if (n_ > 0) {
+    regate(nullptr);
+    cuda_check(cudaStreamSynchronize(nullptr), "regate");
+  }
 }
 
 }  // namespace kb2

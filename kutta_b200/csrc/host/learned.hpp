@@ -20,10 +20,22 @@ class Gnn {
  public:
   static constexpr int kHidden = 32;
   static constexpr int kLayers = 3;
+  static constexpr int kGate = 2;  // the geometry gate's theta (last parameters)
   explicit Gnn(std::uint64_t seed);
   // Parameters: per layer Ws [32][Cin], Wn [32][Cin], b [32] (Cin = 1, 32,
-  // 32), then wo [32].
+  // 32), then wo [32], then the geometry gate's theta [2] (initially 0: no
+  // gating).
   static int parameter_count();
+  // The count without the gate (weights saved before it existed; loading
+  // them leaves theta at 0).
+  static int base_parameter_count() { return parameter_count() - kGate; }
+  // Per-entry geometric coefficients of the matrices bound from now on (a
+  // device array over the bound CSR pattern: |A_f| / |c_N - c_P| per
+  // off-diagonal entry, 0 on the diagonal), or null for none. With them each
+  // edge weight is gated, E_ij = w_ij exp(theta_0 tanh(theta_1 rho_ij)),
+  // rho_ij = log((g_ij / sqrt(G_i G_j)) / w_ij), G_i = sum_j g_ij; takes effect
+  // at the next bind; the array must stay valid while bound.
+  void set_geometry(const float* geometry) { geometry_ = geometry; }
   // Binds the matrix graph (device CSR of the fine level): edge weights and
   // node scales from the values, activation buffers for n rows. The pattern
   // arrays must stay valid while bound; call again after values change.
@@ -72,6 +84,12 @@ class Gnn {
   const int* rows_ = nullptr;
   const int* cols_ = nullptr;
   const float* vals_ = nullptr;
+  const float* geometry_ = nullptr;   // set for the next bind
+  bool gated_ = false;                // the bound graph carries the geometry gate
+  int nnz_ = 0;
+  DArray<float> edge_w_, lift_w_, rho_, node_g_, dedge_, gate_fa_, gate_fb_;
+  // E and lift from the ungated weights and the current theta.
+  void regate(cudaStream_t s);
   DArray<double> partials_;
   DArray<unsigned> ticket_;
   DArray<double> sums_;  // [0] input sum of squares; [1..3] energy-loss dots

@@ -29,6 +29,7 @@ class _KhSystem(ctypes.Structure):
         ("b", ctypes.POINTER(ctypes.c_float)), ("volume", ctypes.POINTER(ctypes.c_double)),
         ("new_to_old", ctypes.POINTER(ctypes.c_int)), ("faces", ctypes.c_int),
         ("centroid", ctypes.POINTER(ctypes.c_double)), ("boundary", ctypes.POINTER(ctypes.c_double)),
+        ("geometry", ctypes.POINTER(ctypes.c_double)),
     ]
 
 
@@ -71,6 +72,7 @@ class HostSystem:
     name: str = ""
     centroid: np.ndarray | None = None   # float64[n, 3] (box meshes)
     boundary: np.ndarray | None = None   # float64[n], Dirichlet term in each diagonal
+    geometry: np.ndarray | None = None   # float64[nnz], |A_f| / |c_N - c_P| per off-diagonal
 
     @property
     def n(self) -> int:
@@ -103,6 +105,8 @@ def _take(ptr) -> HostSystem:
     if s.centroid:
         out.centroid = arr(s.centroid, 3 * n, np.float64).reshape(n, 3)
         out.boundary = arr(s.boundary, n, np.float64)
+    if s.geometry:
+        out.geometry = arr(s.geometry, nnz, np.float64)
     _load().kh_free(ptr)
     return out
 

@@ -203,6 +203,7 @@ _SIGNATURES = {
     "b2_gnn_train_step": (_I, [_P, _P, _P, ctypes.c_float, _P, _P]),
     "b2_gnn_set_wait_limit": (_I, [_P, ctypes.c_longlong]),
     "b2_gnn_gradient": (_I, [_P, _P, _P, _I, _P, ctypes.c_size_t, _P, _P]),
+    "b2_gnn_set_geometry": (_I, [_P, _P]),
     "b2_gnn_get_weights": (_I, [_P, _P, ctypes.c_size_t]),
     "b2_gnn_set_weights": (_I, [_P, _P, ctypes.c_size_t]),
     "b2_mixed_set_learned": (_I, [_P, _P, _I]),
@@ -658,6 +659,13 @@ class LearnedStage:
         self._bound = a
         _check(_load().b2_gnn_bind(self._handle, a.n_rows, _tptr(a.row_ptr), _tptr(a.col),
                                    _tptr(a.diag), _tptr(a.val), _stream()))
+
+    def set_geometry(self, geometry) -> None:
+        """b2_gnn_set_geometry: per-entry geometric face coefficients (a CUDA
+        float32 tensor over the bound pattern, 0 on the diagonal) for the
+        matrices bound from now on, or None. The tensor is kept alive here."""
+        self._geometry = geometry
+        _check(_load().b2_gnn_set_geometry(self._handle, _tptr(geometry)))
 
     def apply(self, r, z, beta: float = 0.0) -> None:
         _check(_load().b2_gnn_apply(self._handle, _tptr(r), _tptr(z), beta, _stream()))

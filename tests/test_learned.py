@@ -400,3 +400,99 @@ def test_stalled_refinement_falls_back_to_the_amg_cycle(cuda):
     st = solver.solve(a, x, b, L.SolveControl(1e-8, 1e-30, 3000))
     assert st.converged and not st.learned_fallback
     solver.set_learned(None)
+
+
+def _gate_inputs(s):
+    """Per entry: the ungated edge weight w, the geometry feature rho and the
+    device geometry array (float32), as the stage computes them at bind."""
+    import torch
+    n = s.n
+    rows = np.repeat(np.arange(n), np.diff(s.row_ptr))
+    vals = s.val.astype(np.float32)
+    d = vals[s.diag]
+    off = rows != s.col
+    w = np.zeros_like(vals)
+    w[off] = -vals[off] / np.sqrt(d[rows[off]] * d[s.col[off]])
+    g = s.geometry.astype(np.float32)
+    G = np.add.reduceat(g.astype(np.float64), s.row_ptr[:-1]).astype(np.float32)
+    gh = np.zeros_like(g)
+    ok = off & (g > 0) & (w > 0)
+    gh[ok] = g[ok] / np.sqrt(G[rows[ok]] * G[s.col[ok]])
+    rho = np.zeros_like(g)
+    rho[ok] = np.clip(np.log(gh[ok] / w[ok]), -20, 20)
+    return rows, w, rho, torch.from_numpy(g).cuda()
+
+
+def _torch_network_gated(s):
+    """The network with the geometry gate E = w exp(theta_0 tanh(theta_1 rho))
+    (the last two parameters), in PyTorch FP32, differentiable in theta."""
+    import torch
+    rows, w, rho, _ = _gate_inputs(s)
+    idx = torch.from_numpy(np.vstack([rows, s.col])).cuda()
+    w_t, rho_t = torch.from_numpy(w).cuda(), torch.from_numpy(rho).cuda()
+    _, scale, _ = _torch_operators(s)
+
+    def f(p, r):
+        layers, wo = _layers(p)
+        gamma = torch.exp(p[-2] * torch.tanh(p[-1] * rho_t))
+        W = torch.sparse_coo_tensor(idx, w_t * gamma, (s.n, s.n))
+        h0 = scale * r
+        rms = torch.sqrt((h0.double() ** 2).mean()).float()
+        h = (h0 / rms)[:, None]
+        for ws, wn, b in layers:
+            m = torch.sparse.mm(W, h)
+            h = torch.relu(h @ ws.T + m @ wn.T + b)
+        return rms * scale * (h @ wo)
+    return f
+
+
+@pytest.mark.gpu
+def test_geometry_gate_is_off_at_zero_theta(cuda):
+    """With theta = 0 the gate is exactly 1: binding the geometry changes no
+    bit of the forward."""
+    import torch
+    s, a, g, r = _setup(seed=5, n_side=9)
+    want = torch.zeros(s.n, device="cuda")
+    g.apply(r, want)
+    _, _, _, geometry = _gate_inputs(s)
+    g.set_geometry(geometry)
+    g.bind(a)
+    z = torch.zeros(s.n, device="cuda")
+    g.apply(r, z)
+    torch.cuda.synchronize()
+    assert torch.equal(z, want)
+
+
+@pytest.mark.gpu
+def test_geometry_gate_forward_and_gradient_match_torch(cuda):
+    """theta = (0.4, 0.3): the tensor-core forward against PyTorch FP32 (3e-2,
+    BF16 operands), and the FP32 backward's gradient, theta included, against
+    autograd (1e-3)."""
+    import torch
+    s, a, g, r = _setup(seed=6, n_side=10)
+    _, _, _, geometry = _gate_inputs(s)
+    g.set_geometry(geometry)
+    w = g.weights()
+    w[-2:] = (0.4, 0.3)
+    g.set_weights(w)
+    g.bind(a)
+    f = _torch_network_gated(s)
+    z = torch.zeros(s.n, device="cuda")
+    g.apply(r, z)
+    want = f(torch.from_numpy(w).cuda(), r)
+    assert _rel(z, want) < 3e-2
+    solver = L.make_mixed_solver(s)
+    solver.refresh(a)
+    t, e, *_ = _pair(s, a, solver)
+    wt = torch.from_numpy(w).cuda().requires_grad_(True)
+    loss_t = _energy_loss(s, f, wt, t, e)
+    loss_t.backward()
+    auto = wt.grad.cpu().numpy().astype(np.float64)
+    fp, loss_fp = g.gradient(t, e, tensor_cores=False)
+    assert loss_fp == pytest.approx(float(loss_t), rel=1e-3, abs=1e-5)
+    scale = np.linalg.norm(auto)
+    for name, sl in _parameter_blocks() + [("theta", slice(-2, None))]:
+        ref = auto[sl]
+        denom = max(np.linalg.norm(ref), 1e-3 * scale)
+        assert np.linalg.norm(fp[sl] - ref) / denom < 1e-3, name
+    assert np.abs(auto[-2:]).max() > 0
