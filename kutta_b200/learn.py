@@ -87,16 +87,28 @@ def pairs(s: harness.HostSystem, a: L.CsrMatrix, mixed: L.MixedSolver, b, x):
     return out
 
 
-def training_set(count: int, n_side: int, rhs_per_system: int, seed0: int):
-    """[(device matrix, t, e)] from `count` systems x `rhs_per_system` solves of
-    the plain FP32 AMG-PCG (the reference's method; to relative 1e-6 or its
-    FP32 floor, whichever it reaches)."""
+def geometry(s: harness.HostSystem):
+    """The system's per-entry geometric face coefficients as a CUDA float32
+    tensor (the learned stage's geometry gate input), or None."""
+    import torch
+    if s.geometry is None:
+        return None
+    return torch.from_numpy(s.geometry.astype(np.float32)).cuda()
+
+
+def training_set(count: int, n_side: int, rhs_per_system: int, seed0: int,
+                 with_geometry: bool = True):
+    """[(device matrix, geometry, t, e)] from `count` systems x
+    `rhs_per_system` solves of the plain FP32 AMG-PCG (the reference's method;
+    to relative 1e-6 or its FP32 floor, whichever it reaches); geometry is
+    None unless with_geometry."""
     import torch
     rng = np.random.default_rng(seed0)
     data = []
     for k in range(count):
         s = system(n_side, seed0 + k)
         a = L.upload(s)
+        geo = geometry(s) if with_geometry else None
         plain = L.make_solver(L.SolverKind.AmgPcg, s, L.SolverOptions(
             structure=L.OperatorStructure.SymmetricMMatrix))
         plain.refresh(a)
@@ -106,7 +118,7 @@ def training_set(count: int, n_side: int, rhs_per_system: int, seed0: int):
             b = torch.from_numpy(fourier_rhs(s, rng)).cuda()
             x = torch.zeros(s.n, dtype=torch.float32, device="cuda")
             plain.solve(a, x, b, L.SolveControl(1e-6, 1e-30, 3000))
-            data.extend((a, t, e) for t, e in pairs(s, a, mixed, b, x.double()))
+            data.extend((a, geo, t, e) for t, e in pairs(s, a, mixed, b, x.double()))
         del plain, mixed
     return data
 
@@ -118,8 +130,9 @@ def train(stage: L.LearnedStage, data, steps: int, learning_rate: float, seed: i
     bound = None
     losses = []
     for step in range(steps):
-        a, t, e = data[order[step]]
+        a, geo, t, e = data[order[step]]
         if bound is not a:
+            stage.set_geometry(geo)
             stage.bind(a)
             bound = a
         # Cosine decay to a tenth of the rate.
@@ -136,8 +149,9 @@ def held_out_loss(stage: L.LearnedStage, data) -> float:
     negligible rate on a copy of the weights (the weights are restored)."""
     w = stage.weights()
     bound, losses = None, []
-    for a, t, e in data:
+    for a, geo, t, e in data:
         if bound is not a:
+            stage.set_geometry(geo)
             stage.bind(a)
             bound = a
         losses.append(stage.train_step(t, e, learning_rate=1e-30))
@@ -145,7 +159,8 @@ def held_out_loss(stage: L.LearnedStage, data) -> float:
     return float(np.mean(losses))
 
 
-def evaluate(stage: L.LearnedStage | None, n_side: int, seeds, rel_tol: float = 1e-6) -> dict:
+def evaluate(stage: L.LearnedStage | None, n_side: int, seeds, rel_tol: float = 1e-6,
+             with_geometry: bool = True) -> dict:
     """Mixed solve with and without the stage, and the plain FP32 AMG-PCG."""
     import torch
     rng = np.random.default_rng(12345)
@@ -153,6 +168,7 @@ def evaluate(stage: L.LearnedStage | None, n_side: int, seeds, rel_tol: float = 
     for seed in seeds:
         s = system(n_side, seed)
         a = L.upload(s)
+        geo = geometry(s) if with_geometry else None
         b = torch.from_numpy(fourier_rhs(s, rng)).cuda()
         row = {"seed": seed, "n": s.n}
         arms = [("mixed", None), ("plain", None)]
@@ -168,6 +184,7 @@ def evaluate(stage: L.LearnedStage | None, n_side: int, seeds, rel_tol: float = 
                 x = torch.zeros(s.n, dtype=torch.float64, device="cuda")
             solver.refresh(a)
             if g is not None:
+                g.set_geometry(geo)
                 solver.set_learned(g, L.LEARNED_CYCLE)
             best, st = None, None
             for _ in range(3):
@@ -189,8 +206,16 @@ def evaluate(stage: L.LearnedStage | None, n_side: int, seeds, rel_tol: float = 
                 plain.refresh(a)
                 x_plain = torch.zeros(s.n, dtype=torch.float32, device="cuda")
                 plain.solve(a, x_plain, b, L.SolveControl(1e-6, 1e-30, 3000))
-                row["held_out_energy_loss"] = held_out_loss(
-                    g, [(a, t, e) for t, e in pairs(s, a, solver, b, x_plain.double())])
+                held_out = [(a, geo, t, e) for t, e in pairs(s, a, solver, b, x_plain.double())]
+                row["held_out_energy_loss"] = held_out_loss(g, held_out)
+                if geo is not None:
+                    # The same weights with the gate off (theta = 0).
+                    w = g.weights()
+                    off = w.copy()
+                    off[-2:] = 0.0
+                    g.set_weights(off)
+                    row["held_out_energy_loss_gate_off"] = held_out_loss(g, held_out)
+                    g.set_weights(w)
             del solver
         results.append(row)
     return {"rel_tol": rel_tol, "mesh": f"{n_side}^3 jittered hex, smooth log-normal D_f "
@@ -245,6 +270,9 @@ def main():
     ap.add_argument("--seed", type=int, default=1000)
     ap.add_argument("--eval-n", type=int, default=128)
     ap.add_argument("--eval-seeds", type=int, default=2)
+    ap.add_argument("--no-geometry", action="store_true",
+                    help="train without the geometry gate (theta stays 0)")
+    ap.add_argument("--init", help="start from these weights (.npy) instead of random ones")
     args = ap.parse_args()
     if args.time_forward:
         print(json.dumps(time_forward(args.time_forward)))
@@ -252,16 +280,20 @@ def main():
     if not args.out:
         ap.error("--out is required for training")
     t0 = time.time()
-    data = training_set(args.systems, args.n, args.rhs, args.seed)
+    data = training_set(args.systems, args.n, args.rhs, args.seed,
+                        with_geometry=not args.no_geometry)
     t1 = time.time()
     stage = L.LearnedStage(seed=args.seed)
+    if args.init:
+        stage.set_weights(np.load(args.init))
     losses = train(stage, data, args.steps, args.lr)
     t2 = time.time()
     np.save(args.out, stage.weights())
     report = {"pairs": len(data), "solutions": len(data) // 2, "data_s": t1 - t0, "train_s": t2 - t1,
               "loss_first": float(np.mean(losses[:50])), "loss_last": float(np.mean(losses[-50:])),
               "evaluation": evaluate(stage, args.eval_n,
-                                     [args.seed + 10_000 + k for k in range(args.eval_seeds)])}
+                                     [args.seed + 10_000 + k for k in range(args.eval_seeds)],
+                                     with_geometry=not args.no_geometry)}
     print(json.dumps(report))
     pathlib.Path(args.out).with_suffix(".json").write_text(json.dumps(report, indent=1))
 
