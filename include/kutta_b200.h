@@ -290,7 +290,7 @@ int b2_mixed_hierarchy_build(int n, int nnz, const int32_t* row_ptr, const int32
 typedef struct b2_gnn b2_gnn;
 /* A stage with weights drawn from `seed`; b2_gnn_set_weights loads trained
  * ones (b2_gnn_parameter_count floats; the count without the geometry gate's
- * two parameters is accepted too, leaving the gate off). */
+ * two parameters is accepted too, giving theta = (0, 0.25): a gate of 1). */
 int b2_gnn_create(uint64_t seed, b2_gnn** out);
 void b2_gnn_destroy(b2_gnn* g);
 int b2_gnn_parameter_count(void);

@@ -4,6 +4,7 @@
 
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <chrono>
 #include <cstdlib>
 #include <string>
@@ -65,6 +66,52 @@ class DArray {
   }
   T* p_ = nullptr;
   std::size_t n_ = 0;
+};
+
+// A stream-ordered device array: cudaMallocAsync on its stream, released with
+// cudaFreeAsync on the same stream, so the release waits for that stream's
+// queued work without synchronising the device, and the memory pool makes
+// repeated allocations cheap. For scratch whose every use is on one stream.
+template <class T>
+class SArray {
+ public:
+  SArray() = default;
+  SArray(std::size_t n, cudaStream_t s) { reset(n, s); }
+  SArray(const SArray&) = delete;
+  SArray& operator=(const SArray&) = delete;
+  SArray(SArray&& o) noexcept
+      : p_(std::exchange(o.p_, nullptr)), n_(std::exchange(o.n_, 0)), s_(o.s_) {}
+  SArray& operator=(SArray&& o) noexcept {
+    if (this != &o) {
+      release();
+      p_ = std::exchange(o.p_, nullptr);
+      n_ = std::exchange(o.n_, 0);
+      s_ = o.s_;
+    }
+    return *this;
+  }
+  ~SArray() { release(); }
+  void reset(std::size_t n, cudaStream_t s) {
+    release();
+    n_ = n;
+    s_ = s;
+    void* p = nullptr;
+    cuda_check(cudaMallocAsync(&p, std::max<std::size_t>(n, 1) * sizeof(T), s), "cudaMallocAsync");
+    p_ = static_cast<T*>(p);
+  }
+  T* get() const { return p_; }
+  std::size_t size() const { return n_; }
+  bool allocated() const { return p_ != nullptr; }
+
+ private:
+  void release() {
+    if (p_) cudaFreeAsync(p_, s_);
+    p_ = nullptr;
+    n_ = 0;
+  }
+  T* p_ = nullptr;
+  std::size_t n_ = 0;
+  cudaStream_t s_ = nullptr;
 };
 
 template <class T>

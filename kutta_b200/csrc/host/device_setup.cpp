@@ -33,6 +33,12 @@ void zero(DArray<int>& a, std::size_t n, cudaStream_t s) {
   if (a.size() < n || !a.allocated()) a.reset(n);
   cuda_check(cudaMemsetAsync(a.get(), 0, sizeof(int) * std::max<std::size_t>(n, 1), s), "memset");
 }
+// The builder's scratch is stream-ordered (SArray): freeing it neither
+// synchronises the device nor pays cudaMalloc's cost again on the next pass.
+void zero(SArray<int>& a, std::size_t n, cudaStream_t s) {
+  if (a.size() < n || !a.allocated()) a.reset(n, s);
+  cuda_check(cudaMemsetAsync(a.get(), 0, sizeof(int) * std::max<std::size_t>(n, 1), s), "memset");
+}
 
 // A device CSR operator of the setup (a level, or an intermediate operator).
 struct Operator {
@@ -58,7 +64,7 @@ class Builder {
   // out[0..n] = exclusive scan of in[0..n); returns the total.
   int scan(int n, const int* in, int* out) {
     const auto need = static_cast<std::size_t>(launch::scan_scratch(n));
-    if (blocks_.size() < need) blocks_.reset(need);
+    if (blocks_.size() < need) blocks_.reset(need, s_);
     launch::exclusive_scan(n, in, out, blocks_.get(), s_);
     return read_int(out + n, s_);
   }
@@ -68,17 +74,18 @@ class Builder {
   int pair(const Operator& a, bool exclude_isolated, DArray<int>& map) {
     const int n = a.n;
     const auto rows = static_cast<std::size_t>(n);
-    DArray<int> count(rows + 1), offsets(rows + 1), state(rows), next(rows), owner(rows);
+    SArray<int> count(rows + 1, s_), offsets(rows + 1, s_), state(rows, s_), next(rows, s_),
+        owner(rows, s_);
     launch::pair_count(n, a.rows, a.cols, a.vals, o_.strength_threshold, exclude_isolated ? 1 : 0,
                        count.get(), state.get(), s_);
     const int total = scan(n, count.get(), offsets.get());
-    DArray<unsigned long long> keys(static_cast<std::size_t>(total));
-    DArray<int> pref(static_cast<std::size_t>(total));
+    SArray<unsigned long long> keys(static_cast<std::size_t>(total), s_);
+    SArray<int> pref(static_cast<std::size_t>(total), s_);
     launch::pair_fill(n, a.rows, a.cols, a.vals, o_.strength_threshold, offsets.get(), keys.get(),
                       pref.get(), s_);
     int* cur = state.get();
     int* nxt = next.get();
-    DArray<int> changed(kSweepBatch);
+    SArray<int> changed(kSweepBatch, s_);
     for (int sweeps = 0;; sweeps += kSweepBatch) {
       KB2_REQUIRE(sweeps < sweep_limit(n), "device aggregation: pairing did not settle");
       cuda_check(cudaMemsetAsync(changed.get(), 0, sizeof(int) * kSweepBatch, s_), "memset");
@@ -94,7 +101,7 @@ class Builder {
       // of the batch left it (and the claims computed from it) as they were.
       if (std::find(flags, flags + kSweepBatch, 0) != flags + kSweepBatch) break;
     }
-    DArray<int> leader(rows + 1), id(rows + 1);
+    SArray<int> leader(rows + 1, s_), id(rows + 1, s_);
     launch::pair_leaders(n, cur, leader.get(), s_);
     const int nc = scan(n, leader.get(), id.get());
     map.reset(rows);
@@ -107,16 +114,16 @@ class Builder {
   int absorb(const Operator& a, int nc, DArray<int>& map) {
     const int n = a.n;
     const auto rows = static_cast<std::size_t>(n);
-    DArray<int> size0;
+    SArray<int> size0;
     zero(size0, static_cast<std::size_t>(nc), s_);
     launch::aggregate_sizes(n, map.get(), size0.get(), s_);
-    DArray<int> first(rows), second(rows);
+    SArray<int> first(rows, s_), second(rows, s_);
     cuda_check(cudaMemcpyAsync(first.get(), map.get(), sizeof(int) * rows, cudaMemcpyDeviceToDevice,
                                s_),
                "copy");
     int* cur = first.get();
     int* nxt = second.get();
-    DArray<int> changed(kSweepBatch);
+    SArray<int> changed(kSweepBatch, s_);
     for (int sweeps = 0;; sweeps += kSweepBatch) {
       KB2_REQUIRE(sweeps < sweep_limit(n), "device aggregation: absorption did not settle");
       cuda_check(cudaMemsetAsync(changed.get(), 0, sizeof(int) * kSweepBatch, s_), "memset");
@@ -132,7 +139,7 @@ class Builder {
       wait(s_);
       if (std::find(flags, flags + kSweepBatch, 0) != flags + kSweepBatch) break;
     }
-    DArray<int> used, renumber(static_cast<std::size_t>(nc) + 1);
+    SArray<int> used, renumber(static_cast<std::size_t>(nc) + 1, s_);
     zero(used, static_cast<std::size_t>(nc) + 1, s_);
     launch::mark_used(n, cur, used.get(), s_);
     const int kept = scan(nc, used.get(), renumber.get());
@@ -147,21 +154,21 @@ class Builder {
   void coarsen(const Operator& fine, const int* aggregate, int nc, Coarse& c) {
     const auto count = static_cast<std::size_t>(nc);
     c.n = nc;
-    DArray<int> size, triples;
+    SArray<int> size, triples;
     zero(size, count + 1, s_);
     zero(triples, count + 1, s_);
     launch::coarsen_count(fine.n, fine.rows, fine.cols, aggregate, size.get(), triples.get(), s_);
     c.member_offsets.reset(count + 1);
     c.active = scan(nc, size.get(), c.member_offsets.get());
-    DArray<int> triple_offsets(count + 1);
+    SArray<int> triple_offsets(count + 1, s_);
     const int total = scan(nc, triples.get(), triple_offsets.get());
     c.members.reset(static_cast<std::size_t>(c.active));
     zero(size, count + 1, s_);  // placement cursors
     launch::place_members(fine.n, aggregate, c.member_offsets.get(), size.get(), c.members.get(),
                           s_);
     launch::sort_members(nc, c.member_offsets.get(), c.members.get(), s_);
-    DArray<int4> sorted(static_cast<std::size_t>(total));
-    DArray<int> unique(count + 1);
+    SArray<int4> sorted(static_cast<std::size_t>(total), s_);
+    SArray<int> unique(count + 1, s_);
     launch::coarsen_triples(nc, fine.rows, fine.cols, aggregate, c.member_offsets.get(),
                             c.members.get(), triple_offsets.get(), o_.m_matrix ? 1 : 0,
                             sorted.get(), unique.get(), s_);
@@ -181,11 +188,10 @@ class Builder {
     c.val.reset(nnz);
     launch::galerkin(c.nnz, c.entry_offsets.get(), c.entries.get(), fine.vals, c.val.get(), s_);
     if (o_.m_matrix) {
-      DArray<float> surplus(static_cast<std::size_t>(fine.n));
+      SArray<float> surplus(static_cast<std::size_t>(fine.n), s_);
       launch::m_matrix_diagonal(fine.n, nc, c.member_offsets.get(), c.members.get(), fine.rows,
                                 fine.diag, fine.vals, c.row_ptr.get(), c.diag.get(), c.val.get(),
                                 surplus.get(), s_);
-      wait(s_);  // the scratch is freed on return
     }
     wait(s_);  // total_host_ is read by the copy above
   }
@@ -210,7 +216,7 @@ class Builder {
  private:
   const Options& o_;
   cudaStream_t s_;
-  DArray<int> blocks_;
+  SArray<int> blocks_;
   DArray<int> out_map_;
   int total_host_ = 0;
 };

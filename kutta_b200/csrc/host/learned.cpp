@@ -57,6 +57,8 @@ Gnn::Gnn(std::uint64_t seed) {
     k += kHidden;  // biases stay 0
   }
   for (int c = 0; c < kHidden; ++c) w[k++] = static_cast<float>((2.0 * uniform(state) - 1.0) * 0.1);
+  w[k++] = 0.0f;               // theta_0: the gate starts at exactly 1
+  w[k++] = kGateSlope;         // theta_1: nonzero, so theta_0's gradient is not 0
   params_.upload(w, nullptr);
   grads_.reset(static_cast<std::size_t>(count));
   m_.reset(static_cast<std::size_t>(count));
@@ -270,7 +272,10 @@ void Gnn::set_weights(const std::vector<float>& w) {
   KB2_REQUIRE(w.size() == count || w.size() == static_cast<std::size_t>(base_parameter_count()),
               "learned stage: wrong number of weights");
   std::vector<float> all(w);
-  all.resize(count, 0.0f);  // weights without the gate: theta = 0
+  if (all.size() < count) {  // weights without the gate: gate exactly 1, as at creation
+    all.resize(count, 0.0f);
+    all[count - 1] = kGateSlope;
+  }
   cuda_check(cudaMemcpy(params_.get(), all.data(), sizeof(float) * count, cudaMemcpyHostToDevice),
              "weights");
   step_ = 0;

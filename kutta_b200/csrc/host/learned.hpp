@@ -21,10 +21,15 @@ class Gnn {
   static constexpr int kHidden = 32;
   static constexpr int kLayers = 3;
   static constexpr int kGate = 2;  // the geometry gate's theta (last parameters)
+  // theta_1 at creation. At theta = (0, 0) both gate gradients vanish (a
+  // saddle: dE/dtheta_0 carries tanh(theta_1 rho), dE/dtheta_1 carries
+  // theta_0), so theta_1 starts nonzero; the gate is exactly 1 while theta_0
+  // is 0.
+  static constexpr float kGateSlope = 0.25f;
   explicit Gnn(std::uint64_t seed);
   // Parameters: per layer Ws [32][Cin], Wn [32][Cin], b [32] (Cin = 1, 32,
-  // 32), then wo [32], then the geometry gate's theta [2] (initially 0: no
-  // gating).
+  // 32), then wo [32], then the geometry gate's theta [2] (initially
+  // (0, kGateSlope): a gate of exactly 1).
   static int parameter_count();
   // The count without the gate (weights saved before it existed; loading
   // them leaves theta at 0).
