@@ -197,7 +197,6 @@ def run_ours(args, rank, world, local):
     b = torch.from_numpy(s.b).to(dev)
     from kutta_b200 import learn
     stage = learn.trained_stage()
-    stage.set_geometry(learn.geometry(s) if getattr(s, "geometry", None) is not None else None)
 
     # ---- learned+mixed: the metric's method, the measured value ----
     # The mixed-precision solve with the trained learned stage as its warm
@@ -383,7 +382,6 @@ def other_configs(args):
         a = L.upload(s)
         control = L.SolveControl(rel_tol, 1e-30, args.max_iter)
         row = {"rows": s.n, "nnz": s.nnz, "rel_tol": rel_tol}
-        stage.set_geometry(learn.geometry(s))
         mixed = L.make_mixed_solver(s)
         x64 = torch.zeros(s.n, dtype=torch.float64, device="cuda")
         for name, mode in (("mixed", 0), ("learned+mixed", L.LEARNED_WARM_START),
@@ -641,7 +639,6 @@ def run_sequence(args):
     control = L.SolveControl(args.rel_tol, 1e-30, args.max_iter)
     from kutta_b200 import learn
     stage = learn.trained_stage()
-    stage.set_geometry(learn.geometry(s))
     arms = {"mixed": L.make_mixed_solver(s), "learned+mixed": L.make_mixed_solver(s),
             "plain": L.make_solver(L.SolverKind.AmgPcg, s, L.SolverOptions(
                 structure=L.OperatorStructure.SymmetricMMatrix))}
