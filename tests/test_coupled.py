@@ -418,3 +418,42 @@ def test_one_block_tail_changes_no_bits(cuda, name, monkeypatch):
     assert (a1.iterations, a1.final_residual) == (b1.iterations, b1.final_residual)
     assert (a2.iterations, a2.final_residual) == (b2.iterations, b2.final_residual)
     assert np.array_equal(bits(ax), bits(bx))
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("tet,dims,kinds,reference", [
+    (False, (32, 32, 32), (1, 2, 0, 0, 3, 3), -1),
+    (True, (16, 14, 12), (1, 4, 0, 3, 0, 0), -1),
+    (False, (24, 20, 16), (0, 0, 0, 0, 0, 0), 7),
+], ids=["hex32_open", "tet16x14x12_open", "hex24x20x16_closed"])
+def test_coupled_matches_reference_at_scale(cuda, tet, dims, kinds, reference):
+    """Larger meshes than the fixtures (16K to 32K cells, 4 to 5 levels, the
+    one-block tail on the small ones), against the reference's CoupledSolver
+    run here when oracle/_ref is present: the right-hand side, the cell data
+    and every coarse level bit for bit, the same iterations, the solution to
+    1e-4."""
+    from oracle import ref
+    if not ref.available():
+        pytest.skip("oracle/_ref not built")
+    from kutta_b200 import coupled_harness as H
+    case = ref.CoupledCase(tet, *dims, patch_kinds=kinds)
+    fields = H.flow_fields(case.arrays, 21, reference=reference)
+    want = case.solve(fields, ref.coupled_options(), rel_tol=1e-3, max_iter=60)
+    meta = {"reference": reference, "options": {}, "control": (1e-3, 1e-12, 60),
+            "density": fields["density"], "velocity_scale": fields["velocity_scale"]}
+    s, st, _ = _solver(meta, case.arrays, fields)
+    assert s.describe() == want["describe"]
+    n = int(case.arrays["sizes"][0])
+    assert np.array_equal(bits(s.copy("rhs")), bits(want["rhs"]))
+    assert np.array_equal(bits(s.copy("cell")), bits(want["cell"][: 27 * n]))
+    sizes, levels = ref_levels({"describe": want["describe"]}, want)
+    for k, lv in enumerate(levels, start=1):
+        got = s.level(k)
+        for key in ("rows", "cols", "diag", "a", "c", "g", "h", "d"):
+            assert np.array_equal(bits(got[key]), bits(lv[key][: len(got[key])])), (k, key)
+    assert st.iterations == want["iterations"]
+    assert st.converged == want["converged"]
+    assert st.final_residual == pytest.approx(want["final_residual"], rel=1e-2)
+    x = s.copy("x")
+    err = np.linalg.norm(x.astype(np.float64) - want["x"]) / np.linalg.norm(want["x"])
+    assert err <= 1e-4, err
