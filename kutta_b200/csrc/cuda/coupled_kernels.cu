@@ -133,7 +133,7 @@ __global__ void k_cpl_face_coefficient(int nf, int internal, const int* __restri
 }
 
 // fv_coupled.kern.h:93-108 (coupled_velocity_block): H_ii into planes 7-9.
-__global__ void k_cpl_velocity_block(int n, int internal, const int* __restrict__ offsets,
+__global__ void __launch_bounds__(kBlock, 8) k_cpl_velocity_block(int n, int internal, const int* __restrict__ offsets,
                                      const int* __restrict__ faces,
                                      const float* __restrict__ sign,
                                      const int* __restrict__ adjacent,
@@ -197,7 +197,7 @@ struct FineGeometry {
 };
 
 // fv_coupled.kern.h:191-208 (coupled_fine_gsum): |G| row sums, 3n planes.
-__global__ void k_cpl_fine_gsum(int n, FineGeometry m, const float* __restrict__ cell,
+__global__ void __launch_bounds__(kBlock, 8) k_cpl_fine_gsum(int n, FineGeometry m, const float* __restrict__ cell,
                                 float* __restrict__ r, float wc) {
   pdl_entry();
   const std::size_t N = n;
@@ -297,6 +297,12 @@ __global__ void k_cpl_fine_pack(int n, int width, FineGeometry m, const float* _
   }
 }
 
+// The fine row kernels are bounded to 32 registers (8 resident blocks of 256
+// per SM), so the fixed 1,184-block grid runs in one wave: at 40 registers
+// the sweep took 142.5 us at 128^3, bounded 122.7 us (0.92 of the measured
+// copy bandwidth). The coarse-level and Galerkin kernels are not bounded: the
+// spills cost them more than the second wave.
+//
 // (J x)_i of the fine level (fv_coupled.kern.h:258-278, coupled_fine_row).
 __device__ __forceinline__ float4 fine_row(int i, int n, int width, const CoupledFine& op,
                                            const float4* __restrict__ x) {
@@ -323,7 +329,7 @@ __device__ __forceinline__ float4 fine_row(int i, int n, int width, const Couple
   return make_float4(yu, yv, yw, yp);
 }
 
-__global__ void __launch_bounds__(kBlock) k_cpl_fine_spmv(int n, int width, CoupledFine op,
+__global__ void __launch_bounds__(kBlock, 8) k_cpl_fine_spmv(int n, int width, CoupledFine op,
                                                           const float4* __restrict__ x,
                                                           float4* __restrict__ y) {
   pdl_entry();
@@ -331,7 +337,7 @@ __global__ void __launch_bounds__(kBlock) k_cpl_fine_spmv(int n, int width, Coup
     y[i] = fine_row(i, n, width, op, x);
 }
 
-__global__ void __launch_bounds__(kBlock) k_cpl_fine_residual(int n, int width, CoupledFine op,
+__global__ void __launch_bounds__(kBlock, 8) k_cpl_fine_residual(int n, int width, CoupledFine op,
                                                               const float4* __restrict__ x,
                                                               const float4* __restrict__ b,
                                                               float4* __restrict__ r) {
@@ -345,7 +351,7 @@ __global__ void __launch_bounds__(kBlock) k_cpl_fine_residual(int n, int width, 
 
 // Damped block Jacobi (fv_coupled.kern.h:294-309, coupled_fine_smooth);
 // first: x is zero and is not read.
-__global__ void __launch_bounds__(kBlock) k_cpl_fine_smooth(int n, int width, CoupledFine op,
+__global__ void __launch_bounds__(kBlock, 8) k_cpl_fine_smooth(int n, int width, CoupledFine op,
                                                             const float4* __restrict__ x,
                                                             const float4* __restrict__ b,
                                                             float4* __restrict__ next, float omega,
@@ -630,7 +636,7 @@ __global__ void k_cpl_coarse_schur(CoupledLevel l, const float* __restrict__ r) 
 
 // fv_coupled.kern.h:554-567: restriction sums members in member order;
 // prolongation adds the aggregate's correction.
-__global__ void k_cpl_restrict(int nc, const int* __restrict__ offsets,
+__global__ void __launch_bounds__(kBlock, 8) k_cpl_restrict(int nc, const int* __restrict__ offsets,
                                const int* __restrict__ members, const float4* __restrict__ fine,
                                float4* __restrict__ coarse) {
   pdl_entry();
@@ -646,7 +652,7 @@ __global__ void k_cpl_restrict(int nc, const int* __restrict__ offsets,
     coarse[i] = s;
   }
 }
-__global__ void k_cpl_prolong(int nf, const int* __restrict__ aggregate,
+__global__ void __launch_bounds__(kBlock, 8) k_cpl_prolong(int nf, const int* __restrict__ aggregate,
                               const float4* __restrict__ coarse, float4* __restrict__ fine) {
   pdl_entry();
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nf; i += gridDim.x * blockDim.x) {
