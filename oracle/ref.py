@@ -198,7 +198,8 @@ def _coupled_lib():
         lib.kref_coupled_solve.argtypes = (
             [P, ctypes.POINTER(CoupledOptions)] + [F] * 14 +
             [ctypes.c_double, ctypes.c_double, ctypes.c_int, ctypes.c_double, ctypes.c_double,
-             ctypes.c_int, ctypes.c_int, I, I, D, ctypes.c_char_p, ctypes.c_int])
+             ctypes.c_int, ctypes.c_int, I, F, F, ctypes.c_double, ctypes.c_double,
+             ctypes.c_float, ctypes.c_float, I, I, D, ctypes.c_char_p, ctypes.c_int])
         lib.kref_coupled_array.restype = ctypes.c_longlong
         lib.kref_coupled_array.argtypes = [P, ctypes.c_char_p, P, ctypes.c_char_p]
         lib.kref_coupled_names.restype = ctypes.c_int
@@ -239,13 +240,15 @@ class CoupledCase:
         return out
 
     def solve(self, fields: dict, opts: CoupledOptions | None = None, *, rel_tol=0.1,
-              abs_tol=1e-12, max_iter=20, capture=True) -> dict:
+              abs_tol=1e-12, max_iter=20, capture=True, low_order=None, pairs=None) -> dict:
         """One CoupledSolver construction + solve + update on this mesh. `fields`
         holds momentum_u/v/w (over the stencil pattern), physical_u/v/w,
         ru/rv/rw, mass, viscosity, physical_diagonal, face_weights,
-        net_outflow (or None), density, velocity_scale and reference. Returns
-        the captured arrays plus iterations, converged, residuals, seconds and
-        describe."""
+        net_outflow (or None), density, velocity_scale and reference.
+        low_order: n int flags or None. pairs: (hi, lo, alpha_u, alpha_p,
+        velocity_slack, pressure_slack) with hi, lo float32 planes of 4n, or
+        None. Returns the captured arrays plus iterations, converged,
+        residuals, seconds and describe."""
         lib = self._lib
         opts = opts or coupled_options()
         f32 = {k: np.ascontiguousarray(fields[k], np.float32) for k in (
@@ -257,6 +260,14 @@ class CoupledCase:
         res = np.zeros(4, np.float64)
         desc = ctypes.create_string_buffer(512)
         F = ctypes.c_float
+        low = None if low_order is None else np.ascontiguousarray(low_order, np.int32)
+        if pairs is not None:
+            hi, lo, au, ap, vs, ps = pairs
+            hi = np.ascontiguousarray(hi, np.float32)
+            lo = np.ascontiguousarray(lo, np.float32)
+        else:
+            hi = lo = None
+            au = ap = vs = ps = 0.0
         rc = lib.kref_coupled_solve(
             self._h, ctypes.byref(opts), *(_ptr(f32[k], F) for k in (
                 "momentum_u", "momentum_v", "momentum_w", "physical_u", "physical_v",
@@ -264,7 +275,9 @@ class CoupledCase:
                 "face_weights")),
             _ptr(net, F) if net is not None else None, float(fields["density"]),
             float(fields["velocity_scale"]), int(fields["reference"]), rel_tol, abs_tol,
-            max_iter, int(capture), ctypes.byref(it), ctypes.byref(conv),
+            max_iter, int(capture), _ptr(low, ctypes.c_int) if low is not None else None,
+            _ptr(hi, F) if hi is not None else None, _ptr(lo, F) if lo is not None else None,
+            float(au), float(ap), float(vs), float(ps), ctypes.byref(it), ctypes.byref(conv),
             _ptr(res, ctypes.c_double), desc, 512)
         if rc != 0:
             raise RuntimeError(lib.kref_coupled_last_error().decode())

@@ -161,6 +161,9 @@ struct kref_coupled_options {
 // three momentum rows (values over the stencil pattern; physical diagonals),
 // solve(residuals) and update(alpha 1, 1) into zero fields. net_outflow may be
 // null. reference < 0: open domain. capture = 0 records nothing (timing).
+// low_order: n flags of cells with low-order pressure faces, or null. With
+// pair_hi / pair_lo (planes u | v | w | p), the float-pair update is also run
+// on those fields and recorded.
 // residuals[4]: initial and final residual, construction and solve seconds
 // (solve: the momentum-diagonal captures excluded, Jacobian assembly included).
 int kref_coupled_solve(void* handle, const kref_coupled_options* o, const float* momentum_u,
@@ -170,8 +173,10 @@ int kref_coupled_solve(void* handle, const kref_coupled_options* o, const float*
                        const float* physical_diagonal, const float* face_weights,
                        const float* net_outflow, double density, double velocity_scale,
                        int reference, double rel_tol, double abs_tol, int max_iter, int capture,
-                       int* iterations, int* converged, double* residuals, char* describe,
-                       int describe_len) {
+                       const int* low_order, const float* pair_hi, const float* pair_lo,
+                       double pair_alpha_u, double pair_alpha_p, float velocity_slack,
+                       float pressure_slack, int* iterations, int* converged, double* residuals,
+                       char* describe, int describe_len) {
   try {
     auto& c = *static_cast<Case*>(handle);
     auto& dev = c.dev;
@@ -223,7 +228,8 @@ int kref_coupled_solve(void* handle, const kref_coupled_options* o, const float*
     if (!capture) dev.observer = nullptr;
     using Clock = std::chrono::steady_clock;
     const auto t0 = Clock::now();
-    CoupledSolver solver(dev, c.mesh, c.stencil, c.host, c.geom, c.kinds, c.lsq, reference, {},
+    std::vector<Index> low(low_order ? low_order : nullptr, low_order ? low_order + n : nullptr);
+    CoupledSolver solver(dev, c.mesh, c.stencil, c.host, c.geom, c.kinds, c.lsq, reference, low,
                          opt);
     const float* momentum[] = {momentum_u, momentum_v, momentum_w};
     const float* physical[] = {physical_u, physical_v, physical_w};
@@ -255,6 +261,26 @@ int kref_coupled_solve(void* handle, const kref_coupled_options* o, const float*
     solver.update(velocity, pressure, 1.0, 1.0);
     c.put_buffer("updated_u", velocity.x);
     c.put_buffer("updated_p", pressure);
+    if (pair_hi && pair_lo) {
+      // The float-pair update (coupled_solver.cpp:524-535) from given hi/lo
+      // fields (planes u | v | w | p of n each).
+      const auto plane = [&](const float* base, int k) {
+        return dev.upload<float>(std::span<const float>(base + static_cast<std::size_t>(k) * n, n));
+      };
+      DeviceVec3 vh{plane(pair_hi, 0), plane(pair_hi, 1), plane(pair_hi, 2)};
+      DeviceVec3 vl{plane(pair_lo, 0), plane(pair_lo, 1), plane(pair_lo, 2)};
+      auto ph = plane(pair_hi, 3), pl = plane(pair_lo, 3);
+      solver.update(vh, ph, CoupledPairs{vl, pl, velocity_slack, pressure_slack}, pair_alpha_u,
+                    pair_alpha_p);
+      const char* hi_names[] = {"paired_u", "paired_v", "paired_w", "paired_p"};
+      const char* lo_names[] = {"paired_u_lo", "paired_v_lo", "paired_w_lo", "paired_p_lo"};
+      const Buffer<float>* his[] = {&vh.x, &vh.y, &vh.z, &ph};
+      const Buffer<float>* los[] = {&vl.x, &vl.y, &vl.z, &pl};
+      for (int k = 0; k < 4; ++k) {
+        c.put_buffer(hi_names[k], *his[k]);
+        c.put_buffer(lo_names[k], *los[k]);
+      }
+    }
     dev.observer = nullptr;
     *iterations = st.iterations;
     *converged = st.converged ? 1 : 0;

@@ -46,6 +46,10 @@ CASES = {
                                   {"pre_sweeps": 2, "post_sweeps": 2, "coarsest_rows": 20,
                                    "recompute": True},
                                   (1e-3, 1e-12, 60), {"net_outflow": True}),
+    # Cells flagged with low-order pressure faces (no extrapolation in Q),
+    # and the float-pair update on seeded hi/lo fields.
+    "coupled_tet5x4x3_loworder_paired": (True, (5, 4, 3), OPEN, -1, 6, {}, (1e-3, 1e-12, 60),
+                                         {"low_order": 0.15, "pairs": True}),
 }
 
 MESH_KEYS = ("sizes", "owner", "neighbour", "area_x", "area_y", "area_z", "face_area",
@@ -74,8 +78,18 @@ def make(name: str) -> None:
         np.add.at(net, m["neighbour"], -fields["mass"][: len(m["neighbour"])].astype(np.float64))
         fields["net_outflow"] = (net * (1 + 0.1 * rng.standard_normal(n))).astype(np.float32)
     rel_tol, abs_tol, max_iter = control
+    n = int(case.arrays["sizes"][0])
+    rng = np.random.default_rng(seed + 200)
+    low = None
+    if extras.get("low_order"):
+        low = (rng.random(n) < extras["low_order"]).astype(np.int32)
+    pairs = None
+    if extras.get("pairs"):
+        hi = (rng.standard_normal(4 * n) * 10).astype(np.float32)
+        lo = (rng.standard_normal(4 * n) * 1e-6).astype(np.float32)
+        pairs = (hi, lo, 0.7, 0.3, 1e-4, 3e-5)
     out = case.solve(fields, ref.coupled_options(**options), rel_tol=rel_tol, abs_tol=abs_tol,
-                     max_iter=max_iter)
+                     max_iter=max_iter, low_order=low, pairs=pairs)
     arrays = {}
     for k in MESH_KEYS:
         arrays["mesh_" + k] = case.arrays[k]
@@ -83,6 +97,10 @@ def make(name: str) -> None:
         arrays["field_" + k] = fields[k]
     if fields.get("net_outflow") is not None:
         arrays["field_net_outflow"] = fields["net_outflow"]
+    if low is not None:
+        arrays["mesh_low_order"] = low
+    if pairs is not None:
+        arrays["pair_hi"], arrays["pair_lo"] = pairs[0], pairs[1]
     for k, v in out.items():
         if isinstance(v, np.ndarray) and k not in case.arrays:
             arrays["ref_" + k] = v
@@ -93,6 +111,7 @@ def make(name: str) -> None:
         "converged": out["converged"], "initial_residual": out["initial_residual"],
         "final_residual": out["final_residual"], "describe": out["describe"],
         "net_outflow": bool(extras.get("net_outflow")),
+        "pairs": list(pairs[2:]) if pairs is not None else None,
     }
     np.savez_compressed(HERE / f"{name}.npz", meta=np.frombuffer(json.dumps(meta).encode(), np.uint8),
                         **arrays)

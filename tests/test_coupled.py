@@ -32,6 +32,7 @@ def load(name):
     mesh = {k[5:]: d[k] for k in d.files if k.startswith("mesh_")}
     fields = {k[6:]: d[k] for k in d.files if k.startswith("field_")}
     refs = {k[4:]: d[k] for k in d.files if k.startswith("ref_")}
+    refs.update({k: d[k] for k in d.files if k in ("pair_hi", "pair_lo")})
     fields.setdefault("net_outflow", None)
     fields.update(density=meta["density"], velocity_scale=meta["velocity_scale"],
                   reference=meta["reference"])
@@ -457,3 +458,63 @@ def test_coupled_matches_reference_at_scale(cuda, tet, dims, kinds, reference):
     x = s.copy("x")
     err = np.linalg.norm(x.astype(np.float64) - want["x"]) / np.linalg.norm(want["x"])
     assert err <= 1e-4, err
+
+
+
+def _paired_oracle(hi, lo, x, n, au, ap, vs, ps, wc, reference):
+    """The reference's paired update restated (coupled_paired_update and, for
+    a closed domain, the paired pick and gauge), planes u | v | w | p."""
+    out = []
+    for k in range(3):
+        out.append(O.pair_add(hi[k * n:(k + 1) * n], lo[k * n:(k + 1) * n],
+                              np.float32(au) * x[k * n:(k + 1) * n], vs))
+    ph, pl = O.pair_add(hi[3 * n:], lo[3 * n:], np.float32(ap * float(wc)) * x[3 * n:], ps)
+    if reference >= 0:
+        shift = -(np.float32(ph[reference]) + np.float32(pl[reference]))
+        ph, pl = O.pair_add(ph, pl, np.full(n, shift, np.float32), ps)
+    out.append((ph, pl))
+    return out
+
+
+def test_oracle_pair_update_reproduces_reference():
+    """The oracle's paired update on the reference's own solution and hi/lo
+    fields gives the reference's paired update bit for bit (kpair_add,
+    prelude.h:139-149)."""
+    meta, mesh, _, refs = load("coupled_tet5x4x3_loworder_paired")
+    n = int(mesh["sizes"][0])
+    au, ap, vs, ps = meta["pairs"]
+    want = _paired_oracle(refs["pair_hi"], refs["pair_lo"], refs["x"], n, au, ap, vs, ps,
+                          wc_of(meta), meta["reference"])
+    for k, c in enumerate("uvwp"):
+        assert np.array_equal(bits(want[k][0]), bits(refs[f"paired_{c}"])), c
+        assert np.array_equal(bits(want[k][1]), bits(refs[f"paired_{c}_lo"])), c
+
+
+@pytest.mark.gpu
+def test_coupled_paired_update_on_low_order_mesh(cuda):
+    """On a mesh with low-order pressure cells: the solve takes the
+    reference's iterations, and the device's paired update equals the
+    oracle's (pinned to the reference above) on the device's solution, and the
+    reference's own result bit for bit when the two solutions agree bit for
+    bit."""
+    import torch
+    name = "coupled_tet5x4x3_loworder_paired"
+    meta, mesh, fields, refs = load(name)
+    assert "low_order" in mesh
+    s, st, _ = _solver(meta, mesh, fields)
+    assert st.iterations == meta["iterations"]
+    n = int(mesh["sizes"][0])
+    au, ap, vs, ps = meta["pairs"]
+    hi = [torch.from_numpy(refs["pair_hi"][k * n:(k + 1) * n].copy()).cuda() for k in range(4)]
+    lo = [torch.from_numpy(refs["pair_lo"][k * n:(k + 1) * n].copy()).cuda() for k in range(4)]
+    s.paired_update(*hi, *lo, au, ap, vs, ps)
+    torch.cuda.synchronize()
+    x = s.copy("x")
+    want = _paired_oracle(refs["pair_hi"], refs["pair_lo"], x, n, au, ap, vs, ps, wc_of(meta),
+                          meta["reference"])
+    same_x = np.array_equal(bits(x), bits(refs["x"]))
+    for k, c in enumerate("uvwp"):
+        assert np.array_equal(bits(hi[k].cpu().numpy()), bits(want[k][0])), c
+        assert np.array_equal(bits(lo[k].cpu().numpy()), bits(want[k][1])), c
+        if same_x:
+            assert np.array_equal(bits(hi[k].cpu().numpy()), bits(refs[f"paired_{c}"])), c
