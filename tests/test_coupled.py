@@ -518,3 +518,25 @@ def test_coupled_paired_update_on_low_order_mesh(cuda):
         assert np.array_equal(bits(lo[k].cpu().numpy()), bits(want[k][1])), c
         if same_x:
             assert np.array_equal(bits(hi[k].cpu().numpy()), bits(refs[f"paired_{c}"])), c
+
+
+@pytest.mark.parametrize("dims,lo,hi", [((3, 2, 2), (0, 0, 0), (3, 2, 2)),
+                                        ((7, 5, 4), (0, 0, 0), (1, 1, 1)),
+                                        ((6, 4, 5), (-1, 0.5, 0), (2, 1, 0.25))])
+def test_box_hex_matches_reference_arrays(dims, lo, hi):
+    """coupled_harness.box_hex (the bench's mesh, built without the reference)
+    gives the reference's arrays for the same box: integer arrays equal, float
+    arrays to the reference's geometric round-off (1e-12 absolute)."""
+    from oracle import ref
+    if not ref.available():
+        pytest.skip("oracle/_ref not built")
+    from kutta_b200 import coupled_harness as H
+    want = ref.CoupledCase(False, *dims, lo=lo, hi=hi).arrays
+    got = H.box_hex(*dims, lo=lo, hi=hi)
+    for k, v in got.items():
+        w = want[k]
+        assert v.shape == w.shape, k
+        if v.dtype.kind == "i":
+            assert np.array_equal(v, w), k
+        else:
+            assert np.allclose(v.astype(np.float64), w.astype(np.float64), rtol=1e-6, atol=1e-12), k
