@@ -366,9 +366,10 @@ def other_configs(args):
     """One device-timed refresh + solve (best of two) of the other
     configurations, at N = 1 after the timed work: the graded near-wall
     matrix to 1e-8 (mixed with and without the learned warm start, against
-    plain FP32 AMG-PCG, which stops at its FP32 floor), and an unseen seed of
+    plain FP32 AMG-PCG, which stops at its FP32 floor), an unseen seed of
     the learned stage's evaluation configuration (128^3 jittered hex, smooth
-    log-normal D_f, Fourier right-hand side) to 1e-6."""
+    log-normal D_f, Fourier right-hand side) to 1e-6, and the Coupled
+    4x4-block solve on a 128^3 hex box (10 solves after 3 warm-ups)."""
     import numpy as np
     import scipy.sparse as sp
     import torch
@@ -425,6 +426,12 @@ def other_configs(args):
         workload="hex128, unseen seed 90001: 128^3 jittered hex, smooth log-normal D_f "
                  "(sigma 1.5, correlation 0.1), 16 Fourier modes + 10 % noise",
         **arms(s, b, 1e-6, 1))
+    # The Coupled 4x4-block solve (`--mode coupled` at its defaults, without
+    # the reference's CPU solve, which that mode adds).
+    import copy
+    cargs = copy.copy(args)
+    cargs.steps, cargs.warmup, cargs.no_cpu_baseline = 10, 3, True
+    out["coupled_hex128"] = run_coupled(cargs)
     return out
 
 
