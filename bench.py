@@ -860,8 +860,10 @@ def run_coupled(args):
     (Jacobian assembly, Galerkin hierarchy refresh, block BiCGStab to the
     steady solver's control: relative 0.1, at most 20 iterations), device-
     timed over --steps after --warmup. The fine damped block-Jacobi sweep is
-    timed on its own for its HBM fraction. The reference's own CPU solve
-    (oracle/_ref) runs on a smaller box of the same kind as the CPU baseline."""
+    timed on its own for its HBM fraction. With --coupled-mesh tet the box is
+    split into six tets per hex (--cells-per-side^3 x 6 cells). The
+    reference's own CPU solve (oracle/_ref) runs on a box of the same kind
+    (--coupled-cpu-side, default the same box) as the CPU baseline."""
     import numpy as np
     import torch
     from kutta_b200 import coupled_harness as H
@@ -869,7 +871,8 @@ def run_coupled(args):
     torch.cuda.set_device(0)
     side = args.cells_per_side
     t0 = time.perf_counter()
-    mesh = H.box_hex(side, side, side)
+    tet = args.coupled_mesh == "tet"
+    mesh = (H.box_tet if tet else H.box_hex)(side, side, side)
     fields = H.flow_fields(mesh, args.seed)
     make_s = time.perf_counter() - t0
     n, nf, ni, entries, nnz = (int(v) for v in mesh["sizes"])
@@ -914,7 +917,8 @@ def run_coupled(args):
     peak, kind = _peaks()
     achieved = sweep_bytes / (sweep_ms * 1e-3) / 1e9
     out = {"mode": "coupled",
-           "workload": f"coupled_hex{side}: {side}^3 hex box, {n} cells, {nf} faces, "
+           "workload": f"coupled_{args.coupled_mesh}{side}: {side}^3 "
+                       f"{'x 6 tet' if tet else 'hex'} box, {n} cells, {nf} faces, "
                        f"{width_slots} internal cell-face slots, 4 unknowns per cell",
            "method": solver.describe(), "control": [control.rel_tol, control.abs_tol,
                                                      control.max_iter],
@@ -930,8 +934,8 @@ def run_coupled(args):
         try:
             from oracle import ref
             if ref.available():
-                cside = args.coupled_cpu_side
-                case = ref.CoupledCase(False, cside, cside, cside)
+                cside = args.coupled_cpu_side or side
+                case = ref.CoupledCase(tet, cside, cside, cside)
                 f = H.flow_fields(case.arrays, args.seed)
                 r = case.solve(f, ref.coupled_options(), rel_tol=control.rel_tol,
                                abs_tol=control.abs_tol, max_iter=control.max_iter, capture=False)
@@ -939,7 +943,8 @@ def run_coupled(args):
                 out["cpu_baseline"] = {
                     "kind": "reference", "cores": 1,
                     "sample": f"the reference's CoupledSolver (oracle/_ref, serial CPU device) "
-                              f"on a {cside}^3 hex box of the same kind ({cells} cells)",
+                              f"on a {cside}^3 {'x 6 tet' if tet else 'hex'} box of the same "
+                              f"kind ({cells} cells)",
                     "ms_per_solve": r["solve_s"] * 1e3, "iterations": r["iterations"],
                     "construct_s": r["setup_s"], "describe": r["describe"],
                     "ns_per_cell_iteration": r["solve_s"] * 1e9 / cells / max(1, r["iterations"])}
@@ -981,8 +986,11 @@ def main():
     ap.add_argument("--cells-per-side", type=int, default=128, help="coupled mode: box side")
     ap.add_argument("--coupled-rel-tol", type=float, default=0.1)
     ap.add_argument("--coupled-max-iter", type=int, default=20)
-    ap.add_argument("--coupled-cpu-side", type=int, default=128,
-                    help="coupled mode: box side of the reference CPU baseline")
+    ap.add_argument("--coupled-mesh", default="hex", choices=["hex", "tet"],
+                    help="coupled mode: hex box, or the box split into six tets per hex")
+    ap.add_argument("--coupled-cpu-side", type=int, default=None,
+                    help="coupled mode: box side of the reference CPU baseline "
+                         "(default --cells-per-side)")
     args = ap.parse_args()
     rank, world, local = _dist()
     if args.mode == "workload":

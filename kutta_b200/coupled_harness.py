@@ -9,7 +9,8 @@ A mesh is a dict of the device-mesh, stencil and least-squares arrays by name
 `lsq_inverse`, `owner_to_face_x`.., `neighbour_to_face_x`.., `volume`,
 `boundary_kind`), as the reference builds them for a box
 (src/kutta/fv/device_mesh.cpp, src/kutta/fv/operators.cpp:43-90) and as
-`box_hex` below builds them for a structured hex box without the reference.
+`box_hex` / `box_tet` below build them, bit for bit, for a structured hex box and
+its six-tet split without the reference.
 
 The fields follow the steady solver's assembly in form, with seeded values:
 a swirling velocity field, its face mass fluxes, an effective viscosity that
@@ -107,62 +108,24 @@ def flow_fields(mesh: dict, seed: int = 1, *, density: float = 1.2, speed: float
     return fields
 
 
-def box_hex(nx: int, ny: int, nz: int, lo=(0.0, 0.0, 0.0), hi=(1.0, 1.0, 1.0),
-            patch_kinds=(INLET, OUTLET, WALL, WALL, SYMMETRY, SYMMETRY)) -> dict:
-    """A structured hex box [lo, hi] with nx x ny x nz cells and the arrays a
-    Coupled solve reads, in the reference's conventions for such a box
-    (src/kutta/io/generators.cpp make_box_hex, src/kutta/fv/device_mesh.cpp,
-    src/kutta/fv/operators.cpp:43-90): cell i + nx (j + ny k); internal faces
-    sorted by (owner, neighbour); boundary faces by patch (xmin, xmax, ymin,
-    ymax, zmin, zmax), each in cell order; each cell's faces in face order;
-    least-squares rows d / |d|^2 toward the neighbour centroid or the boundary
-    face centroid, with every boundary face observed at its centroid (on a box
-    the normal foot of the cell centroid is the face centroid)."""
-    lo = np.asarray(lo, np.float64)
-    hi = np.asarray(hi, np.float64)
-    dims = np.array([nx, ny, nz])
-    h = (hi - lo) / dims
-    n = int(nx * ny * nz)
-    cells = np.arange(n, dtype=np.int64)
-    ijk = np.stack([cells % nx, (cells // nx) % ny, cells // (nx * ny)], 1)
-    centroid = lo + (ijk + 0.5) * h
-    strides = np.array([1, nx, nx * ny])
-    face_area_axis = np.array([h[1] * h[2], h[0] * h[2], h[0] * h[1]])
-    # Internal faces, sorted by (owner, neighbour).
-    own, nei, axis = [], [], []
-    for a in range(3):
-        c = cells[ijk[:, a] < dims[a] - 1]
-        own.append(c)
-        nei.append(c + strides[a])
-        axis.append(np.full(len(c), a))
-    own, nei, axis = (np.concatenate(v) for v in (own, nei, axis))
-    order = np.argsort(own * n + nei, kind="stable")
-    own, nei, axis = own[order], nei[order], axis[order]
-    ni = len(own)
-    # Boundary faces by patch, each in cell order.
-    b_owner, b_axis, b_side, b_kind = [], [], [], []
-    for a in range(3):
-        for side, at in ((-1, 0), (1, dims[a] - 1)):
-            c = cells[ijk[:, a] == at]
-            b_owner.append(c)
-            b_axis.append(np.full(len(c), a))
-            b_side.append(np.full(len(c), side))
-            b_kind.append(np.full(len(c), patch_kinds[2 * a + (side > 0)]))
-    b_owner, b_axis, b_side, b_kind = (np.concatenate(v) for v in (b_owner, b_axis, b_side,
-                                                                   b_kind))
-    nb = len(b_owner)
-    nf = ni + nb
-    owner = np.concatenate([own, b_owner])
-    f_axis = np.concatenate([axis, b_axis])
-    sign_b = np.concatenate([np.ones(ni), b_side])
-    S = np.zeros((nf, 3))
-    S[np.arange(nf), f_axis] = face_area_axis[f_axis] * sign_b
-    fc = np.empty((nf, 3))
-    fc[:ni] = 0.5 * (centroid[own] + centroid[nei])
-    fc[ni:] = centroid[b_owner]
-    fc[ni + np.arange(nb), b_axis] += 0.5 * h[b_axis] * b_side
+def _mesh_arrays(centroid, volume, owner, neighbour, S, fc, b_kind) -> dict:
+    """The device-mesh, stencil and pressure least-squares arrays of a mesh
+    given by its cells (centroids, volumes) and faces (owner for every face,
+    neighbour for the internal ones, which come first; area vectors out of
+    the owner; centroids; the kind of each boundary face), in the reference's
+    conventions (src/kutta/fv/device_mesh.cpp, src/kutta/fv/operators.cpp):
+    each cell's faces in face order; least-squares rows d / |d|^2 toward the
+    neighbour centroid or the boundary face centroid (make_stencil); the
+    pressure fit observes pressure-specified faces at their centroid and every
+    other boundary face at the normal foot of the cell centroid
+    (operators.cpp cell_fit, steady_solver.cpp:348-356)."""
+    n = len(centroid)
+    ni = len(neighbour)
+    nf = len(owner)
+    nb = nf - ni
+    b_owner = owner[ni:]
     # Cell-face entries: each cell's faces in face order.
-    e_cell = np.concatenate([own, nei, b_owner])
+    e_cell = np.concatenate([owner[:ni], neighbour, b_owner])
     e_face = np.concatenate([np.arange(ni), np.arange(ni), ni + np.arange(nb)])
     e_sign = np.concatenate([np.ones(ni), -np.ones(ni), np.ones(nb)])
     order = np.argsort(e_cell * nf + e_face, kind="stable")
@@ -171,17 +134,27 @@ def box_hex(nx: int, ny: int, nz: int, lo=(0.0, 0.0, 0.0), hi=(1.0, 1.0, 1.0),
     np.add.at(offsets, e_cell + 1, 1)
     offsets = np.cumsum(offsets)
     internal = e_face < ni
-    other = np.where(internal, np.where(owner[e_face] == e_cell,
-                                        np.concatenate([nei, np.zeros(nb, np.int64)])[e_face],
+    nei_full = np.concatenate([neighbour, np.zeros(nb, np.int64)])
+    other = np.where(internal, np.where(owner[e_face] == e_cell, nei_full[e_face],
                                         owner[e_face]), -1)
     adjacent = np.where(internal, other, -(e_face - ni + 1))
     target = np.where(internal[:, None], centroid[np.maximum(other, 0)], fc[e_face])
     d = target - centroid[e_cell]
     w = 1.0 / np.einsum("ek,ek->e", d, d)
     rows = d * w[:, None]
+    # The pressure fit's boundary observations.
+    db = fc[ni:] - centroid[b_owner]
+    prescribed = np.isin(b_kind, (OUTLET, OUTLET_NORMAL))
+    sb = S[ni:]
+    foot = sb * (np.einsum("bk,bk->b", db, sb) / np.einsum("bk,bk->b", sb, sb))[:, None]
+    db = np.where(prescribed[:, None], db, foot)
+    wb = 1.0 / np.einsum("bk,bk->b", db, db)
+    bd = db * wb[:, None]
     m = np.zeros((n, 6))
+    ci, di, wi = e_cell[internal], d[internal], w[internal]
     for k, (p, q) in enumerate(((0, 0), (0, 1), (0, 2), (1, 1), (1, 2), (2, 2))):
-        np.add.at(m[:, k], e_cell, w * d[:, p] * d[:, q])
+        np.add.at(m[:, k], ci, wi * di[:, p] * di[:, q])
+        np.add.at(m[:, k], b_owner, wb * db[:, p] * db[:, q])
     a = m.T
     det = a[0] * (a[3] * a[5] - a[4] * a[4]) - a[1] * (a[1] * a[5] - a[4] * a[2]) + \
         a[2] * (a[1] * a[4] - a[3] * a[2])
@@ -189,15 +162,15 @@ def box_hex(nx: int, ny: int, nz: int, lo=(0.0, 0.0, 0.0), hi=(1.0, 1.0, 1.0),
                         (a[1] * a[4] - a[2] * a[3]) / det, (a[0] * a[5] - a[2] * a[2]) / det,
                         (a[1] * a[2] - a[0] * a[4]) / det, (a[0] * a[3] - a[1] * a[1]) / det])
     dfc = np.empty((nf, 3))
-    dfc[:ni] = centroid[nei] - centroid[own]
+    dfc[:ni] = centroid[neighbour] - centroid[owner[:ni]]
     dfc[ni:] = fc[ni:] - centroid[b_owner]
     diffusion = np.einsum("fk,fk->f", S, S) / np.einsum("fk,fk->f", S, dfc)
-    bd = dfc[ni:] / np.einsum("fk,fk->f", dfc[ni:], dfc[ni:])[:, None]
     otf = fc - centroid[owner]
-    ntf = fc[:ni] - centroid[nei]
+    ntf = fc[:ni] - centroid[neighbour]
     # The stencil pattern: each cell's face neighbours and itself, sorted.
-    p_cell = np.concatenate([own, nei, cells])
-    p_col = np.concatenate([nei, own, cells])
+    cells = np.arange(n, dtype=np.int64)
+    p_cell = np.concatenate([owner[:ni], neighbour, cells])
+    p_col = np.concatenate([neighbour, owner[:ni], cells])
     order = np.argsort(p_cell * n + p_col, kind="stable")
     p_cell, p_col = p_cell[order], p_col[order]
     p_rows = np.zeros(n + 1, np.int64)
@@ -207,7 +180,7 @@ def box_hex(nx: int, ny: int, nz: int, lo=(0.0, 0.0, 0.0), hi=(1.0, 1.0, 1.0),
     f32, i32 = np.float32, np.int32
     return {
         "sizes": np.array([n, nf, ni, len(e_cell), len(p_col)], i32),
-        "owner": owner.astype(i32), "neighbour": nei.astype(i32),
+        "owner": owner.astype(i32), "neighbour": neighbour.astype(i32),
         "area_x": S[:, 0].astype(f32), "area_y": S[:, 1].astype(f32),
         "area_z": S[:, 2].astype(f32), "face_area": S.reshape(-1),
         "cell_centroid": centroid.reshape(-1),
@@ -225,5 +198,186 @@ def box_hex(nx: int, ny: int, nz: int, lo=(0.0, 0.0, 0.0), hi=(1.0, 1.0, 1.0),
         "owner_to_face_z": otf[:, 2].astype(f32),
         "neighbour_to_face_x": ntf[:, 0].astype(f32), "neighbour_to_face_y": ntf[:, 1].astype(f32),
         "neighbour_to_face_z": ntf[:, 2].astype(f32),
-        "volume": np.full(n, np.prod(h), f32), "boundary_kind": b_kind.astype(i32),
+        "volume": volume.astype(f32), "boundary_kind": b_kind.astype(i32),
     }
+
+
+def box_hex(nx: int, ny: int, nz: int, lo=(0.0, 0.0, 0.0), hi=(1.0, 1.0, 1.0),
+            patch_kinds=(INLET, OUTLET, WALL, WALL, SYMMETRY, SYMMETRY)) -> dict:
+    """A structured hex box [lo, hi] with nx x ny x nz cells and the arrays a
+    Coupled solve reads, as the reference builds them for the same box
+    (src/kutta/io/generators.cpp make_box_hex): cell i + nx (j + ny k);
+    patches xmin, xmax, ymin, ymax, zmin, zmax with the given kinds."""
+    return _box(nx, ny, nz, lo, hi, patch_kinds, tet=False)
+
+
+def box_tet(nx: int, ny: int, nz: int, lo=(0.0, 0.0, 0.0), hi=(1.0, 1.0, 1.0),
+            patch_kinds=(INLET, OUTLET, WALL, WALL, SYMMETRY, SYMMETRY)) -> dict:
+    """The same box split into six tets per hex around its (0,0,0)-(1,1,1)
+    diagonal (generators.cpp make_box_tet): cell 6 (hex index) + t."""
+    return _box(nx, ny, nz, lo, hi, patch_kinds, tet=True)
+
+
+def _box(nx, ny, nz, lo, hi, patch_kinds, tet):
+    """The box's cells as the generator lists them, then the reference's
+    face construction (src/kutta/mesh/topology.cpp from_cells and pack):
+    faces numbered by first appearance over the cells' local faces, stored
+    with the first cell's node order, reversed where its normal points into
+    that cell; the lower cell owns an internal face; internal faces sorted by
+    (owner, neighbour), boundary faces by patch (the first box side all the
+    face's nodes lie on), each in order of first appearance. The geometry
+    follows in the reference's double operations (`_face_geometry`,
+    `_cell_geometry`), so the arrays are the reference's bit for bit, the
+    least-squares inverse aside (the reference inverts by a Jacobi
+    eigensolve; the two agree to double round-off)."""
+    lo = np.asarray(lo, np.float64)
+    hi = np.asarray(hi, np.float64)
+    dims = np.array([nx, ny, nz])
+    hexes = np.arange(int(nx * ny * nz), dtype=np.int64)
+    i, j, k = hexes % nx, (hexes // nx) % ny, hexes // (nx * ny)
+
+    def node(i, j, k):
+        return (k * (ny + 1) + j) * (nx + 1) + i
+
+    v = np.stack([node(i, j, k), node(i + 1, j, k), node(i + 1, j + 1, k), node(i, j + 1, k),
+                  node(i, j, k + 1), node(i + 1, j, k + 1), node(i + 1, j + 1, k + 1),
+                  node(i, j + 1, k + 1)], 1)
+    if tet:
+        ring = (1, 2, 3, 7, 4, 5)
+        cells = np.stack([np.stack([v[:, 0], v[:, ring[t]], v[:, ring[(t + 1) % 6]], v[:, 6]], 1)
+                          for t in range(6)], 1).reshape(-1, 4)
+        local = [[0, 1, 2], [0, 3, 1], [1, 3, 2], [2, 3, 0]]
+    else:
+        cells = v
+        local = [[0, 3, 2, 1], [4, 5, 6, 7], [0, 1, 5, 4], [1, 2, 6, 5], [2, 3, 7, 6],
+                 [3, 0, 4, 7]]
+    n = len(cells)
+    npts = (nx + 1) * (ny + 1) * (nz + 1)
+    pid = np.arange(npts, dtype=np.int64)
+    pijk = np.stack([pid % (nx + 1), (pid // (nx + 1)) % (ny + 1),
+                     pid // ((nx + 1) * (ny + 1))], 1)
+    points = lo + (hi - lo) * pijk / dims
+    # Every cell's local faces; occurrence (local faces) cell + local face.
+    occ = cells[:, local].reshape(-1, len(local[0]))
+    per_cell = len(local)
+    cell_mid = np.zeros((n, 3))
+    for c in range(cells.shape[1]):
+        cell_mid += points[cells[:, c]]
+    cell_mid /= cells.shape[1]
+    del cells
+    srt = np.sort(occ, axis=1)
+    key_hi = srt[:, 0] * npts + srt[:, 1]
+    key_lo = srt[:, 2] * npts + (srt[:, 3] if srt.shape[1] > 3 else 0)
+    del srt
+    order = np.lexsort((key_lo, key_hi))  # stable: each key's first occurrence leads
+    ks_hi, ks_lo = key_hi[order], key_lo[order]
+    del key_hi, key_lo
+    lead = np.ones(len(order), bool)
+    lead[1:] = (ks_hi[1:] != ks_hi[:-1]) | (ks_lo[1:] != ks_lo[:-1])
+    del ks_hi, ks_lo
+    first = order[lead]
+    group = np.cumsum(lead) - 1
+    owner_f = first // per_cell
+    second = np.full(len(first), -1, np.int64)
+    repeat = ~lead
+    second[group[repeat]] = order[repeat] // per_cell
+    del order, lead, group, repeat
+    # Stored node order: the first cell's, reversed where the polygon's normal
+    # points into that cell (the sign needs no exact doubles).
+    ns = occ[first]
+    del occ
+    corners = points[ns]
+    normal = np.cross(corners[:, 1] - corners[:, 0], corners[:, 2] - corners[:, 0])
+    inward = np.einsum("fk,fk->f", normal, corners.mean(axis=1) - cell_mid[owner_f]) < 0
+    del corners, normal
+    ns[inward] = ns[inward, ::-1]
+    internal = second >= 0
+    nijk = pijk[ns]
+    patch = np.full(len(first), -1)
+    for side in range(6):
+        axis = side // 2
+        at = 0 if side % 2 == 0 else dims[axis]
+        on = np.all(nijk[:, :, axis] == at, axis=1) & ~internal & (patch < 0)
+        patch[on] = side
+    del nijk
+    ii = np.nonzero(internal)[0]
+    ii = ii[np.lexsort((second[ii], owner_f[ii]))]
+    bb = np.nonzero(~internal)[0]
+    bb = bb[np.lexsort((first[bb], patch[bb]))]
+    order = np.concatenate([ii, bb])
+    owner, neighbour = owner_f[order], second[ii]
+    fc, area = _face_geometry(points[ns[order]])
+    centroid, volume = _cell_geometry(fc, area, owner, neighbour, n)
+    b_kind = np.asarray(patch_kinds)[patch[bb]]
+    return _mesh_arrays(centroid, volume, owner, neighbour, area, fc, b_kind)
+
+
+def _dot(a, b):
+    return a[..., 0] * b[..., 0] + a[..., 1] * b[..., 1] + a[..., 2] * b[..., 2]
+
+
+def _cross(a, b):
+    return np.stack([a[..., 1] * b[..., 2] - a[..., 2] * b[..., 1],
+                     a[..., 2] * b[..., 0] - a[..., 0] * b[..., 2],
+                     a[..., 0] * b[..., 1] - a[..., 1] * b[..., 0]], -1)
+
+
+def _face_geometry(corners):
+    """Centroid and area vector of each polygon (faces x nodes x 3), in the
+    reference's double operations and their order (src/kutta/mesh/mesh.cpp
+    face_geometry, src/kutta/mesh/detail.hpp face_center): the node mean
+    about the first node; the area vector as the fan of half cross products
+    about it; the centroid as the fan triangles' moments weighted by their
+    areas projected on the unit normal. A division by s is a product with
+    1 / s, as there."""
+    k = corners.shape[1]
+    origin = corners[:, 0]
+    d = np.zeros_like(origin)
+    for j in range(k):
+        d = d + (corners[:, j] - origin)
+    center = origin + d * (1 / float(k))
+    av = np.zeros_like(origin)
+    for j in range(k):
+        av = av + _cross(corners[:, j] - center, corners[:, (j + 1) % k] - center) * 0.5
+    normal = av * (1 / np.sqrt(_dot(av, av)))[:, None]
+    area = np.zeros(len(origin))
+    moment = np.zeros_like(origin)
+    for j in range(k):
+        a, b = corners[:, j] - center, corners[:, (j + 1) % k] - center
+        w = _dot(_cross(a, b) * 0.5, normal)
+        area = area + w
+        moment = moment + (a + b) * (w / 3)[:, None]
+    return center + moment * (1 / area)[:, None], av
+
+
+def _cell_geometry(fc, area, owner, neighbour, n):
+    """Cell centroids and volumes from the face centroids and area vectors, in
+    the reference's double operations and their order (src/kutta/mesh/mesh.cpp
+    cell_geometry): a first estimate, the mean of the cell's face centroids
+    about its first; then one pyramid per face from that estimate, with volume
+    (sign) S.r / 3 and centroid 3/4 of the way to the face, each cell summed
+    in face order."""
+    ni = len(neighbour)
+    e_cell = np.concatenate([owner[:ni], neighbour, owner[ni:]])
+    e_face = np.concatenate([np.arange(ni), np.arange(ni), np.arange(ni, len(owner))])
+    e_sign = np.concatenate([np.ones(ni), -np.ones(ni), np.ones(len(owner) - ni)])
+    order = np.lexsort((e_face, e_cell))
+    e_cell, e_face, e_sign = e_cell[order], e_face[order], e_sign[order]
+    start = np.searchsorted(e_cell, np.arange(n + 1))
+    count = np.diff(start)
+    anchor = fc[e_face[start[:-1]]]
+    estimate = np.zeros((n, 3))
+    for k in range(int(count.max())):
+        c = np.nonzero(count > k)[0]
+        estimate[c] = estimate[c] + (fc[e_face[start[c] + k]] - anchor[c])
+    estimate = anchor + estimate * (1 / count.astype(np.float64))[:, None]
+    volume = np.zeros(n)
+    centroid = np.zeros((n, 3))
+    for k in range(int(count.max())):
+        c = np.nonzero(count > k)[0]
+        e = start[c] + k
+        r = fc[e_face[e]] - estimate[c]
+        v = e_sign[e] * _dot(area[e_face[e]], r) / 3
+        volume[c] = volume[c] + v
+        centroid[c] = centroid[c] + r * (0.75 * v)[:, None]
+    return estimate + centroid * (1 / volume)[:, None], volume

@@ -902,7 +902,7 @@ class _CoupledResiduals(ctypes.Structure):
 
 class CoupledMesh:
     """The host arrays of b2_coupled_mesh, by name (the keys a reference box
-    case or coupled_harness.box_hex gives; `lsq_x` are the pressure fit's rows,
+    case or coupled_harness.box_hex / box_tet give; `lsq_x` are the pressure fit's rows,
     `low_order` is optional). The arrays are kept alive with the struct."""
 
     def __init__(self, arrays: dict):
