@@ -374,6 +374,21 @@ __global__ void __launch_bounds__(kBlock, 8) k_cpl_fine_smooth(int n, int width,
 // ---- coarse levels ------------------------------------------------------------
 
 // (J x)_i of a coarse level (fv_coupled.kern.h:376-392, coupled_coarse_row).
+// The entries are summed one by one in CSR order, as there. Each entry's
+// product terms are formed whether or not it is the diagonal (only the sum
+// skips the diagonal), so the loads of four entries at a time are issued
+// together: a long row waits for two memory latencies per four entries
+// instead of one or two per entry.
+struct EntryTerms {
+  float u, v, w, p;
+};
+__device__ __forceinline__ EntryTerms coarse_terms(const CoupledLevel& l, int j, const float4& xm) {
+  const std::size_t Z = l.nnz;
+  const float a = l.a[j];
+  return EntryTerms{a * xm.x + l.g[j] * xm.w, a * xm.y + l.g[Z + j] * xm.w,
+                    a * xm.z + l.g[2 * Z + j] * xm.w,
+                    l.h[j] * xm.x + l.h[Z + j] * xm.y + l.h[2 * Z + j] * xm.z + l.c[j] * xm.w};
+}
 __device__ __forceinline__ float4 coarse_row(int i, const CoupledLevel& l,
                                              const float4* __restrict__ x) {
   const std::size_t N = l.n, Z = l.nnz;
@@ -383,14 +398,32 @@ __device__ __forceinline__ float4 coarse_row(int i, const CoupledLevel& l,
   float yv = l.d[N + i] * xi.y + l.g[Z + k] * xi.w;
   float yw = l.d[2 * N + i] * xi.z + l.g[2 * Z + k] * xi.w;
   float yp = l.c[k] * xi.w + l.h[k] * xi.x + l.h[Z + k] * xi.y + l.h[2 * Z + k] * xi.z;
-  for (int j = l.rows[i]; j < l.rows[i + 1]; ++j) {
-    if (j == k) continue;
-    const float4 xm = x[l.cols[j]];
-    const float a = l.a[j];
-    yu += a * xm.x + l.g[j] * xm.w;
-    yv += a * xm.y + l.g[Z + j] * xm.w;
-    yw += a * xm.z + l.g[2 * Z + j] * xm.w;
-    yp += l.h[j] * xm.x + l.h[Z + j] * xm.y + l.h[2 * Z + j] * xm.z + l.c[j] * xm.w;
+  const int end = l.rows[i + 1];
+  int j = l.rows[i];
+  for (; j + 4 <= end; j += 4) {
+    int col[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) col[u] = l.cols[j + u];
+    EntryTerms e[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) e[u] = coarse_terms(l, j + u, x[col[u]]);
+#pragma unroll
+    for (int u = 0; u < 4; ++u)
+      if (j + u != k) {
+        yu += e[u].u;
+        yv += e[u].v;
+        yw += e[u].w;
+        yp += e[u].p;
+      }
+  }
+  for (; j < end; ++j) {
+    const EntryTerms e = coarse_terms(l, j, x[l.cols[j]]);
+    if (j != k) {
+      yu += e.u;
+      yv += e.v;
+      yw += e.w;
+      yp += e.p;
+    }
   }
   return make_float4(yu, yv, yw, yp);
 }
@@ -428,12 +461,43 @@ __global__ void k_cpl_coarse_smooth(CoupledLevel l, const float4* __restrict__ x
   }
 }
 
-// Linear search in one sorted coarse row (fv_coupled.kern.h:418-422).
+// The entry of column `col` in coarse row `row` (fv_coupled.kern.h:418-422
+// searches linearly). A row's columns are sorted and unique (the contracted
+// graph's targets in order, the diagonal in place), so a binary search finds
+// the same entry in log2(row length) loads; rows on the small levels of tet
+// meshes reach 150 entries.
 __device__ __forceinline__ int entry_of(const int* __restrict__ rows, const int* __restrict__ cols,
                                         int row, int col) {
-  for (int j = rows[row]; j < rows[row + 1]; ++j)
-    if (cols[j] == col) return j;
-  return -1;
+  int lo = rows[row];
+  const int end = rows[row + 1];
+  int hi = end;
+  while (lo < hi) {
+    const int mid = (lo + hi) >> 1;
+    if (cols[mid] < col)
+      lo = mid + 1;
+    else
+      hi = mid;
+  }
+  return lo < end && cols[lo] == col ? lo : -1;
+}
+
+// Adds one off-diagonal contribution to entry e. Every load comes before any
+// store, so the eight read-modify-writes overlap instead of each waiting for
+// the last store (the arrays are distinct, the compiler cannot know it); each
+// sum is the same single addition.
+__device__ __forceinline__ void add_entry(const CoupledLevel& l, int e, float a, float c, float gx,
+                                          float gy, float gz, float hx, float hy, float hz) {
+  const std::size_t Z = l.nnz;
+  const float a0 = l.a[e], c0 = l.c[e], gx0 = l.g[e], gy0 = l.g[Z + e], gz0 = l.g[2 * Z + e];
+  const float hx0 = l.h[e], hy0 = l.h[Z + e], hz0 = l.h[2 * Z + e];
+  l.a[e] = a0 + a;
+  l.c[e] = c0 + c;
+  l.g[e] = gx0 + gx;
+  l.g[Z + e] = gy0 + gy;
+  l.g[2 * Z + e] = gz0 + gz;
+  l.h[e] = hx0 + hx;
+  l.h[Z + e] = hy0 + hy;
+  l.h[2 * Z + e] = hz0 + hz;
 }
 
 struct Sums {
@@ -527,14 +591,7 @@ __global__ void k_cpl_galerkin_fine(CoupledLevel l, CoupledTransfer t, FineGeome
           // contracted graph), so the search always finds it.
           const int e = entry_of(l.rows, l.cols, i, target);
           if (e < 0) continue;
-          l.a[e] += uu;
-          l.c[e] += pp;
-          l.g[e] += gx;
-          l.g[Z + e] += gy;
-          l.g[2 * Z + e] += gz;
-          l.h[e] += hx;
-          l.h[Z + e] += hy;
-          l.h[2 * Z + e] += hz;
+          add_entry(l, e, uu, pp, gx, gy, gz, hx, hy, hz);
         }
       }
     }
@@ -573,14 +630,8 @@ __global__ void k_cpl_galerkin_coarse(CoupledLevel l, CoupledTransfer t, Coupled
         } else {
           const int e = entry_of(l.rows, l.cols, i, target);
           if (e < 0) continue;
-          l.a[e] += f.a[j];
-          l.c[e] += f.c[j];
-          l.g[e] += f.g[j];
-          l.g[Z + e] += f.g[FZ + j];
-          l.g[2 * Z + e] += f.g[2 * FZ + j];
-          l.h[e] += f.h[j];
-          l.h[Z + e] += f.h[FZ + j];
-          l.h[2 * Z + e] += f.h[2 * FZ + j];
+          add_entry(l, e, f.a[j], f.c[j], f.g[j], f.g[FZ + j], f.g[2 * FZ + j], f.h[j],
+                    f.h[FZ + j], f.h[2 * FZ + j]);
         }
       }
     }

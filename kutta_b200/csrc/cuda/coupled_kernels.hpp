@@ -67,8 +67,9 @@ struct CoupledTransfer {
   const int* members = nullptr;
 };
 
-// The V-cycle of the small coarse levels (each at most kMaxRows rows) as one
-// single-block launch: levels 0 .. levels-1 of the tail, the first receiving
+// The V-cycle of the small coarse levels (by default each at most kMaxRows
+// rows; the kernel itself takes any size, its block looping over the rows) as
+// one single-block launch: levels 0 .. levels-1 of the tail, the first receiving
 // its right-hand side from the level above; x/tmp are each level's current
 // ping-pong roles.
 struct CoupledTail {

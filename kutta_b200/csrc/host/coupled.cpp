@@ -108,11 +108,14 @@ CoupledSolver::CoupledSolver(const CoupledMeshHost& m, int reference,
     transfers_.push_back(std::move(t));
   }
   // Levels from `tail_` down are small enough for the one-block V-cycle
-  // (KUTTA_B200_COUPLED_TAIL=0: separate launches, the same results).
+  // (KUTTA_B200_COUPLED_TAIL=0: separate launches, the same results;
+  // KUTTA_B200_COUPLED_TAIL_ROWS: the largest level it takes).
   const char* tail = std::getenv("KUTTA_B200_COUPLED_TAIL");
+  const char* tail_rows = std::getenv("KUTTA_B200_COUPLED_TAIL_ROWS");
+  const int max_rows = tail_rows ? std::atoi(tail_rows) : CoupledTail::kMaxRows;
   tail_ = levels_.size();
   if (!(tail && std::string(tail) == "0"))
-    while (tail_ > 0 && levels_[tail_ - 1].op.n <= CoupledTail::kMaxRows &&
+    while (tail_ > 0 && levels_[tail_ - 1].op.n <= max_rows &&
            levels_.size() - (tail_ - 1) <= static_cast<std::size_t>(CoupledTail::kMaxLevels))
       --tail_;
   for (auto* v : {&b_, &r_, &shadow_, &p_, &q_, &sv_, &t_}) own(*v, n);
