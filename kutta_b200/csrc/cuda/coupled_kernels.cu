@@ -428,6 +428,87 @@ __device__ __forceinline__ float4 coarse_row(int i, const CoupledLevel& l,
   return make_float4(yu, yv, yw, yp);
 }
 
+// (J x)_i by one warp, every lane returning the same value: the lanes form
+// the terms of 32 entries at a time in parallel, then every lane adds them
+// in CSR order, each read from its lane by shuffle, so the sums are
+// coarse_row's bit for bit. Called by all 32 lanes of a warp with the same i.
+__device__ __forceinline__ float4 coarse_row_warp(int i, const CoupledLevel& l,
+                                                  const float4* __restrict__ x, int lane) {
+  const std::size_t N = l.n, Z = l.nnz;
+  const int k = l.diag[i];
+  const float4 xi = x[i];
+  float yu = l.d[i] * xi.x + l.g[k] * xi.w;
+  float yv = l.d[N + i] * xi.y + l.g[Z + k] * xi.w;
+  float yw = l.d[2 * N + i] * xi.z + l.g[2 * Z + k] * xi.w;
+  float yp = l.c[k] * xi.w + l.h[k] * xi.x + l.h[Z + k] * xi.y + l.h[2 * Z + k] * xi.z;
+  const int end = l.rows[i + 1];
+  for (int base = l.rows[i]; base < end; base += 32) {
+    const int j = base + lane;
+    EntryTerms e{0.0f, 0.0f, 0.0f, 0.0f};
+    if (j < end) e = coarse_terms(l, j, x[l.cols[j]]);
+    const int count = min(32, end - base);
+    for (int u = 0; u < count; ++u) {
+      const float tu = __shfl_sync(0xffffffffu, e.u, u);
+      const float tv = __shfl_sync(0xffffffffu, e.v, u);
+      const float tw = __shfl_sync(0xffffffffu, e.w, u);
+      const float tp = __shfl_sync(0xffffffffu, e.p, u);
+      if (base + u != k) {
+        yu += tu;
+        yv += tv;
+        yw += tw;
+        yp += tp;
+      }
+    }
+  }
+  return make_float4(yu, yv, yw, yp);
+}
+
+// One damped block-Jacobi update of row i from r = b - (J x)_i (or b when x
+// is zero), fv_coupled.kern.h:401-416.
+__device__ __forceinline__ float4 coarse_update(const CoupledLevel& l, int i, float4 r,
+                                                float4 base, float omega) {
+  const std::size_t N = l.n, Z = l.nnz;
+  const int k = l.diag[i];
+  const float* d = l.d;
+  const float4 s = block_solve(r, l.g[k], l.g[Z + k], l.g[2 * Z + k], d[4 * N + i], d[5 * N + i],
+                               d[6 * N + i], d[7 * N + i], d[8 * N + i], d[9 * N + i],
+                               d[10 * N + i]);
+  return damped(base, s, omega);
+}
+
+// A warp per row (levels flagged wide): the residual and the sweep.
+__global__ void k_cpl_coarse_residual_wide(CoupledLevel l, const float4* __restrict__ x,
+                                           const float4* __restrict__ b,
+                                           float4* __restrict__ r) {
+  pdl_entry();
+  const int lane = threadIdx.x & 31;
+  const int warps = gridDim.x * (blockDim.x >> 5);
+  for (int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < l.n; i += warps) {
+    const float4 y = coarse_row_warp(i, l, x, lane);
+    if (lane == 0) {
+      const float4 bi = b[i];
+      r[i] = make_float4(bi.x - y.x, bi.y - y.y, bi.z - y.z, bi.w - y.w);
+    }
+  }
+}
+__global__ void k_cpl_coarse_smooth_wide(CoupledLevel l, const float4* __restrict__ x,
+                                         const float4* __restrict__ b, float4* __restrict__ next,
+                                         float omega, int first) {
+  pdl_entry();
+  const int lane = threadIdx.x & 31;
+  const int warps = gridDim.x * (blockDim.x >> 5);
+  for (int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < l.n; i += warps) {
+    float4 r = b[i];
+    float4 base = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    if (!first) {
+      const float4 y = coarse_row_warp(i, l, x, lane);
+      r = make_float4(r.x - y.x, r.y - y.y, r.z - y.z, r.w - y.w);
+      base = x[i];
+    }
+    if (lane == 0) next[i] = coarse_update(l, i, r, base, omega);
+  }
+}
+
 __global__ void k_cpl_coarse_residual(CoupledLevel l, const float4* __restrict__ x,
                                       const float4* __restrict__ b, float4* __restrict__ r) {
   pdl_entry();
@@ -726,11 +807,12 @@ __global__ void __launch_bounds__(kBlock, 8) k_cpl_prolong(int nf, const int* __
 // ping-pong roles of each level's x and tmp follow the host's: the kernel
 // starts from the pointers it is given and swaps them as the separate
 // launches would. On a 128^3 box this replaces about 25 launches of 3-6 us
-// per V-cycle by one.
+// per V-cycle by one. Rows stay one per thread here even on levels flagged
+// wide: with 32 warps for the whole level, a warp per row measured slower
+// (388 against 252 us per launch on a 875-row level with 152-entry rows).
 __device__ __forceinline__ void tail_smooth(const CoupledLevel& l, float4*& x, float4*& tmp,
                                             const float4* __restrict__ b, int sweeps, bool first,
                                             float omega) {
-  const std::size_t N = l.n, Z = l.nnz;
   for (int s = 0; s < sweeps; ++s) {
     const bool zero = first && s == 0;
     for (int i = threadIdx.x; i < l.n; i += blockDim.x) {
@@ -741,12 +823,7 @@ __device__ __forceinline__ void tail_smooth(const CoupledLevel& l, float4*& x, f
         r = make_float4(r.x - y.x, r.y - y.y, r.z - y.z, r.w - y.w);
         base = x[i];
       }
-      const int k = l.diag[i];
-      const float* d = l.d;
-      const float4 v = block_solve(r, l.g[k], l.g[Z + k], l.g[2 * Z + k], d[4 * N + i],
-                                   d[5 * N + i], d[6 * N + i], d[7 * N + i], d[8 * N + i],
-                                   d[9 * N + i], d[10 * N + i]);
-      tmp[i] = damped(base, v, omega);
+      tmp[i] = coarse_update(l, i, r, base, omega);
     }
     __syncthreads();
     float4* swap = x;
@@ -978,14 +1055,21 @@ void cpl_coarse_residual(const CoupledLevel& l, const float4* x, const float4* b
                          cudaStream_t s) {
   if (l.n <= 0) return;
   ++counter;
-  pdl(k_cpl_coarse_residual, grid_for(l.n), kBlock, 0, s, l, x, b, r);
+  if (l.wide)
+    pdl(k_cpl_coarse_residual_wide, grid_for(32LL * l.n), kBlock, 0, s, l, x, b, r);
+  else
+    pdl(k_cpl_coarse_residual, grid_for(l.n), kBlock, 0, s, l, x, b, r);
 }
 
 void cpl_coarse_smooth(const CoupledLevel& l, const float4* x, const float4* b, float4* next,
                        float omega, bool first, cudaStream_t s) {
   if (l.n <= 0) return;
   ++counter;
-  pdl(k_cpl_coarse_smooth, grid_for(l.n), kBlock, 0, s, l, x, b, next, omega, first ? 1 : 0);
+  if (l.wide)
+    pdl(k_cpl_coarse_smooth_wide, grid_for(32LL * l.n), kBlock, 0, s, l, x, b, next, omega,
+        first ? 1 : 0);
+  else
+    pdl(k_cpl_coarse_smooth, grid_for(l.n), kBlock, 0, s, l, x, b, next, omega, first ? 1 : 0);
 }
 
 void cpl_restrict(int nc, const int* offsets, const int* members, const float4* fine,

@@ -58,6 +58,10 @@ struct CoupledLevel {
   const int* cols = nullptr;
   const int* diag = nullptr;
   float *a = nullptr, *c = nullptr, *g = nullptr, *h = nullptr, *d = nullptr;
+  // Rows long enough (a hub aggregate bordering a hundred others) that the
+  // separately launched row kernels give each row a warp instead of a
+  // thread; the results are the same bits either way.
+  int wide = 0;
 };
 
 // Level k -> k+1: aggregate of each fine row, member lists of each coarse row.

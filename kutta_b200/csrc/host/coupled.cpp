@@ -4,6 +4,7 @@
 // the scalar Krylov epilogues are this library's reference-parity ones.
 #include "coupled.hpp"
 
+#include <algorithm>
 #include <cmath>
 #include <cstdlib>
 #include <sstream>
@@ -79,8 +80,16 @@ CoupledSolver::CoupledSolver(const CoupledMeshHost& m, int reference,
   own(link_, slots);
   own(face_, nf);
 
+  // A level whose longest row has at least this many entries gets a warp per
+  // row in its row kernels (KUTTA_B200_COUPLED_WIDE_ROWS; the same bits
+  // either way): a thread walking a hub row of ~150 entries stalls a whole
+  // sweep behind it.
+  const char* wide_env = std::getenv("KUTTA_B200_COUPLED_WIDE_ROWS");
+  const int wide_rows = wide_env ? std::atoi(wide_env) : 32;
   for (std::size_t k = 0; k < setup.levels.size(); ++k) {
     auto& src = setup.levels[k];
+    int longest = 0;
+    for (int i = 0; i < src.n; ++i) longest = std::max(longest, src.rows[i + 1] - src.rows[i]);
     Level l;
     own(l.rows, src.rows, s);
     own(l.cols, src.cols, s);
@@ -98,6 +107,7 @@ CoupledSolver::CoupledSolver(const CoupledMeshHost& m, int reference,
     l.tmp = l.store[1].get();
     l.op = CoupledLevel{src.n, src.nnz, l.rows.get(), l.cols.get(), l.diag.get(),
                         l.a.get(),  l.c.get(),   l.g.get(),    l.h.get(),    l.d.get()};
+    l.op.wide = wide_rows > 0 && longest >= wide_rows ? 1 : 0;
     levels_.push_back(std::move(l));
     auto& tsrc = setup.transfers[k];
     Transfer t;

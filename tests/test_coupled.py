@@ -332,12 +332,16 @@ def test_coupled_paired_update_matches_oracle(cuda):
 
 @pytest.mark.gpu
 @pytest.mark.parametrize("name", ["coupled_tet6x5x4_tight", "coupled_hex12x10x8_closed"])
-def test_coupled_coarse_kernels_match_oracle(cuda, name):
+@pytest.mark.parametrize("wide", [None, "1"], ids=["thread_rows", "warp_rows"])
+def test_coupled_coarse_kernels_match_oracle(cuda, name, wide, monkeypatch):
     """On every coarse level: the residual and the damped block-Jacobi sweep
     (from x and from zero), the member-sum restriction and the prolongation,
     on seeded vectors, bit for bit against the oracle on the reference's own
-    level operator."""
+    level operator; with a thread per row (these levels' rows are short) and
+    with every level forced to a warp per row."""
     import torch
+    if wide is not None:
+        monkeypatch.setenv("KUTTA_B200_COUPLED_WIDE_ROWS", wide)
     meta, mesh, fields, refs = load(name)
     s, _, _ = _solver(meta, mesh, fields)
     sizes, levels = ref_levels(meta, refs)
@@ -411,6 +415,29 @@ def test_one_block_tail_changes_no_bits(cuda, name, monkeypatch):
     runs = []
     for tail in ("1", "0"):
         monkeypatch.setenv("KUTTA_B200_COUPLED_TAIL", tail)
+        s, st, d = _solver(meta, mesh, fields)
+        rel, abs_, max_iter = meta["control"]
+        st2 = s.solve(d, L.SolveControl(rel, abs_, max_iter))
+        runs.append((st, st2, s.copy("x")))
+    (a1, a2, ax), (b1, b2, bx) = runs
+    assert (a1.iterations, a1.final_residual) == (b1.iterations, b1.final_residual)
+    assert (a2.iterations, a2.final_residual) == (b2.iterations, b2.final_residual)
+    assert np.array_equal(bits(ax), bits(bx))
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", ["coupled_tet6x5x4_tight", "coupled_hex10x8x6_v22_net"])
+@pytest.mark.parametrize("tail", ["1", "0"], ids=["tail", "separate"])
+def test_warp_rows_change_no_bits(cuda, name, tail, monkeypatch):
+    """Every separately launched coarse level with a warp per row (the levels
+    of the one-block tail keep a thread per row, and with the tail off every
+    level is launched separately) gives the thread-per-row solution and
+    statistics bit for bit, over two solves."""
+    meta, mesh, fields, _ = load(name)
+    monkeypatch.setenv("KUTTA_B200_COUPLED_TAIL", tail)
+    runs = []
+    for wide in ("1", "0"):
+        monkeypatch.setenv("KUTTA_B200_COUPLED_WIDE_ROWS", wide)
         s, st, d = _solver(meta, mesh, fields)
         rel, abs_, max_iter = meta["control"]
         st2 = s.solve(d, L.SolveControl(rel, abs_, max_iter))
