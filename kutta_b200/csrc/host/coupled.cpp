@@ -81,9 +81,10 @@ CoupledSolver::CoupledSolver(const CoupledMeshHost& m, int reference,
   own(face_, nf);
 
   // A level whose longest row has at least this many entries gets a warp per
-  // row in its row kernels (KUTTA_B200_COUPLED_WIDE_ROWS; the same bits
-  // either way): a thread walking a hub row of ~150 entries stalls a whole
-  // sweep behind it.
+  // row in its separately launched row kernels (KUTTA_B200_COUPLED_WIDE_ROWS,
+  // 0 for never; the same bits either way; the one-block tail keeps a thread
+  // per row): a thread walking a hub row of ~150 entries stalls a whole sweep
+  // behind it.
   const char* wide_env = std::getenv("KUTTA_B200_COUPLED_WIDE_ROWS");
   const int wide_rows = wide_env ? std::atoi(wide_env) : 32;
   for (std::size_t k = 0; k < setup.levels.size(); ++k) {
